@@ -1,0 +1,284 @@
+// dsax_corr.cu -- the X-engine correlator on sm_100a tensor cores.
+//
+// Replaces, in one kernel, the reference's CPU reorder/fluff
+// (src/dsaX_reorder_raw.c:153-169, src/dsaX_reorder_raw.c.bak:184-258), the
+// xGPU-stage promoter (src/dsaX_xgpu.cu:67-77) and xgpuCudaXengine
+// (src/dsaX_xgpu.cu:318; FP32 SIMT in the un-vendored xGPU library).
+//
+// Arithmetic.  For one frequency f' (= 2*chan + time-in-packet) and the 128
+// inputs a = 2*station + pol, the products are
+//     V[a][b] = sum_t x_a(t) conj(x_b(t)),   re = ra rb + ia ib,
+//                                            im = ia rb - ra ib.
+// With K = 2 * packets (k = 2p + {0: re, 1: im}) and the int8 operands
+//     A[a][2p..2p+1]     = ( ra,  ia)
+//     Arot[b][2p..2p+1]  = (-ib,  rb)
+// one UMMA  D[128 x 256] = A * [A ; Arot]^T  yields Re V in columns 0..127
+// and Im V in columns 128..255 (s32, exact).  The B operand is the
+// concatenation of A and Arot in shared memory, so A is staged once.
+//
+// Tiling.  One CTA per channel = two frequencies (t = 0, 1); each frequency
+// owns 256 TMEM columns (all 512 used).  K is streamed in stages of 64
+// packets (128 bytes of K per row = one 128-byte swizzle atom).
+//   warps 0-7 : producers -- load the packed 4-bit samples, unpack the
+//               nibbles in registers and write the swizzled K-major A / Arot
+//               tiles (the unpack never touches HBM);
+//               after the K loop they are the epilogue (TMEM -> triangle).
+//   warp  8   : TMEM allocator and single-thread UMMA issuer.
+// Every pipeline wait is bounded (dsax_ptx.cuh).
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dsax_internal.h"
+#include "dsax_ptx.cuh"
+
+namespace dsax {
+
+namespace corr {
+constexpr int kPktPerStage = 64;                 // K bytes per row per stage = 128
+constexpr int kStages = 3;
+constexpr int kTileBytes = 128 * 128;            // 128 rows x 128 B
+constexpr int kFreqBytes = 2 * kTileBytes;       // A + Arot
+constexpr int kStageBytes = 2 * kFreqBytes;      // two frequencies
+constexpr int kProducerThreads = 256;
+constexpr int kThreads = kProducerThreads + 32;  // + MMA warp
+constexpr int kSmemBytes = kStages * kStageBytes + 1024;  // + alignment slack
+constexpr uint32_t kIdesc = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 256);
+}  // namespace corr
+
+// 2 packed samples (bytes s of wa and wb) -> int8 [re_a, im_a, re_b, im_b].
+__device__ __forceinline__ uint32_t unpack_pair(uint32_t wa, uint32_t wb, uint32_t s) {
+  uint32_t x = __byte_perm(wa, wb, s | ((s + 4u) << 4));  // byte0 = wa.s, byte1 = wb.s
+  uint32_t y = (x & 0x000Fu) | ((x & 0x00F0u) << 4) | ((x & 0x0F00u) << 8) |
+               ((x & 0xF000u) << 12);
+  return __vsub4(y ^ 0x08080808u, 0x08080808u);  // sign-extend each nibble
+}
+
+// [re_a, im_a, re_b, im_b] -> [-im_a, re_a, -im_b, re_b]
+__device__ __forceinline__ uint32_t rotate_pair(uint32_t r) {
+  uint32_t sw = __byte_perm(r, 0u, 0x2301u);
+  uint32_t ng = __vneg4(sw);
+  return (ng & 0x00FF00FFu) | (sw & 0xFF00FF00u);
+}
+
+// Loads the 8 packets of one (antenna, packet-group) task and returns, for
+// each of the 4 (time, pol) sample slots, the packed byte quadruple words:
+// w[q] holds, for packet q, bytes [t0p0, t0p1, t1p0, t1p1].
+template <int FMT>
+__device__ __forceinline__ void load_task(const CorrArgs &a, int ch, int ant, int p0,
+                                          uint32_t (&w)[8], uint32_t (&v)[8]) {
+  if (FMT == FMT_CAPTURED) {
+    // [pkt][nant_in][nchan][2 t][2 pol] packed; one 32-bit word per (pkt, ant).
+    const bool ok_ant = ant < a.nant_in;
+    const uint8_t *base = a.in + ((int64_t)ant * a.nchan + ch) * 4;
+    const int64_t pstride = (int64_t)a.nant_in * a.nchan * 4;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int p = p0 + q;
+      w[q] = (ok_ant && p < a.npkt) ? __ldg(reinterpret_cast<const uint32_t *>(base + p * pstride))
+                                    : 0u;
+    }
+  } else if (FMT == FMT_REORDERED) {
+    // [pkt][2*nchan][64][2 pol] packed (the massage() output).
+    const int64_t pstride = (int64_t)2 * a.nchan * 64 * 2;
+    const uint8_t *base = a.in + ((int64_t)(2 * ch) * 64 + ant) * 2;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int p = p0 + q;
+      uint32_t lo = 0, hi = 0;
+      if (p < a.npkt) {
+        lo = __ldg(reinterpret_cast<const uint16_t *>(base + p * pstride));
+        hi = __ldg(reinterpret_cast<const uint16_t *>(base + p * pstride + 128));
+      }
+      w[q] = lo | (hi << 16);
+    }
+  } else {
+    // FMT_XGPU_INT8: [pkt][nfreq][64][2 pol][re, im] int8 (xGPU ComplexInput).
+    const int64_t pstride = (int64_t)2 * a.nchan * 64 * 4;
+    const uint8_t *base = a.in + ((int64_t)(2 * ch) * 64 + ant) * 4;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int p = p0 + q;
+      w[q] = p < a.npkt ? __ldg(reinterpret_cast<const uint32_t *>(base + p * pstride)) : 0u;
+      v[q] = p < a.npkt ? __ldg(reinterpret_cast<const uint32_t *>(base + p * pstride + 256)) : 0u;
+    }
+  }
+}
+
+template <int FMT>
+__global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
+  using namespace corr;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kStages];
+  __shared__ __align__(8) uint64_t empty_bar[kStages];
+  __shared__ __align__(8) uint64_t accum_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const int ch = blockIdx.x;  // channel -> frequencies 2ch, 2ch+1
+
+  // 1024-byte aligned stage area (required by the 128B swizzle atoms).
+  const uint32_t smem_base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full_bar[s], kProducerThreads);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&accum_bar, 1);
+    abort_sh = 0;
+    mbar_fence_init();
+  }
+  if (warp == 8) {
+    tmem_alloc(&tmem_base_sh, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  if ((tmem & 0xFFFFu) != 0u) {  // 512 columns must start at column 0
+    if (tid == 0) { atomicOr(a.err, DEV_ERR_TMEM); }
+    abort_sh = 1;
+  }
+
+  const int nks = (a.npkt + kPktPerStage - 1) / kPktPerStage;
+
+  if (warp < 8) {
+    // ------------------------------------------------------------ producers
+    // lane -> (ant_lo, jbit, ant_hi); warp -> (ant group, packet-group pair)
+    const int ant = 16 * (warp & 3) + 4 * (lane >> 3) + (lane & 3);
+    const int jbit = (lane >> 2) & 1;
+    for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+      const int s = ks % kStages;
+      const uint32_t ph = (uint32_t)(ks / kStages) & 1u;
+      if (!mbar_wait_bounded(&empty_bar[s], ph ^ 1u, &abort_sh, a.err, DEV_ERR_WAIT_EMPTY,
+                             a.wait_limit_ns))
+        break;
+      const uint32_t stage = smem_base + (uint32_t)s * kStageBytes;
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {
+        const int pg = 2 * ((warp >> 2) * 2 + it) + jbit;  // packet group 0..7
+        uint32_t w[8], v[8];
+        load_task<FMT>(a, ch, ant, ks * kPktPerStage + 8 * pg, w, v);
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+#pragma unroll
+          for (int pol = 0; pol < 2; ++pol) {
+            uint32_t c[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+              if (FMT == FMT_XGPU_INT8) {
+                const uint32_t wa = t ? v[2 * h] : w[2 * h];
+                const uint32_t wb = t ? v[2 * h + 1] : w[2 * h + 1];
+                const uint32_t sel = pol ? 0x7632u : 0x5410u;  // bytes (2pol, 2pol+1) of wa, wb
+                c[h] = __byte_perm(wa, wb, sel);
+              } else {
+                c[h] = unpack_pair(w[2 * h], w[2 * h + 1], (uint32_t)(2 * t + pol));
+              }
+            }
+            const uint32_t row = (uint32_t)(2 * ant + pol);
+            const uint32_t off = sw128_offset(row, (uint32_t)pg);
+            const uint32_t tileA = stage + (uint32_t)t * kFreqBytes;
+            st_shared_v4(tileA + off, c[0], c[1], c[2], c[3]);
+            st_shared_v4(tileA + kTileBytes + off, rotate_pair(c[0]), rotate_pair(c[1]),
+                         rotate_pair(c[2]), rotate_pair(c[3]));
+          }
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(&full_bar[s]);
+    }
+  } else {
+    // ------------------------------------------------------------ UMMA issuer
+    for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+      const int s = ks % kStages;
+      const uint32_t ph = (uint32_t)(ks / kStages) & 1u;
+      if (!mbar_wait_bounded(&full_bar[s], ph, &abort_sh, a.err, DEV_ERR_WAIT_FULL,
+                             a.wait_limit_ns))
+        break;
+      tc_fence_after();
+      if (lane == 0) {
+        const uint32_t stage = smem_base + (uint32_t)s * kStageBytes;
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const uint32_t tileA = stage + (uint32_t)t * kFreqBytes;
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {  // 4 x K=32 bytes per 128-byte atom
+            const uint64_t d = umma_desc_sw128(tileA + 32u * kk, 1024u);
+            umma_i8(tmem + (uint32_t)t * 256u, d, d, kIdesc, (ks | kk) != 0);
+          }
+        }
+        umma_commit(&empty_bar[s]);
+      }
+      __syncwarp();
+    }
+    if (lane == 0) umma_commit(&accum_bar);  // fires when every issued UMMA is done
+    __syncwarp();
+  }
+
+  // ---------------------------------------------------------------- epilogue
+  if (warp < 8) {
+    const bool ok = mbar_wait_bounded(&accum_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
+                                      a.wait_limit_ns);
+    tc_fence_after();
+    if (ok && !abort_sh) {
+      const int q = warp & 3;         // TMEM lane quarter of this warp
+      const int t = warp >> 2;        // frequency within the channel
+      const int m = 32 * q + lane;    // row = 2*station + pol
+      const int i = m >> 1, pi = m & 1;
+      float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
+      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
+      const int ncb = 2 * q + 2;      // station chunks of 8 reaching this warp's diagonal
+      for (int cb = 0; cb < ncb; ++cb) {
+        uint32_t re[16], im[16];
+        tmem_ld16(trow + 16u * cb, re);
+        tmem_ld16(trow + 128u + 16u * cb, im);
+        tmem_wait_ld();
+        const int64_t tri = (int64_t)i * (i + 1) / 2;
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int j = 8 * cb + jj;
+          if (j <= i) {
+            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(int32_t)im[2 * jj],
+                                   (float)(int32_t)re[2 * jj + 1], (float)(int32_t)im[2 * jj + 1]);
+            float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
+            if (a.accumulate) {
+              float4 old = *dst;
+              o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
+            }
+            *dst = o;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+int launch_correlate(const CorrArgs &a, int fmt, cudaStream_t st) {
+  static bool attr_done[3] = {false, false, false};
+  const void *fn = fmt == FMT_CAPTURED    ? (const void *)corr_kernel<FMT_CAPTURED>
+                   : fmt == FMT_REORDERED ? (const void *)corr_kernel<FMT_REORDERED>
+                                          : (const void *)corr_kernel<FMT_XGPU_INT8>;
+  if (fmt < 0 || fmt > 2) return -1;
+  if (!attr_done[fmt]) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         corr::kSmemBytes);
+    if (e != cudaSuccess) return -2;
+    attr_done[fmt] = true;
+  }
+  dim3 grid(a.nchan), block(corr::kThreads);
+  void *args[] = {(void *)&a};
+  cudaError_t e = cudaLaunchKernel(fn, grid, block, args, corr::kSmemBytes, st);
+  return e == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace dsax

@@ -1,0 +1,54 @@
+// dsax_ctx.h -- the context object behind the opaque dsax_ctx handle.
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "../../include/dsax.h"
+
+namespace dsax {
+
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+
+ private:
+  int prev_ = -1;
+};
+
+int set_error(dsax_ctx *c, int code, const char *fmt, ...);
+int cuda_check(dsax_ctx *c, cudaError_t e, const char *what);
+int ensure_buffer(dsax_ctx *c, DevBuf &b, size_t nbytes, const char *what);
+int check_device_error(dsax_ctx *c);
+bool aligned16(const void *p);
+
+}  // namespace dsax
+
+struct dsax_ctx {
+  dsax_config cfg{};
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  int *d_err = nullptr;   // device error word written by bounded waits
+  int *h_err = nullptr;   // pinned readback slot
+  dsax::DevBuf in_buf;    // host-mode staging: input block
+  dsax::DevBuf vis_buf;   // host-mode staging: visibilities
+  dsax::DevBuf aux[8];    // per-stage scratch (beamformer / flagger)
+  char errmsg[512] = {0};
+
+  void release_all() {
+    in_buf.release();
+    vis_buf.release();
+    for (auto &b : aux) b.release();
+  }
+};

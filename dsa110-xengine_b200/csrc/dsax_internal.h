@@ -1,0 +1,38 @@
+// dsax_internal.h -- launch-argument structs shared between the kernels and
+// the C-ABI layer (not installed; the public interface is include/dsax.h).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dsax {
+
+// ---- error codes written to the device error word (bit flags) ----
+enum : int {
+  DEV_ERR_WAIT_FULL = 1 << 0,    // consumer gave up waiting for a filled stage
+  DEV_ERR_WAIT_EMPTY = 1 << 1,   // producer gave up waiting for a free stage
+  DEV_ERR_WAIT_ACCUM = 1 << 2,   // epilogue gave up waiting for the accumulator
+  DEV_ERR_TMEM = 1 << 3,         // TMEM allocation returned an unusable address
+  DEV_ERR_BOUNDS = 1 << 4,       // an index check failed (access skipped)
+};
+
+// Input formats accepted by the correlator.
+enum {
+  FMT_CAPTURED = 0,   // [pkt][nant_in][nchan][2 t][2 pol] 4+4-bit (CAPTURED key)
+  FMT_REORDERED = 1,  // [pkt][2 nchan][64][2 pol] 4+4-bit (REORDER key, massage())
+  FMT_XGPU_INT8 = 2,  // [pkt][2 nchan][64][2 pol][re,im] int8 (xGPU ComplexInput)
+};
+
+struct CorrArgs {
+  const uint8_t *in;       // device input block
+  float *vis;              // device output [2 nchan][2080][4][re,im]
+  int *err;                // device error word (bit flags, dsax_ptx.cuh)
+  int npkt;                // packets (xGPU time samples) per block
+  int nant_in;             // antennas present in the captured block (<= 64)
+  int nchan;               // channels (= CTAs); frequencies = 2 * nchan
+  int accumulate;          // 1: vis += block's products (xGPU integration buffer)
+  unsigned long long wait_limit_ns;  // bound on every pipeline wait
+};
+
+int launch_correlate(const CorrArgs &a, int fmt, cudaStream_t st);
+
+}  // namespace dsax

@@ -1,0 +1,224 @@
+"""Python binding of libdsax.so (include/dsax.h) through ctypes.
+
+This is a thin host-side mirror of the C ABI for tests, the benchmark and
+Python callers.  Device buffers are passed as raw pointers (torch tensors'
+data_ptr() or any CUDA allocation); the library itself holds no torch types.
+
+There is no fallback: if libdsax.so is missing or cannot be loaded, every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+_PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_DIR, "libdsax.so")
+HEADER_DIR = os.path.join(os.path.dirname(_PKG_DIR), "include")
+
+DSAX_OK = 0
+DSAX_ERR_ARG = -1
+DSAX_ERR_CUDA = -2
+DSAX_ERR_TIMEOUT = -3
+DSAX_ERR_NOMEM = -4
+DSAX_ERR_UNSUPPORTED = -5
+DSAX_ERR_DEVICE = -6
+
+MEM_HOST = 0
+MEM_DEVICE = 1
+
+FMT_CAPTURED = 0
+FMT_REORDERED = 1
+FMT_XGPU_INT8 = 2
+
+NBL = 2080
+
+
+class DsaxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"dsax status {status}: {msg}")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("npkt", ctypes.c_int),
+        ("nant_in", ctypes.c_int),
+        ("nchan", ctypes.c_int),
+        ("nbeam", ctypes.c_int),
+        ("bf_pkt_per_out", ctypes.c_int),
+        ("bf_scale", ctypes.c_float),
+        ("wait_limit_ns", ctypes.c_ulonglong),
+    ]
+
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Run the package Makefile (nvcc, sm_100a) and return the library path."""
+    args = ["make", "-s", "-C", _PKG_DIR, "-j8"]
+    if force:
+        args.insert(2, "-B")
+    subprocess.check_call(args)
+    return LIB_PATH
+
+
+def lib():
+    """Load libdsax.so (raises OSError if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"libdsax.so not built at {LIB_PATH}; run `make -C {_PKG_DIR}`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+    CP = ctypes.POINTER(Config)
+    L.dsax_default_config.argtypes = [CP]
+    L.dsax_default_config.restype = None
+    for fn in ("dsax_block_bytes",):
+        getattr(L, fn).argtypes = [CP, I]
+        getattr(L, fn).restype = Z
+    for fn in ("dsax_vis_bytes", "dsax_beam_bytes"):
+        getattr(L, fn).argtypes = [CP]
+        getattr(L, fn).restype = Z
+    L.dsax_create.argtypes = [ctypes.POINTER(P), CP, I]
+    L.dsax_create.restype = I
+    L.dsax_destroy.argtypes = [P]
+    L.dsax_destroy.restype = None
+    L.dsax_strerror.argtypes = [I]
+    L.dsax_strerror.restype = ctypes.c_char_p
+    L.dsax_last_error.argtypes = [P]
+    L.dsax_last_error.restype = ctypes.c_char_p
+    L.dsax_stream.argtypes = [P]
+    L.dsax_stream.restype = P
+    L.dsax_sync.argtypes = [P]
+    L.dsax_sync.restype = I
+    L.dsax_host_alloc.argtypes = [P, Z, ctypes.POINTER(P)]
+    L.dsax_host_alloc.restype = I
+    L.dsax_host_free.argtypes = [P, P]
+    L.dsax_host_free.restype = I
+    L.dsax_correlate.argtypes = [P, P, P, I]
+    L.dsax_correlate.restype = I
+    L.dsax_correlate_fmt.argtypes = [P, I, P, P, I, I]
+    L.dsax_correlate_fmt.restype = I
+    _bind_optional(L)
+    _lib = L
+    return L
+
+
+def _bind_optional(L):
+    """Signatures of entry points added beyond the correlator."""
+    P, I, Z, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_float
+    table = {
+        "dsax_set_weights": ([P, P, P, I], I),
+        "dsax_beamform": ([P, P, P, I, I], I),
+        "dsax_beamform_power": ([P, P, P, I, I], I),
+    }
+    for name, (args, res) in table.items():
+        if hasattr(L, name):
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+
+
+def default_config(**kw) -> Config:
+    c = Config()
+    lib().dsax_default_config(ctypes.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def block_bytes(cfg: Config, fmt: int = FMT_CAPTURED) -> int:
+    return int(lib().dsax_block_bytes(ctypes.byref(cfg), fmt))
+
+
+def vis_bytes(cfg: Config) -> int:
+    return int(lib().dsax_vis_bytes(ctypes.byref(cfg)))
+
+
+def beam_bytes(cfg: Config) -> int:
+    return int(lib().dsax_beam_bytes(ctypes.byref(cfg)))
+
+
+def strerror(status: int) -> str:
+    return lib().dsax_strerror(status).decode()
+
+
+def _ptr(x) -> int:
+    """Raw address of a torch tensor, numpy array or int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(f"cannot take the address of {type(x)}")
+
+
+class Context:
+    """One dsax context: one device, one stream, its scratch buffers."""
+
+    def __init__(self, cfg: Config | None = None, device: int = 0):
+        self.cfg = cfg if cfg is not None else default_config()
+        self._h = ctypes.c_void_p()
+        rc = lib().dsax_create(ctypes.byref(self._h), ctypes.byref(self.cfg), device)
+        if rc != DSAX_OK:
+            raise DsaxError(rc, f"dsax_create: {strerror(rc)}")
+        self.device = device
+
+    # -- plumbing ----------------------------------------------------------
+    def _check(self, rc: int, what: str):
+        if rc != DSAX_OK:
+            msg = lib().dsax_last_error(self._h).decode()
+            raise DsaxError(rc, f"{what}: {strerror(rc)} ({msg})")
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return int(lib().dsax_stream(self._h) or 0)
+
+    def sync(self):
+        self._check(lib().dsax_sync(self._h), "dsax_sync")
+
+    def close(self):
+        if self._h:
+            lib().dsax_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- correlator --------------------------------------------------------
+    def correlate(self, blk, vis, mem: int = MEM_DEVICE, fmt: int = FMT_CAPTURED,
+                  accumulate: bool = False):
+        rc = lib().dsax_correlate_fmt(self._h, fmt, _ptr(blk), _ptr(vis), mem, int(accumulate))
+        self._check(rc, "dsax_correlate_fmt")
+
+    # -- beamformer --------------------------------------------------------
+    def set_weights(self, wre, wim, mem: int = MEM_HOST):
+        self._check(lib().dsax_set_weights(self._h, _ptr(wre), _ptr(wim), mem), "dsax_set_weights")
+
+    def beamform(self, blk, out, mem: int = MEM_DEVICE, precision: int = 0):
+        self._check(lib().dsax_beamform(self._h, _ptr(blk), _ptr(out), mem, precision),
+                    "dsax_beamform")
+
+    def beamform_power(self, blk, out, mem: int = MEM_DEVICE, precision: int = 0):
+        self._check(lib().dsax_beamform_power(self._h, _ptr(blk), _ptr(out), mem, precision),
+                    "dsax_beamform_power")

@@ -1,0 +1,122 @@
+/*
+ * dsax.h -- C ABI of the B200 (sm_100a) DSA-110 X-engine hot path.
+ *
+ * One library, libdsax.so, replaces the GPU stages of the reference
+ * pipeline behind plain C calls (pointers, sizes, int status codes):
+ *
+ *   dsax_correlate  <- src/dsaX_reorder_raw.c massage() (:99-219)
+ *                      + src/dsaX_xgpu.cu promoter (:67-77)
+ *                      + xgpuCudaXengine / xgpuClearDeviceIntegrationBuffer
+ *                        (:318, :336)
+ *   dsax_beamform   <- src/dsaX_beamformer.cu promoter/beamformer/adder
+ *                      (:121-416) with calc_weights (:421-449)
+ *   dsax_flag       <- src/gpu_flagger.cu statistics kernels (:175-494)
+ *                      + host flagging (:534-798, :1340-1398)
+ *
+ * The xGPU call shapes used at src/dsaX_xgpu.cu:253-287 are also exported
+ * with their original names by include/xgpu_dsax.h, so a caller written
+ * against xGPU can relink without source changes.
+ *
+ * Conventions
+ *  - Every function returns an int status: DSAX_OK (0) or a negative
+ *    DSAX_ERR_* code.  The library never exits the process.
+ *  - A context owns one CUDA device, one stream and its device scratch.
+ *    Calls on one context are serialised by the caller (a context is not
+ *    thread-safe); several contexts may be used concurrently.
+ *  - mem = DSAX_MEM_HOST: input and output pointers are host memory; the
+ *    call copies in, computes, copies out and synchronises before
+ *    returning.  Pinned host memory (dsax_host_alloc) makes the copies
+ *    asynchronous DMA transfers.
+ *    mem = DSAX_MEM_DEVICE: pointers are device memory on the context's
+ *    device; the work is enqueued on the context stream and the call
+ *    returns without waiting.  dsax_sync() waits and reports any
+ *    device-side error.
+ */
+#ifndef DSAX_H
+#define DSAX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define DSAX_OK 0
+#define DSAX_ERR_ARG (-1)         /* bad argument, size, alignment or layout */
+#define DSAX_ERR_CUDA (-2)        /* CUDA runtime error; see dsax_last_error */
+#define DSAX_ERR_TIMEOUT (-3)     /* a bounded device-side wait expired */
+#define DSAX_ERR_NOMEM (-4)       /* device or host allocation failed */
+#define DSAX_ERR_UNSUPPORTED (-5) /* device is not a compute-capability 10.0 GPU */
+#define DSAX_ERR_DEVICE (-6)      /* a device-side check failed */
+
+/* ---- memory kinds ---- */
+#define DSAX_MEM_HOST 0
+#define DSAX_MEM_DEVICE 1
+
+/* ---- correlator input formats ---- */
+#define DSAX_FMT_CAPTURED 0  /* [pkt][nant_in][nchan][2 t][2 pol], 4+4-bit   */
+#define DSAX_FMT_REORDERED 1 /* [pkt][2*nchan][64][2 pol], 4+4-bit (REORDER key) */
+#define DSAX_FMT_XGPU_INT8 2 /* [pkt][2*nchan][64][2 pol][re,im] int8         */
+
+typedef struct dsax_config {
+    int npkt;            /* packets per block = xGPU NTIME (2048)                 */
+    int nant_in;         /* antennas present in the captured block (63, <= 64)     */
+    int nchan;           /* channels per packet (384); frequencies = 2*nchan      */
+    int nbeam;           /* beams formed (256; multiple of 64)                     */
+    int bf_pkt_per_out;  /* packets per Stokes-I output sample (16 = 32 times)    */
+    float bf_scale;      /* fixed scale before the uint8 quantisation             */
+    unsigned long long wait_limit_ns; /* bound on device waits (0 = 1 s)          */
+} dsax_config;
+
+typedef struct dsax_ctx dsax_ctx;
+
+/* Fills cfg with the reference block geometry (src/dsaX_def.h:72-81,
+ * README.md:34-62): npkt 2048, nant_in 63, nchan 384, nbeam 256,
+ * bf_pkt_per_out 16. */
+void dsax_default_config(dsax_config *cfg);
+
+/* Sizes in bytes of the block layouts for a configuration. */
+size_t dsax_block_bytes(const dsax_config *cfg, int fmt);
+size_t dsax_vis_bytes(const dsax_config *cfg);   /* 2*nchan*2080*4 complex float */
+size_t dsax_beam_bytes(const dsax_config *cfg);  /* (npkt/bf_pkt_per_out)*nbeam*(nchan/8) */
+
+int dsax_create(dsax_ctx **ctx, const dsax_config *cfg, int device);
+void dsax_destroy(dsax_ctx *ctx);
+const char *dsax_strerror(int status);
+const char *dsax_last_error(const dsax_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that enqueue
+ * their own work around DSAX_MEM_DEVICE calls. */
+void *dsax_stream(dsax_ctx *ctx);
+
+/* Waits for all work on the context stream; returns DSAX_ERR_TIMEOUT or
+ * DSAX_ERR_DEVICE if a kernel recorded a device-side error since the last
+ * check (and clears it). */
+int dsax_sync(dsax_ctx *ctx);
+
+/* Pinned host memory for fast transfers (cudaHostAlloc / cudaFreeHost). */
+int dsax_host_alloc(dsax_ctx *ctx, size_t nbytes, void **ptr);
+int dsax_host_free(dsax_ctx *ctx, void *ptr);
+
+/* ---- correlator ----
+ * Replaces massage() + promoter + xgpuCudaXengine(ctx, in, SYNCOP_DUMP)
+ * (src/dsaX_reorder_raw.c:153-169, src/dsaX_xgpu.cu:312-340).
+ * in  : one block in format `fmt` (dsax_block_bytes(cfg, fmt) bytes,
+ *       16-byte aligned).
+ * vis : xGPU triangular visibilities, MATRIX_ORDER_TRIANGULAR:
+ *       vis[((f*2080 + i*(i+1)/2 + j)*4 + 2*pol_i + pol_j)] = {re, im}
+ *       (float), f = 2*chan + time, j <= i, value sum_t x_i conj(x_j).
+ *       Bit-exact to an FP32 accumulation (all sums are integers < 2^24).
+ * accumulate = 0 overwrites vis; 1 adds the block's products to vis (the
+ * xGPU device integration buffer semantics).  Host-memory calls always
+ * overwrite. */
+int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
+int dsax_correlate_fmt(dsax_ctx *ctx, int fmt, const void *in, void *vis, int mem,
+                       int accumulate);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSAX_H */

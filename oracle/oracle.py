@@ -1,0 +1,256 @@
+"""ctypes wrapper around oracle/liboracle.so -- the CPU restatement of the
+DSA-110 X-engine hot path.
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, always as the checker; the product path
+(libdsax.so and its C-ABI) never loads it.
+
+Each function cites the reference code it restates; the C source carries
+the details.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+NST = 64
+NBL = NST * (NST + 1) // 2  # 2080 baselines
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the Makefile beside this file."""
+    srcs = [os.path.join(_HERE, f) for f in ("dsax_oracle.c", "dsax_oracle_flag.c")]
+    if force or not os.path.exists(_LIB_PATH) or any(
+            os.path.getmtime(s) > os.path.getmtime(_LIB_PATH) for s in srcs):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "-B" if force else "liboracle.so"])
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        i32, i64, f32, f64 = ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+        L.oracle_promote.argtypes = [P, P, i64]
+        L.oracle_massage.argtypes = [P, P, i32, i32, i32]
+        L.oracle_fluff_reorder.argtypes = [P, P, i32, i32, i32]
+        L.oracle_correlate.argtypes = [P, i32, i32, i32, i32, i32, P]
+        L.oracle_correlate.restype = i32
+        L.oracle_xengine_int8.argtypes = [P, i32, i32, P]
+        L.oracle_xengine_int8.restype = i32
+        L.oracle_simple_extract.argtypes = [P, i32, P]
+        L.oracle_beamform.argtypes = [P, i32, i32, i32, P, P, i32, i32, i32, i32, P]
+        L.oracle_beamform.restype = i32
+        L.oracle_geometric_weights.argtypes = [P, P, P, i32, i32, f64, f64, P, P]
+        L.oracle_plain_flag.argtypes = [P, P, P, P, P, P, P, P]
+        L.oracle_plain_flag.restype = i32
+        L.oracle_nthreads.restype = i32
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def nthreads() -> int:
+    return int(lib().oracle_nthreads())
+
+
+# --------------------------------------------------------------------------
+# seeded synthetic capture blocks
+# --------------------------------------------------------------------------
+def pack4(re: np.ndarray, im: np.ndarray) -> np.ndarray:
+    """4+4-bit two's complement byte: real in the low nibble, imag in the
+    high nibble (src/dsaX_xgpu.cu:74-75, utils/gen_packet.py:137-147)."""
+    return ((re.astype(np.int16) & 0xF) | ((im.astype(np.int16) & 0xF) << 4)).astype(np.uint8)
+
+
+def unpack4(b: np.ndarray):
+    b = b.astype(np.int16)
+    re = ((b & 0xF) ^ 0x8) - 8
+    im = (((b >> 4) & 0xF) ^ 0x8) - 8
+    return re.astype(np.int8), im.astype(np.int8)
+
+
+def gen_block(seed: int, npkt: int, nant_in: int, nchan: int,
+              dist: str = "uniform", sigma: float = 2.5) -> np.ndarray:
+    """Captured block [npkt][nant_in][nchan][2 t][2 pol] of packed samples.
+
+    dist="uniform": re, im uniform on the integers [-8, 7] (every byte value
+    equally likely).  dist="gauss": re, im = clip(round(N(0, sigma^2)), -8, 7).
+    """
+    shape = (npkt, nant_in, nchan, 2, 2)
+    rng = np.random.default_rng(seed)
+    if dist == "uniform":
+        return rng.integers(0, 256, size=shape, dtype=np.uint8)
+    if dist == "gauss":
+        n = int(np.prod(shape))
+        out = np.empty(n, dtype=np.uint8)
+        step = 1 << 24
+        for s in range(0, n, step):
+            e = min(n, s + step)
+            z = rng.standard_normal((2, e - s), dtype=np.float32) * np.float32(sigma)
+            q = np.clip(np.rint(z), -8, 7).astype(np.int8)
+            out[s:e] = pack4(q[0], q[1])
+        return out.reshape(shape)
+    raise ValueError(dist)
+
+
+# --------------------------------------------------------------------------
+# correlator
+# --------------------------------------------------------------------------
+def correlate(blk: np.ndarray, ch0: int = 0, nch: int | None = None) -> np.ndarray:
+    """X-engine on a captured block; returns vis[2*nch][2080][4][2] float32
+    (xGPU triangular order, f' = 2*chan + time).  See oracle_correlate."""
+    npkt, nant_in, nchan = blk.shape[:3]
+    nch = nchan - ch0 if nch is None else nch
+    blk = np.ascontiguousarray(blk)
+    vis = np.zeros((2 * nch, NBL, 4, 2), dtype=np.float32)
+    rc = lib().oracle_correlate(_ptr(blk), npkt, nant_in, nchan, ch0, nch, _ptr(vis))
+    if rc != 0:
+        raise RuntimeError(f"oracle_correlate failed: {rc}")
+    return vis
+
+
+def massage(blk: np.ndarray) -> np.ndarray:
+    """dsaX_reorder_raw massage(): -> [pkt][2*nchan][64][2 pol] packed bytes."""
+    npkt, nant_in, nchan = blk.shape[:3]
+    out = np.empty((npkt, 2 * nchan, NST, 2), dtype=np.uint8)
+    lib().oracle_massage(_ptr(np.ascontiguousarray(blk)), _ptr(out), npkt, nant_in, nchan)
+    return out
+
+
+def fluff_reorder(blk: np.ndarray) -> np.ndarray:
+    """AVX-512 fluff + transpose: -> [pkt][2*nchan][64][2 pol][re,im] int8."""
+    npkt, nant_in, nchan = blk.shape[:3]
+    out = np.empty((npkt, 2 * nchan, NST, 2, 2), dtype=np.int8)
+    lib().oracle_fluff_reorder(_ptr(np.ascontiguousarray(blk)), _ptr(out), npkt, nant_in, nchan)
+    return out
+
+
+def promote(packed: np.ndarray) -> np.ndarray:
+    out = np.empty(packed.size * 2, dtype=np.int8)
+    lib().oracle_promote(_ptr(np.ascontiguousarray(packed).reshape(-1)), _ptr(out), packed.size)
+    return out
+
+
+def xengine_int8(xin: np.ndarray) -> np.ndarray:
+    """X-engine on xGPU's 8-bit input [ntime][nfreq][64][2][2]."""
+    ntime, nfreq = xin.shape[:2]
+    vis = np.zeros((nfreq, NBL, 4, 2), dtype=np.float32)
+    rc = lib().oracle_xengine_int8(_ptr(np.ascontiguousarray(xin)), ntime, nfreq, _ptr(vis))
+    if rc != 0:
+        raise RuntimeError(f"oracle_xengine_int8 failed: {rc}")
+    return vis
+
+
+def simple_extract(vis: np.ndarray) -> np.ndarray:
+    nchan = vis.shape[0] // 2
+    out = np.empty((NBL, nchan, 2, 2), dtype=np.float32)
+    lib().oracle_simple_extract(_ptr(np.ascontiguousarray(vis)), nchan, _ptr(out))
+    return out
+
+
+# --------------------------------------------------------------------------
+# beamformer
+# --------------------------------------------------------------------------
+def random_phase_weights(seed: int, ngrp: int, nbeam: int):
+    """Unit-magnitude complex weights with seeded uniform phases, FP64,
+    layout [ngrp][2 pol][nbeam][64 ant]."""
+    rng = np.random.default_rng(seed)
+    ph = rng.uniform(0.0, 2.0 * np.pi, size=(ngrp, 2, nbeam, NST))
+    return np.cos(ph), np.sin(ph)
+
+
+def geometric_weights(antpos, cal, flagged, ngrp: int, nbeam: int,
+                      fch1_mhz: float = 1530.0, sep_arcmin: float = 1.0):
+    """calc_weights/init_weights restated in FP64 (see C source)."""
+    antpos = np.ascontiguousarray(antpos, dtype=np.float64)
+    cal = np.ascontiguousarray(cal, dtype=np.float64)
+    fl = np.ascontiguousarray(flagged, dtype=np.int32)
+    wre = np.empty((ngrp, 2, nbeam, NST))
+    wim = np.empty_like(wre)
+    lib().oracle_geometric_weights(_ptr(antpos), _ptr(cal), _ptr(fl), ngrp, nbeam,
+                                   float(fch1_mhz), float(sep_arcmin), _ptr(wre), _ptr(wim))
+    return wre, wim
+
+
+def beamform_power(blk: np.ndarray, wre: np.ndarray, wim: np.ndarray,
+                   pkt_per_out: int = 16, g0: int = 0, ng: int | None = None) -> np.ndarray:
+    """FP64 Stokes-I power [npkt/pkt_per_out][nbeam][ng]."""
+    npkt, nant_in, nchan = blk.shape[:3]
+    nbeam = wre.shape[2]
+    ng = nchan // 8 - g0 if ng is None else ng
+    pw = np.empty((npkt // pkt_per_out, nbeam, ng), dtype=np.float64)
+    rc = lib().oracle_beamform(_ptr(np.ascontiguousarray(blk)), npkt, nant_in, nchan,
+                               _ptr(np.ascontiguousarray(wre)), _ptr(np.ascontiguousarray(wim)),
+                               nbeam, pkt_per_out, g0, ng, _ptr(pw))
+    if rc != 0:
+        raise RuntimeError(f"oracle_beamform failed: {rc}")
+    return pw
+
+
+def quantize_u8(power: np.ndarray, scale: float) -> np.ndarray:
+    """Fixed scaling to uint8: saturate(rint(P * scale)) to [0, 255]."""
+    return np.clip(np.rint(power * scale), 0, 255).astype(np.uint8)
+
+
+# --------------------------------------------------------------------------
+# plain flagger
+# --------------------------------------------------------------------------
+class FlagParams(ctypes.Structure):
+    _fields_ = [("nbeam", ctypes.c_int), ("ntime", ctypes.c_int), ("nchan", ctypes.c_int),
+                ("guard", ctypes.c_int), ("filt", ctypes.c_int), ("tbin", ctypes.c_int),
+                ("fbin", ctypes.c_int), ("ts_base", ctypes.c_int), ("tsflag", ctypes.c_int),
+                ("parity", ctypes.c_int), ("thresh", ctypes.c_float),
+                ("var_add", ctypes.c_float), ("ts_thresh", ctypes.c_float),
+                ("nperm", ctypes.c_int), ("perm", ctypes.c_int * 8)]
+
+
+def flag_params(nbeam, ntime, nchan, guard=None, filt=21, tbin=128, fbin=8,
+                ts_base=None, tsflag=1, parity=0, thresh=5.0, var_add=0.5,
+                ts_thresh=10.0, perm=()):
+    p = FlagParams()
+    p.nbeam, p.ntime, p.nchan = nbeam, ntime, nchan
+    p.guard = int(round(nchan * 128 / 1024)) if guard is None else guard
+    p.filt, p.tbin, p.fbin = filt, tbin, fbin
+    p.ts_base = ntime // 16 if ts_base is None else ts_base
+    p.tsflag, p.parity = tsflag, parity
+    p.thresh, p.var_add, p.ts_thresh = thresh, var_add, ts_thresh
+    p.nperm = len(perm)
+    for i, c in enumerate(perm):
+        p.perm[i] = c
+    return p
+
+
+def plain_flag(x: np.ndarray, params: FlagParams, oldspec=None):
+    """Returns (chanmask[B][C] int32, tsmask[B][T] int32, chan_margin,
+    ts_margin, stats) for a float32 filterbank x[B][T][C]."""
+    B, T, C = x.shape
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    cm = np.zeros((B, C), np.int32)
+    tm = np.zeros((B, T), np.int32)
+    cmg = np.zeros((B, C), np.float32)
+    tmg = np.zeros((B, T), np.float32)
+    st = np.zeros(5 * B * C + B * T, np.float32)
+    old = None if oldspec is None else np.ascontiguousarray(oldspec, dtype=np.float32)
+    lib().oracle_plain_flag(_ptr(x), ctypes.byref(params),
+                            None if old is None else _ptr(old),
+                            _ptr(cm), _ptr(tm), _ptr(cmg), _ptr(tmg), _ptr(st))
+    stats = {
+        "spec": st[0:B * C].reshape(B, C), "var": st[B * C:2 * B * C].reshape(B, C),
+        "max": st[2 * B * C:3 * B * C].reshape(B, C), "pp": st[3 * B * C:4 * B * C].reshape(B, C),
+        "sub": st[4 * B * C:5 * B * C].reshape(B, C), "ts": st[5 * B * C:].reshape(B, T),
+    }
+    return cm, tm, cmg, tmg, stats
