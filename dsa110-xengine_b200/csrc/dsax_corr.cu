@@ -193,14 +193,15 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
     }
   } else {
     // ------------------------------------------------------------ UMMA issuer
-    for (int ks = 0; ks < nks && !abort_sh; ++ks) {
-      const int s = ks % kStages;
-      const uint32_t ph = (uint32_t)(ks / kStages) & 1u;
-      if (!mbar_wait_bounded(&full_bar[s], ph, &abort_sh, a.err, DEV_ERR_WAIT_FULL,
-                             a.wait_limit_ns))
-        break;
-      tc_fence_after();
-      if (lane == 0) {
+    // One thread waits and issues; the other 31 lanes idle until the end.
+    if (lane == 0) {
+      for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+        const int s = ks % kStages;
+        const uint32_t ph = (uint32_t)(ks / kStages) & 1u;
+        if (!mbar_wait_bounded(&full_bar[s], ph, &abort_sh, a.err, DEV_ERR_WAIT_FULL,
+                               a.wait_limit_ns))
+          break;
+        tc_fence_after();
         const uint32_t stage = smem_base + (uint32_t)s * kStageBytes;
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
@@ -213,18 +214,19 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
         }
         umma_commit(&empty_bar[s]);
       }
-      __syncwarp();
+      umma_commit(&accum_bar);  // fires when every issued UMMA is done
     }
-    if (lane == 0) umma_commit(&accum_bar);  // fires when every issued UMMA is done
     __syncwarp();
   }
 
   // ---------------------------------------------------------------- epilogue
   if (warp < 8) {
-    const bool ok = mbar_wait_bounded(&accum_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
-                                      a.wait_limit_ns);
+    bool ok = mbar_wait_bounded(&accum_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
+                                a.wait_limit_ns);
     tc_fence_after();
-    if (ok && !abort_sh) {
+    // tcgen05.ld is .sync.aligned: the whole warp takes the same branch.
+    ok = __all_sync(0xffffffffu, ok && !abort_sh);
+    if (ok) {
       const int q = warp & 3;         // TMEM lane quarter of this warp
       const int t = warp >> 2;        // frequency within the channel
       const int m = 32 * q + lane;    // row = 2*station + pol
@@ -258,6 +260,13 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
   tc_fence_before();
   __syncthreads();
   if (warp == 8) {
+    // Never free TMEM under an in-flight UMMA: wait for the final commit
+    // (bounded, and independent of the abort flag).
+    if (lane == 0) {
+      volatile int no_abort = 0;
+      mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+    }
+    __syncwarp();
     tc_fence_after();
     tmem_dealloc(tmem, 512);
   }
