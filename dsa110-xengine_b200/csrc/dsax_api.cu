@@ -188,6 +188,34 @@ int dsax_host_free(dsax_ctx *c, void *p) {
   return cuda_check(c, cudaFreeHost(p), "cudaFreeHost");
 }
 
+// Enqueues the correlation of one device-resident block on the ctx stream.
+static int correlate_device(dsax_ctx *c, int fmt, const void *in, float *vis, int accumulate) {
+  CorrArgs a{};
+  a.npkt = c->cfg.npkt;
+  a.nant_in = fmt == DSAX_FMT_CAPTURED ? c->cfg.nant_in : 64;
+  a.nchan = c->cfg.nchan;
+  a.err = c->d_err;
+  a.wait_limit_ns = c->cfg.wait_limit_ns;
+  a.accumulate = accumulate ? 1 : 0;
+  a.vis = vis;
+  a.in = static_cast<const uint8_t *>(in);
+  if (fmt == DSAX_FMT_CAPTURED && c->cfg.corr_path != 1) {
+    // corner turn into the context's REORDER-layout buffer, then correlate
+    const size_t nre = dsax_block_bytes(&c->cfg, DSAX_FMT_REORDERED);
+    int rc = ensure_buffer(c, c->aux[AUX_REORDERED], nre, "corner-turned block");
+    if (rc != DSAX_OK) return rc;
+    if (launch_reorder(a.in, static_cast<uint8_t *>(c->aux[AUX_REORDERED].ptr), c->cfg.npkt,
+                       c->cfg.nant_in, c->cfg.nchan, c->stream) != 0)
+      return cuda_check(c, cudaGetLastError(), "corner-turn launch");
+    a.in = static_cast<const uint8_t *>(c->aux[AUX_REORDERED].ptr);
+    a.nant_in = 64;
+    fmt = DSAX_FMT_REORDERED;
+  }
+  if (launch_correlate(a, fmt, c->stream) != 0)
+    return cuda_check(c, cudaGetLastError(), "correlator launch");
+  return DSAX_OK;
+}
+
 int dsax_correlate_fmt(dsax_ctx *c, int fmt, const void *in, void *vis, int mem,
                        int accumulate) {
   if (!c || !in || !vis) return DSAX_ERR_ARG;
@@ -198,34 +226,50 @@ int dsax_correlate_fmt(dsax_ctx *c, int fmt, const void *in, void *vis, int mem,
   DeviceGuard g(c->device);
   const size_t nin = dsax_block_bytes(&c->cfg, fmt);
   const size_t nvis = dsax_vis_bytes(&c->cfg);
-  CorrArgs a{};
-  a.npkt = c->cfg.npkt;
-  a.nant_in = fmt == DSAX_FMT_CAPTURED ? c->cfg.nant_in : 64;
-  a.nchan = c->cfg.nchan;
-  a.err = c->d_err;
-  a.wait_limit_ns = c->cfg.wait_limit_ns;
-  int rc;
   if (mem == DSAX_MEM_DEVICE) {
     if (!aligned16(in) || !aligned16(vis))
       return set_error(c, DSAX_ERR_ARG, "device pointers must be 16-byte aligned");
-    a.in = static_cast<const uint8_t *>(in);
-    a.vis = static_cast<float *>(vis);
-    a.accumulate = accumulate ? 1 : 0;
-    rc = launch_correlate(a, fmt, c->stream);
-    if (rc != 0) return cuda_check(c, cudaGetLastError(), "correlator launch");
-    return DSAX_OK;
+    return correlate_device(c, fmt, in, static_cast<float *>(vis), accumulate);
   }
+  int rc;
   if ((rc = ensure_buffer(c, c->in_buf, nin, "input block")) != DSAX_OK) return rc;
   if ((rc = ensure_buffer(c, c->vis_buf, nvis, "visibilities")) != DSAX_OK) return rc;
   cudaError_t e = cudaMemcpyAsync(c->in_buf.ptr, in, nin, cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "H2D block");
-  a.in = static_cast<const uint8_t *>(c->in_buf.ptr);
-  a.vis = static_cast<float *>(c->vis_buf.ptr);
-  a.accumulate = 0;
-  if (launch_correlate(a, fmt, c->stream) != 0)
-    return cuda_check(c, cudaGetLastError(), "correlator launch");
+  if ((rc = correlate_device(c, fmt, c->in_buf.ptr, static_cast<float *>(c->vis_buf.ptr), 0)) !=
+      DSAX_OK)
+    return rc;
   e = cudaMemcpyAsync(vis, c->vis_buf.ptr, nvis, cudaMemcpyDeviceToHost, c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "D2H visibilities");
+  return dsax_sync(c);
+}
+
+int dsax_reorder(dsax_ctx *c, const void *captured, void *reordered, int mem) {
+  if (!c || !captured || !reordered) return DSAX_ERR_ARG;
+  if (mem != DSAX_MEM_HOST && mem != DSAX_MEM_DEVICE) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  const size_t nin = dsax_block_bytes(&c->cfg, DSAX_FMT_CAPTURED);
+  const size_t nout = dsax_block_bytes(&c->cfg, DSAX_FMT_REORDERED);
+  if (mem == DSAX_MEM_DEVICE) {
+    if (!aligned16(captured) || !aligned16(reordered))
+      return set_error(c, DSAX_ERR_ARG, "device pointers must be 16-byte aligned");
+    if (launch_reorder(static_cast<const uint8_t *>(captured), static_cast<uint8_t *>(reordered),
+                       c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan, c->stream) != 0)
+      return cuda_check(c, cudaGetLastError(), "corner-turn launch");
+    return DSAX_OK;
+  }
+  int rc;
+  if ((rc = ensure_buffer(c, c->in_buf, nin, "input block")) != DSAX_OK) return rc;
+  if ((rc = ensure_buffer(c, c->aux[AUX_REORDER_OUT], nout, "corner-turned block")) != DSAX_OK)
+    return rc;
+  cudaError_t e = cudaMemcpyAsync(c->in_buf.ptr, captured, nin, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_check(c, e, "H2D block");
+  if (launch_reorder(static_cast<const uint8_t *>(c->in_buf.ptr),
+                     static_cast<uint8_t *>(c->aux[AUX_REORDER_OUT].ptr), c->cfg.npkt,
+                     c->cfg.nant_in, c->cfg.nchan, c->stream) != 0)
+    return cuda_check(c, cudaGetLastError(), "corner-turn launch");
+  e = cudaMemcpyAsync(reordered, c->aux[AUX_REORDER_OUT].ptr, nout, cudaMemcpyDeviceToHost, c->stream);
+  if (e != cudaSuccess) return cuda_check(c, e, "D2H corner-turned block");
   return dsax_sync(c);
 }
 

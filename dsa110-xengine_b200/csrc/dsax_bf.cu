@@ -1,0 +1,319 @@
+// dsax_bf.cu -- the Stokes-I beamformer on sm_100a tensor cores (BF16 in,
+// FP32 accumulate in TMEM), with the 4-bit unpack fused into the operand
+// staging and the detect + time/channel/pol sum + uint8 quantisation fused
+// into the epilogue.
+//
+// Replaces src/dsaX_beamformer.cu promoter (:170-193), beamformer (:267-416,
+// wmma m16n16k16 with FP16 accumulators), badder/adder (:79-158).
+//
+// Arithmetic.  For channel group g (8 fine channels), pol p and beam b, the
+// beam voltage of sample s = (packet, chunnel = 2*chan + time) is
+//     B[b][s] = sum_a w[g][p][b][a] * x[a][s]            (no conjugate)
+// and the output is
+//     P[t_out][b][g] = sum_{p} sum_{s in t_out} |B[b][s]|^2
+// over ppo packets x 16 chunnels x 2 pols.
+// As a real GEMM (K = 64 antennas x {re, im} = 128):
+//     A row b      = [ wr_a, -wi_a ]_a   -> Re B
+//     A row 64 + b = [ wi_a,  wr_a ]_a   -> Im B
+//     B column s   = [ xr_a,  xi_a ]_a
+// so one UMMA D[128 x 256] = A * B^T gives Re/Im of 64 beams x 256 samples.
+//
+// Tiling.  A CTA owns (channel group g, beam tile of 64 beams) and a range of
+// stages in time; a stage is 16 packets (256 samples) of one pol.  The
+// weights of both pols (64 KB) stay resident; data stages are double
+// buffered (64 KB each); TMEM holds two 256-column accumulators so the
+// epilogue of stage i overlaps the MMAs of stage i+1.
+//   warps 0-3 : producers (global 4-bit -> BF16 K-major swizzled tiles)
+//   warps 4-7 : epilogue (TMEM -> |.|^2 row sums -> outputs)
+//   warp  8   : weight loader (bulk copy) and single-thread UMMA issuer
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dsax_internal.h"
+#include "dsax_ptx.cuh"
+
+namespace dsax {
+
+namespace bf {
+constexpr int kPktPerStage = 16;                      // N = 16 packets x 16 chunnels = 256
+constexpr int kN = 256;
+constexpr int kKBlockBytes = 128;                     // 64 bf16 = 32 antennas x {re,im}
+constexpr int kWTileBytes = 128 * kKBlockBytes;       // 128 rows x 128 B = 16 KB
+constexpr int kWBytes = 2 /*pol*/ * 2 /*kb*/ * kWTileBytes;  // 64 KB per (g, bt)
+constexpr int kDTileBytes = kN * kKBlockBytes;        // 256 rows x 128 B = 32 KB
+constexpr int kStageBytes = 2 /*kb*/ * kDTileBytes;   // 64 KB
+constexpr int kStages = 2;
+constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes;
+constexpr int kThreads = 288;
+constexpr uint32_t kIdesc = umma_idesc(/*F32*/ 1, /*BF16*/ 1, /*BF16*/ 1, 128, kN);
+}  // namespace bf
+
+__device__ __forceinline__ void bf_decode(int u, int npg, int nbt, int &g, int &bt, int &pg,
+                                          int &pol) {
+  pol = u & 1;
+  const int r = u >> 1;
+  pg = r % npg;
+  const int gb = r / npg;
+  bt = gb % nbt;
+  g = gb / nbt;
+}
+
+__global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
+  using namespace bf;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kStages];
+  __shared__ __align__(8) uint64_t empty_bar[kStages];
+  __shared__ __align__(8) uint64_t tfull_bar[2];
+  __shared__ __align__(8) uint64_t tempty_bar[2];
+  __shared__ __align__(8) uint64_t wload_bar;
+  __shared__ __align__(8) uint64_t wdrain_bar;
+  __shared__ __align__(8) uint64_t final_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+  __shared__ float red[4][64];
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  const uint32_t wsm = base;                  // weights [pol][kb][128 x 128 B]
+  const uint32_t dsm = base + kWBytes;        // data stages [s][kb][256 x 128 B]
+
+  const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / kPktPerStage;
+  const int align = 2 * (a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1);
+  const int nunits = ngrp * nbt * npg * 2;
+  const int nchunks = nunits / align;
+  const int u_lo = (int)((long long)blockIdx.x * nchunks / gridDim.x) * align;
+  const int u_hi = (int)((long long)(blockIdx.x + 1) * nchunks / gridDim.x) * align;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full_bar[s], 128);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], 128);
+    }
+    mbar_init(&wload_bar, 1);
+    mbar_init(&wdrain_bar, 1);
+    mbar_init(&final_bar, 1);
+    abort_sh = 0;
+    mbar_fence_init();
+  }
+  if (warp == 8) {
+    tmem_alloc(&tmem_base_sh, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  if ((tmem & 0xFFFFu) != 0u) {
+    if (tid == 0) atomicOr(a.err, DEV_ERR_TMEM);
+    abort_sh = 1;
+  }
+
+  if (warp < 4) {
+    // ------------------------------------------------------------ producers
+    const int j = lane & 7;
+    const int q = 4 * warp + (lane >> 3);          // packet within the stage
+    const int64_t ant_stride = (int64_t)a.nchan * 4;
+    const int64_t pkt_stride = (int64_t)a.nant_in * ant_stride;
+    for (int u = u_lo, i = 0; u < u_hi && !abort_sh; ++u, ++i) {
+      const int s = i % kStages;
+      const uint32_t ph = (uint32_t)(i / kStages) & 1u;
+      if (!mbar_wait_bounded(&empty_bar[s], ph ^ 1u, &abort_sh, a.err, DEV_ERR_WAIT_EMPTY,
+                             a.wait_limit_ns))
+        break;
+      int g, bt, pg, pol;
+      bf_decode(u, npg, nbt, g, bt, pg, pol);
+      const int p = pg * kPktPerStage + q;
+      const uint32_t sel = (uint32_t)pol | ((4u + pol) << 4) | ((2u + pol) << 8) | ((6u + pol) << 12);
+      const uint32_t stage = dsm + (uint32_t)s * kStageBytes;
+#pragma unroll
+      for (int it = 0; it < 4; ++it) {
+        const int kb = it & 1, h = it >> 1;
+        uint4 U[4];
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+          const int ant = 32 * kb + 4 * j + ii;
+          if (ant < a.nant_in && p < a.npkt) {
+            U[ii] = __ldg(reinterpret_cast<const uint4 *>(a.in + p * pkt_stride + ant * ant_stride +
+                                                          (int64_t)(8 * g) * 4 + 16 * h));
+          } else {
+            U[ii] = make_uint4(0u, 0u, 0u, 0u);
+          }
+        }
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const uint32_t u0 = w == 0 ? U[0].x : w == 1 ? U[0].y : w == 2 ? U[0].z : U[0].w;
+          const uint32_t u1 = w == 0 ? U[1].x : w == 1 ? U[1].y : w == 2 ? U[1].z : U[1].w;
+          const uint32_t u2 = w == 0 ? U[2].x : w == 1 ? U[2].y : w == 2 ? U[2].z : U[2].w;
+          const uint32_t u3 = w == 0 ? U[3].x : w == 1 ? U[3].y : w == 2 ? U[3].z : U[3].w;
+          const uint32_t t01 = __byte_perm(u0, u1, sel);
+          const uint32_t t23 = __byte_perm(u2, u3, sel);
+#pragma unroll
+          for (int odd = 0; odd < 2; ++odd) {
+            const uint32_t x = __byte_perm(t01, t23, odd ? 0x7632u : 0x5410u);
+            uint32_t o[4];
+            nib8_to_bf16x8(x, o);
+            const int k = 8 * h + 2 * w + odd;     // chunnel = 2*chan + time
+            const uint32_t row = (uint32_t)(16 * q + k);
+            st_shared_v4(stage + (uint32_t)kb * kDTileBytes + sw128_offset(row, (uint32_t)j),
+                         o[0], o[1], o[2], o[3]);
+          }
+        }
+      }
+      fence_proxy_async_smem();
+      mbar_arrive(&full_bar[s]);
+    }
+  } else if (warp < 8) {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp - 4;                          // TMEM lane quarter
+    const int m = 32 * q + lane;                     // accumulator row
+    const int nsub = a.ppo < kPktPerStage ? kPktPerStage / a.ppo : 1;  // outputs per stage
+    const int span = kN / nsub;                      // columns per output
+    const int pgs_per_out = a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int u = u_lo, i = 0; u < u_hi; ++u, ++i) {
+      const int b = i & 1;
+      const uint32_t ph = (uint32_t)(i >> 1) & 1u;
+      bool ok = mbar_wait_bounded(&tfull_bar[b], ph, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
+                                  a.wait_limit_ns);
+      tc_fence_after();
+      // The four epilogue warps never leave this loop early: they meet at the
+      // named barriers below, which have no timeout.  After an abort they
+      // skip the TMEM work (tcgen05.ld is .sync.aligned: warp-uniform test).
+      ok = __all_sync(0xffffffffu, ok && !abort_sh);
+      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)b * 256u;
+#pragma unroll
+      for (int c = 0; c < (ok ? kN / 32 : 0); ++c) {
+        uint32_t r[32];
+        tmem_ld32(taddr + 32u * c, r);
+        tmem_wait_ld();
+        float sq = 0.f;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+          const float v = __uint_as_float(r[e]);
+          sq = fmaf(v, v, sq);
+        }
+        const int sub = (32 * c) / span;
+        if (nsub == 1) acc[0] += sq;
+        else if (sub == 0) acc[0] += sq;
+        else if (sub == 1) acc[1] += sq;
+        else if (sub == 2) acc[2] += sq;
+        else acc[3] += sq;
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty_bar[b]);
+
+      int g, bt, pg, pol;
+      bf_decode(u, npg, nbt, g, bt, pg, pol);
+      if (pol == 1 && ((pg + 1) % pgs_per_out) == 0) {
+        // rows m and m + 64 hold Re and Im of the same beam
+        if (m >= 64)
+          for (int sI = 0; sI < nsub; ++sI) red[sI][m - 64] = acc[sI];
+        named_bar(1, 128);
+        if (m < 64 && !abort_sh) {
+          const int beam = 64 * bt + m;
+          for (int sI = 0; sI < nsub; ++sI) {
+            const float P = acc[sI] + red[sI][m];
+            const int to = a.ppo <= kPktPerStage ? pg * nsub + sI : pg / pgs_per_out;
+            const int64_t o = ((int64_t)to * a.nbeam + beam) * ngrp + g;
+            if (a.out_f32) a.out_f32[o] = P;
+            if (a.out_u8) {
+              int v = __float2int_rn(P * a.scale);
+              a.out_u8[o] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+            }
+          }
+        }
+        named_bar(1, 128);
+        acc[0] = acc[1] = acc[2] = acc[3] = 0.f;
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ weights + UMMA
+    if (lane == 0) {
+      int cur_gb = -1;
+      uint32_t nload = 0, ndrain = 0;
+      for (int u = u_lo, i = 0; u < u_hi && !abort_sh; ++u, ++i) {
+        int g, bt, pg, pol;
+        bf_decode(u, npg, nbt, g, bt, pg, pol);
+        const int gb = g * nbt + bt;
+        if (gb != cur_gb) {
+          if (i > 0) {  // no UMMA may still read the old weights
+            umma_commit(&wdrain_bar);
+            if (!mbar_wait_bounded(&wdrain_bar, ndrain & 1u, &abort_sh, a.err,
+                                   DEV_ERR_WAIT_ACCUM, a.wait_limit_ns))
+              break;
+            ++ndrain;
+          }
+          mbar_arrive_expect_tx(&wload_bar, (uint32_t)kWBytes);
+          const uint8_t *src = a.wimg + (int64_t)gb * kWBytes;
+#pragma unroll
+          for (int c = 0; c < kWBytes / 16384; ++c)
+            bulk_g2s(wsm + 16384u * c, src + 16384 * c, 16384u, &wload_bar);
+          if (!mbar_wait_bounded(&wload_bar, nload & 1u, &abort_sh, a.err, DEV_ERR_WAIT_FULL,
+                                 a.wait_limit_ns))
+            break;
+          ++nload;
+          cur_gb = gb;
+        }
+        const int s = i % kStages;
+        const int b = i & 1;
+        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)(i / kStages) & 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+          break;
+        if (!mbar_wait_bounded(&tempty_bar[b], ((uint32_t)(i >> 1) & 1u) ^ 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+          break;
+        tc_fence_after();
+        const uint32_t wpol = wsm + (uint32_t)pol * (2 * kWTileBytes);
+        const uint32_t stage = dsm + (uint32_t)s * kStageBytes;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {   // K = 128 bf16 = 8 x 16
+          const uint32_t kb = kk >> 2, koff = 32u * (kk & 3);
+          const uint64_t ad = umma_desc_sw128(wpol + kb * kWTileBytes + koff, 1024u);
+          const uint64_t bd = umma_desc_sw128(stage + kb * kDTileBytes + koff, 1024u);
+          umma_f16(tmem + (uint32_t)b * 256u, ad, bd, kIdesc, kk > 0);
+        }
+        umma_commit(&empty_bar[s]);
+        umma_commit(&tfull_bar[b]);
+      }
+      umma_commit(&final_bar);
+    }
+    __syncwarp();
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    if (lane == 0) {
+      volatile int no_abort = 0;
+      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+    }
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
+  static bool attr_done = false;
+  if (!attr_done) {
+    if (cudaFuncSetAttribute(bf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bf::kSmemBytes) != cudaSuccess)
+      return -2;
+    attr_done = true;
+  }
+  const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / bf::kPktPerStage;
+  const int align = 2 * (a.ppo > bf::kPktPerStage ? a.ppo / bf::kPktPerStage : 1);
+  const int nchunks = ngrp * nbt * npg * 2 / align;
+  const int grid = nchunks < num_sms ? nchunks : num_sms;
+  void *args[] = {(void *)&a};
+  return cudaLaunchKernel((const void *)bf_kernel, dim3(grid), dim3(bf::kThreads), args,
+                          bf::kSmemBytes, st) == cudaSuccess
+             ? 0
+             : -2;
+}
+
+}  // namespace dsax

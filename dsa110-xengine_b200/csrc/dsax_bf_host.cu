@@ -1,0 +1,131 @@
+// dsax_bf_host.cu -- beamformer entry points of the C-ABI and the host-side
+// conversion of FP64 weights to the BF16 UMMA operand image.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "../../include/dsax.h"
+#include "dsax_ctx.h"
+#include "dsax_internal.h"
+
+using namespace dsax;
+
+namespace {
+
+// Round-to-nearest-even FP32 -> BF16 (keep the upper 16 bits, adding half an
+// ulp of the kept part plus the tie-breaking lsb); NaN stays a quiet NaN.
+uint16_t f32_to_bf16_rne(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+// Byte offset of 16-byte chunk `chunk` of row `row` in a K-major 128-byte
+// swizzled tile (8-row x 128-byte atoms), as the kernels write it.
+uint32_t sw128_off(uint32_t row, uint32_t chunk) {
+  return (row >> 3) * 1024u + (row & 7u) * 128u + (((chunk ^ (row & 7u)) & 7u) << 4);
+}
+
+constexpr size_t kWTile = 16384;  // 128 rows x 128 B
+constexpr size_t kWPerGB = 4 * kWTile;  // [2 pol][2 kb] per (group, beam tile)
+
+}  // namespace
+
+extern "C" {
+
+int dsax_set_weights(dsax_ctx *c, const double *wre, const double *wim) {
+  if (!c || !wre || !wim) return DSAX_ERR_ARG;
+  const int ngrp = c->cfg.nchan / 8, nbeam = c->cfg.nbeam;
+  if (c->cfg.nchan % 8 || nbeam < 64 || nbeam % 64)
+    return set_error(c, DSAX_ERR_ARG, "beamformer needs nchan %% 8 == 0 and nbeam %% 64 == 0");
+  const int nbt = nbeam / 64;
+  const size_t nbytes = (size_t)ngrp * nbt * kWPerGB;
+  std::vector<uint8_t> img(nbytes, 0);
+  for (int g = 0; g < ngrp; ++g)
+    for (int bt = 0; bt < nbt; ++bt)
+      for (int pol = 0; pol < 2; ++pol)
+        for (int kb = 0; kb < 2; ++kb)
+          for (int m = 0; m < 128; ++m)
+            for (int j = 0; j < 8; ++j)
+              for (int i = 0; i < 4; ++i) {
+                const int ant = 32 * kb + 4 * j + i;
+                const int beam = 64 * bt + (m & 63);
+                const size_t wi_ = (((size_t)g * 2 + pol) * nbeam + beam) * 64 + ant;
+                const double wr = wre[wi_], wi = wim[wi_];
+                const double c0 = m < 64 ? wr : wi;     // multiplies x_re
+                const double c1 = m < 64 ? -wi : wr;    // multiplies x_im
+                const size_t off = (((size_t)(g * nbt + bt) * 2 + pol) * 2 + kb) * kWTile +
+                                   sw128_off((uint32_t)m, (uint32_t)j) + 4 * i;
+                const uint16_t b0 = f32_to_bf16_rne((float)c0), b1 = f32_to_bf16_rne((float)c1);
+                memcpy(&img[off], &b0, 2);
+                memcpy(&img[off + 2], &b1, 2);
+              }
+  DeviceGuard dg(c->device);
+  int rc = ensure_buffer(c, c->aux[AUX_WIMG_BF16], nbytes, "beamformer weights");
+  if (rc != DSAX_OK) return rc;
+  cudaError_t e = cudaMemcpyAsync(c->aux[AUX_WIMG_BF16].ptr, img.data(), nbytes,
+                                  cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_check(c, e, "upload weights");
+  c->weights_ready = 1;
+  return DSAX_OK;
+}
+
+int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int mem) {
+  if (!c || !blk || (!out_u8 && !out_f32)) return DSAX_ERR_ARG;
+  if (!c->weights_ready) return set_error(c, DSAX_ERR_ARG, "dsax_set_weights not called");
+  const dsax_config &cf = c->cfg;
+  const int ppo = cf.bf_pkt_per_out;
+  if (cf.nchan % 8 || cf.nbeam % 64 || cf.npkt % 16 || ppo <= 0 || cf.npkt % ppo ||
+      !(ppo == 4 || ppo == 8 || ppo % 16 == 0))
+    return set_error(c, DSAX_ERR_ARG,
+                     "beamformer needs nchan%%8==0, nbeam%%64==0, npkt%%16==0, npkt%%ppo==0, "
+                     "ppo in {4, 8, 16k}");
+  if (mem != DSAX_MEM_HOST && mem != DSAX_MEM_DEVICE) return DSAX_ERR_ARG;
+  DeviceGuard dg(c->device);
+  const size_t nin = dsax_block_bytes(&cf, DSAX_FMT_CAPTURED);
+  const size_t nout = dsax_beam_bytes(&cf);
+  BfArgs a{};
+  a.wimg = static_cast<const uint8_t *>(c->aux[AUX_WIMG_BF16].ptr);
+  a.err = c->d_err;
+  a.npkt = cf.npkt;
+  a.nant_in = cf.nant_in;
+  a.nchan = cf.nchan;
+  a.nbeam = cf.nbeam;
+  a.ppo = ppo;
+  a.scale = cf.bf_scale;
+  a.wait_limit_ns = cf.wait_limit_ns;
+  if (mem == DSAX_MEM_DEVICE) {
+    if (!aligned16(blk)) return set_error(c, DSAX_ERR_ARG, "block must be 16-byte aligned");
+    a.in = static_cast<const uint8_t *>(blk);
+    a.out_u8 = static_cast<uint8_t *>(out_u8);
+    a.out_f32 = static_cast<float *>(out_f32);
+    if (launch_beamform(a, c->num_sms, c->stream) != 0)
+      return cuda_check(c, cudaGetLastError(), "beamformer launch");
+    return DSAX_OK;
+  }
+  int rc;
+  if ((rc = ensure_buffer(c, c->in_buf, nin, "input block")) != DSAX_OK) return rc;
+  if (out_u8 && (rc = ensure_buffer(c, c->aux[AUX_BEAM_U8], nout, "beams")) != DSAX_OK) return rc;
+  if (out_f32 && (rc = ensure_buffer(c, c->aux[AUX_BEAM_F32], nout * 4, "beam power")) != DSAX_OK)
+    return rc;
+  cudaError_t e = cudaMemcpyAsync(c->in_buf.ptr, blk, nin, cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_check(c, e, "H2D block");
+  a.in = static_cast<const uint8_t *>(c->in_buf.ptr);
+  a.out_u8 = out_u8 ? static_cast<uint8_t *>(c->aux[AUX_BEAM_U8].ptr) : nullptr;
+  a.out_f32 = out_f32 ? static_cast<float *>(c->aux[AUX_BEAM_F32].ptr) : nullptr;
+  if (launch_beamform(a, c->num_sms, c->stream) != 0)
+    return cuda_check(c, cudaGetLastError(), "beamformer launch");
+  if (out_u8 && (e = cudaMemcpyAsync(out_u8, a.out_u8, nout, cudaMemcpyDeviceToHost, c->stream)) !=
+                    cudaSuccess)
+    return cuda_check(c, e, "D2H beams");
+  if (out_f32 && (e = cudaMemcpyAsync(out_f32, a.out_f32, nout * 4, cudaMemcpyDeviceToHost,
+                                      c->stream)) != cudaSuccess)
+    return cuda_check(c, e, "D2H beam power");
+  return dsax_sync(c);
+}
+
+}  // extern "C"

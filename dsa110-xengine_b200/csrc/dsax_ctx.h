@@ -7,6 +7,19 @@
 
 namespace dsax {
 
+// Slots of dsax_ctx::aux.
+enum {
+  AUX_WIMG_BF16 = 0,  // beamformer weight operand image (BF16)
+  AUX_WIMG_FP8 = 1,   // beamformer weight operand image (FP8 E4M3)
+  AUX_BEAM_U8 = 2,    // host-mode staging: Stokes-I uint8
+  AUX_BEAM_F32 = 3,   // host-mode staging: FP32 power
+  AUX_FLAG_STATS = 4, // flagger statistics + counts
+  AUX_FLAG_X = 5,     // host-mode staging: filterbank + oldspec
+  AUX_FLAG_MASK = 6,  // host-mode staging: masks
+  AUX_REORDERED = 7,  // corner-turned block for the two-pass correlator path
+  AUX_REORDER_OUT = 8,  // host-mode staging for dsax_reorder output
+};
+
 struct DevBuf {
   void *ptr = nullptr;
   size_t bytes = 0;
@@ -43,7 +56,8 @@ struct dsax_ctx {
   int *h_err = nullptr;   // pinned readback slot
   dsax::DevBuf in_buf;    // host-mode staging: input block
   dsax::DevBuf vis_buf;   // host-mode staging: visibilities
-  dsax::DevBuf aux[8];    // per-stage scratch (beamformer / flagger)
+  dsax::DevBuf aux[16];   // per-stage buffers, indexed by dsax::AUX_*
+  int weights_ready = 0;
   char errmsg[512] = {0};
 
   void release_all() {

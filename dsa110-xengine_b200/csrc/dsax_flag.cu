@@ -1,0 +1,250 @@
+// dsax_flag.cu -- the plain RFI flagger on the GPU: one HBM pass for all
+// per-(beam, channel) and per-(beam, time) statistics, then the
+// median/MAD decisions on the device (the reference does them on the host).
+//
+// Replaces src/gpu_flagger.cu: calc_spectrum (:175-223), calc_varspec
+// (:229-278), calc_maxspec (:283-319; the reference calls calc_spectrum in
+// its place at :1334 -- parity mode keeps that), calc_ppspec (:324-376),
+// make_ts (:414-453), and the host decisions medval/channflag/
+// simple_channflag/simple_tsflag (:534-720) run in the order of
+// :1340-1398.  The shapes the reference hard-codes ([64][16384][1024],
+// ZeroChannels 128, nFiltSize 21, TBIN 128, FBIN 8, T/16) are parameters.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dsax_internal.h"
+#include "dsax_ptx.cuh"
+
+namespace dsax {
+
+namespace flag {
+constexpr int kStatThreads = 512;   // 16 warps per beam
+constexpr int kMaxChan = 64;        // two channels per lane
+constexpr int kDecThreads = 256;
+}  // namespace flag
+
+// ---------------------------------------------------------------- stats
+// One CTA per beam.  Warp w owns the TBIN-sample bins w, w+16, ...; lane l
+// owns channels l and l+32.  Sums are FP64 in sample order within a bin
+// (the oracle's order), max/bin extremes exact.
+__global__ void __launch_bounds__(flag::kStatThreads) flag_stats_kernel(FlagArgs a) {
+  const int b = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  const int T = a.ntime, C = a.nchan, TB = a.tbin;
+  const int nbins = T / TB;
+  const float *xb = a.x + (int64_t)b * T * C;
+  const int c0 = lane, c1 = lane + 32;
+  const bool h0 = c0 < C, h1 = c1 < C;
+
+  double s0 = 0.0, s1 = 0.0, q0 = 0.0, q1 = 0.0;
+  float m0 = -INFINITY, m1 = -INFINITY;
+  double bmax0 = -1e300, bmin0 = 1e300, bmax1 = -1e300, bmin1 = 1e300;
+
+  for (int bin = warp; bin < nbins; bin += nw) {
+    double bs0 = 0.0, bs1 = 0.0;
+    for (int t = bin * TB; t < (bin + 1) * TB; ++t) {
+      const float *row = xb + (int64_t)t * C;
+      const float v0 = h0 ? __ldg(row + c0) : 0.0f;
+      const float v1 = h1 ? __ldg(row + c1) : 0.0f;
+      bs0 += v0; bs1 += v1;
+      q0 += (double)v0 * v0; q1 += (double)v1 * v1;
+      m0 = fmaxf(m0, h0 ? v0 : -INFINITY);
+      m1 = fmaxf(m1, h1 ? v1 : -INFINITY);
+      double r = (double)v0 + (double)v1;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+      if (lane == 0) a.ts[(int64_t)b * T + t] = (float)(r / C);
+    }
+    s0 += bs0; s1 += bs1;
+    const double mb0 = bs0 / TB, mb1 = bs1 / TB;
+    bmax0 = fmax(bmax0, mb0); bmin0 = fmin(bmin0, mb0);
+    bmax1 = fmax(bmax1, mb1); bmin1 = fmin(bmin1, mb1);
+  }
+  // samples beyond the last whole bin (T % TB): sums and max only
+  for (int t = nbins * TB + warp; t < T; t += nw) {
+    const float *row = xb + (int64_t)t * C;
+    const float v0 = h0 ? __ldg(row + c0) : 0.0f;
+    const float v1 = h1 ? __ldg(row + c1) : 0.0f;
+    s0 += v0; s1 += v1;
+    q0 += (double)v0 * v0; q1 += (double)v1 * v1;
+    m0 = fmaxf(m0, h0 ? v0 : -INFINITY);
+    m1 = fmaxf(m1, h1 ? v1 : -INFINITY);
+    double r = (double)v0 + (double)v1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (lane == 0) a.ts[(int64_t)b * T + t] = (float)(r / C);
+  }
+
+  __shared__ double sh_s[16][flag::kMaxChan], sh_q[16][flag::kMaxChan];
+  __shared__ double sh_bmax[16][flag::kMaxChan], sh_bmin[16][flag::kMaxChan];
+  __shared__ float sh_m[16][flag::kMaxChan];
+  sh_s[warp][c0] = s0; sh_s[warp][c1] = s1;
+  sh_q[warp][c0] = q0; sh_q[warp][c1] = q1;
+  sh_m[warp][c0] = m0; sh_m[warp][c1] = m1;
+  sh_bmax[warp][c0] = bmax0; sh_bmax[warp][c1] = bmax1;
+  sh_bmin[warp][c0] = bmin0; sh_bmin[warp][c1] = bmin1;
+  __syncthreads();
+  if (threadIdx.x < C) {
+    const int c = threadIdx.x;
+    double s = 0.0, q = 0.0, bx = -1e300, bn = 1e300;
+    float m = -INFINITY;
+    for (int w = 0; w < nw; ++w) {
+      s += sh_s[w][c]; q += sh_q[w][c];
+      m = fmaxf(m, sh_m[w][c]);
+      bx = fmax(bx, sh_bmax[w][c]); bn = fmin(bn, sh_bmin[w][c]);
+    }
+    const double mean = s / T;
+    const double var = fmax(q / T - mean * mean, 0.0);
+    const int o = b * C + c;
+    a.spec[o] = (float)mean;
+    a.var[o] = (float)var;
+    a.maxs[o] = a.parity ? (float)mean : m;
+    a.pp[o] = nbins > 0 ? (float)(bx - bn) : 0.0f;
+  }
+}
+
+// ---------------------------------------------------------------- decisions
+// Lower median sorted[(n+1)/2 - 1] of v[0..n) in shared memory, by rank
+// counting with ties broken by index (the element a stable sort would put
+// at that position has the same value).  All threads of the block call it.
+__device__ float block_lower_median(const float *v, int n, float *result_slot) {
+  const int k = (n + 1) / 2 - 1;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float x = v[i];
+    int r = 0;
+    for (int j = 0; j < n; ++j) {
+      const float y = v[j];
+      r += (y < x) || (y == x && j < i);
+    }
+    if (r == k) *result_slot = x;
+  }
+  __syncthreads();
+  const float med = *result_slot;
+  __syncthreads();
+  return med;
+}
+
+// channflag() on one statistic of one beam: forward median detrend over
+// `filt` channels (the last windows clamped at C-G-filt), median and MAD
+// over the guard-banded channels, flag |x| > thr*MAD.
+__device__ void channflag_dev(const float *sb, float thr, const FlagArgs &a, uint8_t *mask,
+                              float *corr, float *tmp, float *slot) {
+  const int C = a.nchan, G = a.guard, F = a.filt, n = C - 2 * G;
+  for (int j = G + threadIdx.x; j < C - G; j += blockDim.x) {
+    const int w0 = (C - G - j >= F) ? j : C - G - F;
+    const int k = (F + 1) / 2 - 1;
+    float med = 0.0f;
+    for (int i = 0; i < F; ++i) {   // rank-count median of the window
+      const float x = sb[w0 + i];
+      int r = 0;
+      for (int q = 0; q < F; ++q) {
+        const float y = sb[w0 + q];
+        r += (y < x) || (y == x && q < i);
+      }
+      if (r == k) med = x;
+    }
+    corr[j - G] = sb[j] - med;
+  }
+  __syncthreads();
+  const float med = block_lower_median(corr, n, slot);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = fabsf(corr[i] - med);
+  __syncthreads();
+  const float mad = block_lower_median(tmp, n, slot);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = corr[i];
+    if (v > thr * mad || v < -thr * mad) mask[G + i] = 1;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(flag::kDecThreads) flag_decide_kernel(FlagArgs a) {
+  const int b = blockIdx.x;
+  const int C = a.nchan, G = a.guard, T = a.ntime, n = C - 2 * G;
+  extern __shared__ float dsh[];
+  float *spec = dsh;                    // C
+  float *corr = spec + C;               // C
+  float *tmp = corr + C;                // max(C, ts_base)
+  float *tsb = tmp + (a.ts_base > C ? a.ts_base : C);  // ts_base
+  __shared__ uint8_t cmask[flag::kMaxChan * 2];
+  __shared__ float slot;
+
+  for (int c = threadIdx.x; c < C; c += blockDim.x) cmask[c] = 0;
+  __syncthreads();
+
+  // 1) channflag(spec - oldspec, Thr)
+  for (int c = threadIdx.x; c < C; c += blockDim.x)
+    spec[c] = a.spec[b * C + c] - (a.oldspec ? a.oldspec[b * C + c] : 0.0f);
+  __syncthreads();
+  channflag_dev(spec, a.thresh, a, cmask, corr, tmp, &slot);
+  // 2) channflag(var, Thr + 0.5)
+  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.var[b * C + c];
+  __syncthreads();
+  channflag_dev(spec, a.thresh + a.var_add, a, cmask, corr, tmp, &slot);
+  // 3) channflag(max, Thr)
+  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.maxs[b * C + c];
+  __syncthreads();
+  channflag_dev(spec, a.thresh, a, cmask, corr, tmp, &slot);
+  // 4) simple_channflag(pp, Thr): one-sided, Thr/sqrt(FBIN)
+  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.pp[b * C + c];
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) corr[i] = spec[G + i];
+  __syncthreads();
+  {
+    const float med = block_lower_median(corr, n, &slot);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = fabsf(corr[i] - med);
+    __syncthreads();
+    const float mad = block_lower_median(tmp, n, &slot);
+    const float mythr = a.thresh / sqrtf((float)a.fbin);
+    for (int j = G + threadIdx.x; j < C - G - a.fbin; j += blockDim.x) {
+      float vv = 0.0f;
+      for (int k = 0; k < a.fbin; ++k) vv += a.parity ? spec[j] : spec[j + k];
+      vv = vv / (float)a.fbin - med;
+      if (vv > mythr * mad) cmask[j] = 1;
+    }
+  }
+  __syncthreads();
+  for (int k = 0; k < a.nperm; ++k) {
+    const int j = a.perm[k];
+    if (threadIdx.x == 0 && j >= G && j < C - G) cmask[j] = 1;
+  }
+  __syncthreads();
+  int nflag = 0;
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    a.chanmask[b * C + c] = cmask[c];
+    nflag += cmask[c];
+  }
+  if (nflag) atomicAdd(a.counts, nflag);
+
+  // 5) simple_tsflag(ts, TsThr): median/MAD over the first ts_base samples
+  const float *tb = a.ts + (int64_t)b * T;
+  if (a.tsflag) {
+    for (int i = threadIdx.x; i < a.ts_base; i += blockDim.x) tsb[i] = tb[i];
+    __syncthreads();
+    const float med = block_lower_median(tsb, a.ts_base, &slot);
+    for (int i = threadIdx.x; i < a.ts_base; i += blockDim.x) tmp[i] = fabsf(tsb[i] - med);
+    __syncthreads();
+    const float mad = block_lower_median(tmp, a.ts_base, &slot);
+    int nts = 0;
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+      const uint8_t f = (tb[t] - med) > a.ts_thresh * mad ? 1 : 0;
+      a.tsmask[(int64_t)b * T + t] = f;
+      nts += f;
+    }
+    if (nts) atomicAdd(a.counts + 1, nts);
+  } else {
+    for (int t = threadIdx.x; t < T; t += blockDim.x) a.tsmask[(int64_t)b * T + t] = 0;
+  }
+}
+
+int launch_flag(const FlagArgs &a, cudaStream_t st) {
+  if (a.nchan > flag::kMaxChan || a.ts_base > 4096) return -1;
+  flag_stats_kernel<<<a.nbeam, flag::kStatThreads, 0, st>>>(a);
+  if (cudaGetLastError() != cudaSuccess) return -2;
+  const int tmpn = a.ts_base > a.nchan ? a.ts_base : a.nchan;
+  const size_t sh = sizeof(float) * (2 * a.nchan + tmpn + a.ts_base);
+  flag_decide_kernel<<<a.nbeam, flag::kDecThreads, sh, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace dsax

@@ -36,3 +36,44 @@ struct CorrArgs {
 int launch_correlate(const CorrArgs &a, int fmt, cudaStream_t st);
 
 }  // namespace dsax
+
+namespace dsax {
+
+struct BfArgs {
+  const uint8_t *in;       // captured block [npkt][nant_in][nchan][2 t][2 pol]
+  const uint8_t *wimg;     // weight operand image [ngrp][nbeam/64][2 pol][2 kb][16 KB]
+  uint8_t *out_u8;         // [npkt/ppo][nbeam][nchan/8] Stokes-I uint8 (or null)
+  float *out_f32;          // same layout, FP32 power before scaling (or null)
+  int *err;
+  int npkt, nant_in, nchan, nbeam, ppo;
+  float scale;
+  unsigned long long wait_limit_ns;
+};
+
+int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st);
+
+}  // namespace dsax
+
+namespace dsax {
+
+struct FlagArgs {
+  const float *x;          // filterbank [nbeam][ntime][nchan] FP32 (device)
+  const float *oldspec;    // previous block's spec [nbeam][nchan] or null
+  float *spec, *var, *maxs, *pp, *ts;   // statistics (device)
+  uint8_t *chanmask;       // [nbeam][nchan]
+  uint8_t *tsmask;         // [nbeam][ntime]
+  int *counts;             // [2]: flagged (beam, chan) columns, (beam, t) rows
+  int nbeam, ntime, nchan, guard, filt, tbin, fbin, ts_base, tsflag, parity;
+  float thresh, var_add, ts_thresh;
+  int nperm;
+  int perm[8];
+};
+
+int launch_flag(const FlagArgs &a, cudaStream_t st);
+
+}  // namespace dsax
+
+namespace dsax {
+int launch_reorder(const uint8_t *in, uint8_t *out, int npkt, int nant_in, int nchan,
+                   cudaStream_t st);
+}  // namespace dsax

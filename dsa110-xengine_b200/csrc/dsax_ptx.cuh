@@ -202,3 +202,79 @@ __device__ __forceinline__ void st_shared_v4(uint32_t saddr, uint32_t a, uint32_
 }
 
 }  // namespace dsax
+
+namespace dsax {
+
+// ------------------------------------------------------------ bulk copies
+// Arms `bar` for `bytes` of transaction count (one arrival).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+// Non-tensor bulk copy global -> this CTA's shared memory (no multicast);
+// completion is signalled on `bar` as transaction bytes.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst_smem, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst_smem),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// 32 lanes x 32 bit, 32 consecutive columns per thread.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+}
+
+// Named barrier over `nthreads` threads (ids 1..15; 0 is __syncthreads).
+__device__ __forceinline__ void named_bar(uint32_t id, uint32_t nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// 8 packed 4-bit two's-complement values (nibble 2i = real, 2i+1 = imag of
+// element i) -> four words, word i = bf16(real_i) | bf16(imag_i) << 16.
+// Branch-free: |v| indexes byte tables of the bf16 low/high bytes with
+// PRMT; the sign and the single 3-bit-overflowing magnitude (|-8| = 8) are
+// patched into the high byte.
+__device__ __forceinline__ void nib8_to_bf16x8(uint32_t x, uint32_t (&o)[4]) {
+  const uint32_t S = x & 0x88888888u;            // sign bit of each nibble
+  const uint32_t M = (S >> 3) * 0xFu;            // 0xF in negative nibbles
+  const uint32_t mag = (x ^ M) + (S >> 3);       // |v| per nibble, 0..8, no carries
+  const uint32_t idx = mag & 0x77777777u;
+  // bf16(|v|), |v| = 0..7: low bytes 00 80 00 40 80 A0 C0 E0, high 00 3F 40 40 40 40 40 40
+  const uint32_t TL0 = 0x40008000u, TL1 = 0xE0C0A080u;
+  const uint32_t TH0 = 0x40403F00u, TH1 = 0x40404040u;
+  const uint32_t L03 = __byte_perm(TL0, TL1, idx & 0xFFFFu);
+  const uint32_t L47 = __byte_perm(TL0, TL1, idx >> 16);
+  uint32_t H03 = __byte_perm(TH0, TH1, idx & 0xFFFFu);
+  uint32_t H47 = __byte_perm(TH0, TH1, idx >> 16);
+  // nibble bit 3 (bit 4i+3) -> byte bit 7 (bit 8i+7), nibbles 0..3
+  auto spread = [](uint32_t s) -> uint32_t {
+    return ((s & 0x8u) << 4) | ((s & 0x80u) << 8) | ((s & 0x800u) << 12) | ((s & 0x8000u) << 16);
+  };
+  const uint32_t E = mag & 0x88888888u;          // |v| == 8 (only v = -8)
+  H03 |= spread(S) | ((spread(E) >> 7) * 0x41u);
+  H47 |= spread(S >> 16) | ((spread(E >> 16) >> 7) * 0x41u);
+  o[0] = __byte_perm(L03, H03, 0x5140u);
+  o[1] = __byte_perm(L03, H03, 0x7362u);
+  o[2] = __byte_perm(L47, H47, 0x5140u);
+  o[3] = __byte_perm(L47, H47, 0x7362u);
+}
+
+}  // namespace dsax

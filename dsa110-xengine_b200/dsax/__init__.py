@@ -50,7 +50,30 @@ class Config(ctypes.Structure):
         ("bf_pkt_per_out", ctypes.c_int),
         ("bf_scale", ctypes.c_float),
         ("wait_limit_ns", ctypes.c_ulonglong),
+        ("corr_path", ctypes.c_int),
     ]
+
+
+class FlagParams(ctypes.Structure):
+    _fields_ = [("nbeam", ctypes.c_int), ("ntime", ctypes.c_int), ("nchan", ctypes.c_int),
+                ("guard", ctypes.c_int), ("filt", ctypes.c_int), ("tbin", ctypes.c_int),
+                ("fbin", ctypes.c_int), ("ts_base", ctypes.c_int), ("tsflag", ctypes.c_int),
+                ("parity", ctypes.c_int), ("thresh", ctypes.c_float),
+                ("var_add", ctypes.c_float), ("ts_thresh", ctypes.c_float),
+                ("nperm", ctypes.c_int), ("perm", ctypes.c_int * 8)]
+
+
+def flag_params(nbeam: int, ntime: int, nchan: int, **kw) -> FlagParams:
+    p = FlagParams()
+    lib().dsax_default_flag_params(ctypes.byref(p), nbeam, ntime, nchan)
+    perm = kw.pop("perm", None)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    if perm is not None:
+        p.nperm = len(perm)
+        for i, c in enumerate(perm):
+            p.perm[i] = c
+    return p
 
 
 _lib = None
@@ -109,12 +132,14 @@ def lib():
 
 
 def _bind_optional(L):
-    """Signatures of entry points added beyond the correlator."""
-    P, I, Z, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_float
+    """Signatures of the entry points beyond the correlator."""
+    P, I = ctypes.c_void_p, ctypes.c_int
     table = {
-        "dsax_set_weights": ([P, P, P, I], I),
-        "dsax_beamform": ([P, P, P, I, I], I),
-        "dsax_beamform_power": ([P, P, P, I, I], I),
+        "dsax_set_weights": ([P, P, P], I),
+        "dsax_beamform": ([P, P, P, P, I], I),
+        "dsax_default_flag_params": ([ctypes.POINTER(FlagParams), I, I, I], None),
+        "dsax_flag": ([P, ctypes.POINTER(FlagParams), P, P, P, P, P, P, I], I),
+        "dsax_reorder": ([P, P, P, I], I),
     }
     for name, (args, res) in table.items():
         if hasattr(L, name):
@@ -211,14 +236,26 @@ class Context:
         rc = lib().dsax_correlate_fmt(self._h, fmt, _ptr(blk), _ptr(vis), mem, int(accumulate))
         self._check(rc, "dsax_correlate_fmt")
 
+    def reorder(self, captured, reordered, mem: int = MEM_DEVICE):
+        """massage() on the GPU: captured -> REORDER-key layout."""
+        self._check(lib().dsax_reorder(self._h, _ptr(captured), _ptr(reordered), mem),
+                    "dsax_reorder")
+
     # -- beamformer --------------------------------------------------------
-    def set_weights(self, wre, wim, mem: int = MEM_HOST):
-        self._check(lib().dsax_set_weights(self._h, _ptr(wre), _ptr(wim), mem), "dsax_set_weights")
+    def set_weights(self, wre, wim):
+        """FP64 weights [nchan/8][2][nbeam][64] (numpy, host)."""
+        import numpy as np
+        wre = np.ascontiguousarray(wre, dtype=np.float64)
+        wim = np.ascontiguousarray(wim, dtype=np.float64)
+        self._check(lib().dsax_set_weights(self._h, _ptr(wre), _ptr(wim)), "dsax_set_weights")
 
-    def beamform(self, blk, out, mem: int = MEM_DEVICE, precision: int = 0):
-        self._check(lib().dsax_beamform(self._h, _ptr(blk), _ptr(out), mem, precision),
-                    "dsax_beamform")
+    def beamform(self, blk, out_u8=None, out_f32=None, mem: int = MEM_DEVICE):
+        rc = lib().dsax_beamform(self._h, _ptr(blk), _ptr(out_u8), _ptr(out_f32), mem)
+        self._check(rc, "dsax_beamform")
 
-    def beamform_power(self, blk, out, mem: int = MEM_DEVICE, precision: int = 0):
-        self._check(lib().dsax_beamform_power(self._h, _ptr(blk), _ptr(out), mem, precision),
-                    "dsax_beamform_power")
+    # -- plain flagger -----------------------------------------------------
+    def flag(self, params: FlagParams, x, chanmask, tsmask, oldspec=None, stats=None,
+             counts=None, mem: int = MEM_DEVICE):
+        rc = lib().dsax_flag(self._h, ctypes.byref(params), _ptr(x), _ptr(oldspec),
+                             _ptr(chanmask), _ptr(tsmask), _ptr(stats), _ptr(counts), mem)
+        self._check(rc, "dsax_flag")

@@ -68,6 +68,9 @@ typedef struct dsax_config {
     int bf_pkt_per_out;  /* packets per Stokes-I output sample (16 = 32 times)    */
     float bf_scale;      /* fixed scale before the uint8 quantisation             */
     unsigned long long wait_limit_ns; /* bound on device waits (0 = 1 s)          */
+    int corr_path;       /* captured-block correlation: 0 = default (corner turn),
+                            1 = one fused kernel reading the captured layout,
+                            2 = GPU corner turn (dsax_reorder) + correlate      */
 } dsax_config;
 
 typedef struct dsax_ctx dsax_ctx;
@@ -113,8 +116,70 @@ int dsax_host_free(dsax_ctx *ctx, void *ptr);
  * xGPU device integration buffer semantics).  Host-memory calls always
  * overwrite. */
 int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
+
+/* massage() on the GPU (src/dsaX_reorder_raw.c:153-169): captured block ->
+ * REORDER-key layout [pkt][2*nchan][64][2 pol] (4+4-bit kept packed, padded
+ * antennas zero).  dsax_block_bytes(cfg, DSAX_FMT_REORDERED) bytes out. */
+int dsax_reorder(dsax_ctx *ctx, const void *captured, void *reordered, int mem);
 int dsax_correlate_fmt(dsax_ctx *ctx, int fmt, const void *in, void *vis, int mem,
                        int accumulate);
+
+/* ---- beamformer ----
+ * Replaces the promoter/beamformer/adder chain of src/dsaX_beamformer.cu
+ * (:121-416) and the weight upload of calc_weights (:421-449).
+ *
+ * dsax_set_weights: complex weights in FP64, host memory, layout
+ *   [nchan/8 groups][2 pol][nbeam][64 antennas] (re and im arrays), the
+ *   product of the geometric phase and the calibration as calc_weights
+ *   forms it.  Converted once (round-to-nearest-even) to the BF16 operand
+ *   image kept on the device; FP64 is used only here.
+ * dsax_beamform: one captured block -> Stokes-I
+ *   out[t][beam][group] = sum over 2 pols x bf_pkt_per_out packets x
+ *   8 channels x 2 times of |sum_a w * x|^2 (no conjugate on w, as
+ *   src/dsaX_beamformer.cu:376-378), t = packet / bf_pkt_per_out.
+ *   out_u8  : saturate(rint(P * bf_scale)) in [0, 255] (the reference wraps
+ *             modulo 256 instead, src/dsaX_beamformer.cu:150-156), or NULL;
+ *   out_f32 : P itself (FP32), or NULL.  At least one must be given.
+ *   Requires nchan % 8 == 0, nbeam % 64 == 0, npkt % 16 == 0 and
+ *   bf_pkt_per_out in {4, 8, 16, 32, ...} dividing npkt. */
+int dsax_set_weights(dsax_ctx *ctx, const double *wre, const double *wim);
+int dsax_beamform(dsax_ctx *ctx, const void *blk, void *out_u8, void *out_f32, int mem);
+
+/* ---- plain RFI flagger ----
+ * Replaces src/gpu_flagger.cu: the statistics kernels (:175-494) and the
+ * host decisions run per block (:1340-1398) -- channflag on spec-oldspec
+ * (Thr), on var (Thr + 0.5), on max (Thr), simple_channflag on the
+ * peak-to-peak of TBIN-sample means (Thr / sqrt(FBIN)), simple_tsflag on
+ * the channel-mean time series (TsThr), all with lower medians (medval,
+ * :534-556) and MADs -- on the GPU.  The shapes the reference hard-codes
+ * are parameters here. */
+typedef struct dsax_flag_params {
+    int nbeam, ntime, nchan; /* filterbank [nbeam][ntime][nchan], nchan <= 64      */
+    int guard;     /* ZeroChannels guard band at each edge (128 of 1024)           */
+    int filt;      /* nFiltSize forward median window (21)                          */
+    int tbin;      /* TBIN samples per peak-to-peak bin (128)                       */
+    int fbin;      /* FBIN channels of the simple_channflag boxcar (8)              */
+    int ts_base;   /* samples of the time-series median/MAD baseline (ntime/16)    */
+    int tsflag;    /* 1: time-series flagging (-s)                                  */
+    int parity;    /* 1: reproduce the reference as written: max spectrum = mean
+                      spectrum (:1334) and the FBIN boxcar reads spec[j] (:594)     */
+    float thresh;  /* Thr (-t, 5.0)                                                 */
+    float var_add; /* variance threshold = Thr + var_add (0.5)                      */
+    float ts_thresh; /* TsThr (-s, 10.0)                                            */
+    int nperm;     /* permanent flag channels (flagchannels[], :95)                 */
+    int perm[8];
+} dsax_flag_params;
+
+void dsax_default_flag_params(dsax_flag_params *p, int nbeam, int ntime, int nchan);
+
+/* x: filterbank [nbeam][ntime][nchan] float32.  oldspec: previous block's
+ * mean spectrum [nbeam][nchan] or NULL (zeros).  Outputs: chanmask
+ * [nbeam][nchan] and tsmask [nbeam][ntime] (0/1 bytes); stats (optional)
+ * [spec | var | max | pp] each [nbeam][nchan] then ts [nbeam][ntime];
+ * counts (optional) = {flagged (beam, chan) columns, flagged (beam, t) rows}.
+ * With DSAX_MEM_DEVICE every pointer is device memory. */
+int dsax_flag(dsax_ctx *ctx, const dsax_flag_params *p, const float *x, const float *oldspec,
+              uint8_t *chanmask, uint8_t *tsmask, float *stats, int *counts, int mem);
 
 #ifdef __cplusplus
 }

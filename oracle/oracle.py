@@ -254,3 +254,46 @@ def plain_flag(x: np.ndarray, params: FlagParams, oldspec=None):
         "sub": st[4 * B * C:5 * B * C].reshape(B, C), "ts": st[5 * B * C:].reshape(B, T),
     }
     return cm, tm, cmg, tmg, stats
+
+
+def gen_filterbank(seed: int, nbeam: int = 256, ntime: int = 4096, nchan: int = 48,
+                   n_tones: int | None = None, n_bursts: int | None = None,
+                   n_drift: int | None = None):
+    """Stokes-I filterbank [nbeam][ntime][nchan] float32: chi-square(2) noise
+    (exponential, mean 2, sigma 2) plus seeded RFI:
+      persistent narrowband tones, 1-3 adjacent channels, 5-20 sigma;
+      impulsive broadband bursts, 1-8 samples, all channels, 3-10 sigma;
+      slow drifting tones, one channel wide, 5-15 sigma, drifting up to 8
+      channels across the block.
+    Returns (x, truth) where truth[b][t][c] marks the injected samples."""
+    rng = np.random.default_rng(seed)
+    x = rng.exponential(2.0, size=(nbeam, ntime, nchan)).astype(np.float32)
+    truth = np.zeros((nbeam, ntime, nchan), dtype=bool)
+    sig = 2.0
+    n_tones = nbeam // 4 if n_tones is None else n_tones
+    n_bursts = nbeam // 4 if n_bursts is None else n_bursts
+    n_drift = nbeam // 8 if n_drift is None else n_drift
+    for _ in range(n_tones):
+        b = rng.integers(nbeam)
+        w = int(rng.integers(1, 4))
+        c = int(rng.integers(0, nchan - w + 1))
+        amp = rng.uniform(5, 20) * sig
+        x[b, :, c:c + w] += np.float32(amp)
+        truth[b, :, c:c + w] = True
+    for _ in range(n_bursts):
+        b = rng.integers(nbeam)
+        w = int(rng.integers(1, 9))
+        t = int(rng.integers(0, ntime - w + 1))
+        amp = rng.uniform(3, 10) * sig
+        x[b, t:t + w, :] += np.float32(amp)
+        truth[b, t:t + w, :] = True
+    for _ in range(n_drift):
+        b = rng.integers(nbeam)
+        c0 = rng.uniform(0, nchan - 1)
+        drift = rng.uniform(-8, 8)
+        amp = rng.uniform(5, 15) * sig
+        tt = np.arange(ntime)
+        cc = np.clip(np.rint(c0 + drift * tt / ntime), 0, nchan - 1).astype(int)
+        x[b, tt, cc] += np.float32(amp)
+        truth[b, tt, cc] = True
+    return x, truth

@@ -1,0 +1,101 @@
+"""GPU tests of the tcgen05 BF16 beamformer through the C-ABI against the
+FP64 oracle.  Tolerances: FP32 power within 5e-3 relative of FP64 -- the
+BF16 weight rounding bounds the power error by 2 * 2^-9 = 3.9e-3 when one
+antenna dominates a beam (geometric x calibration weights), and averages to
+well under 1e-3 for unit-magnitude weights; uint8 Stokes-I within 1 LSB of
+the FP64 oracle quantised the same way."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 5e-3
+MEAN_TOL = 1e-3
+
+
+def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None):
+    import torch
+    npkt, nant, nchan = blk.shape[:3]
+    cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
+                              bf_pkt_per_out=ppo, bf_scale=scale)
+    own = ctx is None
+    ctx = ctx or dsax.Context(cfg)
+    try:
+        ctx.set_weights(wre, wim)
+        d_in = torch.from_numpy(blk.reshape(-1)).cuda()
+        nout = (npkt // ppo) * nbeam * (nchan // 8)
+        u8 = torch.zeros(nout, dtype=torch.uint8, device="cuda")
+        f32 = torch.zeros(nout, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.beamform(d_in, u8, f32)
+        ctx.sync()
+        shp = (npkt // ppo, nbeam, nchan // 8)
+        return u8.cpu().numpy().reshape(shp), f32.cpu().numpy().reshape(shp)
+    finally:
+        if own:
+            ctx.close()
+
+
+def _check(oracle, blk, wre, wim, u8, f32, ppo, scale, g0=0, ng=None):
+    ng = f32.shape[2] - g0 if ng is None else ng
+    ref = oracle.beamform_power(blk, wre, wim, pkt_per_out=ppo, g0=g0, ng=ng)
+    got = f32[:, :, g0:g0 + ng].astype(np.float64)
+    rel = np.abs(got - ref) / np.maximum(ref, 1e-30)
+    assert rel.max() < REL_TOL, f"max rel err {rel.max():.3e}"
+    assert rel.mean() < MEAN_TOL, f"mean rel err {rel.mean():.3e}"
+    ref_u8 = oracle.quantize_u8(ref, scale)
+    diff = np.abs(u8[:, :, g0:g0 + ng].astype(int) - ref_u8.astype(int))
+    assert diff.max() <= 1, f"uint8 off by {diff.max()}"
+    return rel, diff
+
+
+def test_beamformer_config3_subset(dsax, oracle):
+    """BASELINE shape: 64 ants (63 populated) x 2 pols x 384 ch x 4096 t,
+    256 beams, unit-magnitude random-phase weights, 32 t x 8 ch sums."""
+    blk = oracle.gen_block(303, 2048, 63, 384, "gauss")
+    wre, wim = oracle.random_phase_weights(9, 48, 256)
+    scale = 128.0 / (512 * 64 * 2 * 6.25)   # E[P] = 512 samples x 64 ants x E|x|^2
+    u8, f32 = _beamform(dsax, blk, wre, wim, 256, 16, scale)
+    assert f32.shape == (128, 256, 48)
+    rel, diff = _check(oracle, blk, wre, wim, u8, f32, 16, scale, g0=5, ng=3)
+    assert np.median(u8) > 60 and np.median(u8) < 200   # fixed scaling lands mid-range
+
+
+@pytest.mark.parametrize("nbeam,ppo,npkt,nant,nchan", [(64, 16, 32, 63, 8), (128, 4, 64, 64, 16),
+                                                       (256, 8, 48, 63, 8), (192, 32, 64, 40, 24)])
+def test_beamformer_shapes(dsax, oracle, nbeam, ppo, npkt, nant, nchan):
+    blk = oracle.gen_block(nbeam + ppo + npkt, npkt, nant, nchan, "gauss")
+    wre, wim = oracle.random_phase_weights(nbeam, nchan // 8, nbeam)
+    scale = 128.0 / (2 * ppo * 16 * nant * 2 * 6.25 * 0.93)
+    u8, f32 = _beamform(dsax, blk, wre, wim, nbeam, ppo, scale)
+    _check(oracle, blk, wre, wim, u8, f32, ppo, scale)
+
+
+def test_beamformer_geometric_weights(dsax, oracle):
+    """calc_weights geometry with calibration and a flagged antenna."""
+    rng = np.random.default_rng(3)
+    pos = rng.uniform(-600, 600, 64)
+    cal = rng.normal(size=(64, 2, 2, 2))
+    flagged = np.zeros(64, np.int32)
+    flagged[[3, 40]] = 1
+    wre, wim = oracle.geometric_weights(pos, cal, flagged, 2, 256)
+    blk = oracle.gen_block(77, 64, 63, 16, "gauss")
+    ref = oracle.beamform_power(blk, wre, wim, pkt_per_out=16)
+    scale = 128.0 / float(np.median(ref))
+    u8, f32 = _beamform(dsax, blk, wre, wim, 256, 16, scale)
+    _check(oracle, blk, wre, wim, u8, f32, 16, scale)
+
+
+def test_beamformer_single_antenna_tone(dsax, oracle):
+    """Only antenna 7 carries a constant 3+2i and weights pick it with
+    magnitude 1: every beam's power is |3+2i|^2 x samples."""
+    blk = np.zeros((16, 63, 8, 2, 2), np.uint8)
+    blk[:, 7] = (3 & 15) | ((2 & 15) << 4)
+    wre = np.zeros((1, 2, 64, 64)); wim = np.zeros_like(wre)
+    ph = np.linspace(0, 2 * np.pi, 64, endpoint=False)
+    wre[:, :, :, 7] = np.cos(ph)[None, None, :]
+    wim[:, :, :, 7] = np.sin(ph)[None, None, :]
+    u8, f32 = _beamform(dsax, blk, wre, wim, 64, 16, 1.0)
+    want = 13.0 * 16 * 16 * 2
+    np.testing.assert_allclose(f32, want, rtol=REL_TOL)
+    assert (u8 == 255).all()   # saturates instead of wrapping

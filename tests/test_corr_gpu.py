@@ -6,12 +6,13 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _run(dsax, blk, fmt=0, nant_in=None, ctx=None, accumulate=False, vis=None):
+def _run(dsax, blk, fmt=0, nant_in=None, ctx=None, accumulate=False, vis=None, corr_path=0):
     import torch
     npkt = blk.shape[0]
     nchan = blk.shape[2] if fmt == 0 else blk.shape[1] // 2
     nant = blk.shape[1] if fmt == 0 else 64
-    cfg = dsax.default_config(npkt=npkt, nant_in=nant if nant_in is None else nant_in, nchan=nchan)
+    cfg = dsax.default_config(npkt=npkt, nant_in=nant if nant_in is None else nant_in, nchan=nchan,
+                              corr_path=corr_path)
     own = ctx is None
     ctx = ctx or dsax.Context(cfg)
     try:
@@ -27,19 +28,39 @@ def _run(dsax, blk, fmt=0, nant_in=None, ctx=None, accumulate=False, vis=None):
             ctx.close()
 
 
-def test_config1_small_uniform_bit_exact(dsax, oracle):
+@pytest.mark.parametrize("corr_path", [1, 2])
+def test_config1_small_uniform_bit_exact(dsax, oracle, corr_path):
     """64 dual-pol antennas, 48 channels, 2048 packets (xGPU NTIME), samples
-    uniform on [-8, 7]: whole output bit-exact."""
+    uniform on [-8, 7]: whole output bit-exact (fused and corner-turn paths)."""
     blk = oracle.gen_block(101, 2048, 64, 48, "uniform")
-    np.testing.assert_array_equal(_run(dsax, blk), oracle.correlate(blk))
+    np.testing.assert_array_equal(_run(dsax, blk, corr_path=corr_path), oracle.correlate(blk))
 
 
-def test_config2_full_block(dsax, oracle):
+def test_reorder_matches_massage(dsax, oracle):
+    """GPU corner turn == massage() of src/dsaX_reorder_raw.c:153-169 (with
+    the padded antenna zeroed), byte for byte, including a channel count
+    that is not a multiple of the 32-channel tile."""
+    import torch
+    for npkt, nant, nch in ((64, 63, 384), (5, 63, 40), (3, 64, 7)):
+        blk = oracle.gen_block(npkt * nch, npkt, nant, nch, "uniform")
+        cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nch)
+        with dsax.Context(cfg) as ctx:
+            d_in = torch.from_numpy(blk.reshape(-1)).cuda()
+            out = torch.full((npkt * 2 * nch * 64 * 2,), 0xAB, dtype=torch.uint8, device="cuda")
+            torch.cuda.synchronize()
+            ctx.reorder(d_in, out)
+            ctx.sync()
+            got = out.cpu().numpy().reshape(npkt, 2 * nch, 64, 2)
+        np.testing.assert_array_equal(got, oracle.massage(blk))
+
+
+@pytest.mark.parametrize("corr_path", [1, 2])
+def test_config2_full_block(dsax, oracle, corr_path):
     """Full block [2048][63->64][384][2][2], Gaussian sigma 2.5 clipped to
     [-8, 7]: bit-exact on 24 channels checked by the oracle, plus
     size-independent properties over all 768 frequencies."""
     blk = oracle.gen_block(202, 2048, 63, 384, "gauss")
-    vis = _run(dsax, blk)
+    vis = _run(dsax, blk, corr_path=corr_path)
     rng = np.random.default_rng(7)
     chans = sorted(rng.choice(384, size=22, replace=False).tolist() + [0, 383])
     for c in chans:
@@ -71,11 +92,12 @@ def test_formats_agree(dsax, oracle):
     np.testing.assert_array_equal(_run(dsax, oracle.fluff_reorder(blk), fmt=2), want)
 
 
+@pytest.mark.parametrize("corr_path", [1, 2])
 @pytest.mark.parametrize("npkt,nant,nchan", [(4, 63, 8), (100, 63, 5), (64, 1, 1), (1, 64, 3),
-                                             (130, 64, 2)])
-def test_ragged_shapes(dsax, oracle, npkt, nant, nchan):
+                                             (130, 64, 2), (64, 63, 33)])
+def test_ragged_shapes(dsax, oracle, npkt, nant, nchan, corr_path):
     blk = oracle.gen_block(npkt + 13 * nant + nchan, npkt, nant, nchan, "uniform")
-    np.testing.assert_array_equal(_run(dsax, blk), oracle.correlate(blk))
+    np.testing.assert_array_equal(_run(dsax, blk, corr_path=corr_path), oracle.correlate(blk))
 
 
 def test_extreme_values(dsax, oracle):
