@@ -195,7 +195,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--corr-path", type=int, default=0,
-                    help="0 default (corner turn + correlate), 1 fused kernel, 2 corner turn")
+                    help="0 default (=3), 1 fused kernel, 2 REORDER-layout corner turn, "
+                         "3 channel-major corner turn + bulk-copy-fed correlator")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -262,8 +263,11 @@ def main():
     kernel_ms = {}
     if cfg.corr_path != 1:
         reo = torch.empty(2048 * 768 * 64 * 2, dtype=torch.uint8, device=f"cuda:{dev}")
-        for name, fn in (("reorder_kernel", lambda s: ctx.reorder(ins[s % nbuf], reo)),
-                         ("corr_kernel", lambda s: ctx.correlate(reo, vis, fmt=dsax.FMT_REORDERED))):
+        tfmt = dsax.FMT_REORDERED if cfg.corr_path == 2 else dsax.FMT_CHANMAJOR
+        names = (("reorder_kernel", "corr_kernel") if cfg.corr_path == 2
+                 else ("reorder_cm_kernel", "corr_cm_kernel"))
+        for name, fn in ((names[0], lambda s: ctx.corner_turn(ins[s % nbuf], reo, tfmt)),
+                         (names[1], lambda s: ctx.correlate(reo, vis, fmt=tfmt))):
             for s in range(3):
                 fn(s)
             ctx.sync()
@@ -318,9 +322,10 @@ def main():
         peak, peak_kind = _peaks()
         # dominant kernel of the step and its algorithmic bytes per launch
         dom = max(kernel_ms, key=kernel_ms.get)
+        corr_ms = [v for k, v in kernel_ms.items() if k.startswith("corr")][0]
         dom_ms = kernel_ms[dom]
         reo_bytes = 2048 * 768 * 64 * 2
-        if dom == "reorder_kernel":
+        if dom.startswith("reorder"):
             alg = BLOCK_IN + reo_bytes
         elif cfg.corr_path != 1:
             alg = reo_bytes + VIS_OUT
@@ -336,7 +341,9 @@ def main():
             "config": {"workload": "full-size correlator block [2048][63->64][384][2][2] "
                                    "-> xGPU triangular 768x2080x4 complex FP32",
                        "block_bytes": BLOCK_IN, "vis_bytes": VIS_OUT,
-                       "corr_path": ["corner turn + correlate", "fused", "corner turn + correlate"][cfg.corr_path],
+                       "corr_path": ["channel-major corner turn + correlate", "fused",
+                                     "REORDER-layout corner turn + correlate",
+                                     "channel-major corner turn + correlate"][cfg.corr_path],
                        "l2": "inputs larger than L2: 3 resident 198 MB blocks rotated",
                        "parallelism": f"blocks independent per GPU x{ws}"},
             "realtime_factor": value / ws * REALTIME_S,
@@ -347,8 +354,8 @@ def main():
                          "traffic": _traffic_from_profiles(dom),
                          "peak_kind": f"{peak_kind} (HBM copy bandwidth)",
                          "alg_bytes_per_launch": alg,
-                         "int8_alg_tops": ALG_OPS / (kernel_ms["corr_kernel"] * 1e-3) / 1e12,
-                         "int8_mma_tops": MMA_OPS / (kernel_ms["corr_kernel"] * 1e-3) / 1e12},
+                         "int8_alg_tops": ALG_OPS / (corr_ms * 1e-3) / 1e12,
+                         "int8_mma_tops": MMA_OPS / (corr_ms * 1e-3) / 1e12},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": BLOCK_IN,
                     "d2h_bytes_per_step": VIS_OUT, "steps": e2e_steps,
                     "ms_per_step": ms_e2e / e2e_steps},

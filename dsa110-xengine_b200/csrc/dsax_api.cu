@@ -94,6 +94,7 @@ size_t dsax_block_bytes(const dsax_config *c, int fmt) {
     case DSAX_FMT_CAPTURED: return (size_t)c->npkt * c->nant_in * c->nchan * 4;
     case DSAX_FMT_REORDERED: return (size_t)c->npkt * 2 * c->nchan * 64 * 2;
     case DSAX_FMT_XGPU_INT8: return (size_t)c->npkt * 2 * c->nchan * 64 * 4;
+    case DSAX_FMT_CHANMAJOR: return (size_t)c->nchan * c->npkt * 64 * 4;
     default: return 0;
   }
 }
@@ -199,17 +200,34 @@ static int correlate_device(dsax_ctx *c, int fmt, const void *in, float *vis, in
   a.accumulate = accumulate ? 1 : 0;
   a.vis = vis;
   a.in = static_cast<const uint8_t *>(in);
+  if (fmt == DSAX_FMT_CHANMAJOR) {
+    a.nant_in = 64;
+    if (launch_correlate_chanmajor(a, c->stream) != 0)
+      return cuda_check(c, cudaGetLastError(), "correlator launch");
+    return DSAX_OK;
+  }
   if (fmt == DSAX_FMT_CAPTURED && c->cfg.corr_path != 1) {
-    // corner turn into the context's REORDER-layout buffer, then correlate
+    // corner turn into the context's buffer, then correlate from it
     const size_t nre = dsax_block_bytes(&c->cfg, DSAX_FMT_REORDERED);
     int rc = ensure_buffer(c, c->aux[AUX_REORDERED], nre, "corner-turned block");
     if (rc != DSAX_OK) return rc;
-    if (launch_reorder(a.in, static_cast<uint8_t *>(c->aux[AUX_REORDERED].ptr), c->cfg.npkt,
-                       c->cfg.nant_in, c->cfg.nchan, c->stream) != 0)
-      return cuda_check(c, cudaGetLastError(), "corner-turn launch");
-    a.in = static_cast<const uint8_t *>(c->aux[AUX_REORDERED].ptr);
-    a.nant_in = 64;
-    fmt = DSAX_FMT_REORDERED;
+    uint8_t *tmp = static_cast<uint8_t *>(c->aux[AUX_REORDERED].ptr);
+    if (c->cfg.corr_path == 2) {   // REORDER-key layout (massage) + row loads
+      if (launch_reorder(a.in, tmp, c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan, c->stream) != 0)
+        return cuda_check(c, cudaGetLastError(), "corner-turn launch");
+      a.in = tmp;
+      a.nant_in = 64;
+      fmt = DSAX_FMT_REORDERED;
+    } else {                       // channel-major streams + bulk-copy-fed correlator
+      if (launch_reorder_chanmajor(a.in, tmp, c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan,
+                                   c->stream) != 0)
+        return cuda_check(c, cudaGetLastError(), "corner-turn launch");
+      a.in = tmp;
+      a.nant_in = 64;
+      if (launch_correlate_chanmajor(a, c->stream) != 0)
+        return cuda_check(c, cudaGetLastError(), "correlator launch");
+      return DSAX_OK;
+    }
   }
   if (launch_correlate(a, fmt, c->stream) != 0)
     return cuda_check(c, cudaGetLastError(), "correlator launch");
@@ -219,7 +237,7 @@ static int correlate_device(dsax_ctx *c, int fmt, const void *in, float *vis, in
 int dsax_correlate_fmt(dsax_ctx *c, int fmt, const void *in, void *vis, int mem,
                        int accumulate) {
   if (!c || !in || !vis) return DSAX_ERR_ARG;
-  if (fmt < DSAX_FMT_CAPTURED || fmt > DSAX_FMT_XGPU_INT8)
+  if (fmt < DSAX_FMT_CAPTURED || fmt > DSAX_FMT_CHANMAJOR)
     return set_error(c, DSAX_ERR_ARG, "unknown input format %d", fmt);
   if (mem != DSAX_MEM_HOST && mem != DSAX_MEM_DEVICE)
     return set_error(c, DSAX_ERR_ARG, "mem must be DSAX_MEM_HOST or DSAX_MEM_DEVICE");
@@ -244,17 +262,24 @@ int dsax_correlate_fmt(dsax_ctx *c, int fmt, const void *in, void *vis, int mem,
   return dsax_sync(c);
 }
 
-int dsax_reorder(dsax_ctx *c, const void *captured, void *reordered, int mem) {
-  if (!c || !captured || !reordered) return DSAX_ERR_ARG;
+int dsax_corner_turn(dsax_ctx *c, const void *captured, void *out, int out_fmt, int mem) {
+  if (!c || !captured || !out) return DSAX_ERR_ARG;
   if (mem != DSAX_MEM_HOST && mem != DSAX_MEM_DEVICE) return DSAX_ERR_ARG;
+  if (out_fmt != DSAX_FMT_REORDERED && out_fmt != DSAX_FMT_CHANMAJOR)
+    return set_error(c, DSAX_ERR_ARG, "corner turn output must be REORDERED or CHANMAJOR");
   DeviceGuard g(c->device);
   const size_t nin = dsax_block_bytes(&c->cfg, DSAX_FMT_CAPTURED);
-  const size_t nout = dsax_block_bytes(&c->cfg, DSAX_FMT_REORDERED);
+  const size_t nout = dsax_block_bytes(&c->cfg, out_fmt);
+  auto launch = [&](const uint8_t *src, uint8_t *dst) {
+    return out_fmt == DSAX_FMT_REORDERED
+               ? launch_reorder(src, dst, c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan, c->stream)
+               : launch_reorder_chanmajor(src, dst, c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan,
+                                          c->stream);
+  };
   if (mem == DSAX_MEM_DEVICE) {
-    if (!aligned16(captured) || !aligned16(reordered))
+    if (!aligned16(captured) || !aligned16(out))
       return set_error(c, DSAX_ERR_ARG, "device pointers must be 16-byte aligned");
-    if (launch_reorder(static_cast<const uint8_t *>(captured), static_cast<uint8_t *>(reordered),
-                       c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan, c->stream) != 0)
+    if (launch(static_cast<const uint8_t *>(captured), static_cast<uint8_t *>(out)) != 0)
       return cuda_check(c, cudaGetLastError(), "corner-turn launch");
     return DSAX_OK;
   }
@@ -264,13 +289,16 @@ int dsax_reorder(dsax_ctx *c, const void *captured, void *reordered, int mem) {
     return rc;
   cudaError_t e = cudaMemcpyAsync(c->in_buf.ptr, captured, nin, cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "H2D block");
-  if (launch_reorder(static_cast<const uint8_t *>(c->in_buf.ptr),
-                     static_cast<uint8_t *>(c->aux[AUX_REORDER_OUT].ptr), c->cfg.npkt,
-                     c->cfg.nant_in, c->cfg.nchan, c->stream) != 0)
+  if (launch(static_cast<const uint8_t *>(c->in_buf.ptr),
+             static_cast<uint8_t *>(c->aux[AUX_REORDER_OUT].ptr)) != 0)
     return cuda_check(c, cudaGetLastError(), "corner-turn launch");
-  e = cudaMemcpyAsync(reordered, c->aux[AUX_REORDER_OUT].ptr, nout, cudaMemcpyDeviceToHost, c->stream);
+  e = cudaMemcpyAsync(out, c->aux[AUX_REORDER_OUT].ptr, nout, cudaMemcpyDeviceToHost, c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "D2H corner-turned block");
   return dsax_sync(c);
+}
+
+int dsax_reorder(dsax_ctx *c, const void *captured, void *reordered, int mem) {
+  return dsax_corner_turn(c, captured, reordered, DSAX_FMT_REORDERED, mem);
 }
 
 int dsax_correlate(dsax_ctx *c, const void *in, void *vis, int mem) {

@@ -272,6 +272,219 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Channel-major variant: the input is [nchan][npkt][64 ant][4 B] (one
+// contiguous stream per channel, written by reorder_cm_kernel).  A loader
+// warp streams 64-packet stages (16 KB) into shared memory with bulk
+// copies, four stages ahead; the producer warps unpack from shared memory
+// (no global-memory latency on their critical path) into the same A / Arot
+// operand tiles as corr_kernel.
+namespace corrcm {
+constexpr int kRawStages = 4;
+constexpr int kRawBytes = 64 * 64 * 4;           // 64 packets x 64 antennas x 4 B
+constexpr int kStages = 2;                       // operand stages
+constexpr int kThreads = 320;                    // 8 producer warps + MMA warp + loader warp
+constexpr int kSmemBytes = 1024 + kStages * corr::kStageBytes + kRawStages * kRawBytes;
+}  // namespace corrcm
+
+__global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a) {
+  using namespace corr;
+  using corrcm::kRawStages;
+  using corrcm::kRawBytes;
+  constexpr int kOpStages = corrcm::kStages;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kOpStages];
+  __shared__ __align__(8) uint64_t empty_bar[kOpStages];
+  __shared__ __align__(8) uint64_t rfull_bar[kRawStages];
+  __shared__ __align__(8) uint64_t rempty_bar[kRawStages];
+  __shared__ __align__(8) uint64_t accum_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ch = blockIdx.x;
+  const uint32_t smem_base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  const uint32_t raw_base = smem_base + kOpStages * kStageBytes;
+  const uint8_t *raw_gen = smem_raw + (raw_base - smem_u32(smem_raw));  // generic view
+
+  if (tid == 0) {
+    for (int s = 0; s < kOpStages; ++s) {
+      mbar_init(&full_bar[s], kProducerThreads);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int r = 0; r < kRawStages; ++r) {
+      mbar_init(&rfull_bar[r], 1);
+      mbar_init(&rempty_bar[r], kProducerThreads);
+    }
+    mbar_init(&accum_bar, 1);
+    abort_sh = 0;
+    mbar_fence_init();
+  }
+  if (warp == 8) {
+    tmem_alloc(&tmem_base_sh, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  if ((tmem & 0xFFFFu) != 0u) {
+    if (tid == 0) atomicOr(a.err, DEV_ERR_TMEM);
+    abort_sh = 1;
+  }
+  const int nks = (a.npkt + kPktPerStage - 1) / kPktPerStage;
+  const uint8_t *chan_src = a.in + (int64_t)ch * a.npkt * 256;
+
+  if (warp < 8) {
+    // ------------------------------------------------------------ producers
+    const int ant = 16 * (warp & 3) + 4 * (lane >> 3) + (lane & 3);
+    const int jbit = (lane >> 2) & 1;
+    for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+      const int s = ks % kOpStages, r = ks % kRawStages;
+      if (!mbar_wait_bounded(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
+                             DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+        break;
+      if (!mbar_wait_bounded(&empty_bar[s], ((uint32_t)(ks / kOpStages) & 1u) ^ 1u, &abort_sh,
+                             a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+        break;
+      const uint32_t *rw = reinterpret_cast<const uint32_t *>(raw_gen + r * kRawBytes);
+      const uint32_t stage = smem_base + (uint32_t)s * kStageBytes;
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {
+        const int pg = 2 * ((warp >> 2) * 2 + it) + jbit;
+        uint32_t w[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int p = ks * kPktPerStage + 8 * pg + q;
+          w[q] = p < a.npkt ? rw[(8 * pg + q) * 64 + ant] : 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+#pragma unroll
+          for (int pol = 0; pol < 2; ++pol) {
+            uint32_t c[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+              c[h] = unpack_pair(w[2 * h], w[2 * h + 1], (uint32_t)(2 * t + pol));
+            const uint32_t row = (uint32_t)(2 * ant + pol);
+            const uint32_t off = sw128_offset(row, (uint32_t)pg);
+            const uint32_t tileA = stage + (uint32_t)t * kFreqBytes;
+            st_shared_v4(tileA + off, c[0], c[1], c[2], c[3]);
+            st_shared_v4(tileA + kTileBytes + off, rotate_pair(c[0]), rotate_pair(c[1]),
+                         rotate_pair(c[2]), rotate_pair(c[3]));
+          }
+        }
+      }
+      mbar_arrive(&rempty_bar[r]);   // raw stage consumed (generic-proxy reads only)
+      fence_proxy_async_smem();
+      mbar_arrive(&full_bar[s]);
+    }
+  } else if (warp == 9) {
+    // ------------------------------------------------------------ bulk loader
+    if (lane == 0) {
+      for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+        const int r = ks % kRawStages;
+        if (!mbar_wait_bounded(&rempty_bar[r], ((uint32_t)(ks / kRawStages) & 1u) ^ 1u, &abort_sh,
+                               a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+          break;
+        const int npk = min(kPktPerStage, a.npkt - ks * kPktPerStage);
+        const uint32_t bytes = (uint32_t)npk * 256u;
+        mbar_arrive_expect_tx(&rfull_bar[r], bytes);
+        bulk_g2s(raw_base + (uint32_t)r * kRawBytes, chan_src + (int64_t)ks * kPktPerStage * 256,
+                 bytes, &rfull_bar[r]);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ UMMA issuer
+    if (lane == 0) {
+      for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+        const int s = ks % kOpStages;
+        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)(ks / kOpStages) & 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+          break;
+        tc_fence_after();
+        const uint32_t stage = smem_base + (uint32_t)s * kStageBytes;
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const uint32_t tileA = stage + (uint32_t)t * kFreqBytes;
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint64_t d = umma_desc_sw128(tileA + 32u * kk, 1024u);
+            umma_i8(tmem + (uint32_t)t * 256u, d, d, kIdesc, (ks | kk) != 0);
+          }
+        }
+        umma_commit(&empty_bar[s]);
+      }
+      umma_commit(&accum_bar);
+    }
+    __syncwarp();
+  }
+
+  // ---------------------------------------------------------------- epilogue
+  if (warp < 8) {
+    bool ok = mbar_wait_bounded(&accum_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
+                                a.wait_limit_ns);
+    tc_fence_after();
+    ok = __all_sync(0xffffffffu, ok && !abort_sh);
+    if (ok) {
+      const int q = warp & 3, t = warp >> 2;
+      const int m = 32 * q + lane;
+      const int i = m >> 1, pi = m & 1;
+      float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
+      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
+      const int ncb = 2 * q + 2;
+      for (int cb = 0; cb < ncb; ++cb) {
+        uint32_t re[16], im[16];
+        tmem_ld16(trow + 16u * cb, re);
+        tmem_ld16(trow + 128u + 16u * cb, im);
+        tmem_wait_ld();
+        const int64_t tri = (int64_t)i * (i + 1) / 2;
+#pragma unroll
+        for (int jj = 0; jj < 8; ++jj) {
+          const int j = 8 * cb + jj;
+          if (j <= i) {
+            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(int32_t)im[2 * jj],
+                                   (float)(int32_t)re[2 * jj + 1], (float)(int32_t)im[2 * jj + 1]);
+            float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
+            if (a.accumulate) {
+              const float4 old = *dst;
+              o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
+            }
+            *dst = o;
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    if (lane == 0) {
+      volatile int no_abort = 0;
+      mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+    }
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st) {
+  static bool attr_done = false;
+  if (!attr_done) {
+    if (cudaFuncSetAttribute(corr_cm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             corrcm::kSmemBytes) != cudaSuccess)
+      return -2;
+    attr_done = true;
+  }
+  void *args[] = {(void *)&a};
+  return cudaLaunchKernel((const void *)corr_cm_kernel, dim3(a.nchan), dim3(corrcm::kThreads), args,
+                          corrcm::kSmemBytes, st) == cudaSuccess
+             ? 0
+             : -2;
+}
+
 int launch_correlate(const CorrArgs &a, int fmt, cudaStream_t st) {
   static bool attr_done[3] = {false, false, false};
   const void *fn = fmt == FMT_CAPTURED    ? (const void *)corr_kernel<FMT_CAPTURED>

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/dsax.h"
+#include "dsax_lflag.h"
 
 namespace dsax {
 
@@ -18,6 +19,9 @@ enum {
   AUX_FLAG_MASK = 6,  // host-mode staging: masks
   AUX_REORDERED = 7,  // corner-turned block for the two-pass correlator path
   AUX_REORDER_OUT = 8,  // host-mode staging for dsax_reorder output
+  AUX_LF_STATE = 9,     // learned flagger: params, grads, Adam m, v
+  AUX_LF_WLAYOUT = 10,  // learned flagger: forward / data-gradient weight layouts
+  AUX_LF_SCRATCH = 11,  // learned flagger: activations, gradients, partials
 };
 
 struct DevBuf {
@@ -58,6 +62,8 @@ struct dsax_ctx {
   dsax::DevBuf vis_buf;   // host-mode staging: visibilities
   dsax::DevBuf aux[16];   // per-stage buffers, indexed by dsax::AUX_*
   int weights_ready = 0;
+  dsax::LfNet lf_storage;
+  dsax::LfNet *lf = &lf_storage;
   char errmsg[512] = {0};
 
   void release_all() {

@@ -77,3 +77,10 @@ namespace dsax {
 int launch_reorder(const uint8_t *in, uint8_t *out, int npkt, int nant_in, int nchan,
                    cudaStream_t st);
 }  // namespace dsax
+
+namespace dsax {
+// Channel-major corner turn: [nchan][npkt][64][4 B] (internal layout).
+int launch_reorder_chanmajor(const uint8_t *in, uint8_t *out, int npkt, int nant_in, int nchan,
+                             cudaStream_t st);
+int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st);
+}  // namespace dsax

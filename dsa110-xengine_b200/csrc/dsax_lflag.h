@@ -1,0 +1,44 @@
+// dsax_lflag.h -- learned-flagger network state and kernel launchers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dsax {
+
+constexpr int kLfLayers = 4;
+constexpr int kLfCin[kLfLayers] = {4, 32, 64, 64};
+constexpr int kLfCout[kLfLayers] = {32, 64, 64, 1};
+
+// Offsets of layer l's weights / bias in the flat parameter vector:
+// for each layer W[co][3][3][ci] then b[co].
+inline int lf_w_offset(int l) {
+  int o = 0;
+  for (int k = 0; k < l; ++k) o += kLfCout[k] * 9 * kLfCin[k] + kLfCout[k];
+  return o;
+}
+inline int lf_b_offset(int l) { return lf_w_offset(l) + kLfCout[l] * 9 * kLfCin[l]; }
+inline int lf_nparams() { return lf_w_offset(kLfLayers); }
+
+struct LfNet {
+  float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;  // flat, FP32
+  float *w[kLfLayers] = {}, *b[kLfLayers] = {};      // views into params
+  float *gw[kLfLayers] = {}, *gb[kLfLayers] = {};    // views into grads
+  float *wt[kLfLayers] = {}, *wf[kLfLayers] = {};    // forward / data-gradient layouts
+  int step = 0;
+};
+
+int lf_features(const float *x, float *F, int B, int T, int C, int tds, cudaStream_t st);
+int lf_labels(const uint8_t *cm, const uint8_t *tm, uint8_t *L, int B, int T, int C, int tds,
+              int guard, cudaStream_t st);
+int lf_prepare_weights(const LfNet &net, cudaStream_t st);
+int lf_forward(const LfNet &net, float *const acts[5], int B, int H, int W, cudaStream_t st);
+int lf_backward(const LfNet &net, float *const acts[5], float *d4, float *d_a, float *d_b,
+                float *part, int B, int H, int W, cudaStream_t st);
+int lf_bce(const float *z, const uint8_t *L, float *dz, double *loss_acc, int B, int H, int W,
+           int guard, float pos_weight, float inv_n, cudaStream_t st);
+int lf_adam(LfNet &net, float lr, cudaStream_t st);
+int lf_mask(const float *z, uint8_t *mask, int64_t n, int W, int guard, float thresh_logit,
+            cudaStream_t st);
+size_t lf_part_floats(int B, int H);   // partial-gradient scratch size
+
+}  // namespace dsax

@@ -1,0 +1,230 @@
+// dsax_lflag_host.cu -- learned-flagger entry points of the C-ABI: network
+// state on the context, one training step (features -> labels -> forward ->
+// BCE -> backward -> Adam), inference to a pixel mask.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "../../include/dsax.h"
+#include "dsax_ctx.h"
+#include "dsax_internal.h"
+#include "dsax_lflag.h"
+
+using namespace dsax;
+
+namespace {
+
+uint64_t splitmix64(uint64_t &s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Standard normal by Box-Muller on two SplitMix64 uniforms in (0, 1).
+double normal(uint64_t &s) {
+  const double u1 = ((splitmix64(s) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  const double u2 = ((splitmix64(s) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+int ensure_net(dsax_ctx *c) {
+  LfNet &n = *c->lf;
+  if (n.params) return DSAX_OK;
+  const int np = lf_nparams();
+  int rc = ensure_buffer(c, c->aux[AUX_LF_STATE], sizeof(float) * 4 * np, "learned-flagger state");
+  if (rc != DSAX_OK) return rc;
+  rc = ensure_buffer(c, c->aux[AUX_LF_WLAYOUT], sizeof(float) * 2 * np, "learned-flagger layouts");
+  if (rc != DSAX_OK) return rc;
+  float *base = static_cast<float *>(c->aux[AUX_LF_STATE].ptr);
+  n.params = base;
+  n.grads = base + np;
+  n.m = base + 2 * np;
+  n.v = base + 3 * np;
+  float *lay = static_cast<float *>(c->aux[AUX_LF_WLAYOUT].ptr);
+  for (int l = 0; l < kLfLayers; ++l) {
+    n.w[l] = n.params + lf_w_offset(l);
+    n.b[l] = n.params + lf_b_offset(l);
+    n.gw[l] = n.grads + lf_w_offset(l);
+    n.gb[l] = n.grads + lf_b_offset(l);
+    n.wt[l] = lay + lf_w_offset(l);
+    n.wf[l] = lay + np + lf_w_offset(l);
+  }
+  cudaMemsetAsync(base, 0, sizeof(float) * 4 * np, c->stream);
+  n.step = 0;
+  return DSAX_OK;
+}
+
+int check_lf_shape(dsax_ctx *c, const dsax_flag_params *p, int tds) {
+  if (!p || tds < 1 || p->ntime % tds || p->nchan % 4 || p->nchan > 64 ||
+      (size_t)2 * (p->ntime / tds) * p->nchan * 4 > 190 * 1024)
+    return set_error(c, DSAX_ERR_ARG,
+                     "learned flagger needs ntime %% tds == 0, nchan %% 4 == 0, nchan <= 64");
+  return DSAX_OK;
+}
+
+// Scratch for B beams on an H x W grid.
+struct LfScratch {
+  float *F, *a1, *a2, *a3, *z, *d4, *da, *db, *part;
+  uint8_t *L;
+  double *loss;
+};
+
+int lf_scratch(dsax_ctx *c, int B, int H, int W, LfScratch &s) {
+  const size_t px = (size_t)B * H * W;
+  const size_t nf = px * (4 + 32 + 64 + 64 + 1 + 1 + 64 + 64) + lf_part_floats(B, H);
+  int rc = ensure_buffer(c, c->aux[AUX_LF_SCRATCH], nf * 4 + px + 64, "learned-flagger scratch");
+  if (rc != DSAX_OK) return rc;
+  float *f = static_cast<float *>(c->aux[AUX_LF_SCRATCH].ptr);
+  s.loss = reinterpret_cast<double *>(f);  f += 16;
+  s.F = f;  f += px * 4;
+  s.a1 = f; f += px * 32;
+  s.a2 = f; f += px * 64;
+  s.a3 = f; f += px * 64;
+  s.z = f;  f += px;
+  s.d4 = f; f += px;
+  s.da = f; f += px * 64;
+  s.db = f; f += px * 64;
+  s.part = f; f += lf_part_floats(B, H);
+  s.L = reinterpret_cast<uint8_t *>(f);
+  return DSAX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dsax_lf_init(dsax_ctx *c, unsigned long long seed) {
+  if (!c) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  int rc = ensure_net(c);
+  if (rc != DSAX_OK) return rc;
+  std::vector<float> h(lf_nparams(), 0.f);
+  uint64_t s = seed;
+  for (int l = 0; l < kLfLayers; ++l) {
+    const double sd = sqrt(2.0 / (9.0 * kLfCin[l]));
+    float *w = h.data() + lf_w_offset(l);
+    for (int i = 0; i < kLfCout[l] * 9 * kLfCin[l]; ++i) w[i] = (float)(sd * normal(s));
+  }
+  return dsax_lf_set_params(c, h.data(), lf_nparams());
+}
+
+int dsax_lf_nparams(void) { return lf_nparams(); }
+
+int dsax_lf_set_params(dsax_ctx *c, const float *params, int n) {
+  if (!c || !params || n != lf_nparams()) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  int rc = ensure_net(c);
+  if (rc != DSAX_OK) return rc;
+  LfNet &net = *c->lf;
+  cudaError_t e = cudaMemcpyAsync(net.params, params, sizeof(float) * n, cudaMemcpyHostToDevice,
+                                  c->stream);
+  if (e != cudaSuccess) return cuda_check(c, e, "upload parameters");
+  cudaMemsetAsync(net.m, 0, sizeof(float) * 2 * n, c->stream);  // m and v
+  net.step = 0;
+  return dsax_sync(c);
+}
+
+int dsax_lf_get_params(dsax_ctx *c, float *params, int n) {
+  if (!c || !params || n != lf_nparams() || !c->lf->params) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  cudaError_t e = cudaMemcpyAsync(params, c->lf->params, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                                  c->stream);
+  if (e != cudaSuccess) return cuda_check(c, e, "download parameters");
+  return dsax_sync(c);
+}
+
+int dsax_lf_features(dsax_ctx *c, const float *x, const dsax_flag_params *p, int tds, float *F) {
+  if (!c || !x || !F) return DSAX_ERR_ARG;
+  int rc = check_lf_shape(c, p, tds);
+  if (rc != DSAX_OK) return rc;
+  DeviceGuard g(c->device);
+  if (lf_features(x, F, p->nbeam, p->ntime, p->nchan, tds, c->stream) != 0)
+    return cuda_check(c, cudaGetLastError(), "feature launch");
+  return DSAX_OK;
+}
+
+int dsax_lf_train_step(dsax_ctx *c, const float *x, const uint8_t *chanmask, const uint8_t *tsmask,
+                       const dsax_flag_params *p, int tds, float lr, float pos_weight, int update,
+                       float *loss, float *grads) {
+  if (!c || !x || !chanmask || !tsmask) return DSAX_ERR_ARG;
+  int rc = check_lf_shape(c, p, tds);
+  if (rc != DSAX_OK) return rc;
+  if (!c->lf->params) return set_error(c, DSAX_ERR_ARG, "dsax_lf_init not called");
+  DeviceGuard g(c->device);
+  const int B = p->nbeam, H = p->ntime / tds, W = p->nchan;
+  LfScratch s;
+  if ((rc = lf_scratch(c, B, H, W, s)) != DSAX_OK) return rc;
+  LfNet &net = *c->lf;
+  float *acts[5] = {s.F, s.a1, s.a2, s.a3, s.z};
+  const int nvalid = B * H * (W - 2 * p->guard);
+  int e = 0;
+  e |= lf_features(x, s.F, B, p->ntime, W, tds, c->stream);
+  e |= lf_labels(chanmask, tsmask, s.L, B, p->ntime, W, tds, p->guard, c->stream);
+  e |= lf_prepare_weights(net, c->stream);
+  e |= lf_forward(net, acts, B, H, W, c->stream);
+  cudaMemsetAsync(s.loss, 0, sizeof(double), c->stream);
+  e |= lf_bce(s.z, s.L, s.d4, s.loss, B, H, W, p->guard, pos_weight, 1.0f / (float)nvalid,
+              c->stream);
+  e |= lf_backward(net, acts, s.d4, s.da, s.db, s.part, B, H, W, c->stream);
+  if (update) e |= lf_adam(net, lr, c->stream);
+  if (e) return cuda_check(c, cudaGetLastError(), "training step launch");
+  if (loss) {
+    double h = 0.0;
+    cudaError_t ce = cudaMemcpyAsync(&h, s.loss, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (ce != cudaSuccess) return cuda_check(c, ce, "loss readback");
+    if ((rc = dsax_sync(c)) != DSAX_OK) return rc;
+    *loss = (float)(h / nvalid);
+  }
+  if (grads) {
+    cudaError_t ce = cudaMemcpyAsync(grads, net.grads, sizeof(float) * lf_nparams(),
+                                     cudaMemcpyDeviceToHost, c->stream);
+    if (ce != cudaSuccess) return cuda_check(c, ce, "gradient readback");
+    return dsax_sync(c);
+  }
+  return DSAX_OK;
+}
+
+int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, int tds,
+                      uint8_t *mask, float *logits, int mem) {
+  if (!c || !x || !mask) return DSAX_ERR_ARG;
+  int rc = check_lf_shape(c, p, tds);
+  if (rc != DSAX_OK) return rc;
+  if (!c->lf->params) return set_error(c, DSAX_ERR_ARG, "dsax_lf_init not called");
+  if (mem != DSAX_MEM_HOST && mem != DSAX_MEM_DEVICE) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  const int B = p->nbeam, H = p->ntime / tds, W = p->nchan;
+  LfScratch s;
+  if ((rc = lf_scratch(c, B, H, W, s)) != DSAX_OK) return rc;
+  LfNet &net = *c->lf;
+  const float *xd = x;
+  const size_t px = (size_t)B * H * W;
+  if (mem == DSAX_MEM_HOST) {
+    const size_t nx = (size_t)B * p->ntime * W * 4;
+    if ((rc = ensure_buffer(c, c->aux[AUX_FLAG_X], nx, "filterbank")) != DSAX_OK) return rc;
+    cudaError_t ce = cudaMemcpyAsync(c->aux[AUX_FLAG_X].ptr, x, nx, cudaMemcpyHostToDevice, c->stream);
+    if (ce != cudaSuccess) return cuda_check(c, ce, "H2D filterbank");
+    xd = static_cast<const float *>(c->aux[AUX_FLAG_X].ptr);
+  }
+  float *acts[5] = {s.F, s.a1, s.a2, s.a3, s.z};
+  int e = 0;
+  e |= lf_features(xd, s.F, B, p->ntime, W, tds, c->stream);
+  e |= lf_prepare_weights(net, c->stream);
+  e |= lf_forward(net, acts, B, H, W, c->stream);
+  uint8_t *dmask = mem == DSAX_MEM_DEVICE ? mask : s.L;
+  e |= lf_mask(s.z, dmask, (int64_t)px, W, p->guard, 0.0f, c->stream);
+  if (e) return cuda_check(c, cudaGetLastError(), "learned flagger launch");
+  if (mem == DSAX_MEM_DEVICE) {
+    if (logits)
+      cudaMemcpyAsync(logits, s.z, px * 4, cudaMemcpyDeviceToDevice, c->stream);
+    return DSAX_OK;
+  }
+  cudaError_t ce = cudaMemcpyAsync(mask, s.L, px, cudaMemcpyDeviceToHost, c->stream);
+  if (ce == cudaSuccess && logits)
+    ce = cudaMemcpyAsync(logits, s.z, px * 4, cudaMemcpyDeviceToHost, c->stream);
+  if (ce != cudaSuccess) return cuda_check(c, ce, "D2H learned mask");
+  return dsax_sync(c);
+}
+
+}  // extern "C"

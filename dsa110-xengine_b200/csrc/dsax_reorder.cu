@@ -60,3 +60,73 @@ int launch_reorder(const uint8_t *in, uint8_t *out, int npkt, int nant_in, int n
 }
 
 }  // namespace dsax
+
+namespace dsax {
+
+namespace reorder_cm {
+constexpr int kPkt = 4;          // packets per CTA
+constexpr int kChan = 32;        // channels per CTA
+constexpr int kThreads = 256;
+constexpr int kAStride = 65;     // words per channel row (64 antennas + 1 pad)
+}  // namespace reorder_cm
+
+// Captured [pkt][nant_in][nchan][4 B] -> channel-major [nchan][npkt][64][4 B]
+// (padded antennas zero): each channel's samples become one contiguous
+// stream, so the correlator can fetch a 64-packet stage with one bulk copy.
+__global__ void __launch_bounds__(reorder_cm::kThreads) reorder_cm_kernel(
+    const uint8_t *__restrict__ in, uint8_t *__restrict__ out, int npkt, int nant_in, int nchan) {
+  using namespace reorder_cm;
+  __shared__ uint32_t W[kPkt * kChan * kAStride];  // [pkt][chan][ant]
+  const int c0 = blockIdx.x * kChan;
+  const int p0 = blockIdx.y * kPkt;
+  const int nc = min(kChan, nchan - c0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // load: lanes cover 8 x 16 B (32 channels) of 4 antenna rows
+  for (int r = warp; r < kPkt * 16; r += kThreads / 32) {   // 4 pkts x 16 groups of 4 ants
+    const int pq = r >> 4;
+    const int a = 4 * (r & 15) + (lane >> 3);
+    const int cq = lane & 7;
+    const int p = p0 + pq;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (p < npkt && a < nant_in && 4 * cq < nc) {
+      const uint8_t *src = in + (((int64_t)p * nant_in + a) * nchan + c0 + 4 * cq) * 4;
+      if (4 * cq + 4 <= nc && ((nchan & 3) == 0)) {
+        v = __ldg(reinterpret_cast<const uint4 *>(src));
+      } else {
+        const uint32_t *s32 = reinterpret_cast<const uint32_t *>(src);
+        v.x = s32[0];
+        v.y = 4 * cq + 1 < nc ? s32[1] : 0u;
+        v.z = 4 * cq + 2 < nc ? s32[2] : 0u;
+        v.w = 4 * cq + 3 < nc ? s32[3] : 0u;
+      }
+    }
+    uint32_t *w = W + (pq * kChan + 4 * cq) * kAStride + a;
+    w[0] = v.x;
+    w[kAStride] = v.y;
+    w[2 * kAStride] = v.z;
+    w[3 * kAStride] = v.w;
+  }
+  __syncthreads();
+  // store: per channel, kPkt x 256 B contiguous; a warp writes one channel
+  for (int c = warp; c < nc; c += kThreads / 32) {
+    uint8_t *dst = out + ((int64_t)(c0 + c) * npkt + p0) * 256;
+    for (int k = lane; k < kPkt * 16; k += 32) {   // 16-byte chunks
+      const int pq = k >> 4, a = 4 * (k & 15);
+      if (p0 + pq >= npkt) continue;
+      const uint32_t *w = W + (pq * kChan + c) * kAStride + a;
+      *reinterpret_cast<uint4 *>(dst + 16 * k) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+int launch_reorder_chanmajor(const uint8_t *in, uint8_t *out, int npkt, int nant_in, int nchan,
+                             cudaStream_t st) {
+  using namespace reorder_cm;
+  if (npkt < 1 || nant_in < 1 || nant_in > 64 || nchan < 1) return -1;
+  dim3 grid((nchan + kChan - 1) / kChan, (npkt + kPkt - 1) / kPkt);
+  if (grid.y > 65535) return -1;
+  reorder_cm_kernel<<<grid, kThreads, 0, st>>>(in, out, npkt, nant_in, nchan);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace dsax

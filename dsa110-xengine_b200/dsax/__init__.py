@@ -31,6 +31,7 @@ MEM_DEVICE = 1
 FMT_CAPTURED = 0
 FMT_REORDERED = 1
 FMT_XGPU_INT8 = 2
+FMT_CHANMAJOR = 3
 
 NBL = 2080
 
@@ -140,6 +141,15 @@ def _bind_optional(L):
         "dsax_default_flag_params": ([ctypes.POINTER(FlagParams), I, I, I], None),
         "dsax_flag": ([P, ctypes.POINTER(FlagParams), P, P, P, P, P, P, I], I),
         "dsax_reorder": ([P, P, P, I], I),
+        "dsax_corner_turn": ([P, P, P, I, I], I),
+        "dsax_lf_nparams": ([], I),
+        "dsax_lf_init": ([P, ctypes.c_ulonglong], I),
+        "dsax_lf_set_params": ([P, P, I], I),
+        "dsax_lf_get_params": ([P, P, I], I),
+        "dsax_lf_features": ([P, P, ctypes.POINTER(FlagParams), I, P], I),
+        "dsax_lf_train_step": ([P, P, P, P, ctypes.POINTER(FlagParams), I, ctypes.c_float,
+                                ctypes.c_float, I, P, P], I),
+        "dsax_flag_learned": ([P, P, ctypes.POINTER(FlagParams), I, P, P, I], I),
     }
     for name, (args, res) in table.items():
         if hasattr(L, name):
@@ -241,6 +251,10 @@ class Context:
         self._check(lib().dsax_reorder(self._h, _ptr(captured), _ptr(reordered), mem),
                     "dsax_reorder")
 
+    def corner_turn(self, captured, out, out_fmt: int = FMT_CHANMAJOR, mem: int = MEM_DEVICE):
+        self._check(lib().dsax_corner_turn(self._h, _ptr(captured), _ptr(out), out_fmt, mem),
+                    "dsax_corner_turn")
+
     # -- beamformer --------------------------------------------------------
     def set_weights(self, wre, wim):
         """FP64 weights [nchan/8][2][nbeam][64] (numpy, host)."""
@@ -259,3 +273,40 @@ class Context:
         rc = lib().dsax_flag(self._h, ctypes.byref(params), _ptr(x), _ptr(oldspec),
                              _ptr(chanmask), _ptr(tsmask), _ptr(stats), _ptr(counts), mem)
         self._check(rc, "dsax_flag")
+
+    # -- learned flagger ---------------------------------------------------
+    def lf_init(self, seed: int = 0):
+        self._check(lib().dsax_lf_init(self._h, seed), "dsax_lf_init")
+
+    def lf_set_params(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(lib().dsax_lf_set_params(self._h, _ptr(p), p.size), "dsax_lf_set_params")
+
+    def lf_get_params(self):
+        import numpy as np
+        p = np.zeros(lib().dsax_lf_nparams(), np.float32)
+        self._check(lib().dsax_lf_get_params(self._h, _ptr(p), p.size), "dsax_lf_get_params")
+        return p
+
+    def lf_features(self, params: FlagParams, x, F, tds: int = 32):
+        self._check(lib().dsax_lf_features(self._h, _ptr(x), ctypes.byref(params), tds, _ptr(F)),
+                    "dsax_lf_features")
+
+    def lf_train_step(self, params: FlagParams, x, chanmask, tsmask, tds: int = 32,
+                      lr: float = 1e-3, pos_weight: float = 1.0, update: bool = True,
+                      want_grads: bool = False):
+        import numpy as np
+        loss = ctypes.c_float(0.0)
+        g = np.zeros(lib().dsax_lf_nparams(), np.float32) if want_grads else None
+        rc = lib().dsax_lf_train_step(self._h, _ptr(x), _ptr(chanmask), _ptr(tsmask),
+                                      ctypes.byref(params), tds, lr, pos_weight, int(update),
+                                      ctypes.byref(loss), _ptr(g))
+        self._check(rc, "dsax_lf_train_step")
+        return (loss.value, g) if want_grads else loss.value
+
+    def flag_learned(self, params: FlagParams, x, mask, logits=None, tds: int = 32,
+                     mem: int = MEM_DEVICE):
+        rc = lib().dsax_flag_learned(self._h, _ptr(x), ctypes.byref(params), tds, _ptr(mask),
+                                     _ptr(logits), mem)
+        self._check(rc, "dsax_flag_learned")

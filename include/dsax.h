@@ -59,6 +59,7 @@ extern "C" {
 #define DSAX_FMT_CAPTURED 0  /* [pkt][nant_in][nchan][2 t][2 pol], 4+4-bit   */
 #define DSAX_FMT_REORDERED 1 /* [pkt][2*nchan][64][2 pol], 4+4-bit (REORDER key) */
 #define DSAX_FMT_XGPU_INT8 2 /* [pkt][2*nchan][64][2 pol][re,im] int8         */
+#define DSAX_FMT_CHANMAJOR 3 /* [nchan][pkt][64][2 t][2 pol], 4+4-bit (corner-turned) */
 
 typedef struct dsax_config {
     int npkt;            /* packets per block = xGPU NTIME (2048)                 */
@@ -68,9 +69,11 @@ typedef struct dsax_config {
     int bf_pkt_per_out;  /* packets per Stokes-I output sample (16 = 32 times)    */
     float bf_scale;      /* fixed scale before the uint8 quantisation             */
     unsigned long long wait_limit_ns; /* bound on device waits (0 = 1 s)          */
-    int corr_path;       /* captured-block correlation: 0 = default (corner turn),
+    int corr_path;       /* captured-block correlation: 0 = default (= 3),
                             1 = one fused kernel reading the captured layout,
-                            2 = GPU corner turn (dsax_reorder) + correlate      */
+                            2 = corner turn to the REORDER layout + correlate,
+                            3 = corner turn to channel-major streams + bulk-
+                                copy-fed correlate                              */
 } dsax_config;
 
 typedef struct dsax_ctx dsax_ctx;
@@ -121,6 +124,11 @@ int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
  * REORDER-key layout [pkt][2*nchan][64][2 pol] (4+4-bit kept packed, padded
  * antennas zero).  dsax_block_bytes(cfg, DSAX_FMT_REORDERED) bytes out. */
 int dsax_reorder(dsax_ctx *ctx, const void *captured, void *reordered, int mem);
+
+/* Corner turn of a captured block into out_fmt = DSAX_FMT_REORDERED (as
+ * dsax_reorder) or DSAX_FMT_CHANMAJOR (one contiguous stream per channel,
+ * the layout the default correlator path reads). */
+int dsax_corner_turn(dsax_ctx *ctx, const void *captured, void *out, int out_fmt, int mem);
 int dsax_correlate_fmt(dsax_ctx *ctx, int fmt, const void *in, void *vis, int mem,
                        int accumulate);
 
@@ -180,6 +188,35 @@ void dsax_default_flag_params(dsax_flag_params *p, int nbeam, int ntime, int nch
  * With DSAX_MEM_DEVICE every pointer is device memory. */
 int dsax_flag(dsax_ctx *ctx, const dsax_flag_params *p, const float *x, const float *oldspec,
               uint8_t *chanmask, uint8_t *tsmask, float *stats, int *counts, int mem);
+
+/* ---- learned RFI flagger (no reference counterpart) ----
+ * A 4-layer 3x3 conv net (4 -> 32 -> 64 -> 64 -> 1 channels, ReLU,
+ * 57,185 FP32 parameters) over the filterbank downsampled by tds samples,
+ * with four features per pixel (z-scores of the pixel mean, pixel max,
+ * row channel-mean and column mean, log-compressed).  It is trained on the
+ * plain flagger's masks and predicts the pixel mask the plain flagger
+ * applies: (chanmask[b][c]) or (tsmask in the pixel's samples and inside
+ * the guard band).  The plain flagger (dsax_flag) stays the fallback and
+ * the judge.  Parameter vector: for each layer W[co][3][3][ci] then b[co].
+ * Filterbank, masks and feature pointers of dsax_lf_features and
+ * dsax_lf_train_step are device memory. */
+int dsax_lf_nparams(void);
+int dsax_lf_init(dsax_ctx *ctx, unsigned long long seed);
+int dsax_lf_set_params(dsax_ctx *ctx, const float *params, int n);
+int dsax_lf_get_params(dsax_ctx *ctx, float *params, int n);
+/* features [nbeam][ntime/tds][nchan][4] float32 */
+int dsax_lf_features(dsax_ctx *ctx, const float *x, const dsax_flag_params *p, int tds, float *F);
+/* One training step on p->nbeam beams: weighted BCE-with-logits (positive
+ * pixels weighted by pos_weight, guard band excluded) on the plain
+ * flagger's masks, then Adam (lr) if update != 0.  loss (host, optional):
+ * mean loss; grads (host, optional): the flat gradient vector. */
+int dsax_lf_train_step(dsax_ctx *ctx, const float *x, const uint8_t *chanmask,
+                       const uint8_t *tsmask, const dsax_flag_params *p, int tds, float lr,
+                       float pos_weight, int update, float *loss, float *grads);
+/* Inference: mask [nbeam][ntime/tds][nchan] (0/1, guard band 0) and
+ * optionally the logits (float32, same layout). */
+int dsax_flag_learned(dsax_ctx *ctx, const float *x, const dsax_flag_params *p, int tds,
+                      uint8_t *mask, float *logits, int mem);
 
 #ifdef __cplusplus
 }

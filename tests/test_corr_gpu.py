@@ -9,7 +9,8 @@ pytestmark = pytest.mark.gpu
 def _run(dsax, blk, fmt=0, nant_in=None, ctx=None, accumulate=False, vis=None, corr_path=0):
     import torch
     npkt = blk.shape[0]
-    nchan = blk.shape[2] if fmt == 0 else blk.shape[1] // 2
+    nchan = blk.shape[2] if fmt == 0 else (blk.shape[0] if fmt == 3 else blk.shape[1] // 2)
+    npkt = blk.shape[1] if fmt == 3 else npkt
     nant = blk.shape[1] if fmt == 0 else 64
     cfg = dsax.default_config(npkt=npkt, nant_in=nant if nant_in is None else nant_in, nchan=nchan,
                               corr_path=corr_path)
@@ -28,7 +29,7 @@ def _run(dsax, blk, fmt=0, nant_in=None, ctx=None, accumulate=False, vis=None, c
             ctx.close()
 
 
-@pytest.mark.parametrize("corr_path", [1, 2])
+@pytest.mark.parametrize("corr_path", [1, 2, 3])
 def test_config1_small_uniform_bit_exact(dsax, oracle, corr_path):
     """64 dual-pol antennas, 48 channels, 2048 packets (xGPU NTIME), samples
     uniform on [-8, 7]: whole output bit-exact (fused and corner-turn paths)."""
@@ -54,7 +55,7 @@ def test_reorder_matches_massage(dsax, oracle):
         np.testing.assert_array_equal(got, oracle.massage(blk))
 
 
-@pytest.mark.parametrize("corr_path", [1, 2])
+@pytest.mark.parametrize("corr_path", [1, 2, 3])
 def test_config2_full_block(dsax, oracle, corr_path):
     """Full block [2048][63->64][384][2][2], Gaussian sigma 2.5 clipped to
     [-8, 7]: bit-exact on 24 channels checked by the oracle, plus
@@ -84,15 +85,37 @@ def test_config2_full_block(dsax, oracle, corr_path):
 
 
 def test_formats_agree(dsax, oracle):
-    """REORDER-key (massage) and xGPU int8 inputs give the same products."""
+    """REORDER-key (massage), xGPU int8 and channel-major inputs give the
+    same products."""
     blk = oracle.gen_block(303, 256, 63, 32, "gauss")
     want = oracle.correlate(blk)
     np.testing.assert_array_equal(_run(dsax, blk), want)
     np.testing.assert_array_equal(_run(dsax, oracle.massage(blk), fmt=1), want)
     np.testing.assert_array_equal(_run(dsax, oracle.fluff_reorder(blk), fmt=2), want)
+    cm = np.zeros((32, 256, 64, 4), np.uint8)
+    cm[:, :, :63] = np.transpose(blk.reshape(256, 63, 32, 4), (2, 0, 1, 3))
+    np.testing.assert_array_equal(_run(dsax, cm, fmt=3), want)
 
 
-@pytest.mark.parametrize("corr_path", [1, 2])
+def test_corner_turn_chanmajor(dsax, oracle):
+    """Channel-major corner turn: [nchan][npkt][64][4 B], padded antenna zero."""
+    import torch
+    for npkt, nant, nch in ((64, 63, 384), (5, 63, 40), (7, 64, 3)):
+        blk = oracle.gen_block(npkt * nch + 1, npkt, nant, nch, "uniform")
+        cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nch)
+        with dsax.Context(cfg) as ctx:
+            d_in = torch.from_numpy(blk.reshape(-1)).cuda()
+            out = torch.full((nch * npkt * 64 * 4,), 0xCD, dtype=torch.uint8, device="cuda")
+            torch.cuda.synchronize()
+            ctx.corner_turn(d_in, out, dsax.FMT_CHANMAJOR)
+            ctx.sync()
+            got = out.cpu().numpy().reshape(nch, npkt, 64, 4)
+        want = np.zeros((nch, npkt, 64, 4), np.uint8)
+        want[:, :, :nant] = np.transpose(blk.reshape(npkt, nant, nch, 4), (2, 0, 1, 3))
+        np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("corr_path", [1, 2, 3])
 @pytest.mark.parametrize("npkt,nant,nchan", [(4, 63, 8), (100, 63, 5), (64, 1, 1), (1, 64, 3),
                                              (130, 64, 2), (64, 63, 33)])
 def test_ragged_shapes(dsax, oracle, npkt, nant, nchan, corr_path):
