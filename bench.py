@@ -32,6 +32,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "dsa110-xengine_b200")
 for _p in (PKG, os.path.join(ROOT, "oracle")):
@@ -185,6 +187,123 @@ def cpu_baseline_sample(budget_s: float = 12.0):
             "sample": f"{done} of 384 channels of one full block ({t_total:.1f} s), scaled"}
 
 
+BF_FLOPS = 8 * 256 * 64 * 2 * 384 * 4096      # config 3 beamformer, per block
+
+
+def _bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured"
+    except Exception:
+        return 1590.0, 1400.0, "fallback"
+
+
+def _time_loop(stream, fn, steps, warm=3):
+    import torch
+    for i in range(warm):
+        fn(i)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        fn(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def bench_beamformer(dsax, synth, dev, blk_dev, steps):
+    """Config 3: 256 beams, 32 t x 8 ch Stokes-I from a full block (BF16)."""
+    import torch
+    cfg = dsax.default_config(bf_scale=128.0 / (512 * 64 * 2 * 6.25))
+    with dsax.Context(cfg, device=dev) as ctx:
+        wre, wim = synth.random_phase_weights(9, 48, 256)
+        ctx.set_weights(wre, wim)
+        out = torch.empty(128 * 256 * 48, dtype=torch.uint8, device=f"cuda:{dev}")
+        st = torch.cuda.ExternalStream(ctx.stream)
+        ms = _time_loop(st, lambda i: ctx.beamform(blk_dev[i % len(blk_dev)], out), steps)
+        ctx.sync()
+    burst, sust, kind = _bf16_peak()
+    tf = BF_FLOPS / (ms * 1e-3) / 1e12
+    return {"workload": "64 ant x 2 pol x 384 ch x 4096 t -> 128 x 256 x 48 uint8, 256 beams, BF16",
+            "blocks_per_s": 1e3 / ms, "ms_per_block": ms, "realtime_factor": 1e3 / ms * REALTIME_S,
+            "gpu_launches_per_block": 1,
+            "roofline": {"bound": "tensor", "kernel": "bf_kernel", "achieved": tf,
+                         "peak": burst, "unit": "TFLOP/s", "frac": tf / burst,
+                         "frac_of_sustained": tf / sust, "peak_kind": f"{kind} BF16 dense"}}
+
+
+def bench_flaggers(dsax, synth, dev, steps):
+    """Config 4: plain vs learned flagger on [256][4096][48] FP32 (chi2(2)+RFI).
+    The learned net is trained here first (outside the timed regions)."""
+    import torch
+    from dsax import lflag
+    x, _ = synth.gen_filterbank(4040)
+    xd = torch.from_numpy(x).to(f"cuda:{dev}")
+    B, T, C = x.shape
+    tds = 32
+    p = dsax.flag_params(B, T, C)
+    with dsax.Context(dsax.default_config(npkt=16, nchan=8), device=dev) as ctx:
+        st = torch.cuda.ExternalStream(ctx.stream)
+        cm = torch.zeros(B * C, dtype=torch.uint8, device=xd.device)
+        tm = torch.zeros(B * T, dtype=torch.uint8, device=xd.device)
+        plain_ms = _time_loop(st, lambda i: ctx.flag(p, xd, cm, tm), steps)
+        train = [torch.from_numpy(synth.gen_filterbank(5000 + k, nbeam=64)[0]).to(xd.device)
+                 for k in range(4)]
+        ctx.lf_init(11)
+        t0 = time.perf_counter()
+        lflag.train(ctx, train, steps=300, beams_per_step=16, tds=tds)
+        ctx.sync()
+        train_s = time.perf_counter() - t0
+        mask = torch.zeros(B * (T // tds) * C, dtype=torch.uint8, device=xd.device)
+        learned_ms = _time_loop(st, lambda i: ctx.flag_learned(p, xd, mask, tds=tds), steps)
+        ctx.sync()
+        pred, ref = lflag.evaluate(ctx, xd, tds)
+    P, R, F1 = lflag.prf1(pred, ref)
+    npx = B * T * C
+    return {"workload": "256 beams x 4096 t x 48 ch FP32 chi2(2) + tones/bursts/drifts",
+            "plain": {"ms_per_block": plain_ms, "samples_per_s": npx / (plain_ms * 1e-3),
+                      "gpu_launches_per_block": 2},
+            "learned": {"ms_per_block": learned_ms, "samples_per_s": npx / (learned_ms * 1e-3),
+                        "precision": P, "recall": R, "f1": F1, "train_s": train_s,
+                        "train_steps": 300, "params": dsax.lib().dsax_lf_nparams()},
+            "learned_vs_plain_speed": plain_ms / learned_ms}
+
+
+def bench_batch(dsax, synth, dev, steps):
+    """Config 5: 16 blocks, widths from {192, 384, 768}, corner turn +
+    correlate + beamform + flag each, one CUDA graph vs per-block launches."""
+    import torch
+    rng = np.random.default_rng(55)
+    widths = [int(w) for w in rng.choice([192, 384, 768], size=16)]
+    cfg = dsax.default_config(nchan=768, bf_scale=128.0 / (512 * 64 * 2 * 6.25))
+    base = synth.gen_block(5150, 2048, 63, 768, "gauss")
+    with dsax.Context(cfg, device=dev) as ctx:
+        wre, wim = synth.random_phase_weights(5, 96, 256)
+        ctx.set_weights(wre, wim)
+        descs = []
+        for k, w in enumerate(widths):
+            blk = np.ascontiguousarray(base[:, :, (7 * k) % (768 - w + 1):][:, :, :w])
+            descs.append({"blk": torch.from_numpy(blk.reshape(-1)).to(f"cuda:{dev}"), "nchan": w,
+                          "vis": torch.empty(2 * w * 2080 * 8, dtype=torch.float32, device=f"cuda:{dev}"),
+                          "beams": torch.empty(128 * 256 * (w // 8), dtype=torch.uint8, device=f"cuda:{dev}"),
+                          "chanmask": torch.empty(256 * (w // 8), dtype=torch.uint8, device=f"cuda:{dev}"),
+                          "tsmask": torch.empty(256 * 128, dtype=torch.uint8, device=f"cuda:{dev}")})
+        st = torch.cuda.ExternalStream(ctx.stream)
+        graph_ms = _time_loop(st, lambda i: ctx.run_batch(descs, use_graph=True), steps)
+        eager_ms = _time_loop(st, lambda i: ctx.run_batch(descs, use_graph=False), steps)
+        ctx.sync()
+    nb = len(widths)
+    return {"workload": "16 blocks x 2048 pkt x 63 ant, widths " + ",".join(map(str, widths)),
+            "widths": widths,
+            "graph": {"blocks_per_s": nb * 1e3 / graph_ms, "ms_per_batch": graph_ms},
+            "per_block_launches": {"blocks_per_s": nb * 1e3 / eager_ms, "ms_per_batch": eager_ms},
+            "realtime_factor_graph": nb * 1e3 / graph_ms * REALTIME_S * 384.0 / np.mean(widths),
+            "gpu_launches_per_batch": 5 * nb}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,6 +313,8 @@ def main():
     ap.add_argument("--ref-channels", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the beamformer / flagger / batch side measurements")
     ap.add_argument("--corr-path", type=int, default=0,
                     help="0 default (=3), 1 fused kernel, 2 REORDER-layout corner turn, "
                          "3 channel-major corner turn + bulk-copy-fed correlator")
@@ -217,8 +338,8 @@ def main():
     dev = local
     torch.cuda.set_device(dev)
 
-    import oracle  # input generator only (seeded synthetic block)
-    blk = oracle.gen_block(4242 + rank, 2048, 63, 384, "gauss")
+    from dsax import synth
+    blk = synth.gen_block(4242 + rank, 2048, 63, 384, "gauss")
     cfg = dsax.default_config(corr_path=args.corr_path)
     ctx = dsax.Context(cfg, device=dev)
     nbuf = 3
@@ -363,6 +484,14 @@ def main():
         }
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline_sample()
+        if not args.no_extras and ws == 1:
+            for key, fn in (("beamformer", lambda: bench_beamformer(dsax, synth, dev, ins, 20)),
+                            ("flagger", lambda: bench_flaggers(dsax, synth, dev, 20)),
+                            ("batch", lambda: bench_batch(dsax, synth, dev, 5))):
+                try:
+                    line[key] = fn()
+                except Exception as exc:  # reported, never silently dropped
+                    line[key] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

@@ -158,6 +158,7 @@ void dsax_destroy(dsax_ctx *c) {
   if (!c) return;
   DeviceGuard g(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  release_batch_plan(c);
   c->release_all();
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_err) cudaFreeHost(c->h_err);

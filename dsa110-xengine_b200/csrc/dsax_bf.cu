@@ -220,6 +220,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
             const int to = a.ppo <= kPktPerStage ? pg * nsub + sI : pg / pgs_per_out;
             const int64_t o = ((int64_t)to * a.nbeam + beam) * ngrp + g;
             if (a.out_f32) a.out_f32[o] = P;
+            if (a.out_fb) a.out_fb[((int64_t)beam * (a.npkt / a.ppo) + to) * ngrp + g] = P;
             if (a.out_u8) {
               int v = __float2int_rn(P * a.scale);
               a.out_u8[o] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));

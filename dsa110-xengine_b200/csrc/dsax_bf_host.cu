@@ -71,6 +71,7 @@ int dsax_set_weights(dsax_ctx *c, const double *wre, const double *wim) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "upload weights");
   c->weights_ready = 1;
+  c->weights_nchan = c->cfg.nchan;
   return DSAX_OK;
 }
 

@@ -273,25 +273,42 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Channel-major variant: the input is [nchan][npkt][64 ant][4 B] (one
-// contiguous stream per channel, written by reorder_cm_kernel).  A loader
-// warp streams 64-packet stages (16 KB) into shared memory with bulk
-// copies, four stages ahead; the producer warps unpack from shared memory
-// (no global-memory latency on their critical path) into the same A / Arot
-// operand tiles as corr_kernel.
+// Channel-major correlator.  Input [nchan][npkt][64 ant][4 B] (one contiguous
+// stream per channel, written by reorder_cm_kernel).
+//
+// Arithmetic without negated operands: with R, I the int8 real and
+// imaginary parts (rows = 2*station + pol, K = packets),
+//     Re V = R R^T + I I^T,   C = I R^T,   Im V[a][b] = C[a][b] - C[b][a].
+// Three M128 N128 UMMAs per K step (25 % less tensor work than one M128
+// N256 product with a rotated copy), C transposed in the epilogue through
+// shared memory.
+//
+// Stage = 128 packets.  The loader warp bulk-copies each packet's 256 B
+// into a raw row of 272 B (the 16-byte pad makes the unpack reads bank-
+// conflict free).  A thread unpacks 8 packets P = pg + 16 q of one antenna:
+// K position k(P) = 8 (P mod 16) + P / 16 puts them in 8 consecutive bytes
+// of the R and I rows (K order is a free permutation shared by A and B).
 namespace corrcm {
-constexpr int kRawStages = 4;
-constexpr int kRawBytes = 64 * 64 * 4;           // 64 packets x 64 antennas x 4 B
-constexpr int kStages = 2;                       // operand stages
-constexpr int kThreads = 320;                    // 8 producer warps + MMA warp + loader warp
-constexpr int kSmemBytes = 1024 + kStages * corr::kStageBytes + kRawStages * kRawBytes;
+constexpr int kPktPerStage = 128;
+constexpr int kRawRow = 272;                     // bytes per packet row in shared memory
+constexpr int kRawBytes = kPktPerStage * kRawRow;  // 34,816
+constexpr int kRawStages = 2;
+constexpr int kTile = 128 * 128;                 // 128 rows x 128 B of K
+constexpr int kFreqBytes = 2 * kTile;            // R + I
+constexpr int kStageBytes = 2 * kFreqBytes;      // two frequencies
+constexpr int kOpStages = 2;
+constexpr int kThreads = 320;                    // 8 unpack/epilogue warps + UMMA warp + loader warp
+constexpr int kSmemBytes = 1024 + kOpStages * kStageBytes + kRawStages * kRawBytes;
+constexpr uint32_t kIdesc = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 128);
 }  // namespace corrcm
 
+// Sign-extend the low nibble of each byte: v | (bit3 ? 0xF0 : 0).
+__device__ __forceinline__ uint32_t sext_nib4(uint32_t v) {
+  return v | ((v & 0x08080808u) * 0x1Eu);
+}
+
 __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a) {
-  using namespace corr;
-  using corrcm::kRawStages;
-  using corrcm::kRawBytes;
-  constexpr int kOpStages = corrcm::kStages;
+  using namespace corrcm;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kOpStages];
   __shared__ __align__(8) uint64_t empty_bar[kOpStages];
@@ -303,18 +320,18 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ch = blockIdx.x;
-  const uint32_t smem_base = (smem_u32(smem_raw) + 1023u) & ~1023u;
-  const uint32_t raw_base = smem_base + kOpStages * kStageBytes;
-  const uint8_t *raw_gen = smem_raw + (raw_base - smem_u32(smem_raw));  // generic view
+  const uint32_t sbase = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  const uint32_t raw_base = sbase + kOpStages * kStageBytes;
+  uint8_t *const gbase = smem_raw + (sbase - smem_u32(smem_raw));   // generic view of sbase
 
   if (tid == 0) {
     for (int s = 0; s < kOpStages; ++s) {
-      mbar_init(&full_bar[s], kProducerThreads);
+      mbar_init(&full_bar[s], 256);
       mbar_init(&empty_bar[s], 1);
     }
     for (int r = 0; r < kRawStages; ++r) {
       mbar_init(&rfull_bar[r], 1);
-      mbar_init(&rempty_bar[r], kProducerThreads);
+      mbar_init(&rempty_bar[r], 256);
     }
     mbar_init(&accum_bar, 1);
     abort_sh = 0;
@@ -336,9 +353,8 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
   const uint8_t *chan_src = a.in + (int64_t)ch * a.npkt * 256;
 
   if (warp < 8) {
-    // ------------------------------------------------------------ producers
-    const int ant = 16 * (warp & 3) + 4 * (lane >> 3) + (lane & 3);
-    const int jbit = (lane >> 2) & 1;
+    // ------------------------------------------------------------ unpack
+    const int ant_lo = lane & 3, pg_lo = lane >> 2;
     for (int ks = 0; ks < nks && !abort_sh; ++ks) {
       const int s = ks % kOpStages, r = ks % kRawStages;
       if (!mbar_wait_bounded(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
@@ -347,35 +363,52 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
       if (!mbar_wait_bounded(&empty_bar[s], ((uint32_t)(ks / kOpStages) & 1u) ^ 1u, &abort_sh,
                              a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
         break;
-      const uint32_t *rw = reinterpret_cast<const uint32_t *>(raw_gen + r * kRawBytes);
-      const uint32_t stage = smem_base + (uint32_t)s * kStageBytes;
+      const uint32_t *rw = reinterpret_cast<const uint32_t *>(gbase + kOpStages * kStageBytes +
+                                                              r * kRawBytes);
+      const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
+      const int pvalid = a.npkt - ks * kPktPerStage;   // packets of this stage that exist
 #pragma unroll
-      for (int it = 0; it < 2; ++it) {
-        const int pg = 2 * ((warp >> 2) * 2 + it) + jbit;
+      for (int it = 0; it < 4; ++it) {
+        const int pg = pg_lo + 8 * (it & 1);
+        const int ant = 4 * (2 * warp + (it >> 1)) + ant_lo;
         uint32_t w[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const int p = ks * kPktPerStage + 8 * pg + q;
-          w[q] = p < a.npkt ? rw[(8 * pg + q) * 64 + ant] : 0u;
+          const int P = pg + 16 * q;
+          w[q] = P < pvalid ? rw[P * (kRawRow / 4) + ant] : 0u;
+        }
+        // 4x4 byte transposes: X[sl][h] = sample slot sl (= 2t + pol) of
+        // packets q = 4h .. 4h+3
+        uint32_t X[4][2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t t0 = __byte_perm(w[4 * h], w[4 * h + 1], 0x5140u);
+          const uint32_t t1 = __byte_perm(w[4 * h], w[4 * h + 1], 0x7362u);
+          const uint32_t t2 = __byte_perm(w[4 * h + 2], w[4 * h + 3], 0x5140u);
+          const uint32_t t3 = __byte_perm(w[4 * h + 2], w[4 * h + 3], 0x7362u);
+          X[0][h] = __byte_perm(t0, t2, 0x5410u);
+          X[1][h] = __byte_perm(t0, t2, 0x7632u);
+          X[2][h] = __byte_perm(t1, t3, 0x5410u);
+          X[3][h] = __byte_perm(t1, t3, 0x7632u);
         }
 #pragma unroll
-        for (int t = 0; t < 2; ++t) {
-#pragma unroll
-          for (int pol = 0; pol < 2; ++pol) {
-            uint32_t c[4];
-#pragma unroll
-            for (int h = 0; h < 4; ++h)
-              c[h] = unpack_pair(w[2 * h], w[2 * h + 1], (uint32_t)(2 * t + pol));
-            const uint32_t row = (uint32_t)(2 * ant + pol);
-            const uint32_t off = sw128_offset(row, (uint32_t)pg);
-            const uint32_t tileA = stage + (uint32_t)t * kFreqBytes;
-            st_shared_v4(tileA + off, c[0], c[1], c[2], c[3]);
-            st_shared_v4(tileA + kTileBytes + off, rotate_pair(c[0]), rotate_pair(c[1]),
-                         rotate_pair(c[2]), rotate_pair(c[3]));
-          }
+        for (int sl = 0; sl < 4; ++sl) {
+          const int t = sl >> 1, pol = sl & 1;
+          const uint32_t re0 = sext_nib4(X[sl][0] & 0x0F0F0F0Fu);
+          const uint32_t re1 = sext_nib4(X[sl][1] & 0x0F0F0F0Fu);
+          const uint32_t im0 = sext_nib4((X[sl][0] >> 4) & 0x0F0F0F0Fu);
+          const uint32_t im1 = sext_nib4((X[sl][1] >> 4) & 0x0F0F0F0Fu);
+          const uint32_t row = (uint32_t)(2 * ant + pol);
+          const uint32_t off = sw128_offset(row, (uint32_t)(pg >> 1)) + 8u * (pg & 1);
+          const uint32_t tR = stage + (uint32_t)t * kFreqBytes;
+          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(tR + off), "r"(re0), "r"(re1)
+                       : "memory");
+          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(tR + kTile + off), "r"(im0),
+                       "r"(im1)
+                       : "memory");
         }
       }
-      mbar_arrive(&rempty_bar[r]);   // raw stage consumed (generic-proxy reads only)
+      mbar_arrive(&rempty_bar[r]);
       fence_proxy_async_smem();
       mbar_arrive(&full_bar[s]);
     }
@@ -388,10 +421,11 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
                                a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
           break;
         const int npk = min(kPktPerStage, a.npkt - ks * kPktPerStage);
-        const uint32_t bytes = (uint32_t)npk * 256u;
-        mbar_arrive_expect_tx(&rfull_bar[r], bytes);
-        bulk_g2s(raw_base + (uint32_t)r * kRawBytes, chan_src + (int64_t)ks * kPktPerStage * 256,
-                 bytes, &rfull_bar[r]);
+        mbar_arrive_expect_tx(&rfull_bar[r], (uint32_t)npk * 256u);
+        const uint8_t *src = chan_src + (int64_t)ks * kPktPerStage * 256;
+        const uint32_t dst = raw_base + (uint32_t)r * kRawBytes;
+        for (int p = 0; p < npk; ++p)
+          bulk_g2s(dst + (uint32_t)p * kRawRow, src + (int64_t)p * 256, 256u, &rfull_bar[r]);
       }
     }
     __syncwarp();
@@ -404,14 +438,18 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
                                DEV_ERR_WAIT_FULL, a.wait_limit_ns))
           break;
         tc_fence_after();
-        const uint32_t stage = smem_base + (uint32_t)s * kStageBytes;
+        const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-          const uint32_t tileA = stage + (uint32_t)t * kFreqBytes;
+          const uint32_t tR = stage + (uint32_t)t * kFreqBytes, tI = tR + kTile;
+          const uint32_t dre = tmem + (uint32_t)t * 256u, dc = dre + 128u;
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {
-            const uint64_t d = umma_desc_sw128(tileA + 32u * kk, 1024u);
-            umma_i8(tmem + (uint32_t)t * 256u, d, d, kIdesc, (ks | kk) != 0);
+          for (int kk = 0; kk < 4; ++kk) {   // 4 x K = 32 bytes per 128-byte row
+            const uint64_t dR = umma_desc_sw128(tR + 32u * kk, 1024u);
+            const uint64_t dI = umma_desc_sw128(tI + 32u * kk, 1024u);
+            umma_i8(dre, dR, dR, kIdesc, (ks | kk) != 0);   // Re += R R^T
+            umma_i8(dre, dI, dI, kIdesc, 1u);               // Re += I I^T
+            umma_i8(dc, dI, dR, kIdesc, (ks | kk) != 0);    // C  += I R^T
           }
         }
         umma_commit(&empty_bar[s]);
@@ -427,25 +465,43 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
                                 a.wait_limit_ns);
     tc_fence_after();
     ok = __all_sync(0xffffffffu, ok && !abort_sh);
+    const int q = warp & 3, t = warp >> 2;
+    const int m = 32 * q + lane;                   // row = 2 * station + pol
+    const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
+    // C^T through shared memory (operand stage t is free now): row m of C
+    // stored at word (b ^ (m & 31)) of a 512-byte row.
+    uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase + t * kStageBytes);
     if (ok) {
-      const int q = warp & 3, t = warp >> 2;
-      const int m = 32 * q + lane;
+#pragma unroll
+      for (int cb = 0; cb < 8; ++cb) {
+        uint32_t cv[16];
+        tmem_ld16(trow + 128u + 16u * cb, cv);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
+      }
+    }
+    named_bar(1, 256);
+    if (ok) {
       const int i = m >> 1, pi = m & 1;
       float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
-      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
+      const int64_t tri = (int64_t)i * (i + 1) / 2;
       const int ncb = 2 * q + 2;
       for (int cb = 0; cb < ncb; ++cb) {
-        uint32_t re[16], im[16];
+        uint32_t re[16], cr[16];
         tmem_ld16(trow + 16u * cb, re);
-        tmem_ld16(trow + 128u + 16u * cb, im);
+        tmem_ld16(trow + 128u + 16u * cb, cr);
         tmem_wait_ld();
-        const int64_t tri = (int64_t)i * (i + 1) / 2;
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
           const int j = 8 * cb + jj;
           if (j <= i) {
-            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(int32_t)im[2 * jj],
-                                   (float)(int32_t)re[2 * jj + 1], (float)(int32_t)im[2 * jj + 1]);
+            const int b0 = 2 * j, b1 = 2 * j + 1;
+            const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
+            const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
+            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)((int32_t)cr[2 * jj] - ct0),
+                                   (float)(int32_t)re[2 * jj + 1],
+                                   (float)((int32_t)cr[2 * jj + 1] - ct1));
             float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
             if (a.accumulate) {
               const float4 old = *dst;

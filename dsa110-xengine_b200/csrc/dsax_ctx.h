@@ -22,6 +22,7 @@ enum {
   AUX_LF_STATE = 9,     // learned flagger: params, grads, Adam m, v
   AUX_LF_WLAYOUT = 10,  // learned flagger: forward / data-gradient weight layouts
   AUX_LF_SCRATCH = 11,  // learned flagger: activations, gradients, partials
+  AUX_BATCH_SCRATCH = 12,  // batch: corner-turned block, beam filterbank, flag statistics
 };
 
 struct DevBuf {
@@ -47,6 +48,7 @@ int set_error(dsax_ctx *c, int code, const char *fmt, ...);
 int cuda_check(dsax_ctx *c, cudaError_t e, const char *what);
 int ensure_buffer(dsax_ctx *c, DevBuf &b, size_t nbytes, const char *what);
 int check_device_error(dsax_ctx *c);
+void release_batch_plan(dsax_ctx *c);
 bool aligned16(const void *p);
 
 }  // namespace dsax
@@ -62,6 +64,8 @@ struct dsax_ctx {
   dsax::DevBuf vis_buf;   // host-mode staging: visibilities
   dsax::DevBuf aux[16];   // per-stage buffers, indexed by dsax::AUX_*
   int weights_ready = 0;
+  int weights_nchan = 0;      // channels covered by the weight image
+  void *batch_plan = nullptr; // captured batch graph (dsax_batch.cu)
   dsax::LfNet lf_storage;
   dsax::LfNet *lf = &lf_storage;
   char errmsg[512] = {0};

@@ -19,87 +19,89 @@ namespace dsax {
 
 namespace flag {
 constexpr int kStatThreads = 512;   // 16 warps per beam
-constexpr int kMaxChan = 64;        // two channels per lane
+constexpr int kMaxChan = 128;       // four channels per lane
 constexpr int kDecThreads = 256;
 }  // namespace flag
 
 // ---------------------------------------------------------------- stats
 // One CTA per beam.  Warp w owns the TBIN-sample bins w, w+16, ...; lane l
-// owns channels l and l+32.  Sums are FP64 in sample order within a bin
-// (the oracle's order), max/bin extremes exact.
+// owns channels l, l+32, l+64, l+96.  Sums are FP64 in sample order within a
+// bin (the oracle's order), max/bin extremes exact.
 __global__ void __launch_bounds__(flag::kStatThreads) flag_stats_kernel(FlagArgs a) {
+  constexpr int NL = flag::kMaxChan / 32;   // channels per lane
   const int b = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nw = blockDim.x >> 5;
   const int T = a.ntime, C = a.nchan, TB = a.tbin;
   const int nbins = T / TB;
   const float *xb = a.x + (int64_t)b * T * C;
-  const int c0 = lane, c1 = lane + 32;
-  const bool h0 = c0 < C, h1 = c1 < C;
 
-  double s0 = 0.0, s1 = 0.0, q0 = 0.0, q1 = 0.0;
-  float m0 = -INFINITY, m1 = -INFINITY;
-  double bmax0 = -1e300, bmin0 = 1e300, bmax1 = -1e300, bmin1 = 1e300;
-
-  for (int bin = warp; bin < nbins; bin += nw) {
-    double bs0 = 0.0, bs1 = 0.0;
-    for (int t = bin * TB; t < (bin + 1) * TB; ++t) {
-      const float *row = xb + (int64_t)t * C;
-      const float v0 = h0 ? __ldg(row + c0) : 0.0f;
-      const float v1 = h1 ? __ldg(row + c1) : 0.0f;
-      bs0 += v0; bs1 += v1;
-      q0 += (double)v0 * v0; q1 += (double)v1 * v1;
-      m0 = fmaxf(m0, h0 ? v0 : -INFINITY);
-      m1 = fmaxf(m1, h1 ? v1 : -INFINITY);
-      double r = (double)v0 + (double)v1;
+  double s[NL], q[NL], bmax[NL], bmin[NL], bs[NL];
+  float m[NL];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-      if (lane == 0) a.ts[(int64_t)b * T + t] = (float)(r / C);
-    }
-    s0 += bs0; s1 += bs1;
-    const double mb0 = bs0 / TB, mb1 = bs1 / TB;
-    bmax0 = fmax(bmax0, mb0); bmin0 = fmin(bmin0, mb0);
-    bmax1 = fmax(bmax1, mb1); bmin1 = fmin(bmin1, mb1);
+  for (int k = 0; k < NL; ++k) {
+    s[k] = 0.0; q[k] = 0.0; bmax[k] = -1e300; bmin[k] = 1e300; m[k] = -INFINITY;
   }
-  // samples beyond the last whole bin (T % TB): sums and max only
-  for (int t = nbins * TB + warp; t < T; t += nw) {
-    const float *row = xb + (int64_t)t * C;
-    const float v0 = h0 ? __ldg(row + c0) : 0.0f;
-    const float v1 = h1 ? __ldg(row + c1) : 0.0f;
-    s0 += v0; s1 += v1;
-    q0 += (double)v0 * v0; q1 += (double)v1 * v1;
-    m0 = fmaxf(m0, h0 ? v0 : -INFINITY);
-    m1 = fmaxf(m1, h1 ? v1 : -INFINITY);
-    double r = (double)v0 + (double)v1;
+  auto row = [&](int t, bool bin) {
+    const float *rp = xb + (int64_t)t * C;
+    double r = 0.0;
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+      const int c = lane + 32 * k;
+      const float v = c < C ? __ldg(rp + c) : 0.0f;
+      if (bin) bs[k] += v; else s[k] += v;
+      q[k] += (double)v * v;
+      if (c < C) m[k] = fmaxf(m[k], v);
+      r += v;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
     if (lane == 0) a.ts[(int64_t)b * T + t] = (float)(r / C);
+  };
+  for (int bin = warp; bin < nbins; bin += nw) {
+#pragma unroll
+    for (int k = 0; k < NL; ++k) bs[k] = 0.0;
+    for (int t = bin * TB; t < (bin + 1) * TB; ++t) row(t, true);
+#pragma unroll
+    for (int k = 0; k < NL; ++k) {
+      s[k] += bs[k];
+      const double mb = bs[k] / TB;
+      bmax[k] = fmax(bmax[k], mb);
+      bmin[k] = fmin(bmin[k], mb);
+    }
   }
+  // samples beyond the last whole bin (T % TB): sums and max only
+  for (int t = nbins * TB + warp; t < T; t += nw) row(t, false);
 
-  __shared__ double sh_s[16][flag::kMaxChan], sh_q[16][flag::kMaxChan];
-  __shared__ double sh_bmax[16][flag::kMaxChan], sh_bmin[16][flag::kMaxChan];
-  __shared__ float sh_m[16][flag::kMaxChan];
-  sh_s[warp][c0] = s0; sh_s[warp][c1] = s1;
-  sh_q[warp][c0] = q0; sh_q[warp][c1] = q1;
-  sh_m[warp][c0] = m0; sh_m[warp][c1] = m1;
-  sh_bmax[warp][c0] = bmax0; sh_bmax[warp][c1] = bmax1;
-  sh_bmin[warp][c0] = bmin0; sh_bmin[warp][c1] = bmin1;
+  extern __shared__ double fsh[];
+  double *sh_s = fsh, *sh_q = sh_s + 16 * flag::kMaxChan;
+  double *sh_bmax = sh_q + 16 * flag::kMaxChan, *sh_bmin = sh_bmax + 16 * flag::kMaxChan;
+  float *sh_m = reinterpret_cast<float *>(sh_bmin + 16 * flag::kMaxChan);
+#pragma unroll
+  for (int k = 0; k < NL; ++k) {
+    const int c = lane + 32 * k;
+    sh_s[warp * flag::kMaxChan + c] = s[k];
+    sh_q[warp * flag::kMaxChan + c] = q[k];
+    sh_m[warp * flag::kMaxChan + c] = m[k];
+    sh_bmax[warp * flag::kMaxChan + c] = bmax[k];
+    sh_bmin[warp * flag::kMaxChan + c] = bmin[k];
+  }
   __syncthreads();
   if (threadIdx.x < C) {
     const int c = threadIdx.x;
-    double s = 0.0, q = 0.0, bx = -1e300, bn = 1e300;
-    float m = -INFINITY;
+    double ss = 0.0, qq = 0.0, bx = -1e300, bn = 1e300;
+    float mm = -INFINITY;
     for (int w = 0; w < nw; ++w) {
-      s += sh_s[w][c]; q += sh_q[w][c];
-      m = fmaxf(m, sh_m[w][c]);
-      bx = fmax(bx, sh_bmax[w][c]); bn = fmin(bn, sh_bmin[w][c]);
+      ss += sh_s[w * flag::kMaxChan + c]; qq += sh_q[w * flag::kMaxChan + c];
+      mm = fmaxf(mm, sh_m[w * flag::kMaxChan + c]);
+      bx = fmax(bx, sh_bmax[w * flag::kMaxChan + c]); bn = fmin(bn, sh_bmin[w * flag::kMaxChan + c]);
     }
-    const double mean = s / T;
-    const double var = fmax(q / T - mean * mean, 0.0);
+    const double mean = ss / T;
+    const double var = fmax(qq / T - mean * mean, 0.0);
     const int o = b * C + c;
     a.spec[o] = (float)mean;
     a.var[o] = (float)var;
-    a.maxs[o] = a.parity ? (float)mean : m;
+    a.maxs[o] = a.parity ? (float)mean : mm;
     a.pp[o] = nbins > 0 ? (float)(bx - bn) : 0.0f;
   }
 }
@@ -239,7 +241,13 @@ __global__ void __launch_bounds__(flag::kDecThreads) flag_decide_kernel(FlagArgs
 
 int launch_flag(const FlagArgs &a, cudaStream_t st) {
   if (a.nchan > flag::kMaxChan || a.ts_base > 4096) return -1;
-  flag_stats_kernel<<<a.nbeam, flag::kStatThreads, 0, st>>>(a);
+  static bool attr = false;
+  const size_t ssh = 16 * flag::kMaxChan * (4 * sizeof(double) + sizeof(float));
+  if (!attr) {
+    cudaFuncSetAttribute(flag_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssh);
+    attr = true;
+  }
+  flag_stats_kernel<<<a.nbeam, flag::kStatThreads, ssh, st>>>(a);
   if (cudaGetLastError() != cudaSuccess) return -2;
   const int tmpn = a.ts_base > a.nchan ? a.ts_base : a.nchan;
   const size_t sh = sizeof(float) * (2 * a.nchan + tmpn + a.ts_base);

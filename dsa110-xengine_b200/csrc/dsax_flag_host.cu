@@ -33,10 +33,10 @@ int dsax_flag(dsax_ctx *c, const dsax_flag_params *p, const float *x, const floa
               uint8_t *chanmask, uint8_t *tsmask, float *stats, int *counts, int mem) {
   if (!c || !p || !x || !chanmask || !tsmask) return DSAX_ERR_ARG;
   const int B = p->nbeam, T = p->ntime, C = p->nchan;
-  if (B < 1 || T < 1 || C < 1 || C > 64 || p->guard < 0 || C - 2 * p->guard < 1 ||
+  if (B < 1 || T < 1 || C < 1 || C > 128 || p->guard < 0 || C - 2 * p->guard < 1 ||
       p->filt < 1 || p->filt > C - 2 * p->guard || p->tbin < 1 || p->fbin < 1 ||
       p->ts_base < 1 || p->ts_base > T || p->ts_base > 4096 || p->nperm < 0 || p->nperm > 8)
-    return set_error(c, DSAX_ERR_ARG, "flag parameters out of range (nchan <= 64, ts_base <= 4096)");
+    return set_error(c, DSAX_ERR_ARG, "flag parameters out of range (nchan <= 128, ts_base <= 4096)");
   if (mem != DSAX_MEM_HOST && mem != DSAX_MEM_DEVICE) return DSAX_ERR_ARG;
   DeviceGuard dg(c->device);
   const size_t nbc = (size_t)B * C, nbt = (size_t)B * T;

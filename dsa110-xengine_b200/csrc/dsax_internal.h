@@ -44,6 +44,7 @@ struct BfArgs {
   const uint8_t *wimg;     // weight operand image [ngrp][nbeam/64][2 pol][2 kb][16 KB]
   uint8_t *out_u8;         // [npkt/ppo][nbeam][nchan/8] Stokes-I uint8 (or null)
   float *out_f32;          // same layout, FP32 power before scaling (or null)
+  float *out_fb;           // [nbeam][npkt/ppo][nchan/8] FP32 power (filterbank order, or null)
   int *err;
   int npkt, nant_in, nchan, nbeam, ppo;
   float scale;

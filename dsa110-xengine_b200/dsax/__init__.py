@@ -64,6 +64,12 @@ class FlagParams(ctypes.Structure):
                 ("nperm", ctypes.c_int), ("perm", ctypes.c_int * 8)]
 
 
+class BlockDesc(ctypes.Structure):
+    _fields_ = [("blk", ctypes.c_void_p), ("nchan", ctypes.c_int), ("vis", ctypes.c_void_p),
+                ("beams", ctypes.c_void_p), ("chanmask", ctypes.c_void_p),
+                ("tsmask", ctypes.c_void_p)]
+
+
 def flag_params(nbeam: int, ntime: int, nchan: int, **kw) -> FlagParams:
     p = FlagParams()
     lib().dsax_default_flag_params(ctypes.byref(p), nbeam, ntime, nchan)
@@ -150,6 +156,7 @@ def _bind_optional(L):
         "dsax_lf_train_step": ([P, P, P, P, ctypes.POINTER(FlagParams), I, ctypes.c_float,
                                 ctypes.c_float, I, P, P], I),
         "dsax_flag_learned": ([P, P, ctypes.POINTER(FlagParams), I, P, P, I], I),
+        "dsax_run_batch": ([P, ctypes.POINTER(BlockDesc), I, I], I),
     }
     for name, (args, res) in table.items():
         if hasattr(L, name):
@@ -310,3 +317,18 @@ class Context:
         rc = lib().dsax_flag_learned(self._h, _ptr(x), ctypes.byref(params), tds, _ptr(mask),
                                      _ptr(logits), mem)
         self._check(rc, "dsax_flag_learned")
+
+    # -- batches -----------------------------------------------------------
+    def run_batch(self, descs, use_graph: bool = True):
+        """descs: list of dicts with keys blk, nchan, vis, beams, chanmask,
+        tsmask (device tensors or None)."""
+        arr = (BlockDesc * len(descs))()
+        for i, d in enumerate(descs):
+            arr[i].blk = _ptr(d["blk"])
+            arr[i].nchan = int(d["nchan"])
+            arr[i].vis = _ptr(d.get("vis"))
+            arr[i].beams = _ptr(d.get("beams"))
+            arr[i].chanmask = _ptr(d.get("chanmask"))
+            arr[i].tsmask = _ptr(d.get("tsmask"))
+        self._check(lib().dsax_run_batch(self._h, arr, len(descs), int(use_graph)),
+                    "dsax_run_batch")

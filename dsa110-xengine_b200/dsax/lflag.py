@@ -14,7 +14,9 @@ def plain_masks(ctx, x_dev, params: FlagParams):
     B, T, C = params.nbeam, params.ntime, params.nchan
     cm = torch.zeros(B * C, dtype=torch.uint8, device=x_dev.device)
     tm = torch.zeros(B * T, dtype=torch.uint8, device=x_dev.device)
+    torch.cuda.synchronize(x_dev.device)   # inputs ready before the library stream reads them
     ctx.flag(params, x_dev, cm, tm)
+    ctx.sync()                             # masks complete before torch or the host reads them
     return cm, tm
 
 
@@ -37,6 +39,7 @@ def train(ctx, blocks, steps: int = 300, beams_per_step: int = 16, tds: int = 32
     pfull = flag_params(B, T, C)
     labels = [plain_masks(ctx, x, pfull) for x in blocks]
     pb = flag_params(beams_per_step, T, C)
+    torch.cuda.synchronize(blocks[0].device)
     losses = []
     for it in range(steps):
         k = int(rng.integers(len(blocks)))
@@ -60,6 +63,20 @@ def evaluate(ctx, x_dev, tds: int = 32):
     cm, tm = plain_masks(ctx, x_dev, p)
     ref = pixel_labels(cm.cpu().numpy(), tm.cpu().numpy(), B, T, C, tds, p.guard)
     mask = torch.zeros(B * (T // tds) * C, dtype=torch.uint8, device=x_dev.device)
+    torch.cuda.synchronize(x_dev.device)
     ctx.flag_learned(p, x_dev, mask, tds=tds)
     ctx.sync()
     return mask.cpu().numpy().reshape(B, T // tds, C).astype(bool), ref
+
+
+def prf1(pred, truth):
+    """Precision, recall and F1 of a boolean mask against a reference mask."""
+    pred = np.asarray(pred, bool)
+    truth = np.asarray(truth, bool)
+    tp = int((pred & truth).sum())
+    fp = int((pred & ~truth).sum())
+    fn = int((~pred & truth).sum())
+    p = tp / (tp + fp) if tp + fp else 1.0
+    r = tp / (tp + fn) if tp + fn else 1.0
+    f1 = 2 * p * r / (p + r) if p + r else 0.0
+    return p, r, f1

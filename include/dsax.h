@@ -162,7 +162,7 @@ int dsax_beamform(dsax_ctx *ctx, const void *blk, void *out_u8, void *out_f32, i
  * :534-556) and MADs -- on the GPU.  The shapes the reference hard-codes
  * are parameters here. */
 typedef struct dsax_flag_params {
-    int nbeam, ntime, nchan; /* filterbank [nbeam][ntime][nchan], nchan <= 64      */
+    int nbeam, ntime, nchan; /* filterbank [nbeam][ntime][nchan], nchan <= 128     */
     int guard;     /* ZeroChannels guard band at each edge (128 of 1024)           */
     int filt;      /* nFiltSize forward median window (21)                          */
     int tbin;      /* TBIN samples per peak-to-peak bin (128)                       */
@@ -188,6 +188,26 @@ void dsax_default_flag_params(dsax_flag_params *p, int nbeam, int ntime, int nch
  * With DSAX_MEM_DEVICE every pointer is device memory. */
 int dsax_flag(dsax_ctx *ctx, const dsax_flag_params *p, const float *x, const float *oldspec,
               uint8_t *chanmask, uint8_t *tsmask, float *stats, int *counts, int mem);
+
+/* ---- batches of blocks ----
+ * Many consecutive capture blocks in one submission, each with its own
+ * subband width (nchan, a multiple of 8, at most the nchan the context
+ * and its weights were set up with).  Per block: corner turn + correlate
+ * (if vis), beamform (if beams or chanmask), plain flagger on the block's
+ * beam filterbank [nbeam][npkt/bf_pkt_per_out][nchan/8] (if chanmask; the
+ * ts mask too if tsmask).  Device pointers only.  use_graph = 1 captures
+ * the whole batch into a CUDA graph on the first call and replays it while
+ * the descriptors stay the same.  Enqueued on the context stream. */
+typedef struct dsax_block_desc {
+    const void *blk;      /* captured block [npkt][nant_in][nchan][2][2]      */
+    int nchan;            /* subband width of this block                       */
+    float *vis;           /* [2*nchan][2080][4][re,im] or NULL                 */
+    uint8_t *beams;       /* [npkt/ppo][nbeam][nchan/8] uint8 or NULL          */
+    uint8_t *chanmask;    /* [nbeam][nchan/8] or NULL                          */
+    uint8_t *tsmask;      /* [nbeam][npkt/ppo] or NULL                         */
+} dsax_block_desc;
+
+int dsax_run_batch(dsax_ctx *ctx, const dsax_block_desc *blocks, int nblk, int use_graph);
 
 /* ---- learned RFI flagger (no reference counterpart) ----
  * A 4-layer 3x3 conv net (4 -> 32 -> 64 -> 64 -> 1 channels, ReLU,
