@@ -14,6 +14,7 @@
 
 #include "dsax_internal.h"
 #include "dsax_ptx.cuh"
+#include "../../include/dsax.h"
 
 namespace dsax {
 
@@ -256,3 +257,72 @@ int launch_flag(const FlagArgs &a, cudaStream_t st) {
 }
 
 }  // namespace dsax
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the plain flagger for callers that cannot call
+// cudaMalloc (a process whose device memory is owned by another runtime or
+// pool, a real-time thread that must not enter the allocator, or code that
+// runs while a CUDA graph is being recorded by someone else).  The
+// statistics live in this file-scope device array instead of a context
+// buffer: every GPU that loads the library holds it until the process
+// exits, every call shares it, and it keeps the last call's contents.
+namespace dsax {
+
+constexpr long long kNoAllocScratchFloats = 1572864;  // 6 MiB
+static __device__ __align__(256) float g_flag_scratch[kNoAllocScratchFloats];
+
+namespace {
+constexpr int kMaxDevices = 64;
+float *g_scratch_addr[kMaxDevices] = {};   // device address per device, set up once
+}  // namespace
+
+// Resolves the array's device address on the current device (once per
+// device).  Returns nullptr on failure.
+static float *noalloc_scratch(int dev) {
+  if (dev < 0 || dev >= kMaxDevices) return nullptr;
+  if (!g_scratch_addr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_flag_scratch) != cudaSuccess) return nullptr;
+    g_scratch_addr[dev] = static_cast<float *>(p);
+  }
+  return g_scratch_addr[dev];
+}
+
+}  // namespace dsax
+
+extern "C" int dsax_flag_noalloc(const dsax_flag_params *p, const float *x, const float *oldspec,
+                                 uint8_t *chanmask, uint8_t *tsmask, int *counts, void *stream) {
+  using namespace dsax;
+  if (!p || !x || !chanmask || !tsmask) return DSAX_ERR_ARG;
+  const int B = p->nbeam, T = p->ntime, C = p->nchan;
+  if (B < 1 || T < 1 || C < 1 || C > 128 || p->guard < 0 || C - 2 * p->guard < 1 ||
+      p->filt < 1 || p->filt > C - 2 * p->guard || p->tbin < 1 || p->fbin < 1 ||
+      p->ts_base < 1 || p->ts_base > T || p->ts_base > 4096 || p->nperm < 0 || p->nperm > 8)
+    return DSAX_ERR_ARG;
+  const long long nbc = (long long)B * C, nbt = (long long)B * T;
+  const long long need = 4 * nbc + nbt + 2;   // spec, var, max, pp, ts, two counters
+  if (need > kNoAllocScratchFloats) return DSAX_ERR_ARG;   // beyond the fixed 6 MiB
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DSAX_ERR_CUDA;
+  float *s = noalloc_scratch(dev);
+  if (!s) return DSAX_ERR_CUDA;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  FlagArgs a{};
+  a.x = x; a.oldspec = oldspec; a.chanmask = chanmask; a.tsmask = tsmask;
+  a.nbeam = B; a.ntime = T; a.nchan = C;
+  a.guard = p->guard; a.filt = p->filt; a.tbin = p->tbin; a.fbin = p->fbin;
+  a.ts_base = p->ts_base; a.tsflag = p->tsflag; a.parity = p->parity;
+  a.thresh = p->thresh; a.var_add = p->var_add; a.ts_thresh = p->ts_thresh;
+  a.nperm = p->nperm;
+  for (int i = 0; i < p->nperm; ++i) a.perm[i] = p->perm[i];
+  a.spec = s; a.var = s + nbc; a.maxs = s + 2 * nbc; a.pp = s + 3 * nbc; a.ts = s + 4 * nbc;
+  a.counts = reinterpret_cast<int *>(s + 4 * nbc + nbt);
+  // the counters accumulate with atomics: clear them (the array keeps the
+  // previous call's values)
+  if (cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), st) != cudaSuccess) return DSAX_ERR_CUDA;
+  if (launch_flag(a, st) != 0) return DSAX_ERR_CUDA;
+  if (counts && cudaMemcpyAsync(counts, a.counts, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st) !=
+                    cudaSuccess)
+    return DSAX_ERR_CUDA;
+  return DSAX_OK;
+}

@@ -189,6 +189,23 @@ void dsax_default_flag_params(dsax_flag_params *p, int nbeam, int ntime, int nch
 int dsax_flag(dsax_ctx *ctx, const dsax_flag_params *p, const float *x, const float *oldspec,
               uint8_t *chanmask, uint8_t *tsmask, float *stats, int *counts, int mem);
 
+/* Allocation-free plain flagger.  No counterpart in the reference: it is for
+ * callers that cannot call cudaMalloc -- a process whose device memory is
+ * owned by another runtime's pool, a real-time thread that must not enter
+ * the allocator, or code running while someone else records a CUDA graph.
+ * Same computation and outputs as dsax_flag, without a context: it runs on
+ * the current device and the given cudaStream_t (NULL = default stream),
+ * and every pointer (x, oldspec, chanmask, tsmask, counts) is device memory.
+ * The statistics use a fixed 6 MiB device array compiled into the library
+ * (held on every GPU that loads it until the process exits), so
+ * 4*nbeam*nchan + nbeam*ntime + 2 must not exceed 1,572,864 floats; larger
+ * sizes return DSAX_ERR_ARG.  The first call on a device looks up that
+ * array's address; make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller.  Nothing is allocated or freed. */
+int dsax_flag_noalloc(const dsax_flag_params *p, const float *x, const float *oldspec,
+                      uint8_t *chanmask, uint8_t *tsmask, int *counts, void *stream);
+
 /* ---- batches of blocks ----
  * Many consecutive capture blocks in one submission, each with its own
  * subband width (nchan, a multiple of 8, at most the nchan the context
