@@ -254,7 +254,7 @@ def bench_flaggers(dsax, synth, dev, steps):
                  for k in range(4)]
         ctx.lf_init(11)
         t0 = time.perf_counter()
-        lflag.train(ctx, train, steps=300, beams_per_step=16, tds=tds)
+        lflag.train(ctx, train, steps=600, beams_per_step=16, tds=tds)
         ctx.sync()
         train_s = time.perf_counter() - t0
         mask = torch.zeros(B * (T // tds) * C, dtype=torch.uint8, device=xd.device)
@@ -268,7 +268,7 @@ def bench_flaggers(dsax, synth, dev, steps):
                       "gpu_launches_per_block": 2},
             "learned": {"ms_per_block": learned_ms, "samples_per_s": npx / (learned_ms * 1e-3),
                         "precision": P, "recall": R, "f1": F1, "train_s": train_s,
-                        "train_steps": 300, "params": dsax.lib().dsax_lf_nparams()},
+                        "train_steps": 600, "params": dsax.lib().dsax_lf_nparams()},
             "learned_vs_plain_speed": plain_ms / learned_ms}
 
 

@@ -23,6 +23,7 @@ enum {
   AUX_LF_WLAYOUT = 10,  // learned flagger: forward / data-gradient weight layouts
   AUX_LF_SCRATCH = 11,  // learned flagger: activations, gradients, partials
   AUX_BATCH_SCRATCH = 12,  // batch: corner-turned block, beam filterbank, flag statistics
+  AUX_TUNE = 13,           // autotuner: synthetic block + visibilities
 };
 
 struct DevBuf {

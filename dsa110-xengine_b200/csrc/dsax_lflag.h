@@ -6,7 +6,7 @@
 namespace dsax {
 
 constexpr int kLfLayers = 4;
-constexpr int kLfCin[kLfLayers] = {4, 32, 64, 64};
+constexpr int kLfCin[kLfLayers] = {8, 32, 64, 64};
 constexpr int kLfCout[kLfLayers] = {32, 64, 64, 1};
 
 // Offsets of layer l's weights / bias in the flat parameter vector:

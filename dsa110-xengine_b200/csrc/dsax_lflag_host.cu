@@ -58,7 +58,7 @@ int ensure_net(dsax_ctx *c) {
 
 int check_lf_shape(dsax_ctx *c, const dsax_flag_params *p, int tds) {
   if (!p || tds < 1 || p->ntime % tds || p->nchan % 4 || p->nchan > 64 ||
-      (size_t)2 * (p->ntime / tds) * p->nchan * 4 > 190 * 1024)
+      ((size_t)2 * (p->ntime / tds) * p->nchan + 2 * (p->ntime / tds)) * 4 > 190 * 1024)
     return set_error(c, DSAX_ERR_ARG,
                      "learned flagger needs ntime %% tds == 0, nchan %% 4 == 0, nchan <= 64");
   return DSAX_OK;
@@ -73,12 +73,12 @@ struct LfScratch {
 
 int lf_scratch(dsax_ctx *c, int B, int H, int W, LfScratch &s) {
   const size_t px = (size_t)B * H * W;
-  const size_t nf = px * (4 + 32 + 64 + 64 + 1 + 1 + 64 + 64) + lf_part_floats(B, H);
+  const size_t nf = px * (8 + 32 + 64 + 64 + 1 + 1 + 64 + 64) + lf_part_floats(B, H);
   int rc = ensure_buffer(c, c->aux[AUX_LF_SCRATCH], nf * 4 + px + 64, "learned-flagger scratch");
   if (rc != DSAX_OK) return rc;
   float *f = static_cast<float *>(c->aux[AUX_LF_SCRATCH].ptr);
   s.loss = reinterpret_cast<double *>(f);  f += 16;
-  s.F = f;  f += px * 4;
+  s.F = f;  f += px * 8;
   s.a1 = f; f += px * 32;
   s.a2 = f; f += px * 64;
   s.a3 = f; f += px * 64;

@@ -1,0 +1,79 @@
+// dsax_tune.cu -- autotuner: times the interchangeable kernel variants of
+// a stage on the context's own geometry and device, keeps the fastest in
+// the context, and reports every timing.  Candidates for the captured-block
+// correlator: (1) one fused kernel on the captured layout, (2) corner turn
+// to the REORDER layout + row-load correlator, (3) corner turn to channel-
+// major streams + bulk-copy-fed correlator (two kinds of operand staging
+// and tile shape: 64-packet stages of [re,im | -im,re] vs 128-packet R/I
+// stages).
+#include <cstring>
+#include <cuda_runtime.h>
+
+#include "../../include/dsax.h"
+#include "dsax_ctx.h"
+#include "dsax_internal.h"
+
+using namespace dsax;
+
+namespace {
+
+__global__ void fill_pattern(uint8_t *p, size_t n, uint32_t seed) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t h = (uint32_t)i * 2654435761u ^ seed;
+    h ^= h >> 15;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    p[i] = (uint8_t)h;
+  }
+}
+
+}  // namespace
+
+extern "C" int dsax_autotune(dsax_ctx *c, int reps, float *times_ms, int ntimes, int *best_path) {
+  if (!c || reps < 1) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  const size_t nin = dsax_block_bytes(&c->cfg, DSAX_FMT_CAPTURED);
+  const size_t nvis = dsax_vis_bytes(&c->cfg);
+  int rc;
+  if ((rc = ensure_buffer(c, c->aux[AUX_TUNE], nin + nvis + 256, "autotune block")) != DSAX_OK)
+    return rc;
+  uint8_t *blk = static_cast<uint8_t *>(c->aux[AUX_TUNE].ptr);
+  float *vis = reinterpret_cast<float *>(blk + ((nin + 255) & ~(size_t)255));
+  fill_pattern<<<1024, 256, 0, c->stream>>>(blk, nin, 12345u);
+  const int saved = c->cfg.corr_path;
+  const int paths[3] = {1, 2, 3};
+  float best = 1e30f;
+  int bestp = 3;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int k = 0; k < 3; ++k) {
+    c->cfg.corr_path = paths[k];
+    for (int w = 0; w < 2; ++w)
+      if ((rc = dsax_correlate_fmt(c, DSAX_FMT_CAPTURED, blk, vis, DSAX_MEM_DEVICE, 0)) != DSAX_OK)
+        break;
+    if (rc != DSAX_OK) break;
+    cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps; ++r)
+      if ((rc = dsax_correlate_fmt(c, DSAX_FMT_CAPTURED, blk, vis, DSAX_MEM_DEVICE, 0)) != DSAX_OK)
+        break;
+    cudaEventRecord(e1, c->stream);
+    if (rc != DSAX_OK) break;
+    if ((rc = dsax_sync(c)) != DSAX_OK) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= reps;
+    if (times_ms && k < ntimes) times_ms[k] = ms;
+    if (ms < best) { best = ms; bestp = paths[k]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != DSAX_OK) {
+    c->cfg.corr_path = saved;
+    return rc;
+  }
+  c->cfg.corr_path = bestp;
+  if (best_path) *best_path = bestp;
+  return DSAX_OK;
+}

@@ -157,6 +157,7 @@ def _bind_optional(L):
                                 ctypes.c_float, I, P, P], I),
         "dsax_flag_learned": ([P, P, ctypes.POINTER(FlagParams), I, P, P, I], I),
         "dsax_run_batch": ([P, ctypes.POINTER(BlockDesc), I, I], I),
+        "dsax_autotune": ([P, I, P, I, P], I),
     }
     for name, (args, res) in table.items():
         if hasattr(L, name):
@@ -317,6 +318,17 @@ class Context:
         rc = lib().dsax_flag_learned(self._h, _ptr(x), ctypes.byref(params), tds, _ptr(mask),
                                      _ptr(logits), mem)
         self._check(rc, "dsax_flag_learned")
+
+    # -- autotuner ---------------------------------------------------------
+    def autotune(self, reps: int = 10):
+        """Returns ({corr_path: ms}, chosen corr_path); the context keeps the choice."""
+        import numpy as np
+        t = np.zeros(3, np.float32)
+        best = ctypes.c_int(0)
+        self._check(lib().dsax_autotune(self._h, reps, _ptr(t), 3, ctypes.byref(best)),
+                    "dsax_autotune")
+        self.cfg.corr_path = best.value
+        return {1: float(t[0]), 2: float(t[1]), 3: float(t[2])}, best.value
 
     # -- batches -----------------------------------------------------------
     def run_batch(self, descs, use_graph: bool = True):

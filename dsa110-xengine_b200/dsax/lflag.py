@@ -29,10 +29,11 @@ def pixel_labels(cm, tm, B, T, C, tds, guard):
     return cm[:, None, :] | (ts[:, :, None] & inside[None, None, :])
 
 
-def train(ctx, blocks, steps: int = 300, beams_per_step: int = 16, tds: int = 32,
-          lr: float = 2e-3, pos_weight: float = 2.0, seed: int = 0, log=None):
+def train(ctx, blocks, steps: int = 600, beams_per_step: int = 16, tds: int = 32,
+          lr: float = 3e-3, pos_weight: float = 3.0, seed: int = 0, log=None):
     """blocks: list of device filterbanks [B][T][C] (torch float32).  Labels
-    come from the GPU plain flagger on each whole block."""
+    come from the GPU plain flagger on each whole block.  Adam with a cosine
+    learning-rate decay from lr to lr/20."""
     import torch
     rng = np.random.default_rng(seed)
     B, T, C = blocks[0].shape
@@ -47,8 +48,9 @@ def train(ctx, blocks, steps: int = 300, beams_per_step: int = 16, tds: int = 32
         x = blocks[k][b0:b0 + beams_per_step]
         cm = labels[k][0].view(B, C)[b0:b0 + beams_per_step]
         tm = labels[k][1].view(B, T)[b0:b0 + beams_per_step]
+        lr_t = lr * (0.05 + 0.95 * 0.5 * (1.0 + np.cos(np.pi * it / max(steps - 1, 1))))
         loss = ctx.lf_train_step(pb, x.contiguous(), cm.contiguous(), tm.contiguous(), tds=tds,
-                                 lr=lr, pos_weight=pos_weight)
+                                 lr=lr_t, pos_weight=pos_weight)
         losses.append(loss)
         if log and (it % 50 == 0 or it == steps - 1):
             log(f"step {it} loss {loss:.4f}")

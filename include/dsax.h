@@ -120,6 +120,12 @@ int dsax_host_free(dsax_ctx *ctx, void *ptr);
  * overwrite. */
 int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
 
+/* Autotuner: times the captured-block correlator variants (corr_path 1, 2,
+ * 3) on a synthetic block of the context's geometry (reps launches each),
+ * sets the context's corr_path to the fastest, and returns the per-variant
+ * milliseconds (times_ms[0..2] for paths 1..3, if given) and the choice. */
+int dsax_autotune(dsax_ctx *ctx, int reps, float *times_ms, int ntimes, int *best_path);
+
 /* massage() on the GPU (src/dsaX_reorder_raw.c:153-169): captured block ->
  * REORDER-key layout [pkt][2*nchan][64][2 pol] (4+4-bit kept packed, padded
  * antennas zero).  dsax_block_bytes(cfg, DSAX_FMT_REORDERED) bytes out. */
@@ -227,10 +233,13 @@ typedef struct dsax_block_desc {
 int dsax_run_batch(dsax_ctx *ctx, const dsax_block_desc *blocks, int nblk, int use_graph);
 
 /* ---- learned RFI flagger (no reference counterpart) ----
- * A 4-layer 3x3 conv net (4 -> 32 -> 64 -> 64 -> 1 channels, ReLU,
- * 57,185 FP32 parameters) over the filterbank downsampled by tds samples,
- * with four features per pixel (z-scores of the pixel mean, pixel max,
- * row channel-mean and column mean, log-compressed).  It is trained on the
+ * A 4-layer 3x3 conv net (8 -> 32 -> 64 -> 64 -> 1 channels, ReLU,
+ * 58,337 FP32 parameters) over the filterbank downsampled by tds samples,
+ * with eight features per pixel (log-compressed z-scores of the pixel mean
+ * and max, the row channel-mean, the max of the channel-mean series inside
+ * the pixel, and the column mean, max, variance and peak-to-peak of
+ * 128-sample means -- the statistics the plain flagger thresholds).  It is
+ * trained on the
  * plain flagger's masks and predicts the pixel mask the plain flagger
  * applies: (chanmask[b][c]) or (tsmask in the pixel's samples and inside
  * the guard band).  The plain flagger (dsax_flag) stays the fallback and
@@ -241,7 +250,7 @@ int dsax_lf_nparams(void);
 int dsax_lf_init(dsax_ctx *ctx, unsigned long long seed);
 int dsax_lf_set_params(dsax_ctx *ctx, const float *params, int n);
 int dsax_lf_get_params(dsax_ctx *ctx, float *params, int n);
-/* features [nbeam][ntime/tds][nchan][4] float32 */
+/* features [nbeam][ntime/tds][nchan][8] float32 */
 int dsax_lf_features(dsax_ctx *ctx, const float *x, const dsax_flag_params *p, int tds, float *F);
 /* One training step on p->nbeam beams: weighted BCE-with-logits (positive
  * pixels weighted by pos_weight, guard band excluded) on the plain

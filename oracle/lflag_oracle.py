@@ -9,13 +9,14 @@ the label rule below restates how that flagger's masks are applied
 (flag :459-474 replaces whole (beam, channel) columns, flagts :479-494
 replaces (beam, time) rows inside the guard band).
 
-Layouts (NHWC): features [B][H=T/tds][W=C][4]; weights [Cout][3][3][Cin].
+Layouts (NHWC): features [B][H=T/tds][W=C][8]; weights [Cout][3][3][Cin].
 """
 from __future__ import annotations
 
 import numpy as np
 
-LAYERS = [(4, 32), (32, 64), (64, 64), (64, 1)]
+LAYERS = [(8, 32), (32, 64), (64, 64), (64, 1)]
+TBIN = 128
 
 
 def n_params() -> int:
@@ -23,8 +24,8 @@ def n_params() -> int:
 
 
 def init_params(seed: int):
-    """He-normal weights, zero biases (the CUDA init draws the same values
-    from the same counter-based generator; see lf_init_kernel)."""
+    """He-normal weights, zero biases from numpy's generator (tests copy
+    these into the library with dsax_lf_set_params)."""
     rng = np.random.default_rng(seed)
     ps = []
     for ci, co in LAYERS:
@@ -38,11 +39,13 @@ def _slog(v):
 
 
 def features(x: np.ndarray, tds: int = 32) -> np.ndarray:
-    """x [B][T][C] -> [B][T/tds][C][4]:
-    f0 = slog(z of the tds-sample mean), f1 = slog((max - mu)/sigma),
-    f2 = slog(z of the row's channel-mean), f3 = slog(z of the column mean),
-    with mu, sigma the mean and standard deviation of the whole beam and
-    slog(v) = sign(v) log(1 + |v|)."""
+    """x [B][T][C] -> [B][T/tds][C][8], slog(v) = sign(v) log(1 + |v|) of
+    z-scores against the beam mean mu and standard deviation sigma:
+    f0 pixel mean (x sqrt(tds)), f1 pixel max, f2 row channel-mean
+    (x sqrt(tds C)), f3 column mean (x sqrt(T)), f4 max over the pixel's
+    samples of the channel-mean series (x sqrt(C)), f5 column max,
+    f6 (column variance / sigma^2 - 1) x sqrt(T/2), f7 column peak-to-peak
+    of TBIN-sample means / sigma x sqrt(TBIN)."""
     B, T, C = x.shape
     H = T // tds
     xd = x[:, :H * tds].astype(np.float64)
@@ -52,16 +55,30 @@ def features(x: np.ndarray, tds: int = 32) -> np.ndarray:
     pm = blk.mean(axis=2)
     px = blk.max(axis=2)
     rm = pm.mean(axis=2)                          # [B][H]
+    tsmax = blk.mean(axis=3).max(axis=2)          # [B][H]
     cm = x.astype(np.float64).mean(axis=1)        # [B][C]
+    cmax = x.max(axis=1).astype(np.float64)
+    cvar = x.astype(np.float64).var(axis=1)
+    pb = max(TBIN // tds, 1)
+    nb = H // pb
+    if nb > 0:
+        bm = pm[:, :nb * pb].reshape(B, nb, pb, C).mean(axis=2)
+        cpp = bm.max(axis=1) - bm.min(axis=1)
+    else:
+        cpp = np.zeros((B, C))
     m = mu[:, None, None]
     s = sd[:, None, None]
-    f = np.empty((B, H, C, 4))
+    ones_c = np.ones((1, 1, C))
+    ones_h = np.ones((1, H, 1))
+    f = np.empty((B, H, C, 8))
     f[..., 0] = _slog((pm - m) / s * np.sqrt(tds))
     f[..., 1] = _slog((px - m) / s)
-    f[..., 2] = _slog(((rm - mu[:, None]) / sd[:, None] * np.sqrt(tds * C))[:, :, None]
-                      * np.ones((1, 1, C)))
-    f[..., 3] = _slog(((cm - mu[:, None]) / sd[:, None] * np.sqrt(T))[:, None, :]
-                      * np.ones((1, H, 1)))
+    f[..., 2] = _slog(((rm - mu[:, None]) / sd[:, None] * np.sqrt(tds * C))[:, :, None] * ones_c)
+    f[..., 3] = _slog(((cm - mu[:, None]) / sd[:, None] * np.sqrt(T))[:, None, :] * ones_h)
+    f[..., 4] = _slog(((tsmax - mu[:, None]) / sd[:, None] * np.sqrt(C))[:, :, None] * ones_c)
+    f[..., 5] = _slog(((cmax - mu[:, None]) / sd[:, None])[:, None, :] * ones_h)
+    f[..., 6] = _slog(((cvar / (sd[:, None] ** 2) - 1.0) * np.sqrt(0.5 * T))[:, None, :] * ones_h)
+    f[..., 7] = _slog((cpp / sd[:, None] * np.sqrt(max(TBIN, tds)))[:, None, :] * ones_h)
     return f
 
 

@@ -176,3 +176,20 @@ def test_misaligned_device_pointer_rejected(dsax):
         with pytest.raises(dsax.DsaxError) as ei:
             ctx.correlate(buf.data_ptr() + 4, vis)
         assert ei.value.status == dsax.DSAX_ERR_ARG
+
+
+def test_autotune_picks_fastest_and_stays_exact(dsax, oracle):
+    import torch
+    blk = oracle.gen_block(606, 256, 63, 64, "gauss")
+    cfg = dsax.default_config(npkt=256, nant_in=63, nchan=64)
+    with dsax.Context(cfg) as ctx:
+        times, best = ctx.autotune(reps=3)
+        assert best in (1, 2, 3) and all(t > 0 for t in times.values())
+        assert times[best] == min(times.values())
+        d_in = torch.from_numpy(blk.reshape(-1)).cuda()
+        vis = torch.zeros(128 * 2080 * 8, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.correlate(d_in, vis)
+        ctx.sync()
+        np.testing.assert_array_equal(vis.cpu().numpy().reshape(128, 2080, 4, 2),
+                                      oracle.correlate(blk))

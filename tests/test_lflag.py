@@ -11,7 +11,7 @@ import lflag_oracle as LO
 def test_oracle_gradients_finite_difference():
     rng = np.random.default_rng(0)
     params = LO.init_params(1)
-    f = rng.standard_normal((1, 5, 8, 4))
+    f = rng.standard_normal((1, 5, 8, 8))
     y = rng.random((1, 5, 8)) < 0.3
     valid = np.ones((1, 5, 8))
     valid[..., :1] = 0
@@ -39,7 +39,7 @@ def test_oracle_gradients_finite_difference():
 
 
 def test_param_count():
-    assert LO.n_params() == 57185
+    assert LO.n_params() == 58337
 
 
 def _flat(params):
@@ -63,10 +63,12 @@ def test_features_match_oracle(dsax, oracle):
     x, _ = oracle.gen_filterbank(11, nbeam=4, ntime=1024, nchan=48)
     p = dsax.flag_params(4, 1024, 48)
     with dsax.Context(dsax.default_config(npkt=16, nchan=8)) as ctx:
-        F = torch.zeros(4 * 32 * 48 * 4, dtype=torch.float32, device="cuda")
-        ctx.lf_features(p, torch.from_numpy(x).cuda(), F, tds=32)
+        F = torch.zeros(4 * 32 * 48 * 8, dtype=torch.float32, device="cuda")
+        xd = torch.from_numpy(x).cuda()
+        torch.cuda.synchronize()
+        ctx.lf_features(p, xd, F, tds=32)
         ctx.sync()
-        got = F.cpu().numpy().reshape(4, 32, 48, 4)
+        got = F.cpu().numpy().reshape(4, 32, 48, 8)
     want = LO.features(x, 32)
     np.testing.assert_allclose(got, want, rtol=2e-4, atol=2e-4)
 
@@ -121,20 +123,22 @@ def test_training_reaches_plain_flagger_masks(dsax, oracle):
     with dsax.Context(dsax.default_config(npkt=16, nchan=8)) as ctx:
         ctx.lf_init(7)
         untrained = [LO.prf1(*lflag.evaluate(ctx, xb, tds)) for xb in test_blocks]
-        lflag.train(ctx, train_blocks, steps=400, beams_per_step=16, tds=tds)
+        losses = lflag.train(ctx, train_blocks, steps=600, beams_per_step=16, tds=tds)
+        print("loss first/last", losses[0], losses[-1])
         trained = [LO.prf1(*lflag.evaluate(ctx, xb, tds)) for xb in test_blocks]
         # threshold rule on one feature (no learning): best over features and cuts
         p = dsax.flag_params(B, T, C)
         best_rule = 0.0
         for xb in test_blocks:
-            F = torch.zeros(B * (T // tds) * C * 4, device="cuda")
+            F = torch.zeros(B * (T // tds) * C * 8, device="cuda")
+            torch.cuda.synchronize()
             ctx.lf_features(p, xb, F, tds=tds)
             ctx.sync()
-            F = F.cpu().numpy().reshape(B, T // tds, C, 4)
+            F = F.cpu().numpy().reshape(B, T // tds, C, 8)
             _, ref = lflag.evaluate(ctx, xb, tds)
             inside = np.zeros(C, bool)
             inside[p.guard:C - p.guard] = True
-            for k in range(4):
+            for k in range(8):
                 for cut in (1.0, 2.0, 3.0, 4.0, 5.0, 6.0):
                     best_rule = max(best_rule, LO.prf1((F[..., k] > cut) & inside, ref)[2])
     print("untrained P/R/F1", untrained)
