@@ -313,6 +313,8 @@ def main():
     ap.add_argument("--ref-channels", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["beamformer", "flagger", "batch"], default=None,
+                    help="run one side workload alone (profiling); prints its JSON")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the beamformer / flagger / batch side measurements")
     ap.add_argument("--corr-path", type=int, default=0,
@@ -329,6 +331,20 @@ def main():
     import dsax
 
     ws, rank, local = _dist()
+    if args.only:
+        from dsax import synth
+        torch.cuda.set_device(local)
+        ins = None
+        if args.only == "beamformer":
+            blk = synth.gen_block(4242, 2048, 63, 384, "gauss")
+            ins = [torch.from_numpy(blk.reshape(-1)).to(f"cuda:{local}")]
+            res = bench_beamformer(dsax, synth, local, ins, args.steps)
+        elif args.only == "flagger":
+            res = bench_flaggers(dsax, synth, local, args.steps)
+        else:
+            res = bench_batch(dsax, synth, local, args.steps)
+        print(json.dumps({"only": args.only, **res}), flush=True)
+        return 0
     dist = None
     if ws > 1:
         import datetime
