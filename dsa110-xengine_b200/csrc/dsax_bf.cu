@@ -18,11 +18,15 @@
 //     B column s   = [ xr_a,  xi_a ]_a
 // so one UMMA D[128 x 256] = A * B^T gives Re/Im of 64 beams x 256 samples.
 //
-// Tiling.  A CTA owns (channel group g, beam tile of 64 beams) and a range of
-// stages in time; a stage is 16 packets (256 samples) of one pol.  The
-// weights of both pols (64 KB) stay resident; data stages are double
-// buffered (64 KB each); TMEM holds two 256-column accumulators so the
-// epilogue of stage i overlaps the MMAs of stage i+1.
+// Tiling.  A CTA owns one beam tile of 64 beams and a range of (channel
+// group g, packet group) pairs; the nbt CTAs of the beam tiles share the
+// range and run it together, so L2 serves their common input.  A stage is
+// 16 packets (256 samples) of one pol.  The weights of both pols (64 KB) of
+// the current g stay resident; data stages are double buffered (64 KB
+// each); the producers stage the next packet group's raw bytes (32 KB)
+// with cp.async while they build the current one; TMEM holds two
+// 256-column accumulators so the epilogue of stage i overlaps the MMAs of
+// stage i+1.
 //   warps 0-3 : producers (global 4-bit -> BF16 K-major swizzled tiles)
 //   warps 4-7 : epilogue (TMEM -> |.|^2 row sums -> outputs)
 //   warp  8   : weight loader (bulk copy) and single-thread UMMA issuer
@@ -43,19 +47,20 @@ constexpr int kWBytes = 2 /*pol*/ * 2 /*kb*/ * kWTileBytes;  // 64 KB per (g, bt
 constexpr int kDTileBytes = kN * kKBlockBytes;        // 256 rows x 128 B = 32 KB
 constexpr int kStageBytes = 2 /*kb*/ * kDTileBytes;   // 64 KB
 constexpr int kStages = 2;
-constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes;
+constexpr int kRawRowBytes = 128 * 16;                // one 16 B load per producer thread
+constexpr int kRawBytes = 16 * kRawRowBytes;          // 32 KB: one packet group, both pols
+constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
 constexpr int kThreads = 288;
 constexpr uint32_t kIdesc = umma_idesc(/*F32*/ 1, /*BF16*/ 1, /*BF16*/ 1, 128, kN);
 }  // namespace bf
 
-__device__ __forceinline__ void bf_decode(int u, int npg, int nbt, int &g, int &bt, int &pg,
-                                          int &pol) {
+// Unit u of a CTA's range: r = u / 2 enumerates (channel group g, packet
+// group pg) as g * npg + pg; pol = u % 2.  The beam tile is fixed per CTA.
+__device__ __forceinline__ void bf_decode(int u, int npg, int &g, int &pg, int &pol) {
   pol = u & 1;
   const int r = u >> 1;
   pg = r % npg;
-  const int gb = r / npg;
-  bt = gb % nbt;
-  g = gb / nbt;
+  g = r / npg;
 }
 
 __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
@@ -76,13 +81,18 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   const uint32_t wsm = base;                  // weights [pol][kb][128 x 128 B]
   const uint32_t dsm = base + kWBytes;        // data stages [s][kb][256 x 128 B]
+  const uint32_t raw = dsm + kStages * kStageBytes;   // producer staging [16][128][16 B]
 
+  // Work split: the nbt CTAs of a slot (consecutive blockIdx) own the same
+  // (g, pg) range, one beam tile each, and run it in lockstep, so each
+  // input sector is fetched from HBM about once and then served by L2.
+  // Ranges are whole output times (pgs_per_out packet groups).
   const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / kPktPerStage;
   const int align = 2 * (a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1);
-  const int nunits = ngrp * nbt * npg * 2;
-  const int nchunks = nunits / align;
-  const int u_lo = (int)((long long)blockIdx.x * nchunks / gridDim.x) * align;
-  const int u_hi = (int)((long long)(blockIdx.x + 1) * nchunks / gridDim.x) * align;
+  const int nchunks = ngrp * npg * 2 / align;
+  const int nslots = gridDim.x / nbt, slot = blockIdx.x / nbt, bt = blockIdx.x % nbt;
+  const int u_lo = (int)((long long)slot * nchunks / nslots) * align;
+  const int u_hi = (int)((long long)(slot + 1) * nchunks / nslots) * align;
 
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -114,37 +124,69 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
 
   if (warp < 4) {
     // ------------------------------------------------------------ producers
+    // Thread (q, j): packet q of the stage, antennas 4j..4j+3 of each K
+    // block.  The 16 B loads of a (g, pg) carry both pols: they are issued
+    // once, one packet group ahead (while the previous group's two pol
+    // stages are built), and reused for the pol-1 stage.
     const int j = lane & 7;
     const int q = 4 * warp + (lane >> 3);          // packet within the stage
     const int64_t ant_stride = (int64_t)a.nchan * 4;
     const int64_t pkt_stride = (int64_t)a.nant_in * ant_stride;
+    // Each thread stages its own 16 loads of the next packet group in a
+    // private slice of `raw` ([16][128 threads][16 B], conflict free) with
+    // cp.async (zero fill for the padded antenna), and reads them back into
+    // registers when that group starts, which frees the slice for the next
+    // group's copies.
+    const uint32_t myraw = raw + 16u * (uint32_t)tid;
+    uint4 Ucur[16];
+    auto stage_group = [&](int r) {
+      const int g = r / npg, pg = r % npg;
+      const int p = pg * kPktPerStage + q;
+#pragma unroll
+      for (int it = 0; it < 4; ++it) {
+        const int kb = it & 1, h = it >> 1;
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii) {
+          const int ant = 32 * kb + 4 * j + ii;
+          const bool ok = ant < a.nant_in && p < a.npkt;
+          const uint8_t *src = a.in + (ok ? p * pkt_stride + ant * ant_stride + (int64_t)(8 * g) * 4 +
+                                                16 * h
+                                          : 0);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                           myraw + (uint32_t)(4 * it + ii) * (kRawRowBytes)),
+                       "l"(src), "r"(ok ? 16 : 0)
+                       : "memory");
+        }
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (u_lo < u_hi) stage_group(u_lo >> 1);
     for (int u = u_lo, i = 0; u < u_hi && !abort_sh; ++u, ++i) {
       const int s = i % kStages;
       const uint32_t ph = (uint32_t)(i / kStages) & 1u;
+      const int pol = u & 1;
+      if (pol == 0) {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+                       : "=r"(Ucur[k].x), "=r"(Ucur[k].y), "=r"(Ucur[k].z), "=r"(Ucur[k].w)
+                       : "r"(myraw + (uint32_t)k * kRawRowBytes)
+                       : "memory");
+        }
+        if (u + 2 < u_hi) stage_group((u >> 1) + 1);
+      }
       if (!mbar_wait_bounded(&empty_bar[s], ph ^ 1u, &abort_sh, a.err, DEV_ERR_WAIT_EMPTY,
                              a.wait_limit_ns))
         break;
-      int g, bt, pg, pol;
-      bf_decode(u, npg, nbt, g, bt, pg, pol);
-      const int p = pg * kPktPerStage + q;
       const uint32_t sel = (uint32_t)pol | ((4u + pol) << 4) | ((2u + pol) << 8) | ((6u + pol) << 12);
       const uint32_t stage = dsm + (uint32_t)s * kStageBytes;
 #pragma unroll
       for (int it = 0; it < 4; ++it) {
         const int kb = it & 1, h = it >> 1;
-        uint4 U[4];
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii) {
-          const int ant = 32 * kb + 4 * j + ii;
-          if (ant < a.nant_in && p < a.npkt) {
-            U[ii] = __ldg(reinterpret_cast<const uint4 *>(a.in + p * pkt_stride + ant * ant_stride +
-                                                          (int64_t)(8 * g) * 4 + 16 * h));
-          } else {
-            U[ii] = make_uint4(0u, 0u, 0u, 0u);
-          }
-        }
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
+          const uint4 *U = Ucur + 4 * it;
           const uint32_t u0 = w == 0 ? U[0].x : w == 1 ? U[0].y : w == 2 ? U[0].z : U[0].w;
           const uint32_t u1 = w == 0 ? U[1].x : w == 1 ? U[1].y : w == 2 ? U[1].z : U[1].w;
           const uint32_t u2 = w == 0 ? U[2].x : w == 1 ? U[2].y : w == 2 ? U[2].z : U[2].w;
@@ -166,6 +208,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       fence_proxy_async_smem();
       mbar_arrive(&full_bar[s]);
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");   // no copy outlives an aborted loop
   } else if (warp < 8) {
     // ------------------------------------------------------------ epilogue
     const int q = warp - 4;                          // TMEM lane quarter
@@ -206,8 +249,8 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       tc_fence_before();
       mbar_arrive(&tempty_bar[b]);
 
-      int g, bt, pg, pol;
-      bf_decode(u, npg, nbt, g, bt, pg, pol);
+      int g, pg, pol;
+      bf_decode(u, npg, g, pg, pol);
       if (pol == 1 && ((pg + 1) % pgs_per_out) == 0) {
         // rows m and m + 64 hold Re and Im of the same beam
         if (m >= 64)
@@ -237,8 +280,8 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       int cur_gb = -1;
       uint32_t nload = 0, ndrain = 0;
       for (int u = u_lo, i = 0; u < u_hi && !abort_sh; ++u, ++i) {
-        int g, bt, pg, pol;
-        bf_decode(u, npg, nbt, g, bt, pg, pol);
+        int g, pg, pol;
+        bf_decode(u, npg, g, pg, pol);
         const int gb = g * nbt + bt;
         if (gb != cur_gb) {
           if (i > 0) {  // no UMMA may still read the old weights
@@ -308,8 +351,11 @@ int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
   }
   const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / bf::kPktPerStage;
   const int align = 2 * (a.ppo > bf::kPktPerStage ? a.ppo / bf::kPktPerStage : 1);
-  const int nchunks = ngrp * nbt * npg * 2 / align;
-  const int grid = nchunks < num_sms ? nchunks : num_sms;
+  const int nchunks = ngrp * npg * 2 / align;
+  int nslots = num_sms / nbt;
+  if (nslots < 1) nslots = 1;
+  if (nslots > nchunks) nslots = nchunks;
+  const int grid = nslots * nbt;
   void *args[] = {(void *)&a};
   return cudaLaunchKernel((const void *)bf_kernel, dim3(grid), dim3(bf::kThreads), args,
                           bf::kSmemBytes, st) == cudaSuccess

@@ -276,35 +276,42 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
 // Channel-major correlator.  Input [nchan][npkt][64 ant][4 B] (one contiguous
 // stream per channel, written by reorder_cm_kernel).
 //
-// Arithmetic without negated operands: with R, I the int8 real and
-// imaginary parts (rows = 2*station + pol, K = packets),
-//     Re V = R R^T + I I^T,   C = I R^T,   Im V[a][b] = C[a][b] - C[b][a].
-// Three M128 N128 UMMAs per K step (25 % less tensor work than one M128
-// N256 product with a rotated copy), C transposed in the epilogue through
-// shared memory.
-//
-// Stage = 128 packets.  The loader warp bulk-copies each packet's 256 B
-// into a raw row of 272 B (the 16-byte pad makes the unpack reads bank-
-// conflict free).  A thread unpacks 8 packets P = pg + 16 q of one antenna:
-// K position k(P) = 8 (P mod 16) + P / 16 puts them in 8 consecutive bytes
-// of the R and I rows (K order is a free permutation shared by A and B).
+// Same product as corr_kernel -- D[128 x 256] = A [A ; Arot]^T per 32-byte
+// K step, Re in columns 0..127, Im in 128..255 -- with K laid out per 64-
+// packet stage as [64 real parts | 64 imaginary parts]:
+//     A row    = [ R  | I ]        Arot row = [ -I | R ]
+// Packet P of the stage sits at K byte k(P) = 8 (P mod 8) + P / 8 (a free
+// permutation: A and B share it), so the 16 packets P = 2c + e + 8q
+// (e = 0, 1; q = 0..7) fill 16-byte chunk c of the real half and chunk
+// c + 4 of the imaginary half.  Thread (antenna, c) reads those 16 words
+// (lanes = consecutive antennas: conflict-free), transposes bytes, and
+// sign-extends / negates nibbles with SWAR arithmetic.  Lanes 4..7 of each
+// group of 8 store the two pols in the opposite order, so every 16-byte
+// store instruction covers all eight bank groups of the 128-byte swizzle.
+// One loader thread brings each 64-packet stage (16 KB, contiguous) in with
+// a single bulk copy, four stages ahead.
 namespace corrcm {
-constexpr int kPktPerStage = 128;
-constexpr int kRawRow = 272;                     // bytes per packet row in shared memory
-constexpr int kRawBytes = kPktPerStage * kRawRow;  // 34,816
-constexpr int kRawStages = 2;
-constexpr int kTile = 128 * 128;                 // 128 rows x 128 B of K
-constexpr int kFreqBytes = 2 * kTile;            // R + I
-constexpr int kStageBytes = 2 * kFreqBytes;      // two frequencies
+constexpr int kPktPerStage = 64;
+constexpr int kRawBytes = kPktPerStage * 256;      // 16 KB
+constexpr int kRawStages = 4;
+constexpr int kTile = 128 * 128;                   // 128 rows x 128 B of K
+constexpr int kFreqBytes = 2 * kTile;              // A + Arot
+constexpr int kStageBytes = 2 * kFreqBytes;        // two frequencies
 constexpr int kOpStages = 2;
-constexpr int kThreads = 320;                    // 8 unpack/epilogue warps + UMMA warp + loader warp
+constexpr int kThreads = 320;                      // 8 unpack/epilogue warps + UMMA warp + loader warp
 constexpr int kSmemBytes = 1024 + kOpStages * kStageBytes + kRawStages * kRawBytes;
-constexpr uint32_t kIdesc = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 128);
 }  // namespace corrcm
 
-// Sign-extend the low nibble of each byte: v | (bit3 ? 0xF0 : 0).
+// Low nibble of each byte (0..15) -> sign-extended int8: v | (bit3 ? 0xF0 : 0).
 __device__ __forceinline__ uint32_t sext_nib4(uint32_t v) {
   return v | ((v & 0x08080808u) * 0x1Eu);
+}
+
+// Bytewise two's-complement negation (no carries between bytes); exact for
+// bytes in [-8, 7].
+__device__ __forceinline__ uint32_t neg_bytes(uint32_t x) {
+  const uint32_t t = (~x & 0x7F7F7F7Fu) + 0x01010101u;
+  return t ^ (~x & 0x80808080u);
 }
 
 __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a) {
@@ -322,7 +329,7 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
   const int ch = blockIdx.x;
   const uint32_t sbase = (smem_u32(smem_raw) + 1023u) & ~1023u;
   const uint32_t raw_base = sbase + kOpStages * kStageBytes;
-  uint8_t *const gbase = smem_raw + (sbase - smem_u32(smem_raw));   // generic view of sbase
+  const uint8_t *raw_gen = smem_raw + (raw_base - smem_u32(smem_raw));   // generic view
 
   if (tid == 0) {
     for (int s = 0; s < kOpStages; ++s) {
@@ -354,7 +361,9 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
 
   if (warp < 8) {
     // ------------------------------------------------------------ unpack
-    const int ant_lo = lane & 3, pg_lo = lane >> 2;
+    const int ant = lane + 32 * (warp & 1);
+    const uint32_t c = (uint32_t)(warp >> 1);          // K chunk of the real half (0..3)
+    const uint32_t flip = (uint32_t)(lane >> 2) & 1u;  // store pol 1 first
     for (int ks = 0; ks < nks && !abort_sh; ++ks) {
       const int s = ks % kOpStages, r = ks % kRawStages;
       if (!mbar_wait_bounded(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
@@ -363,52 +372,58 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
       if (!mbar_wait_bounded(&empty_bar[s], ((uint32_t)(ks / kOpStages) & 1u) ^ 1u, &abort_sh,
                              a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
         break;
-      const uint32_t *rw = reinterpret_cast<const uint32_t *>(gbase + kOpStages * kStageBytes +
-                                                              r * kRawBytes);
-      const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
+      const uint32_t *rw = reinterpret_cast<const uint32_t *>(raw_gen + r * kRawBytes);
       const int pvalid = a.npkt - ks * kPktPerStage;   // packets of this stage that exist
+      // w[e][q]: packet 2c + e + 8q, word = bytes [t0p0, t0p1, t1p0, t1p1]
+      uint32_t w[2][8];
 #pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        const int pg = pg_lo + 8 * (it & 1);
-        const int ant = 4 * (2 * warp + (it >> 1)) + ant_lo;
-        uint32_t w[8];
+      for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const int P = pg + 16 * q;
-          w[q] = P < pvalid ? rw[P * (kRawRow / 4) + ant] : 0u;
+          const int P = 2 * (int)c + e + 8 * q;
+          w[e][q] = P < pvalid ? rw[P * 64 + ant] : 0u;
         }
-        // 4x4 byte transposes: X[sl][h] = sample slot sl (= 2t + pol) of
-        // packets q = 4h .. 4h+3
-        uint32_t X[4][2];
+      mbar_arrive(&rempty_bar[r]);   // raw stage consumed (generic-proxy reads only)
+      // X[sl][e][h]: sample slot sl = 2t + pol of packets q = 4h .. 4h+3
+      uint32_t X[4][2][2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const uint32_t t0 = __byte_perm(w[4 * h], w[4 * h + 1], 0x5140u);
-          const uint32_t t1 = __byte_perm(w[4 * h], w[4 * h + 1], 0x7362u);
-          const uint32_t t2 = __byte_perm(w[4 * h + 2], w[4 * h + 3], 0x5140u);
-          const uint32_t t3 = __byte_perm(w[4 * h + 2], w[4 * h + 3], 0x7362u);
-          X[0][h] = __byte_perm(t0, t2, 0x5410u);
-          X[1][h] = __byte_perm(t0, t2, 0x7632u);
-          X[2][h] = __byte_perm(t1, t3, 0x5410u);
-          X[3][h] = __byte_perm(t1, t3, 0x7632u);
+          const uint32_t *v = &w[e][4 * h];
+          const uint32_t t0 = __byte_perm(v[0], v[1], 0x5140u);
+          const uint32_t t1 = __byte_perm(v[0], v[1], 0x7362u);
+          const uint32_t t2 = __byte_perm(v[2], v[3], 0x5140u);
+          const uint32_t t3 = __byte_perm(v[2], v[3], 0x7362u);
+          X[0][e][h] = __byte_perm(t0, t2, 0x5410u);
+          X[1][e][h] = __byte_perm(t0, t2, 0x7632u);
+          X[2][e][h] = __byte_perm(t1, t3, 0x5410u);
+          X[3][e][h] = __byte_perm(t1, t3, 0x7632u);
         }
+      const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
 #pragma unroll
-        for (int sl = 0; sl < 4; ++sl) {
-          const int t = sl >> 1, pol = sl & 1;
-          const uint32_t re0 = sext_nib4(X[sl][0] & 0x0F0F0F0Fu);
-          const uint32_t re1 = sext_nib4(X[sl][1] & 0x0F0F0F0Fu);
-          const uint32_t im0 = sext_nib4((X[sl][0] >> 4) & 0x0F0F0F0Fu);
-          const uint32_t im1 = sext_nib4((X[sl][1] >> 4) & 0x0F0F0F0Fu);
-          const uint32_t row = (uint32_t)(2 * ant + pol);
-          const uint32_t off = sw128_offset(row, (uint32_t)(pg >> 1)) + 8u * (pg & 1);
-          const uint32_t tR = stage + (uint32_t)t * kFreqBytes;
-          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(tR + off), "r"(re0), "r"(re1)
-                       : "memory");
-          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(tR + kTile + off), "r"(im0),
-                       "r"(im1)
-                       : "memory");
+      for (int t = 0; t < 2; ++t) {
+#pragma unroll
+        for (int sp = 0; sp < 2; ++sp) {
+          const uint32_t pol = (uint32_t)sp ^ flip;
+          uint32_t re[4], im[4], ni[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {   // chunk word k = (e, h) = (k >> 1, k & 1)
+            const uint32_t x0 = X[2 * t][k >> 1][k & 1], x1 = X[2 * t + 1][k >> 1][k & 1];
+            const uint32_t x = pol ? x1 : x0;
+            re[k] = sext_nib4(x & 0x0F0F0F0Fu);
+            im[k] = sext_nib4((x >> 4) & 0x0F0F0F0Fu);
+            ni[k] = neg_bytes(im[k]);
+          }
+          const uint32_t row = (uint32_t)(2 * ant) + pol;
+          const uint32_t tA = stage + (uint32_t)t * kFreqBytes, tB = tA + kTile;
+          const uint32_t o_re = sw128_offset(row, c), o_im = sw128_offset(row, c + 4u);
+          st_shared_v4(tA + o_re, re[0], re[1], re[2], re[3]);
+          st_shared_v4(tA + o_im, im[0], im[1], im[2], im[3]);
+          st_shared_v4(tB + o_re, ni[0], ni[1], ni[2], ni[3]);
+          st_shared_v4(tB + o_im, re[0], re[1], re[2], re[3]);
         }
       }
-      mbar_arrive(&rempty_bar[r]);
       fence_proxy_async_smem();
       mbar_arrive(&full_bar[s]);
     }
@@ -421,11 +436,10 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
                                a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
           break;
         const int npk = min(kPktPerStage, a.npkt - ks * kPktPerStage);
-        mbar_arrive_expect_tx(&rfull_bar[r], (uint32_t)npk * 256u);
-        const uint8_t *src = chan_src + (int64_t)ks * kPktPerStage * 256;
-        const uint32_t dst = raw_base + (uint32_t)r * kRawBytes;
-        for (int p = 0; p < npk; ++p)
-          bulk_g2s(dst + (uint32_t)p * kRawRow, src + (int64_t)p * 256, 256u, &rfull_bar[r]);
+        const uint32_t bytes = (uint32_t)npk * 256u;
+        mbar_arrive_expect_tx(&rfull_bar[r], bytes);
+        bulk_g2s(raw_base + (uint32_t)r * kRawBytes, chan_src + (int64_t)ks * kPktPerStage * 256,
+                 bytes, &rfull_bar[r]);
       }
     }
     __syncwarp();
@@ -441,15 +455,11 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
         const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-          const uint32_t tR = stage + (uint32_t)t * kFreqBytes, tI = tR + kTile;
-          const uint32_t dre = tmem + (uint32_t)t * 256u, dc = dre + 128u;
+          const uint32_t tA = stage + (uint32_t)t * kFreqBytes;
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {   // 4 x K = 32 bytes per 128-byte row
-            const uint64_t dR = umma_desc_sw128(tR + 32u * kk, 1024u);
-            const uint64_t dI = umma_desc_sw128(tI + 32u * kk, 1024u);
-            umma_i8(dre, dR, dR, kIdesc, (ks | kk) != 0);   // Re += R R^T
-            umma_i8(dre, dI, dI, kIdesc, 1u);               // Re += I I^T
-            umma_i8(dc, dI, dR, kIdesc, (ks | kk) != 0);    // C  += I R^T
+            const uint64_t d = umma_desc_sw128(tA + 32u * kk, 1024u);
+            umma_i8(tmem + (uint32_t)t * 256u, d, d, corr::kIdesc, (ks | kk) != 0);
           }
         }
         umma_commit(&empty_bar[s]);
@@ -465,43 +475,25 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
                                 a.wait_limit_ns);
     tc_fence_after();
     ok = __all_sync(0xffffffffu, ok && !abort_sh);
-    const int q = warp & 3, t = warp >> 2;
-    const int m = 32 * q + lane;                   // row = 2 * station + pol
-    const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
-    // C^T through shared memory (operand stage t is free now): row m of C
-    // stored at word (b ^ (m & 31)) of a 512-byte row.
-    uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase + t * kStageBytes);
     if (ok) {
-#pragma unroll
-      for (int cb = 0; cb < 8; ++cb) {
-        uint32_t cv[16];
-        tmem_ld16(trow + 128u + 16u * cb, cv);
-        tmem_wait_ld();
-#pragma unroll
-        for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
-      }
-    }
-    named_bar(1, 256);
-    if (ok) {
+      const int q = warp & 3, t = warp >> 2;
+      const int m = 32 * q + lane;
       const int i = m >> 1, pi = m & 1;
       float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
-      const int64_t tri = (int64_t)i * (i + 1) / 2;
+      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
       const int ncb = 2 * q + 2;
+      const int64_t tri = (int64_t)i * (i + 1) / 2;
       for (int cb = 0; cb < ncb; ++cb) {
-        uint32_t re[16], cr[16];
+        uint32_t re[16], im[16];
         tmem_ld16(trow + 16u * cb, re);
-        tmem_ld16(trow + 128u + 16u * cb, cr);
+        tmem_ld16(trow + 128u + 16u * cb, im);
         tmem_wait_ld();
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
           const int j = 8 * cb + jj;
           if (j <= i) {
-            const int b0 = 2 * j, b1 = 2 * j + 1;
-            const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
-            const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
-            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)((int32_t)cr[2 * jj] - ct0),
-                                   (float)(int32_t)re[2 * jj + 1],
-                                   (float)((int32_t)cr[2 * jj + 1] - ct1));
+            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(int32_t)im[2 * jj],
+                                   (float)(int32_t)re[2 * jj + 1], (float)(int32_t)im[2 * jj + 1]);
             float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
             if (a.accumulate) {
               const float4 old = *dst;

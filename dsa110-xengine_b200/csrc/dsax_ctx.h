@@ -24,6 +24,7 @@ enum {
   AUX_LF_SCRATCH = 11,  // learned flagger: activations, gradients, partials
   AUX_BATCH_SCRATCH = 12,  // batch: corner-turned block, beam filterbank, flag statistics
   AUX_TUNE = 13,           // autotuner: synthetic block + visibilities
+  AUX_LF_TCW = 14,         // learned flagger: BF16 weight images of the tensor-core path
 };
 
 struct DevBuf {

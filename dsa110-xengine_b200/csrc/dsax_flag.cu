@@ -107,20 +107,217 @@ __global__ void __launch_bounds__(flag::kStatThreads) flag_stats_kernel(FlagArgs
   }
 }
 
+// ---------------------------------------------------------------- stats, staged
+// Same statistics as flag_stats_kernel for the common shapes (nchan a
+// multiple of 4, one TBIN-sample bin <= 32 KB): one CTA per beam streams the
+// beam's bins through a 3-stage cp.async ring in shared memory (each bin is
+// one contiguous TB x C x 4-byte run of the [T][C] filterbank), so the HBM
+// reads stay in flight while the previous bin is reduced.  Thread (p, c4)
+// owns channels 4c4..4c4+3 and rows p, p+P, ... of every bin; per-row sums
+// (the time series) and per-bin sums are finished in shared memory in a
+// fixed order, so results do not depend on scheduling.
+namespace flag {
+constexpr int kFastThreads = 256;
+constexpr int kFastStages = 3;
+constexpr int kFastStageMax = 32768;
+}  // namespace flag
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(flag::kFastThreads, 2) flag_stats_staged_kernel(FlagArgs a) {
+  constexpr int S = flag::kFastStages;
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const int T = a.ntime, C = a.nchan, TB = a.tbin;
+  const int C4 = C >> 2, P = flag::kFastThreads / C4;
+  const int p = tid / C4, c4 = tid - p * C4;
+  const bool active = p < P;
+  const int nbins = T / TB;
+  const int stage_f4 = TB * C4;                     // float4 per bin
+  const int stage_bytes = (stage_f4 * 16 + 127) & ~127;
+  const float4 *xb = reinterpret_cast<const float4 *>(a.x + (int64_t)b * T * C);
+
+  extern __shared__ __align__(16) uint8_t fs_raw[];
+  const uint32_t sbase = smem_u32(fs_raw);
+  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * stage_bytes);   // [TB][C4]
+  double *sm_bp = sm_rs + TB * C4;                                         // [P][C]
+
+  auto issue = [&](int bin) {
+    if (bin < nbins) {
+      const float4 *src = xb + (int64_t)bin * stage_f4;
+      const uint32_t dst = sbase + (uint32_t)(bin % S) * stage_bytes;
+      for (int i = tid; i < stage_f4; i += flag::kFastThreads) cp_async16(dst + 16u * i, src + i);
+    }
+    cp_async_commit();
+  };
+
+  double s[4], q[4];
+  float m[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) { s[j] = 0.0; q[j] = 0.0; m[j] = -INFINITY; }
+  double bmax = -1e300, bmin = 1e300;   // owned by thread tid < C (channel tid)
+
+#pragma unroll
+  for (int i = 0; i < S - 1; ++i) issue(i);
+  for (int bin = 0; bin < nbins; ++bin) {
+    issue(bin + S - 1);
+    cp_async_wait<S - 1>();
+    __syncthreads();
+    if (active) {
+      const float4 *st = reinterpret_cast<const float4 *>(fs_raw + (bin % S) * stage_bytes);
+      double bs[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int t = p; t < TB; t += P) {
+        const float4 v4 = st[t * C4 + c4];
+        const float v[4] = {v4.x, v4.y, v4.z, v4.w};
+        double r = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          bs[j] += v[j];
+          q[j] += (double)v[j] * v[j];
+          m[j] = fmaxf(m[j], v[j]);
+          r += v[j];
+        }
+        sm_rs[t * C4 + c4] = r;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        s[j] += bs[j];
+        sm_bp[p * C + 4 * c4 + j] = bs[j];
+      }
+    }
+    if (a.pix_sum) {   // downsampled spectrogram: tbin / tds whole pixel rows per bin
+      const float *sf = reinterpret_cast<const float *>(fs_raw + (bin % S) * stage_bytes);
+      const int npr = TB / a.tds, H = T / a.tds;
+      for (int i = tid; i < npr * C; i += flag::kFastThreads) {
+        const int pr = i / C, c = i - pr * C;
+        float sum = 0.f, mx = -INFINITY;
+        for (int r = 0; r < a.tds; ++r) {
+          const float v = sf[(pr * a.tds + r) * C + c];
+          sum += v;
+          mx = fmaxf(mx, v);
+        }
+        const int64_t o = ((int64_t)b * H + bin * npr + pr) * C + c;
+        a.pix_sum[o] = sum;
+        a.pix_max[o] = mx;
+      }
+    }
+    __syncthreads();
+    if (tid < TB) {
+      double r = 0.0;
+      for (int k = 0; k < C4; ++k) r += sm_rs[tid * C4 + k];
+      a.ts[(int64_t)b * T + (int64_t)bin * TB + tid] = (float)(r / C);
+    }
+    if (tid < C) {
+      double bsum = 0.0;
+      for (int k = 0; k < P; ++k) bsum += sm_bp[k * C + tid];
+      const double mb = bsum / TB;
+      bmax = fmax(bmax, mb);
+      bmin = fmin(bmin, mb);
+    }
+  }
+  cp_async_wait<0>();
+  // rows beyond the last whole bin (T % TB): sums, squares, max and the
+  // time series, read directly
+  for (int t0 = nbins * TB; t0 < T; t0 += TB) {
+    __syncthreads();
+    const int rows = min(TB, T - t0);
+    if (active) {
+      for (int t = p; t < rows; t += P) {
+        const float4 v4 = __ldg(xb + (int64_t)(t0 + t) * C4 + c4);
+        const float v[4] = {v4.x, v4.y, v4.z, v4.w};
+        double r = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          s[j] += v[j];
+          q[j] += (double)v[j] * v[j];
+          m[j] = fmaxf(m[j], v[j]);
+          r += v[j];
+        }
+        sm_rs[t * C4 + c4] = r;
+      }
+    }
+    __syncthreads();
+    if (tid < rows) {
+      double r = 0.0;
+      for (int k = 0; k < C4; ++k) r += sm_rs[tid * C4 + k];
+      a.ts[(int64_t)b * T + t0 + tid] = (float)(r / C);
+    }
+  }
+  // per-channel totals over the P row phases, in phase order
+  double tot[3] = {0.0, 0.0, -INFINITY};
+#pragma unroll
+  for (int pass = 0; pass < 3; ++pass) {
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        sm_bp[p * C + 4 * c4 + j] = pass == 0 ? s[j] : pass == 1 ? q[j] : (double)m[j];
+    }
+    __syncthreads();
+    if (tid < C) {
+      for (int k = 0; k < P; ++k) {
+        const double v = sm_bp[k * C + tid];
+        tot[pass] = pass < 2 ? tot[pass] + v : fmax(tot[pass], v);
+      }
+    }
+  }
+  if (tid < C) {
+    const double mean = tot[0] / T;
+    const double var = fmax(tot[1] / T - mean * mean, 0.0);
+    const int o = b * C + tid;
+    a.spec[o] = (float)mean;
+    a.var[o] = (float)var;
+    a.maxs[o] = a.parity ? (float)mean : (float)tot[2];
+    a.pp[o] = nbins > 0 ? (float)(bmax - bmin) : 0.0f;
+  }
+}
+
+bool flag_stats_staged_ok(const FlagArgs &a) {
+  const bool pix_ok = !a.pix_sum || (a.tds > 0 && a.tbin % a.tds == 0 && a.ntime % a.tbin == 0);
+  return a.nchan % 4 == 0 && (reinterpret_cast<uintptr_t>(a.x) & 15u) == 0 &&
+         (int64_t)a.tbin * a.nchan * 4 <= flag::kFastStageMax && a.tbin <= flag::kFastThreads &&
+         pix_ok;
+}
+
+static size_t staged_stats_smem(const FlagArgs &a) {
+  const int C4 = a.nchan / 4, P = flag::kFastThreads / C4;
+  const size_t stage = ((size_t)a.tbin * a.nchan * 4 + 127) & ~(size_t)127;
+  return flag::kFastStages * stage + sizeof(double) * ((size_t)a.tbin * C4 + (size_t)P * a.nchan);
+}
+
 // ---------------------------------------------------------------- decisions
 // Lower median sorted[(n+1)/2 - 1] of v[0..n) in shared memory, by rank
 // counting with ties broken by index (the element a stable sort would put
 // at that position has the same value).  All threads of the block call it.
 __device__ float block_lower_median(const float *v, int n, float *result_slot) {
   const int k = (n + 1) / 2 - 1;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float x = v[i];
+  // gs threads (a power of two <= 32) share one element's count
+  int gs = 1;
+  while (gs < 32 && gs * 2 * n <= (int)blockDim.x) gs *= 2;
+  const int sub = threadIdx.x & (gs - 1);
+  const int per = (n + gs - 1) / gs;
+  const int rounds = (n * gs + blockDim.x - 1) / blockDim.x;   // uniform trip count
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int i = (rd * (int)blockDim.x + (int)threadIdx.x) / gs;
+    const bool live = i < n;
+    const float x = live ? v[i] : 0.0f;
     int r = 0;
-    for (int j = 0; j < n; ++j) {
-      const float y = v[j];
-      r += (y < x) || (y == x && j < i);
+    if (live) {
+      const int j0 = sub * per, j1 = min(n, j0 + per);
+#pragma unroll 8
+      for (int j = j0; j < j1; ++j) {
+        const float y = v[j];
+        r += (y < x) || (y == x && j < i);
+      }
     }
-    if (r == k) *result_slot = x;
+    for (int o = gs >> 1; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (live && sub == 0 && r == k) *result_slot = x;
   }
   __syncthreads();
   const float med = *result_slot;
@@ -128,28 +325,34 @@ __device__ float block_lower_median(const float *v, int n, float *result_slot) {
   return med;
 }
 
+// corr[j - G] = sb[j] - lower median of sb[w0 .. w0 + F), w0 = j, or
+// C - G - F for the last windows (channflag's forward detrend), for j in
+// [G, C - G); one thread per (channel, window element) rank count.
+__device__ void window_detrend(const float *sb, const FlagArgs &a, float *corr) {
+  const int C = a.nchan, G = a.guard, F = a.filt, n = C - 2 * G;
+  const int k = (F + 1) / 2 - 1;
+  for (int idx = threadIdx.x; idx < n * F; idx += blockDim.x) {
+    const int jj = idx / F, i = idx - jj * F;
+    const int j = G + jj;
+    const int w0 = (C - G - j >= F) ? j : C - G - F;
+    const float x = sb[w0 + i];
+    int r = 0;
+    for (int q = 0; q < F; ++q) {
+      const float y = sb[w0 + q];
+      r += (y < x) || (y == x && q < i);
+    }
+    if (r == k) corr[jj] = sb[j] - x;
+  }
+  __syncthreads();
+}
+
 // channflag() on one statistic of one beam: forward median detrend over
 // `filt` channels (the last windows clamped at C-G-filt), median and MAD
 // over the guard-banded channels, flag |x| > thr*MAD.
 __device__ void channflag_dev(const float *sb, float thr, const FlagArgs &a, uint8_t *mask,
                               float *corr, float *tmp, float *slot) {
-  const int C = a.nchan, G = a.guard, F = a.filt, n = C - 2 * G;
-  for (int j = G + threadIdx.x; j < C - G; j += blockDim.x) {
-    const int w0 = (C - G - j >= F) ? j : C - G - F;
-    const int k = (F + 1) / 2 - 1;
-    float med = 0.0f;
-    for (int i = 0; i < F; ++i) {   // rank-count median of the window
-      const float x = sb[w0 + i];
-      int r = 0;
-      for (int q = 0; q < F; ++q) {
-        const float y = sb[w0 + q];
-        r += (y < x) || (y == x && q < i);
-      }
-      if (r == k) med = x;
-    }
-    corr[j - G] = sb[j] - med;
-  }
-  __syncthreads();
+  const int C = a.nchan, G = a.guard, n = C - 2 * G;
+  window_detrend(sb, a, corr);
   const float med = block_lower_median(corr, n, slot);
   for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = fabsf(corr[i] - med);
   __syncthreads();
@@ -159,6 +362,167 @@ __device__ void channflag_dev(const float *sb, float thr, const FlagArgs &a, uin
     if (v > thr * mad || v < -thr * mad) mask[G + i] = 1;
   }
   __syncthreads();
+}
+
+// channflag()'s test statistic as a number: corr[j] / (thr * MAD), so the
+// channel is flagged exactly when |z| > 1 (z = +-1e6 when the MAD is 0 and
+// corr is not; 0 in the guard band).  Used as a learned-flagger feature.
+__device__ void channflag_z(const float *sb, float thr, const FlagArgs &a, float *zout,
+                            float *corr, float *tmp, float *slot) {
+  const int C = a.nchan, G = a.guard, n = C - 2 * G;
+  for (int j = threadIdx.x; j < C; j += blockDim.x) zout[j] = 0.0f;
+  window_detrend(sb, a, corr);
+  const float med = block_lower_median(corr, n, slot);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = fabsf(corr[i] - med);
+  __syncthreads();
+  const float mad = block_lower_median(tmp, n, slot);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float v = corr[i];
+    zout[G + i] = mad > 0.0f ? v / (thr * mad) : (v > 0.0f ? 1e6f : (v < 0.0f ? -1e6f : 0.0f));
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ float slogf(float v) { return copysignf(log1pf(fabsf(v)), v); }
+
+// Learned-flagger input features of one beam (one CTA per beam) from the
+// statistics pass: the plain flagger's four channel test statistics and its
+// time-series statistic, each scaled so that the plain rule fires at 1,
+// plus the downsampled spectrogram.  F[b][h][c][8], log-compressed by
+// slog(v) = sign(v) log(1 + |v|):
+//   f0 (pixel mean - mu) / sigma * sqrt(tds)   f1 (pixel max - mu) / sigma
+//   f2 max over the pixel's samples of z_ts    f3 z_spec   f4 z_var
+//   f5 z_max   f6 z_pp   f7 mean over the pixel's samples of z_ts
+// mu, sigma: mean and standard deviation of the beam's samples (from the
+// per-channel mean and variance).
+__global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(FlagArgs a, float *F,
+                                                                            uint16_t *Fbf) {
+  const int b = blockIdx.x;
+  const int C = a.nchan, G = a.guard, T = a.ntime, n = C - 2 * G, tds = a.tds, H = T / tds;
+  extern __shared__ float lsh[];
+  float *spec = lsh;                                   // C
+  float *corr = spec + C;                              // C
+  float *tmp = corr + C;                               // max(C, ts_base)
+  float *z = tmp + (a.ts_base > C ? a.ts_base : C);    // [4][C]
+  float *zt = z + 4 * C;                               // T
+  float *rmax = zt + T;                                // H
+  float *rmean = rmax + H;                             // H
+  __shared__ float slot;
+  __shared__ float mu_sd[2];
+
+  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.spec[b * C + c];
+  __syncthreads();
+  channflag_z(spec, a.thresh, a, z, corr, tmp, &slot);
+  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.var[b * C + c];
+  __syncthreads();
+  channflag_z(spec, a.thresh + a.var_add, a, z + C, corr, tmp, &slot);
+  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.maxs[b * C + c];
+  __syncthreads();
+  channflag_z(spec, a.thresh, a, z + 2 * C, corr, tmp, &slot);
+  // simple_channflag(pp): one-sided, FBIN-channel mean against med + Thr/sqrt(FBIN) MAD
+  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.pp[b * C + c];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) corr[i] = a.pp[b * C + G + i];
+  __syncthreads();
+  {
+    const float med = block_lower_median(corr, n, &slot);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = fabsf(corr[i] - med);
+    __syncthreads();
+    const float mad = block_lower_median(tmp, n, &slot);
+    const float mythr = a.thresh / sqrtf((float)a.fbin);
+    for (int j = threadIdx.x; j < C; j += blockDim.x) {
+      float zz = 0.0f;
+      if (j >= G && j < C - G - a.fbin) {
+        float vv = 0.0f;
+        for (int k = 0; k < a.fbin; ++k) vv += a.parity ? spec[j] : spec[j + k];
+        vv = vv / (float)a.fbin - med;
+        zz = mad > 0.0f ? vv / (mythr * mad) : (vv > 0.0f ? 1e6f : (vv < 0.0f ? -1e6f : 0.0f));
+      }
+      z[3 * C + j] = zz;
+    }
+  }
+  __syncthreads();
+  // simple_tsflag: median and MAD over the first ts_base samples
+  const float *tsb = a.ts + (int64_t)b * T;
+  for (int i = threadIdx.x; i < a.ts_base; i += blockDim.x) tmp[i] = tsb[i];
+  __syncthreads();
+  {
+    const float med = block_lower_median(tmp, a.ts_base, &slot);
+    for (int i = threadIdx.x; i < a.ts_base; i += blockDim.x) tmp[i] = fabsf(tsb[i] - med);
+    __syncthreads();
+    const float mad = block_lower_median(tmp, a.ts_base, &slot);
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+      const float vv = tsb[t] - med;
+      float zz = mad > 0.0f ? vv / (a.ts_thresh * mad) : (vv > 0.0f ? 1e6f : (vv < 0.0f ? -1e6f : 0.0f));
+      zt[t] = a.tsflag ? zz : 0.0f;
+    }
+  }
+  if (threadIdx.x == 0) {
+    double s = 0.0, q = 0.0;
+    for (int c = 0; c < C; ++c) {
+      const double m = a.spec[b * C + c];
+      s += m;
+      q += (double)a.var[b * C + c] + m * m;
+    }
+    const double mu = s / C;
+    mu_sd[0] = (float)mu;
+    mu_sd[1] = (float)sqrt(fmax(q / C - mu * mu, 1e-30));
+  }
+  __syncthreads();
+  for (int h = threadIdx.x; h < H; h += blockDim.x) {
+    float mx = -INFINITY, sm = 0.0f;
+    for (int r = 0; r < tds; ++r) {
+      const float v = zt[h * tds + r];
+      mx = fmaxf(mx, v);
+      sm += v;
+    }
+    rmax[h] = mx;
+    rmean[h] = sm / tds;
+  }
+  __syncthreads();
+  const float mu = mu_sd[0], inv = 1.0f / mu_sd[1], kpix = sqrtf((float)tds);
+  float4 *Fb = F ? reinterpret_cast<float4 *>(F + (int64_t)b * H * C * 8) : nullptr;
+  const float *ps = a.pix_sum + (int64_t)b * H * C;
+  const float *pm = a.pix_max + (int64_t)b * H * C;
+  for (int i = threadIdx.x; i < H * C; i += blockDim.x) {
+    const int h = i / C, c = i - h * C;
+    float4 f, g;
+    f.x = slogf((ps[i] / tds - mu) * inv * kpix);
+    f.y = slogf((pm[i] - mu) * inv);
+    f.z = slogf(rmax[h]);
+    f.w = slogf(z[c]);
+    g.x = slogf(z[C + c]);
+    g.y = slogf(z[2 * C + c]);
+    g.z = slogf(z[3 * C + c]);
+    g.w = slogf(rmean[h]);
+    if (F) {
+      Fb[2 * i] = f;
+      Fb[2 * i + 1] = g;
+    }
+    if (Fbf) {
+      uint4 o;
+      asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.x) : "f"(f.y), "f"(f.x));
+      asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.y) : "f"(f.w), "f"(f.z));
+      asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.z) : "f"(g.y), "f"(g.x));
+      asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.w) : "f"(g.w), "f"(g.z));
+      reinterpret_cast<uint4 *>(Fbf)[(int64_t)b * H * C + i] = o;
+    }
+  }
+}
+
+int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStream_t st) {
+  if (!a.pix_sum || a.tds < 1 || a.ntime % a.tds || a.nchan > flag::kMaxChan) return -1;
+  const int H = a.ntime / a.tds;
+  const size_t sh = sizeof(float) * (2 * a.nchan + (a.ts_base > a.nchan ? a.ts_base : a.nchan) +
+                                     4 * a.nchan + a.ntime + 2 * H);
+  if (sh > 200 * 1024) return -1;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(lf_stat_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    attr = true;
+  }
+  lf_stat_features_kernel<<<a.nbeam, flag::kDecThreads, sh, st>>>(a, F, Fbf);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 __global__ void __launch_bounds__(flag::kDecThreads) flag_decide_kernel(FlagArgs a) {
@@ -240,16 +604,33 @@ __global__ void __launch_bounds__(flag::kDecThreads) flag_decide_kernel(FlagArgs
   }
 }
 
+int launch_flag_stats(const FlagArgs &a, cudaStream_t st) {
+  if (a.nchan > flag::kMaxChan) return -1;
+  if (flag_stats_staged_ok(a)) {
+    static bool attr2 = false;
+    if (!attr2) {
+      const int mx = flag::kFastStages * flag::kFastStageMax + 48 * 1024;
+      cudaFuncSetAttribute(flag_stats_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      attr2 = true;
+    }
+    flag_stats_staged_kernel<<<a.nbeam, flag::kFastThreads, staged_stats_smem(a), st>>>(a);
+  } else {
+    if (a.pix_sum) return -1;
+    static bool attr = false;
+    const size_t ssh = 16 * flag::kMaxChan * (4 * sizeof(double) + sizeof(float));
+    if (!attr) {
+      cudaFuncSetAttribute(flag_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssh);
+      attr = true;
+    }
+    flag_stats_kernel<<<a.nbeam, flag::kStatThreads, ssh, st>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 int launch_flag(const FlagArgs &a, cudaStream_t st) {
   if (a.nchan > flag::kMaxChan || a.ts_base > 4096) return -1;
-  static bool attr = false;
-  const size_t ssh = 16 * flag::kMaxChan * (4 * sizeof(double) + sizeof(float));
-  if (!attr) {
-    cudaFuncSetAttribute(flag_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssh);
-    attr = true;
-  }
-  flag_stats_kernel<<<a.nbeam, flag::kStatThreads, ssh, st>>>(a);
-  if (cudaGetLastError() != cudaSuccess) return -2;
+  const int rc = launch_flag_stats(a, st);
+  if (rc != 0) return rc;
   const int tmpn = a.ts_base > a.nchan ? a.ts_base : a.nchan;
   const size_t sh = sizeof(float) * (2 * a.nchan + tmpn + a.ts_base);
   flag_decide_kernel<<<a.nbeam, flag::kDecThreads, sh, st>>>(a);

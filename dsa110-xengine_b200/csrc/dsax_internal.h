@@ -68,9 +68,21 @@ struct FlagArgs {
   float thresh, var_add, ts_thresh;
   int nperm;
   int perm[8];
+  // optional downsampled spectrogram (staged statistics kernel only; needs
+  // tbin % tds == 0): per (beam, pixel row of tds samples, chan) sum and max
+  float *pix_sum = nullptr, *pix_max = nullptr;
+  int tds = 0;
 };
 
 int launch_flag(const FlagArgs &a, cudaStream_t st);
+// Statistics pass only (spec, var, max, pp, ts and the optional pixel sums);
+// returns -1 when the staged kernel cannot take the shape.
+int launch_flag_stats(const FlagArgs &a, cudaStream_t st);
+bool flag_stats_staged_ok(const FlagArgs &a);
+// Learned-flagger features F[B][T/tds][C][8] from a finished statistics pass
+// (spec, var, maxs, pp, ts, pix_sum, pix_max of `a`).
+// F (FP32, may be null) and / or Fbf (BF16, may be null).
+int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStream_t st);
 
 }  // namespace dsax
 

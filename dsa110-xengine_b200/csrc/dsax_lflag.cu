@@ -5,8 +5,8 @@
 // of src/gpu_flagger.cu, which stay the label source, judge and fallback.
 //
 // Kernels (NHWC activations, FP32):
-//   lf_features_kernel : x[B][T][C] -> F[B][H = T/tds][C][8]; one HBM pass
-//                        per beam (the features are listed at the kernel)
+//   (features: the plain flagger's staged statistics pass plus
+//    lf_stat_features_kernel, both in dsax_flag.cu)
 //   lf_labels_kernel   : plain-flagger masks -> pixel labels on the H x C grid
 //   conv3x3_kernel     : out = conv(in, w) + b (+ReLU); with flipped and
 //                        transposed weights it is also the data gradient,
@@ -25,117 +25,6 @@
 namespace dsax {
 
 __device__ __forceinline__ float slog(float v) { return copysignf(log1pf(fabsf(v)), v); }
-
-// ---------------------------------------------------------------- features
-// One CTA (512 threads) per beam; warp w owns pixel rows h = w, w+16, ...;
-// lane l owns channels l and l+32.  Needs C <= 64, T % tds == 0.
-// Eight features per pixel (z-scores against the beam's mean mu and
-// standard deviation sigma, log-compressed by slog):
-//   f0 pixel mean, f1 pixel max, f2 row channel-mean, f3 column mean,
-//   f4 max over the pixel's samples of the channel-mean time series,
-//   f5 column max, f6 column variance ratio, f7 column peak-to-peak of
-//   128-sample means (the statistics the plain flagger thresholds).
-constexpr int kLfTbin = 128;
-
-__global__ void __launch_bounds__(512) lf_features_kernel(const float *__restrict__ x, float *F,
-                                                          int T, int C, int tds) {
-  extern __shared__ float fsh[];
-  const int H = T / tds;
-  float *psum = fsh;               // [H][C] pixel sums
-  float *pmax = psum + H * C;      // [H][C] pixel maxima
-  float *rsum = pmax + H * C;      // [H] row sums
-  float *tsmx = rsum + H;          // [H] max of the channel-mean series in the pixel
-  __shared__ double red[2][16];
-  __shared__ float csq[16][64];
-  __shared__ float colmean[64], colmax[64], colvar[64], colpp[64];
-  const int b = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const float *xb = x + (int64_t)b * T * C;
-  const int c0 = lane, c1 = lane + 32;
-  const bool h0 = c0 < C, h1 = c1 < C;
-  double s = 0.0, q = 0.0;
-  float q0 = 0.f, q1 = 0.f;
-  for (int h = warp; h < H; h += 16) {
-    float a0 = 0.f, a1 = 0.f, m0 = -INFINITY, m1 = -INFINITY, tm = -INFINITY;
-    for (int t = h * tds; t < (h + 1) * tds; ++t) {
-      const float v0 = h0 ? __ldg(xb + (int64_t)t * C + c0) : 0.f;
-      const float v1 = h1 ? __ldg(xb + (int64_t)t * C + c1) : 0.f;
-      a0 += v0; a1 += v1;
-      q0 = fmaf(v0, v0, q0); q1 = fmaf(v1, v1, q1);
-      q += (double)v0 * v0 + (double)v1 * v1;
-      if (h0) m0 = fmaxf(m0, v0);
-      if (h1) m1 = fmaxf(m1, v1);
-      float r = v0 + v1;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-      tm = fmaxf(tm, r);
-    }
-    s += (double)a0 + (double)a1;
-    if (h0) { psum[h * C + c0] = a0; pmax[h * C + c0] = m0; }
-    if (h1) { psum[h * C + c1] = a1; pmax[h * C + c1] = m1; }
-    float r = a0 + a1;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-    if (lane == 0) { rsum[h] = r; tsmx[h] = tm / C; }
-  }
-  csq[warp][c0] = q0;
-  csq[warp][c1] = q1;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    s += __shfl_xor_sync(0xffffffffu, s, o);
-    q += __shfl_xor_sync(0xffffffffu, q, o);
-  }
-  if (lane == 0) { red[0][warp] = s; red[1][warp] = q; }
-  __syncthreads();
-  if (threadIdx.x < C) {
-    const int c = threadIdx.x;
-    const int pb = kLfTbin / tds > 0 ? kLfTbin / tds : 1;   // pixels per TBIN bin
-    float cs = 0.f, cx = -INFINITY, bs = 0.f, bmax = -INFINITY, bmin = INFINITY;
-    for (int h = 0; h < H; ++h) {
-      cs += psum[h * C + c];
-      cx = fmaxf(cx, pmax[h * C + c]);
-      bs += psum[h * C + c];
-      if ((h + 1) % pb == 0) {
-        const float mb = bs / (float)(pb * tds);
-        bmax = fmaxf(bmax, mb);
-        bmin = fminf(bmin, mb);
-        bs = 0.f;
-      }
-    }
-    float sq = 0.f;
-    for (int w = 0; w < 16; ++w) sq += csq[w][c];
-    const float mean = cs / (float)T;
-    colmean[c] = mean;
-    colmax[c] = cx;
-    colvar[c] = fmaxf(sq / (float)T - mean * mean, 0.f);
-    colpp[c] = bmax >= bmin ? bmax - bmin : 0.f;
-  }
-  __syncthreads();
-  double S = 0.0, Q = 0.0;
-  for (int w = 0; w < 16; ++w) { S += red[0][w]; Q += red[1][w]; }
-  const double n = (double)T * C;
-  const float mu = (float)(S / n);
-  const float var = (float)fmax(Q / n - (S / n) * (S / n), 1e-30);
-  const float sd = sqrtf(var);
-  const float inv = 1.0f / sd;
-  const float kpix = sqrtf((float)tds), krow = sqrtf((float)tds * C), kcol = sqrtf((float)T);
-  const float kts = sqrtf((float)C), kvar = sqrtf(0.5f * T);
-  const float kpp = sqrtf((float)(kLfTbin > tds ? kLfTbin : tds));
-  float4 *Fb = reinterpret_cast<float4 *>(F + (int64_t)b * H * C * 8);
-  for (int i = threadIdx.x; i < H * C; i += blockDim.x) {
-    const int h = i / C, c = i % C;
-    float4 f, g;
-    f.x = slog((psum[i] / tds - mu) * inv * kpix);
-    f.y = slog((pmax[i] - mu) * inv);
-    f.z = slog((rsum[h] / (tds * C) - mu) * inv * krow);
-    f.w = slog((colmean[c] - mu) * inv * kcol);
-    g.x = slog((tsmx[h] - mu) * inv * kts);
-    g.y = slog((colmax[c] - mu) * inv);
-    g.z = slog((colvar[c] / var - 1.f) * kvar);
-    g.w = slog(colpp[c] * inv * kpp);
-    Fb[2 * i] = f;
-    Fb[2 * i + 1] = g;
-  }
-}
 
 // pixel label = chan flag, or (any ts flag in the tds samples and inside the
 // guard band)
@@ -344,12 +233,17 @@ __global__ void lf_adam_kernel(float *p, const float *g, float *m, float *v, int
 }
 
 // sigmoid(z) > 0.5  <=>  z > 0; guard band never flagged.
+// Pixel mask from the logits; the permanently flagged channels of the
+// plain flagger's configuration (inside the guard band) are always set.
 __global__ void lf_mask_kernel(const float *z, uint8_t *mask, int64_t n, int W, int guard,
-                               float thresh_logit) {
+                               float thresh_logit, LfPerm perm) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int c = (int)(i % W);
-    mask[i] = (c >= guard && c < W - guard && z[i] > thresh_logit) ? 1 : 0;
+    const bool inside = c >= guard && c < W - guard;
+    bool pm = false;
+    for (int k = 0; k < perm.n; ++k) pm |= perm.ch[k] == c;
+    mask[i] = (inside && (z[i] > thresh_logit || pm)) ? 1 : 0;
   }
 }
 
@@ -388,19 +282,6 @@ int wgrad_launch(const float *in, const float *dz, const float *gate, int cout, 
 
 }  // namespace
 
-int lf_features(const float *x, float *F, int B, int T, int C, int tds, cudaStream_t st) {
-  const int H = T / tds;
-  const size_t sh = ((size_t)2 * H * C + 2 * H) * sizeof(float);
-  if (sh > 200 * 1024 || C > 64) return -1;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(lf_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    attr = true;
-  }
-  lf_features_kernel<<<B, 512, sh, st>>>(x, F, T, C, tds);
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
-}
 
 int lf_labels(const uint8_t *cm, const uint8_t *tm, uint8_t *L, int B, int T, int C, int tds,
               int guard, cudaStream_t st) {
@@ -475,8 +356,8 @@ int lf_adam(LfNet &net, float lr, cudaStream_t st) {
 }
 
 int lf_mask(const float *z, uint8_t *mask, int64_t n, int W, int guard, float thresh_logit,
-            cudaStream_t st) {
-  lf_mask_kernel<<<1024, 256, 0, st>>>(z, mask, n, W, guard, thresh_logit);
+            const LfPerm &perm, cudaStream_t st) {
+  lf_mask_kernel<<<1024, 256, 0, st>>>(z, mask, n, W, guard, thresh_logit, perm);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

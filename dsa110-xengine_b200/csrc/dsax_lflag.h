@@ -27,7 +27,12 @@ struct LfNet {
   int step = 0;
 };
 
-int lf_features(const float *x, float *F, int B, int T, int C, int tds, cudaStream_t st);
+// Permanently flagged channels of the plain flagger's configuration.
+struct LfPerm {
+  int n = 0;
+  int ch[8] = {};
+};
+
 int lf_labels(const uint8_t *cm, const uint8_t *tm, uint8_t *L, int B, int T, int C, int tds,
               int guard, cudaStream_t st);
 int lf_prepare_weights(const LfNet &net, cudaStream_t st);
@@ -38,7 +43,23 @@ int lf_bce(const float *z, const uint8_t *L, float *dz, double *loss_acc, int B,
            int guard, float pos_weight, float inv_n, cudaStream_t st);
 int lf_adam(LfNet &net, float lr, cudaStream_t st);
 int lf_mask(const float *z, uint8_t *mask, int64_t n, int W, int guard, float thresh_logit,
-            cudaStream_t st);
+            const LfPerm &perm, cudaStream_t st);
 size_t lf_part_floats(int B, int H);   // partial-gradient scratch size
+
+// Tensor-core inference (dsax_lflag_tc.cu).
+struct LfTcBuffers {
+  const uint16_t *feat_bf16 = nullptr;  // [npx][8] BF16 features
+  uint16_t *act1 = nullptr;             // [npx][32] BF16
+  uint16_t *act2 = nullptr;             // [npx][64] BF16
+  float *z9 = nullptr;                  // [9][npx] last-layer tap projections
+  float *logit = nullptr;               // [npx] (may be null)
+  uint8_t *mask = nullptr;              // [npx]
+  const uint8_t *wimg = nullptr;        // weight images of layers 0..2 (lf_tc_wimg_bytes)
+};
+size_t lf_tc_wimg_bytes();
+int lf_tc_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st);
+int lf_tc_forward(const LfNet &net, const LfTcBuffers &bufs, int B, int H, int W, int guard,
+                  const LfPerm &perm, int num_sms, int *err, uint64_t wait_limit_ns,
+                  cudaStream_t st);
 
 }  // namespace dsax

@@ -57,24 +57,34 @@ int ensure_net(dsax_ctx *c) {
 }
 
 int check_lf_shape(dsax_ctx *c, const dsax_flag_params *p, int tds) {
-  if (!p || tds < 1 || p->ntime % tds || p->nchan % 4 || p->nchan > 64 ||
-      ((size_t)2 * (p->ntime / tds) * p->nchan + 2 * (p->ntime / tds)) * 4 > 190 * 1024)
+  if (!p) return DSAX_ERR_ARG;
+  const int B = p->nbeam, T = p->ntime, C = p->nchan;
+  if (B < 1 || T < 1 || C < 1 || p->guard < 0 || C - 2 * p->guard < 1 || p->filt < 1 ||
+      p->filt > C - 2 * p->guard || p->tbin < 1 || p->fbin < 1 || p->ts_base < 1 ||
+      p->ts_base > T || p->ts_base > 4096 || p->nperm < 0 || p->nperm > 8)
+    return set_error(c, DSAX_ERR_ARG, "flag parameters out of range");
+  if (tds < 1 || T % tds || C % 4 || C > 64 || p->tbin % tds || T % p->tbin ||
+      p->tbin > 256 || (size_t)p->tbin * C * 4 > 32768 ||
+      sizeof(float) * ((size_t)6 * C + p->ts_base + T + 2 * (T / tds)) > 200 * 1024)
     return set_error(c, DSAX_ERR_ARG,
-                     "learned flagger needs ntime %% tds == 0, nchan %% 4 == 0, nchan <= 64");
+                     "learned flagger needs ntime %% tbin == 0, tbin %% tds == 0, nchan %% 4 == 0, "
+                     "nchan <= 64, tbin * nchan <= 8192");
   return DSAX_OK;
 }
 
-// Scratch for B beams on an H x W grid.
+// Scratch for B beams on an H x W grid (T samples per beam).
 struct LfScratch {
   float *F, *a1, *a2, *a3, *z, *d4, *da, *db, *part;
+  float *stats, *pix;   // statistics pass: spec, var, max, pp [B][W]; ts [B][T]; pixel sum, max
   uint8_t *L;
   double *loss;
 };
 
-int lf_scratch(dsax_ctx *c, int B, int H, int W, LfScratch &s) {
+int lf_scratch(dsax_ctx *c, int B, int H, int W, int T, LfScratch &s) {
   const size_t px = (size_t)B * H * W;
-  const size_t nf = px * (8 + 32 + 64 + 64 + 1 + 1 + 64 + 64) + lf_part_floats(B, H);
-  int rc = ensure_buffer(c, c->aux[AUX_LF_SCRATCH], nf * 4 + px + 64, "learned-flagger scratch");
+  const size_t nstat = (size_t)4 * B * W + (size_t)B * T;
+  const size_t nf = px * (8 + 32 + 64 + 64 + 1 + 1 + 64 + 64) + lf_part_floats(B, H) + nstat + 2 * px;
+  int rc = ensure_buffer(c, c->aux[AUX_LF_SCRATCH], nf * 4 + px + 64 + 64, "learned-flagger scratch");
   if (rc != DSAX_OK) return rc;
   float *f = static_cast<float *>(c->aux[AUX_LF_SCRATCH].ptr);
   s.loss = reinterpret_cast<double *>(f);  f += 16;
@@ -87,8 +97,34 @@ int lf_scratch(dsax_ctx *c, int B, int H, int W, LfScratch &s) {
   s.da = f; f += px * 64;
   s.db = f; f += px * 64;
   s.part = f; f += lf_part_floats(B, H);
+  s.stats = f; f += nstat;
+  s.pix = f; f += 2 * px;
   s.L = reinterpret_cast<uint8_t *>(f);
   return DSAX_OK;
+}
+
+// Features of a device filterbank: the statistics pass (the plain flagger's
+// staged kernel, also writing the downsampled spectrogram) then the
+// per-beam feature kernel.
+int lf_make_features(const dsax_flag_params *p, const float *x, int tds, const LfScratch &s,
+                     float *F, uint16_t *Fbf, cudaStream_t st) {
+  const int B = p->nbeam, T = p->ntime, C = p->nchan, H = T / tds;
+  FlagArgs a{};
+  a.x = x;
+  a.nbeam = B; a.ntime = T; a.nchan = C;
+  a.guard = p->guard; a.filt = p->filt; a.tbin = p->tbin; a.fbin = p->fbin;
+  a.ts_base = p->ts_base; a.tsflag = p->tsflag; a.parity = p->parity;
+  a.thresh = p->thresh; a.var_add = p->var_add; a.ts_thresh = p->ts_thresh;
+  const size_t nbc = (size_t)B * C;
+  a.spec = s.stats; a.var = s.stats + nbc; a.maxs = s.stats + 2 * nbc; a.pp = s.stats + 3 * nbc;
+  a.ts = s.stats + 4 * nbc;
+  a.pix_sum = s.pix;
+  a.pix_max = s.pix + (size_t)B * H * C;
+  a.tds = tds;
+  if (!flag_stats_staged_ok(a)) return -1;
+  int rc = launch_flag_stats(a, st);
+  if (rc != 0) return rc;
+  return launch_lf_stat_features(a, F, Fbf, st);
 }
 
 }  // namespace
@@ -140,7 +176,9 @@ int dsax_lf_features(dsax_ctx *c, const float *x, const dsax_flag_params *p, int
   int rc = check_lf_shape(c, p, tds);
   if (rc != DSAX_OK) return rc;
   DeviceGuard g(c->device);
-  if (lf_features(x, F, p->nbeam, p->ntime, p->nchan, tds, c->stream) != 0)
+  LfScratch s;
+  if ((rc = lf_scratch(c, p->nbeam, p->ntime / tds, p->nchan, p->ntime, s)) != DSAX_OK) return rc;
+  if (lf_make_features(p, x, tds, s, F, nullptr, c->stream) != 0)
     return cuda_check(c, cudaGetLastError(), "feature launch");
   return DSAX_OK;
 }
@@ -155,12 +193,12 @@ int dsax_lf_train_step(dsax_ctx *c, const float *x, const uint8_t *chanmask, con
   DeviceGuard g(c->device);
   const int B = p->nbeam, H = p->ntime / tds, W = p->nchan;
   LfScratch s;
-  if ((rc = lf_scratch(c, B, H, W, s)) != DSAX_OK) return rc;
+  if ((rc = lf_scratch(c, B, H, W, p->ntime, s)) != DSAX_OK) return rc;
   LfNet &net = *c->lf;
   float *acts[5] = {s.F, s.a1, s.a2, s.a3, s.z};
   const int nvalid = B * H * (W - 2 * p->guard);
   int e = 0;
-  e |= lf_features(x, s.F, B, p->ntime, W, tds, c->stream);
+  e |= lf_make_features(p, x, tds, s, s.F, nullptr, c->stream);
   e |= lf_labels(chanmask, tsmask, s.L, B, p->ntime, W, tds, p->guard, c->stream);
   e |= lf_prepare_weights(net, c->stream);
   e |= lf_forward(net, acts, B, H, W, c->stream);
@@ -196,7 +234,7 @@ int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, in
   DeviceGuard g(c->device);
   const int B = p->nbeam, H = p->ntime / tds, W = p->nchan;
   LfScratch s;
-  if ((rc = lf_scratch(c, B, H, W, s)) != DSAX_OK) return rc;
+  if ((rc = lf_scratch(c, B, H, W, p->ntime, s)) != DSAX_OK) return rc;
   LfNet &net = *c->lf;
   const float *xd = x;
   const size_t px = (size_t)B * H * W;
@@ -207,13 +245,28 @@ int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, in
     if (ce != cudaSuccess) return cuda_check(c, ce, "H2D filterbank");
     xd = static_cast<const float *>(c->aux[AUX_FLAG_X].ptr);
   }
-  float *acts[5] = {s.F, s.a1, s.a2, s.a3, s.z};
+  // Inference on the tensor cores: BF16 features and activations in the
+  // FP32 training buffers' space, FP32 accumulation.
+  if ((rc = ensure_buffer(c, c->aux[AUX_LF_TCW], lf_tc_wimg_bytes(), "learned-flagger weight images")) !=
+      DSAX_OK)
+    return rc;
+  LfTcBuffers tb;
+  uint16_t *fbf = reinterpret_cast<uint16_t *>(s.F);
+  tb.feat_bf16 = fbf;
+  tb.act1 = reinterpret_cast<uint16_t *>(s.a1);
+  tb.act2 = reinterpret_cast<uint16_t *>(s.a2);
+  tb.z9 = s.a3;
+  tb.logit = s.z;
+  tb.mask = mem == DSAX_MEM_DEVICE ? mask : s.L;
+  tb.wimg = static_cast<const uint8_t *>(c->aux[AUX_LF_TCW].ptr);
+  LfPerm perm;
+  perm.n = p->nperm;
+  for (int k = 0; k < p->nperm; ++k) perm.ch[k] = p->perm[k];
   int e = 0;
-  e |= lf_features(xd, s.F, B, p->ntime, W, tds, c->stream);
-  e |= lf_prepare_weights(net, c->stream);
-  e |= lf_forward(net, acts, B, H, W, c->stream);
-  uint8_t *dmask = mem == DSAX_MEM_DEVICE ? mask : s.L;
-  e |= lf_mask(s.z, dmask, (int64_t)px, W, p->guard, 0.0f, c->stream);
+  e |= lf_make_features(p, xd, tds, s, nullptr, fbf, c->stream);
+  e |= lf_tc_prepare(net, static_cast<uint8_t *>(c->aux[AUX_LF_TCW].ptr), c->stream);
+  e |= lf_tc_forward(net, tb, B, H, W, p->guard, perm, c->num_sms, c->d_err, c->cfg.wait_limit_ns,
+                     c->stream);
   if (e) return cuda_check(c, cudaGetLastError(), "learned flagger launch");
   if (mem == DSAX_MEM_DEVICE) {
     if (logits)

@@ -249,32 +249,18 @@ __device__ __forceinline__ void named_bar(uint32_t id, uint32_t nthreads) {
 
 // 8 packed 4-bit two's-complement values (nibble 2i = real, 2i+1 = imag of
 // element i) -> four words, word i = bf16(real_i) | bf16(imag_i) << 16.
-// Branch-free: |v| indexes byte tables of the bf16 low/high bytes with
-// PRMT; the sign and the single 3-bit-overflowing magnitude (|-8| = 8) are
-// patched into the high byte.
+// v + 8 (= nibble ^ 8, 0..15) placed in the mantissa of bf16(128) gives
+// bf16(136 + v) exactly; one packed bf16 subtraction of 136 leaves v.
 __device__ __forceinline__ void nib8_to_bf16x8(uint32_t x, uint32_t (&o)[4]) {
-  const uint32_t S = x & 0x88888888u;            // sign bit of each nibble
-  const uint32_t M = (S >> 3) * 0xFu;            // 0xF in negative nibbles
-  const uint32_t mag = (x ^ M) + (S >> 3);       // |v| per nibble, 0..8, no carries
-  const uint32_t idx = mag & 0x77777777u;
-  // bf16(|v|), |v| = 0..7: low bytes 00 80 00 40 80 A0 C0 E0, high 00 3F 40 40 40 40 40 40
-  const uint32_t TL0 = 0x40008000u, TL1 = 0xE0C0A080u;
-  const uint32_t TH0 = 0x40403F00u, TH1 = 0x40404040u;
-  const uint32_t L03 = __byte_perm(TL0, TL1, idx & 0xFFFFu);
-  const uint32_t L47 = __byte_perm(TL0, TL1, idx >> 16);
-  uint32_t H03 = __byte_perm(TH0, TH1, idx & 0xFFFFu);
-  uint32_t H47 = __byte_perm(TH0, TH1, idx >> 16);
-  // nibble bit 3 (bit 4i+3) -> byte bit 7 (bit 8i+7), nibbles 0..3
-  auto spread = [](uint32_t s) -> uint32_t {
-    return ((s & 0x8u) << 4) | ((s & 0x80u) << 8) | ((s & 0x800u) << 12) | ((s & 0x8000u) << 16);
-  };
-  const uint32_t E = mag & 0x88888888u;          // |v| == 8 (only v = -8)
-  H03 |= spread(S) | ((spread(E) >> 7) * 0x41u);
-  H47 |= spread(S >> 16) | ((spread(E >> 16) >> 7) * 0x41u);
-  o[0] = __byte_perm(L03, H03, 0x5140u);
-  o[1] = __byte_perm(L03, H03, 0x7362u);
-  o[2] = __byte_perm(L47, H47, 0x5140u);
-  o[3] = __byte_perm(L47, H47, 0x7362u);
+  const uint32_t xx = x ^ 0x88888888u;
+  const uint32_t lo = xx & 0x0F0F0F0Fu;             // real parts + 8, byte i
+  const uint32_t hi = (xx >> 4) & 0x0F0F0F0Fu;      // imaginary parts + 8, byte i
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t sel = (uint32_t)i | ((uint32_t)i << 4) | ((4u + i) << 8) | ((4u + i) << 12);
+    const uint32_t w = (__byte_perm(lo, hi, sel) & 0x00FF00FFu) | 0x43004300u;
+    asm("sub.rn.bf16x2 %0, %1, %2;" : "=r"(o[i]) : "r"(w), "r"(0x43084308u));
+  }
 }
 
 }  // namespace dsax

@@ -81,35 +81,49 @@ __global__ void __launch_bounds__(reorder_cm::kThreads) reorder_cm_kernel(
   const int p0 = blockIdx.y * kPkt;
   const int nc = min(kChan, nchan - c0);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // load: lanes cover 8 x 16 B (32 channels) of 4 antenna rows
-  for (int r = warp; r < kPkt * 16; r += kThreads / 32) {   // 4 pkts x 16 groups of 4 ants
+  // load: lanes cover 8 x 16 B (32 channels) of 4 antenna rows; each warp
+  // issues all of its rows' loads before the shared-memory stores, so eight
+  // 16-byte loads per thread are in flight
+  constexpr int kRows = kPkt * 16 / (kThreads / 32);   // rows per warp
+  uint4 v[kRows];
+#pragma unroll
+  for (int i = 0; i < kRows; ++i) {
+    const int r = warp + i * (kThreads / 32);           // 4 pkts x 16 groups of 4 ants
     const int pq = r >> 4;
     const int a = 4 * (r & 15) + (lane >> 3);
     const int cq = lane & 7;
     const int p = p0 + pq;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    v[i] = make_uint4(0u, 0u, 0u, 0u);
     if (p < npkt && a < nant_in && 4 * cq < nc) {
       const uint8_t *src = in + (((int64_t)p * nant_in + a) * nchan + c0 + 4 * cq) * 4;
       if (4 * cq + 4 <= nc && ((nchan & 3) == 0)) {
-        v = __ldg(reinterpret_cast<const uint4 *>(src));
+        v[i] = __ldg(reinterpret_cast<const uint4 *>(src));
       } else {
         const uint32_t *s32 = reinterpret_cast<const uint32_t *>(src);
-        v.x = s32[0];
-        v.y = 4 * cq + 1 < nc ? s32[1] : 0u;
-        v.z = 4 * cq + 2 < nc ? s32[2] : 0u;
-        v.w = 4 * cq + 3 < nc ? s32[3] : 0u;
+        v[i].x = s32[0];
+        v[i].y = 4 * cq + 1 < nc ? s32[1] : 0u;
+        v[i].z = 4 * cq + 2 < nc ? s32[2] : 0u;
+        v[i].w = 4 * cq + 3 < nc ? s32[3] : 0u;
       }
     }
+  }
+#pragma unroll
+  for (int i = 0; i < kRows; ++i) {
+    const int r = warp + i * (kThreads / 32);
+    const int pq = r >> 4;
+    const int a = 4 * (r & 15) + (lane >> 3);
+    const int cq = lane & 7;
     uint32_t *w = W + (pq * kChan + 4 * cq) * kAStride + a;
-    w[0] = v.x;
-    w[kAStride] = v.y;
-    w[2 * kAStride] = v.z;
-    w[3 * kAStride] = v.w;
+    w[0] = v[i].x;
+    w[kAStride] = v[i].y;
+    w[2 * kAStride] = v[i].z;
+    w[3 * kAStride] = v[i].w;
   }
   __syncthreads();
   // store: per channel, kPkt x 256 B contiguous; a warp writes one channel
   for (int c = warp; c < nc; c += kThreads / 32) {
     uint8_t *dst = out + ((int64_t)(c0 + c) * npkt + p0) * 256;
+#pragma unroll
     for (int k = lane; k < kPkt * 16; k += 32) {   // 16-byte chunks
       const int pq = k >> 4, a = 4 * (k & 15);
       if (p0 + pq >= npkt) continue;

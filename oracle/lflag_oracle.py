@@ -10,6 +10,9 @@ the label rule below restates how that flagger's masks are applied
 replaces (beam, time) rows inside the guard band).
 
 Layouts (NHWC): features [B][H=T/tds][W=C][8]; weights [Cout][3][3][Cin].
+The features restate lf_stat_features_kernel: the plain flagger's own test
+statistics (scaled so that its rule fires at 1) and the downsampled
+spectrogram, from one statistics pass.
 """
 from __future__ import annotations
 
@@ -38,47 +41,122 @@ def _slog(v):
     return np.sign(v) * np.log1p(np.abs(v))
 
 
-def features(x: np.ndarray, tds: int = 32) -> np.ndarray:
-    """x [B][T][C] -> [B][T/tds][C][8], slog(v) = sign(v) log(1 + |v|) of
-    z-scores against the beam mean mu and standard deviation sigma:
-    f0 pixel mean (x sqrt(tds)), f1 pixel max, f2 row channel-mean
-    (x sqrt(tds C)), f3 column mean (x sqrt(T)), f4 max over the pixel's
-    samples of the channel-mean series (x sqrt(C)), f5 column max,
-    f6 (column variance / sigma^2 - 1) x sqrt(T/2), f7 column peak-to-peak
-    of TBIN-sample means / sigma x sqrt(TBIN)."""
+def _lower_median(v):
+    """sorted(v)[(n+1)/2 - 1] (src/gpu_flagger.cu medval :534-560)."""
+    s = np.sort(np.asarray(v, np.float32), kind="stable")
+    return s[(len(s) + 1) // 2 - 1]
+
+
+def _ratio(num, den):
+    """num / den in float32, +-1e6 (0 for num == 0) where den == 0."""
+    num = np.float32(num)
+    if den > 0:
+        return np.float32(num / np.float32(den))
+    return np.float32(1e6) * np.float32(np.sign(num))
+
+
+def flag_stats(x, tbin):
+    """Per-(beam, chan) mean, variance, max and peak-to-peak of tbin-sample
+    bin means, and the per-(beam, t) channel mean (src/gpu_flagger.cu
+    calc_spectrum :175-223, calc_varspec :229-278, calc_maxspec :283-319,
+    calc_ppspec :324-376, make_ts :414-453), accumulated in float64 and
+    stored float32."""
+    B, T, C = x.shape
+    xd = x.astype(np.float64)
+    spec = xd.mean(axis=1)
+    var = np.maximum((xd * xd).mean(axis=1) - spec * spec, 0.0)
+    mx = x.max(axis=1).astype(np.float64)
+    nb = T // tbin
+    if nb > 0:
+        bm = xd[:, :nb * tbin].reshape(B, nb, tbin, C).sum(axis=2) / tbin
+        pp = bm.max(axis=1) - bm.min(axis=1)
+    else:
+        pp = np.zeros((B, C))
+    ts = xd.mean(axis=2)
+    f = np.float32
+    return spec.astype(f), var.astype(f), mx.astype(f), pp.astype(f), ts.astype(f)
+
+
+def test_statistics(x, p):
+    """The plain flagger's test statistics scaled so that its rule fires at
+    1 (src/gpu_flagger.cu:1340-1398): z[k][b][c] for channflag on the mean
+    (Thr), variance (Thr + 0.5) and max (Thr): corr / (thr * MAD) after the
+    forward filt-channel median detrend (:655-720; flag when |z| > 1, 0 in
+    the guard band); simple_channflag on pp (:562-610): (mean of the next
+    fbin pp values - median) / (Thr / sqrt(fbin) * MAD) (flag when z > 1);
+    and simple_tsflag (:612-653): zt[b][t] = (ts - median) / (TsThr * MAD)
+    over the first ts_base samples (flag when zt > 1; 0 when tsflag is off)."""
+    B, T, C = x.shape
+    G, F, FB = p.guard, p.filt, p.fbin
+    spec, var, mx, pp, ts = flag_stats(x, p.tbin)
+    if p.parity:
+        mx = spec
+    n = C - 2 * G
+    z = np.zeros((4, B, C), np.float32)
+    thrs = [p.thresh, p.thresh + p.var_add, p.thresh]
+    for k, S in enumerate([spec, var, mx]):
+        thr = np.float32(thrs[k])
+        for b in range(B):
+            sb = S[b]
+            corr = np.zeros(n, np.float32)
+            for j in range(G, C - G):
+                w0 = j if C - G - j >= F else C - G - F
+                corr[j - G] = sb[j] - _lower_median(sb[w0:w0 + F])
+            med = _lower_median(corr)
+            mad = _lower_median(np.abs(corr - med))
+            for i in range(n):
+                z[k, b, G + i] = _ratio(corr[i], thr * mad)
+    mythr = np.float32(p.thresh) / np.sqrt(np.float32(FB))
+    for b in range(B):
+        sb = pp[b]
+        med = _lower_median(sb[G:C - G])
+        mad = _lower_median(np.abs(sb[G:C - G] - med))
+        for j in range(G, C - G - FB):
+            vv = np.float32(0.0)
+            for k in range(FB):
+                vv = np.float32(vv + (sb[j] if p.parity else sb[j + k]))
+            vv = np.float32(vv / np.float32(FB)) - med
+            z[3, b, j] = _ratio(vv, mythr * mad)
+    zt = np.zeros((B, T), np.float32)
+    if p.tsflag:
+        for b in range(B):
+            med = _lower_median(ts[b, :p.ts_base])
+            mad = _lower_median(np.abs(ts[b, :p.ts_base] - med))
+            den = np.float32(p.ts_thresh) * mad
+            vv = (ts[b] - med).astype(np.float32)
+            zt[b] = (vv / den if den > 0 else np.float32(1e6) * np.sign(vv)).astype(np.float32)
+    return z, zt, spec, var
+
+
+def features(x: np.ndarray, tds: int, p) -> np.ndarray:
+    """x [B][T][C] -> [B][H = T/tds][C][8], slog(v) = sign(v) log(1 + |v|):
+    f0 (pixel mean - mu) / sigma * sqrt(tds), f1 (pixel max - mu) / sigma,
+    f2 max and f7 mean over the pixel's samples of zt, f3..f6 the channel
+    statistics z (mean, variance, max, pp) of test_statistics; mu and sigma
+    are the beam's sample mean and standard deviation, from the per-channel
+    mean and variance.  p: the plain flagger's parameters (guard, filt,
+    tbin, fbin, ts_base, tsflag, parity, thresh, var_add, ts_thresh)."""
     B, T, C = x.shape
     H = T // tds
-    xd = x[:, :H * tds].astype(np.float64)
-    mu = x.reshape(B, -1).astype(np.float64).mean(axis=1)
-    sd = x.reshape(B, -1).astype(np.float64).std(axis=1)
-    blk = xd.reshape(B, H, tds, C)
-    pm = blk.mean(axis=2)
-    px = blk.max(axis=2)
-    rm = pm.mean(axis=2)                          # [B][H]
-    tsmax = blk.mean(axis=3).max(axis=2)          # [B][H]
-    cm = x.astype(np.float64).mean(axis=1)        # [B][C]
-    cmax = x.max(axis=1).astype(np.float64)
-    cvar = x.astype(np.float64).var(axis=1)
-    pb = max(TBIN // tds, 1)
-    nb = H // pb
-    if nb > 0:
-        bm = pm[:, :nb * pb].reshape(B, nb, pb, C).mean(axis=2)
-        cpp = bm.max(axis=1) - bm.min(axis=1)
-    else:
-        cpp = np.zeros((B, C))
+    z, zt, spec, var = test_statistics(x, p)
+    f = np.empty((B, H, C, 8))
+    blk = x[:, :H * tds].reshape(B, H, tds, C)
+    pm = blk.astype(np.float64).sum(axis=2) / tds
+    px = blk.max(axis=2).astype(np.float64)
+    mu = spec.astype(np.float64).mean(axis=1)
+    ex2 = (var.astype(np.float64) + spec.astype(np.float64) ** 2).mean(axis=1)
+    sd = np.sqrt(np.maximum(ex2 - mu * mu, 1e-30))
     m = mu[:, None, None]
     s = sd[:, None, None]
+    ztp = zt[:, :H * tds].reshape(B, H, tds).astype(np.float64)
     ones_c = np.ones((1, 1, C))
     ones_h = np.ones((1, H, 1))
-    f = np.empty((B, H, C, 8))
     f[..., 0] = _slog((pm - m) / s * np.sqrt(tds))
     f[..., 1] = _slog((px - m) / s)
-    f[..., 2] = _slog(((rm - mu[:, None]) / sd[:, None] * np.sqrt(tds * C))[:, :, None] * ones_c)
-    f[..., 3] = _slog(((cm - mu[:, None]) / sd[:, None] * np.sqrt(T))[:, None, :] * ones_h)
-    f[..., 4] = _slog(((tsmax - mu[:, None]) / sd[:, None] * np.sqrt(C))[:, :, None] * ones_c)
-    f[..., 5] = _slog(((cmax - mu[:, None]) / sd[:, None])[:, None, :] * ones_h)
-    f[..., 6] = _slog(((cvar / (sd[:, None] ** 2) - 1.0) * np.sqrt(0.5 * T))[:, None, :] * ones_h)
-    f[..., 7] = _slog((cpp / sd[:, None] * np.sqrt(max(TBIN, tds)))[:, None, :] * ones_h)
+    f[..., 2] = _slog(ztp.max(axis=2)[:, :, None] * ones_c)
+    for k in range(4):
+        f[..., 3 + k] = _slog(z[k].astype(np.float64)[:, None, :] * ones_h)
+    f[..., 7] = _slog(ztp.mean(axis=2)[:, :, None] * ones_c)
     return f
 
 
@@ -129,6 +207,29 @@ def forward(params, f):
         h = np.maximum(z, 0.0) if li < len(params) - 1 else z
         acts.append(h)
     return acts  # acts[-1] = logits [B][H][W][1]
+
+
+def to_bf16(v):
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    u = np.asarray(v, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward_bf16(params, f):
+    """The tensor-core inference path: BF16 features, weights of layers 1-3
+    and activations of layers 1-2 (round to nearest even), wide
+    accumulation, layer-3 activations and the last layer in FP32.
+    Returns logits [B][H][W]."""
+    h = to_bf16(f)
+    for li in range(3):
+        w, b = params[li]
+        z = conv3x3(h, to_bf16(w), b)
+        h = np.maximum(z, 0.0)
+        if li < 2:
+            h = to_bf16(h)
+    w, b = params[3]
+    return conv3x3(h, w, b)[..., 0]
 
 
 def bce_loss_grad(logits, y, valid, pos_weight: float):

@@ -38,6 +38,29 @@ def test_oracle_gradients_finite_difference():
         assert abs((lp - lm) / (2 * eps) - gb[0]) < 1e-5 * max(1.0, abs(gb[0]))
 
 
+def test_oracle_features_encode_plain_rule(oracle):
+    """The channel and time features are the plain flagger's own test
+    statistics: thresholding them at 1 (slog: log 2) reproduces the C
+    oracle's masks exactly, so a net can reach F1 = 1 from them."""
+    from types import SimpleNamespace
+    B, T, C, tds = 12, 4096, 48, 32
+    x, _ = oracle.gen_filterbank(1000, nbeam=B)
+    po = oracle.flag_params(B, T, C, guard=6, filt=21, tbin=128, fbin=8, ts_base=T // 16,
+                            tsflag=1, parity=0, thresh=5.0, var_add=0.5, ts_thresh=10.0, perm=[])
+    p = SimpleNamespace(guard=6, filt=21, tbin=128, fbin=8, ts_base=T // 16, tsflag=1, parity=0,
+                        thresh=5.0, var_add=0.5, ts_thresh=10.0)
+    cm, tm, _, _, _ = oracle.plain_flag(x, po, None)
+    f = LO.features(x, tds, p)
+    y = LO.labels(cm, tm, tds, 6)
+    t = np.log(2.0)
+    pred = ((np.abs(f[..., 3]) > t) | (np.abs(f[..., 4]) > t) | (np.abs(f[..., 5]) > t)
+            | (f[..., 6] > t) | (f[..., 2] > t))
+    pred[..., :6] = False
+    pred[..., C - 6:] = False
+    assert y.sum() > 0
+    assert np.array_equal(pred, y)
+
+
 def test_param_count():
     assert LO.n_params() == 58337
 
@@ -69,8 +92,46 @@ def test_features_match_oracle(dsax, oracle):
         ctx.lf_features(p, xd, F, tds=32)
         ctx.sync()
         got = F.cpu().numpy().reshape(4, 32, 48, 8)
-    want = LO.features(x, 32)
+    want = LO.features(x, 32, p)
     np.testing.assert_allclose(got, want, rtol=2e-4, atol=2e-4)
+
+
+@pytest.mark.gpu
+def test_tensor_core_inference_matches_oracle(dsax, oracle):
+    """dsax_flag_learned (tcgen05 BF16 implicit-GEMM convolutions) against
+    the oracle's restatement of the same arithmetic (BF16 operands, wide
+    accumulation): logits within 5e-3 of their scale, the mask identical
+    away from the decision boundary."""
+    import torch
+    B, T, C, tds = 6, 1024, 48, 32
+    x, _ = oracle.gen_filterbank(21, nbeam=B, ntime=T, nchan=C)
+    p = dsax.flag_params(B, T, C)
+    rng = np.random.default_rng(9)
+    params = LO.init_params(4)
+    for i, (w, b) in enumerate(params):
+        params[i] = (w, rng.normal(scale=0.1, size=b.shape))
+    H = T // tds
+    with dsax.Context(dsax.default_config(npkt=16, nchan=8)) as ctx:
+        ctx.lf_set_params(_flat(params))
+        xd = torch.from_numpy(x).cuda()
+        mask = torch.zeros(B * H * C, dtype=torch.uint8, device="cuda")
+        logit = torch.zeros(B * H * C, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.flag_learned(p, xd, mask, logits=logit, tds=tds)
+        ctx.sync()
+        got = logit.cpu().numpy().reshape(B, H, C)
+        gmask = mask.cpu().numpy().reshape(B, H, C).astype(bool)
+    pw = _unflat(_flat(params))
+    want = LO.forward_bf16(pw, LO.features(x, tds, p))
+    scale = np.abs(want).max()
+    err = np.abs(got - want)
+    assert err.max() < 5e-3 * scale, (err.max(), scale)
+    assert err.mean() < 5e-4 * scale
+    inside = np.zeros(C, bool)
+    inside[p.guard:C - p.guard] = True
+    wmask = (want > 0) & inside
+    sure = np.abs(want) > 1e-2 * scale
+    assert np.array_equal(gmask[sure], wmask[sure])
 
 
 @pytest.mark.gpu
@@ -80,7 +141,7 @@ def test_gradients_match_oracle(dsax, oracle):
     import torch
     B, T, C, tds = 2, 256, 16, 32
     x, _ = oracle.gen_filterbank(12, nbeam=B, ntime=T, nchan=C, n_tones=2, n_bursts=2, n_drift=1)
-    p = dsax.flag_params(B, T, C, guard=2)
+    p = dsax.flag_params(B, T, C, guard=2, filt=9)
     rng = np.random.default_rng(5)
     cm = (rng.random((B, C)) < 0.2).astype(np.uint8)
     tm = (rng.random((B, T)) < 0.02).astype(np.uint8)
@@ -92,7 +153,7 @@ def test_gradients_match_oracle(dsax, oracle):
         loss, g = ctx.lf_train_step(p, torch.from_numpy(x).cuda(), torch.from_numpy(cm).cuda(),
                                     torch.from_numpy(tm).cuda(), tds=tds, pos_weight=2.0,
                                     update=False, want_grads=True)
-    f = LO.features(x, tds)
+    f = LO.features(x, tds, p)
     y = LO.labels(cm, tm, tds, 2)
     valid = np.zeros(y.shape)
     valid[..., 2:C - 2] = 1
@@ -139,8 +200,9 @@ def test_training_reaches_plain_flagger_masks(dsax, oracle):
             inside = np.zeros(C, bool)
             inside[p.guard:C - p.guard] = True
             for k in range(8):
-                for cut in (1.0, 2.0, 3.0, 4.0, 5.0, 6.0):
-                    best_rule = max(best_rule, LO.prf1((F[..., k] > cut) & inside, ref)[2])
+                for cut in np.linspace(0.25, 6.0, 24):
+                    best_rule = max(best_rule, LO.prf1((F[..., k] > cut) & inside, ref)[2],
+                                    LO.prf1((np.abs(F[..., k]) > cut) & inside, ref)[2])
     print("untrained P/R/F1", untrained)
     print("trained   P/R/F1", trained)
     print("best single-feature threshold F1", best_rule)
