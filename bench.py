@@ -235,7 +235,7 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps):
                          "frac_of_sustained": tf / sust, "peak_kind": f"{kind} BF16 dense"}}
 
 
-def bench_flaggers(dsax, synth, dev, steps):
+def bench_flaggers(dsax, synth, dev, steps, train_steps=1000):
     """Config 4: plain vs learned flagger on [256][4096][48] FP32 (chi2(2)+RFI).
     The learned net is trained here first (outside the timed regions)."""
     import torch
@@ -254,7 +254,7 @@ def bench_flaggers(dsax, synth, dev, steps):
                  for k in range(4)]
         ctx.lf_init(11)
         t0 = time.perf_counter()
-        lflag.train(ctx, train, steps=600, beams_per_step=16, tds=tds)
+        lflag.train(ctx, train, steps=train_steps, beams_per_step=16, tds=tds)
         ctx.sync()
         train_s = time.perf_counter() - t0
         mask = torch.zeros(B * (T // tds) * C, dtype=torch.uint8, device=xd.device)
@@ -268,7 +268,8 @@ def bench_flaggers(dsax, synth, dev, steps):
                       "gpu_launches_per_block": 2},
             "learned": {"ms_per_block": learned_ms, "samples_per_s": npx / (learned_ms * 1e-3),
                         "precision": P, "recall": R, "f1": F1, "train_s": train_s,
-                        "train_steps": 600, "params": dsax.lib().dsax_lf_nparams()},
+                        "train_steps": train_steps, "params": dsax.lib().dsax_lf_nparams(),
+                        "gpu_launches_per_block": 9},
             "learned_vs_plain_speed": plain_ms / learned_ms}
 
 
@@ -315,6 +316,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["beamformer", "flagger", "batch"], default=None,
                     help="run one side workload alone (profiling); prints its JSON")
+    ap.add_argument("--lf-train-steps", type=int, default=1000,
+                    help="training steps of the learned flagger before it is timed")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the beamformer / flagger / batch side measurements")
     ap.add_argument("--corr-path", type=int, default=0,
@@ -340,7 +343,7 @@ def main():
             ins = [torch.from_numpy(blk.reshape(-1)).to(f"cuda:{local}")]
             res = bench_beamformer(dsax, synth, local, ins, args.steps)
         elif args.only == "flagger":
-            res = bench_flaggers(dsax, synth, local, args.steps)
+            res = bench_flaggers(dsax, synth, local, args.steps, args.lf_train_steps)
         else:
             res = bench_batch(dsax, synth, local, args.steps)
         print(json.dumps({"only": args.only, **res}), flush=True)
@@ -478,9 +481,10 @@ def main():
             "config": {"workload": "full-size correlator block [2048][63->64][384][2][2] "
                                    "-> xGPU triangular 768x2080x4 complex FP32",
                        "block_bytes": BLOCK_IN, "vis_bytes": VIS_OUT,
-                       "corr_path": ["channel-major corner turn + correlate", "fused",
+                       "corr_path": ["channel-major corner turn + bulk-fed correlate", "fused",
                                      "REORDER-layout corner turn + correlate",
-                                     "channel-major corner turn + correlate"][cfg.corr_path],
+                                     "channel-major corner turn + directly fed correlate",
+                                     "channel-major corner turn + bulk-fed correlate"][cfg.corr_path],
                        "l2": "inputs larger than L2: 3 resident 198 MB blocks rotated",
                        "parallelism": f"blocks independent per GPU x{ws}"},
             "realtime_factor": value / ws * REALTIME_S,
@@ -502,7 +506,8 @@ def main():
             line["cpu_baseline"] = cpu_baseline_sample()
         if not args.no_extras and ws == 1:
             for key, fn in (("beamformer", lambda: bench_beamformer(dsax, synth, dev, ins, 20)),
-                            ("flagger", lambda: bench_flaggers(dsax, synth, dev, 20)),
+                            ("flagger", lambda: bench_flaggers(dsax, synth, dev, 20,
+                                                               args.lf_train_steps)),
                             ("batch", lambda: bench_batch(dsax, synth, dev, 5))):
                 try:
                     line[key] = fn()

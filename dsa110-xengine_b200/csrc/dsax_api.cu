@@ -203,7 +203,7 @@ static int correlate_device(dsax_ctx *c, int fmt, const void *in, float *vis, in
   a.in = static_cast<const uint8_t *>(in);
   if (fmt == DSAX_FMT_CHANMAJOR) {
     a.nant_in = 64;
-    if (launch_correlate_chanmajor(a, c->stream) != 0)
+    if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path != 3) != 0)
       return cuda_check(c, cudaGetLastError(), "correlator launch");
     return DSAX_OK;
   }
@@ -219,13 +219,13 @@ static int correlate_device(dsax_ctx *c, int fmt, const void *in, float *vis, in
       a.in = tmp;
       a.nant_in = 64;
       fmt = DSAX_FMT_REORDERED;
-    } else {                       // channel-major streams + bulk-copy-fed correlator
+    } else {                       // channel-major streams + correlator (3: direct, else bulk-fed)
       if (launch_reorder_chanmajor(a.in, tmp, c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan,
                                    c->stream) != 0)
         return cuda_check(c, cudaGetLastError(), "corner-turn launch");
       a.in = tmp;
       a.nant_in = 64;
-      if (launch_correlate_chanmajor(a, c->stream) != 0)
+      if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path != 3) != 0)
         return cuda_check(c, cudaGetLastError(), "correlator launch");
       return DSAX_OK;
     }

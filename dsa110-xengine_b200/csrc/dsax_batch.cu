@@ -37,7 +37,7 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     a.nant_in = 64;
     a.nchan = nchan;
     a.wait_limit_ns = cf.wait_limit_ns;
-    if (launch_correlate_chanmajor(a, c->stream) != 0) return -2;
+    if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path != 3) != 0) return -2;
   }
   if (d.beams || d.chanmask) {
     BfArgs b{};

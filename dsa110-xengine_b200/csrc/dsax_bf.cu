@@ -27,9 +27,10 @@
 // with cp.async while they build the current one; TMEM holds two
 // 256-column accumulators so the epilogue of stage i overlaps the MMAs of
 // stage i+1.
-//   warps 0-3 : producers (global 4-bit -> BF16 K-major swizzled tiles)
-//   warps 4-7 : epilogue (TMEM -> |.|^2 row sums -> outputs)
-//   warp  8   : weight loader (bulk copy) and single-thread UMMA issuer
+//   warps 0-7 : producers (global 4-bit -> BF16 K-major swizzled tiles)
+//   warps 8-11: epilogue (TMEM -> |.|^2 row sums -> outputs)
+//   warp  12  : TMEM allocation, weight loader (bulk copy), single-thread
+//               UMMA issuer
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -47,10 +48,11 @@ constexpr int kWBytes = 2 /*pol*/ * 2 /*kb*/ * kWTileBytes;  // 64 KB per (g, bt
 constexpr int kDTileBytes = kN * kKBlockBytes;        // 256 rows x 128 B = 32 KB
 constexpr int kStageBytes = 2 /*kb*/ * kDTileBytes;   // 64 KB
 constexpr int kStages = 2;
-constexpr int kRawRowBytes = 128 * 16;                // one 16 B load per producer thread
-constexpr int kRawBytes = 16 * kRawRowBytes;          // 32 KB: one packet group, both pols
+constexpr int kProducers = 256;                       // 8 producer warps
+constexpr int kRawRowBytes = kProducers * 16;         // one 16 B load per producer thread
+constexpr int kRawBytes = 8 * kRawRowBytes;           // 32 KB: one packet group, both pols
 constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
-constexpr int kThreads = 288;
+constexpr int kThreads = kProducers + 128 + 32;       // + 4 epilogue warps + UMMA warp
 constexpr uint32_t kIdesc = umma_idesc(/*F32*/ 1, /*BF16*/ 1, /*BF16*/ 1, 128, kN);
 }  // namespace bf
 
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
 
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full_bar[s], 128);
+      mbar_init(&full_bar[s], kProducers);
       mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -109,7 +111,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
     abort_sh = 0;
     mbar_fence_init();
   }
-  if (warp == 8) {
+  if (warp == 12) {
     tmem_alloc(&tmem_base_sh, 512);
     tmem_relinquish();
   }
@@ -122,29 +124,29 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
     abort_sh = 1;
   }
 
-  if (warp < 4) {
+  if (warp < 8) {
     // ------------------------------------------------------------ producers
-    // Thread (q, j): packet q of the stage, antennas 4j..4j+3 of each K
-    // block.  The 16 B loads of a (g, pg) carry both pols: they are issued
-    // once, one packet group ahead (while the previous group's two pol
-    // stages are built), and reused for the pol-1 stage.
-    const int j = lane & 7;
-    const int q = 4 * warp + (lane >> 3);          // packet within the stage
+    // Thread (kb, q, j): K block kb, packet q of the stage, antennas
+    // 32 kb + 4j .. +3.  The 16 B loads of a (g, pg) carry both pols: they
+    // are issued once, one packet group ahead (while the previous group's
+    // two pol stages are built), and reused for the pol-1 stage.
+    const int j = tid & 7;
+    const int q = (tid >> 3) & 15;                   // packet within the stage
+    const int kb = tid >> 7;
     const int64_t ant_stride = (int64_t)a.nchan * 4;
     const int64_t pkt_stride = (int64_t)a.nant_in * ant_stride;
-    // Each thread stages its own 16 loads of the next packet group in a
-    // private slice of `raw` ([16][128 threads][16 B], conflict free) with
+    // Each thread stages its own 8 loads of the next packet group in a
+    // private slice of `raw` ([8][256 threads][16 B], conflict free) with
     // cp.async (zero fill for the padded antenna), and reads them back into
     // registers when that group starts, which frees the slice for the next
     // group's copies.
     const uint32_t myraw = raw + 16u * (uint32_t)tid;
-    uint4 Ucur[16];
+    uint4 Ucur[8];
     auto stage_group = [&](int r) {
       const int g = r / npg, pg = r % npg;
       const int p = pg * kPktPerStage + q;
 #pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        const int kb = it & 1, h = it >> 1;
+      for (int h = 0; h < 2; ++h) {
 #pragma unroll
         for (int ii = 0; ii < 4; ++ii) {
           const int ant = 32 * kb + 4 * j + ii;
@@ -153,7 +155,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
                                                 16 * h
                                           : 0);
           asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
-                           myraw + (uint32_t)(4 * it + ii) * (kRawRowBytes)),
+                           myraw + (uint32_t)(4 * h + ii) * (kRawRowBytes)),
                        "l"(src), "r"(ok ? 16 : 0)
                        : "memory");
         }
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       if (pol == 0) {
         asm volatile("cp.async.wait_all;" ::: "memory");
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
+        for (int k = 0; k < 8; ++k) {
           asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
                        : "=r"(Ucur[k].x), "=r"(Ucur[k].y), "=r"(Ucur[k].z), "=r"(Ucur[k].w)
                        : "r"(myraw + (uint32_t)k * kRawRowBytes)
@@ -180,13 +182,12 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
                              a.wait_limit_ns))
         break;
       const uint32_t sel = (uint32_t)pol | ((4u + pol) << 4) | ((2u + pol) << 8) | ((6u + pol) << 12);
-      const uint32_t stage = dsm + (uint32_t)s * kStageBytes;
+      const uint32_t tile = dsm + (uint32_t)s * kStageBytes + (uint32_t)kb * kDTileBytes;
 #pragma unroll
-      for (int it = 0; it < 4; ++it) {
-        const int kb = it & 1, h = it >> 1;
+      for (int h = 0; h < 2; ++h) {
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
-          const uint4 *U = Ucur + 4 * it;
+          const uint4 *U = Ucur + 4 * h;
           const uint32_t u0 = w == 0 ? U[0].x : w == 1 ? U[0].y : w == 2 ? U[0].z : U[0].w;
           const uint32_t u1 = w == 0 ? U[1].x : w == 1 ? U[1].y : w == 2 ? U[1].z : U[1].w;
           const uint32_t u2 = w == 0 ? U[2].x : w == 1 ? U[2].y : w == 2 ? U[2].z : U[2].w;
@@ -200,8 +201,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
             nib8_to_bf16x8(x, o);
             const int k = 8 * h + 2 * w + odd;     // chunnel = 2*chan + time
             const uint32_t row = (uint32_t)(16 * q + k);
-            st_shared_v4(stage + (uint32_t)kb * kDTileBytes + sw128_offset(row, (uint32_t)j),
-                         o[0], o[1], o[2], o[3]);
+            st_shared_v4(tile + sw128_offset(row, (uint32_t)j), o[0], o[1], o[2], o[3]);
           }
         }
       }
@@ -209,12 +209,12 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       mbar_arrive(&full_bar[s]);
     }
     asm volatile("cp.async.wait_all;" ::: "memory");   // no copy outlives an aborted loop
-  } else if (warp < 8) {
+  } else if (warp < 12) {
     // ------------------------------------------------------------ epilogue
-    const int q = warp - 4;                          // TMEM lane quarter
+    const int q = warp & 3;                          // TMEM lane quarter (warp % 4)
     const int m = 32 * q + lane;                     // accumulator row
     const int nsub = a.ppo < kPktPerStage ? kPktPerStage / a.ppo : 1;  // outputs per stage
-    const int span = kN / nsub;                      // columns per output
+    const int span = kN / nsub;                      // columns per output (>= 64)
     const int pgs_per_out = a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     for (int u = u_lo, i = 0; u < u_hi; ++u, ++i) {
@@ -230,15 +230,20 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)b * 256u;
 #pragma unroll
       for (int c = 0; c < (ok ? kN / 32 : 0); ++c) {
-        uint32_t r[32];
-        tmem_ld32(taddr + 32u * c, r);
+        uint32_t r0[32];
+        tmem_ld32(taddr + 32u * c, r0);
         tmem_wait_ld();
-        float sq = 0.f;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;   // four independent chains
 #pragma unroll
-        for (int e = 0; e < 32; ++e) {
-          const float v = __uint_as_float(r[e]);
-          sq = fmaf(v, v, sq);
+        for (int e = 0; e < 32; e += 4) {
+          const float v0 = __uint_as_float(r0[e]), v1 = __uint_as_float(r0[e + 1]);
+          const float v2 = __uint_as_float(r0[e + 2]), v3 = __uint_as_float(r0[e + 3]);
+          s0 = fmaf(v0, v0, s0);
+          s1 = fmaf(v1, v1, s1);
+          s2 = fmaf(v2, v2, s2);
+          s3 = fmaf(v3, v3, s3);
         }
+        const float sq = (s0 + s1) + (s2 + s3);
         const int sub = (32 * c) / span;
         if (nsub == 1) acc[0] += sq;
         else if (sub == 0) acc[0] += sq;
@@ -253,12 +258,17 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       bf_decode(u, npg, g, pg, pol);
       if (pol == 1 && ((pg + 1) % pgs_per_out) == 0) {
         // rows m and m + 64 hold Re and Im of the same beam
-        if (m >= 64)
-          for (int sI = 0; sI < nsub; ++sI) red[sI][m - 64] = acc[sI];
+        if (m >= 64) {
+#pragma unroll
+          for (int sI = 0; sI < 4; ++sI)
+            if (sI < nsub) red[sI][m - 64] = acc[sI];
+        }
         named_bar(1, 128);
         if (m < 64 && !abort_sh) {
           const int beam = 64 * bt + m;
-          for (int sI = 0; sI < nsub; ++sI) {
+#pragma unroll
+          for (int sI = 0; sI < 4; ++sI) {
+            if (sI >= nsub) break;
             const float P = acc[sI] + red[sI][m];
             const int to = a.ppo <= kPktPerStage ? pg * nsub + sI : pg / pgs_per_out;
             const int64_t o = ((int64_t)to * a.nbeam + beam) * ngrp + g;
@@ -330,7 +340,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
 
   tc_fence_before();
   __syncthreads();
-  if (warp == 8) {
+  if (warp == 12) {
     if (lane == 0) {
       volatile int no_abort = 0;
       mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);

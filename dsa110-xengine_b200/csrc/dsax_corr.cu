@@ -276,45 +276,50 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
 // Channel-major correlator.  Input [nchan][npkt][64 ant][4 B] (one contiguous
 // stream per channel, written by reorder_cm_kernel).
 //
-// Same product as corr_kernel -- D[128 x 256] = A [A ; Arot]^T per 32-byte
-// K step, Re in columns 0..127, Im in 128..255 -- with K laid out per 64-
-// packet stage as [64 real parts | 64 imaginary parts]:
-//     A row    = [ R  | I ]        Arot row = [ -I | R ]
-// Packet P of the stage sits at K byte k(P) = 8 (P mod 8) + P / 8 (a free
-// permutation: A and B share it), so the 16 packets P = 2c + e + 8q
-// (e = 0, 1; q = 0..7) fill 16-byte chunk c of the real half and chunk
-// c + 4 of the imaginary half.  Thread (antenna, c) reads those 16 words
-// (lanes = consecutive antennas: conflict-free), transposes bytes, and
-// sign-extends / negates nibbles with SWAR arithmetic.  Lanes 4..7 of each
-// group of 8 store the two pols in the opposite order, so every 16-byte
-// store instruction covers all eight bank groups of the 128-byte swizzle.
-// One loader thread brings each 64-packet stage (16 KB, contiguous) in with
-// a single bulk copy, four stages ahead.
+// Per 64-packet stage and time slot t, one K-major operand tile
+//     A row (2 ant + pol) = [ R (64 B) | I (64 B) ]
+// with packet P at K byte 8 (P mod 8) + P / 8 of each half (a permutation
+// shared by every operand).  Two MMA groups per tile:
+//     Re = A A^T           (K = 128: R R^T + I I^T)     TMEM cols t*256 + [0, 128)
+//     C  = I R^T           (K = 64, I and R halves)     TMEM cols t*256 + [128, 256)
+// and the epilogue forms Im = C - C^T (C^T through shared memory), so the
+// tile needs neither a negated copy nor a second rotated tile.
+// Thread (antenna, c) owns the 16 packets P = 2c + e + 8q (e = 0, 1;
+// q = 0..7), i.e. 16-byte chunk c of each half.  Its 16 words come either
+// straight from global memory (kBulk = false: lanes = consecutive
+// antennas, coalesced, two stages ahead in registers) or from 16 KB stages
+// that a loader warp brings in with one cp.async.bulk each, four ahead
+// (kBulk = true; conflict-free shared reads).  It transposes bytes with
+// prmt and sign-extends nibbles with carry-free bytewise adds.  Lanes 4..7 of each group of 8
+// store the two pols in the opposite order, so every 16-byte store
+// instruction covers all eight bank groups of the 128-byte swizzle.
 namespace corrcm {
 constexpr int kPktPerStage = 64;
-constexpr int kRawBytes = kPktPerStage * 256;      // 16 KB
-constexpr int kRawStages = 4;
 constexpr int kTile = 128 * 128;                   // 128 rows x 128 B of K
-constexpr int kFreqBytes = 2 * kTile;              // A + Arot
-constexpr int kStageBytes = 2 * kFreqBytes;        // two frequencies
-constexpr int kOpStages = 2;
-constexpr int kThreads = 320;                      // 8 unpack/epilogue warps + UMMA warp + loader warp
-constexpr int kSmemBytes = 1024 + kOpStages * kStageBytes + kRawStages * kRawBytes;
+constexpr int kStageBytes = 2 * kTile;             // two time slots
+constexpr int kOpStages = 4;
+constexpr int kRawBytes = kPktPerStage * 256;      // bulk-fed variant: one 16 KB stage
+constexpr int kRawStages = 4;
+// 8 unpack/epilogue warps + UMMA warp (+ loader warp for the bulk-fed variant)
+template <bool kBulk> constexpr int threads() { return kBulk ? 320 : 288; }
+template <bool kBulk> constexpr int smem_bytes() {
+  return 1024 + kOpStages * kStageBytes + (kBulk ? kRawStages * kRawBytes : 0);
+}
+constexpr uint32_t kIdescN128 = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 128);
+static_assert(kOpStages * kStageBytes >= 2 * 128 * 128 * 4, "C^T scratch reuses the stages");
 }  // namespace corrcm
 
-// Low nibble of each byte (0..15) -> sign-extended int8: v | (bit3 ? 0xF0 : 0).
-__device__ __forceinline__ uint32_t sext_nib4(uint32_t v) {
-  return v | ((v & 0x08080808u) * 0x1Eu);
+// Low / high nibble of each byte (4-bit two's complement) -> int8, bytewise
+// without carries: x = nibble ^ 8 = v + 8 in [0, 15]; (x + 0x78) ^ 0x80 = v.
+__device__ __forceinline__ uint32_t sext_lo4(uint32_t w) {
+  return (((w & 0x0F0F0F0Fu) ^ 0x08080808u) + 0x78787878u) ^ 0x80808080u;
+}
+__device__ __forceinline__ uint32_t sext_hi4(uint32_t w) {
+  return ((((w >> 4) & 0x0F0F0F0Fu) ^ 0x08080808u) + 0x78787878u) ^ 0x80808080u;
 }
 
-// Bytewise two's-complement negation (no carries between bytes); exact for
-// bytes in [-8, 7].
-__device__ __forceinline__ uint32_t neg_bytes(uint32_t x) {
-  const uint32_t t = (~x & 0x7F7F7F7Fu) + 0x01010101u;
-  return t ^ (~x & 0x80808080u);
-}
-
-__global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a) {
+template <bool kBulk>
+__global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(CorrArgs a) {
   using namespace corrcm;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kOpStages];
@@ -328,8 +333,7 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ch = blockIdx.x;
   const uint32_t sbase = (smem_u32(smem_raw) + 1023u) & ~1023u;
-  const uint32_t raw_base = sbase + kOpStages * kStageBytes;
-  const uint8_t *raw_gen = smem_raw + (raw_base - smem_u32(smem_raw));   // generic view
+  uint8_t *const gbase = smem_raw + (sbase - smem_u32(smem_raw));   // generic view of sbase
 
   if (tid == 0) {
     for (int s = 0; s < kOpStages; ++s) {
@@ -348,6 +352,7 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
     tmem_alloc(&tmem_base_sh, 512);
     tmem_relinquish();
   }
+  const uint32_t raw_base = sbase + kOpStages * kStageBytes;   // kBulk only
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -357,33 +362,36 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
     abort_sh = 1;
   }
   const int nks = (a.npkt + kPktPerStage - 1) / kPktPerStage;
-  const uint8_t *chan_src = a.in + (int64_t)ch * a.npkt * 256;
+  const uint32_t *chan_src = reinterpret_cast<const uint32_t *>(a.in + (int64_t)ch * a.npkt * 256);
 
   if (warp < 8) {
     // ------------------------------------------------------------ unpack
     const int ant = lane + 32 * (warp & 1);
-    const uint32_t c = (uint32_t)(warp >> 1);          // K chunk of the real half (0..3)
+    const uint32_t c = (uint32_t)(warp >> 1);          // 16-byte chunk of each half (0..3)
     const uint32_t flip = (uint32_t)(lane >> 2) & 1u;  // store pol 1 first
-    for (int ks = 0; ks < nks && !abort_sh; ++ks) {
-      const int s = ks % kOpStages, r = ks % kRawStages;
-      if (!mbar_wait_bounded(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
-                             DEV_ERR_WAIT_FULL, a.wait_limit_ns))
-        break;
-      if (!mbar_wait_bounded(&empty_bar[s], ((uint32_t)(ks / kOpStages) & 1u) ^ 1u, &abort_sh,
-                             a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
-        break;
-      const uint32_t *rw = reinterpret_cast<const uint32_t *>(raw_gen + r * kRawBytes);
-      const int pvalid = a.npkt - ks * kPktPerStage;   // packets of this stage that exist
-      // w[e][q]: packet 2c + e + 8q, word = bytes [t0p0, t0p1, t1p0, t1p1]
-      uint32_t w[2][8];
+    // tile offsets of this thread's chunks, store order sp = 0, 1 (pol = sp ^ flip)
+    uint32_t o_re[2], o_im[2];
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) {
+      const uint32_t row = (uint32_t)(2 * ant) + ((uint32_t)sp ^ flip);
+      o_re[sp] = sw128_offset(row, c);
+      o_im[sp] = sw128_offset(row, c + 4u);
+    }
+    // w[e][q]: packet 2c + e + 8q of the stage, word = bytes [t0p0, t0p1, t1p0, t1p1]
+    auto load = [&](int ks, uint32_t (&w)[2][8]) {
 #pragma unroll
       for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const int P = 2 * (int)c + e + 8 * q;
-          w[e][q] = P < pvalid ? rw[P * 64 + ant] : 0u;
+          const int p = ks * kPktPerStage + 2 * (int)c + e + 8 * q;
+          w[e][q] = (ks < nks && p < a.npkt) ? __ldg(chan_src + (int64_t)p * 64 + ant) : 0u;
         }
-      mbar_arrive(&rempty_bar[r]);   // raw stage consumed (generic-proxy reads only)
+    };
+    auto unpack_store = [&](int ks, const uint32_t (&w)[2][8]) -> bool {
+      const int s = ks % kOpStages;
+      if (!mbar_wait_bounded(&empty_bar[s], ((uint32_t)(ks / kOpStages) & 1u) ^ 1u, &abort_sh,
+                             a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+        return false;
       // X[sl][e][h]: sample slot sl = 2t + pol of packets q = 4h .. 4h+3
       uint32_t X[4][2][2];
 #pragma unroll
@@ -406,28 +414,60 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
 #pragma unroll
         for (int sp = 0; sp < 2; ++sp) {
           const uint32_t pol = (uint32_t)sp ^ flip;
-          uint32_t re[4], im[4], ni[4];
+          uint32_t re[4], im[4];
 #pragma unroll
           for (int k = 0; k < 4; ++k) {   // chunk word k = (e, h) = (k >> 1, k & 1)
             const uint32_t x0 = X[2 * t][k >> 1][k & 1], x1 = X[2 * t + 1][k >> 1][k & 1];
             const uint32_t x = pol ? x1 : x0;
-            re[k] = sext_nib4(x & 0x0F0F0F0Fu);
-            im[k] = sext_nib4((x >> 4) & 0x0F0F0F0Fu);
-            ni[k] = neg_bytes(im[k]);
+            re[k] = sext_lo4(x);
+            im[k] = sext_hi4(x);
           }
-          const uint32_t row = (uint32_t)(2 * ant) + pol;
-          const uint32_t tA = stage + (uint32_t)t * kFreqBytes, tB = tA + kTile;
-          const uint32_t o_re = sw128_offset(row, c), o_im = sw128_offset(row, c + 4u);
-          st_shared_v4(tA + o_re, re[0], re[1], re[2], re[3]);
-          st_shared_v4(tA + o_im, im[0], im[1], im[2], im[3]);
-          st_shared_v4(tB + o_re, ni[0], ni[1], ni[2], ni[3]);
-          st_shared_v4(tB + o_im, re[0], re[1], re[2], re[3]);
+          const uint32_t tile = stage + (uint32_t)t * kTile;
+          st_shared_v4(tile + o_re[sp], re[0], re[1], re[2], re[3]);
+          st_shared_v4(tile + o_im[sp], im[0], im[1], im[2], im[3]);
         }
       }
       fence_proxy_async_smem();
       mbar_arrive(&full_bar[s]);
+      return true;
+    };
+    if (kBulk) {
+      const uint32_t *rw_base = reinterpret_cast<const uint32_t *>(gbase + kOpStages * kStageBytes);
+      for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+        const int r = ks % kRawStages;
+        if (!mbar_wait_bounded(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+          break;
+        const uint32_t *rw = rw_base + r * (kRawBytes / 4);
+        const int pvalid = a.npkt - ks * kPktPerStage;
+        uint32_t w[2][8];
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int P = 2 * (int)c + e + 8 * q;
+            w[e][q] = P < pvalid ? rw[P * 64 + ant] : 0u;
+          }
+        mbar_arrive(&rempty_bar[r]);   // raw stage consumed (generic-proxy reads only)
+        if (!unpack_store(ks, w)) break;
+      }
+    } else {
+      // two stages of loads in flight ahead of the stage being unpacked
+      uint32_t wa[2][8], wb[2][8], wc[2][8];
+      load(0, wa);
+      load(1, wb);
+      for (int ks = 0; ks < nks && !abort_sh; ks += 3) {
+        load(ks + 2, wc);
+        if (!unpack_store(ks, wa)) break;
+        if (ks + 1 >= nks) break;
+        load(ks + 3, wa);
+        if (!unpack_store(ks + 1, wb)) break;
+        if (ks + 2 >= nks) break;
+        load(ks + 4, wb);
+        if (!unpack_store(ks + 2, wc)) break;
+      }
     }
-  } else if (warp == 9) {
+  } else if (kBulk && warp == 9) {
     // ------------------------------------------------------------ bulk loader
     if (lane == 0) {
       for (int ks = 0; ks < nks && !abort_sh; ++ks) {
@@ -438,8 +478,9 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
         const int npk = min(kPktPerStage, a.npkt - ks * kPktPerStage);
         const uint32_t bytes = (uint32_t)npk * 256u;
         mbar_arrive_expect_tx(&rfull_bar[r], bytes);
-        bulk_g2s(raw_base + (uint32_t)r * kRawBytes, chan_src + (int64_t)ks * kPktPerStage * 256,
-                 bytes, &rfull_bar[r]);
+        bulk_g2s(raw_base + (uint32_t)r * kRawBytes,
+                 a.in + (int64_t)ch * a.npkt * 256 + (int64_t)ks * kPktPerStage * 256, bytes,
+                 &rfull_bar[r]);
       }
     }
     __syncwarp();
@@ -455,11 +496,18 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
         const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-          const uint32_t tA = stage + (uint32_t)t * kFreqBytes;
+          const uint32_t tile = stage + (uint32_t)t * kTile;
+          const uint32_t dre = tmem + (uint32_t)t * 256u, dc = dre + 128u;
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {   // 4 x K = 32 bytes per 128-byte row
-            const uint64_t d = umma_desc_sw128(tA + 32u * kk, 1024u);
-            umma_i8(tmem + (uint32_t)t * 256u, d, d, corr::kIdesc, (ks | kk) != 0);
+          for (int kk = 0; kk < 4; ++kk) {   // Re: K = 128 bytes = 4 x 32
+            const uint64_t d = umma_desc_sw128(tile + 32u * kk, 1024u);
+            umma_i8(dre, d, d, kIdescN128, (ks | kk) != 0);
+          }
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {   // C = I R^T: K = 64 bytes = 2 x 32
+            const uint64_t di = umma_desc_sw128(tile + 64u + 32u * kk, 1024u);
+            const uint64_t dr = umma_desc_sw128(tile + 32u * kk, 1024u);
+            umma_i8(dc, di, dr, kIdescN128, (ks | kk) != 0);
           }
         }
         umma_commit(&empty_bar[s]);
@@ -475,25 +523,43 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
                                 a.wait_limit_ns);
     tc_fence_after();
     ok = __all_sync(0xffffffffu, ok && !abort_sh);
+    const int q = warp & 3, t = warp >> 2;
+    const int m = 32 * q + lane;                   // row = 2 * antenna + pol
+    const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
+    // C^T through shared memory (every MMA has completed, so the operand
+    // stages are free): row m of C at word (col ^ (m & 31)) of a 512-byte row.
+    uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase + t * (128 * 128 * 4));
     if (ok) {
-      const int q = warp & 3, t = warp >> 2;
-      const int m = 32 * q + lane;
+#pragma unroll
+      for (int cb = 0; cb < 8; ++cb) {
+        uint32_t cv[16];
+        tmem_ld16(trow + 128u + 16u * cb, cv);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
+      }
+    }
+    named_bar(1, 256);
+    if (ok) {
       const int i = m >> 1, pi = m & 1;
       float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
-      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
-      const int ncb = 2 * q + 2;
       const int64_t tri = (int64_t)i * (i + 1) / 2;
+      const int ncb = 2 * q + 2;
       for (int cb = 0; cb < ncb; ++cb) {
-        uint32_t re[16], im[16];
+        uint32_t re[16], cr[16];
         tmem_ld16(trow + 16u * cb, re);
-        tmem_ld16(trow + 128u + 16u * cb, im);
+        tmem_ld16(trow + 128u + 16u * cb, cr);
         tmem_wait_ld();
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
           const int j = 8 * cb + jj;
           if (j <= i) {
-            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(int32_t)im[2 * jj],
-                                   (float)(int32_t)re[2 * jj + 1], (float)(int32_t)im[2 * jj + 1]);
+            const int b0 = 2 * j, b1 = 2 * j + 1;
+            const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
+            const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
+            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)((int32_t)cr[2 * jj] - ct0),
+                                   (float)(int32_t)re[2 * jj + 1],
+                                   (float)((int32_t)cr[2 * jj + 1] - ct1));
             float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
             if (a.accumulate) {
               const float4 old = *dst;
@@ -518,19 +584,25 @@ __global__ void __launch_bounds__(corrcm::kThreads, 1) corr_cm_kernel(CorrArgs a
   }
 }
 
-int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st) {
+template <bool kBulk>
+static int launch_cm(const CorrArgs &a, cudaStream_t st) {
   static bool attr_done = false;
   if (!attr_done) {
-    if (cudaFuncSetAttribute(corr_cm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             corrcm::kSmemBytes) != cudaSuccess)
+    if (cudaFuncSetAttribute(corr_cm_kernel<kBulk>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             corrcm::smem_bytes<kBulk>()) != cudaSuccess)
       return -2;
     attr_done = true;
   }
   void *args[] = {(void *)&a};
-  return cudaLaunchKernel((const void *)corr_cm_kernel, dim3(a.nchan), dim3(corrcm::kThreads), args,
-                          corrcm::kSmemBytes, st) == cudaSuccess
+  return cudaLaunchKernel((const void *)corr_cm_kernel<kBulk>, dim3(a.nchan),
+                          dim3(corrcm::threads<kBulk>()), args, corrcm::smem_bytes<kBulk>(),
+                          st) == cudaSuccess
              ? 0
              : -2;
+}
+
+int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, bool bulk_fed) {
+  return bulk_fed ? launch_cm<true>(a, st) : launch_cm<false>(a, st);
 }
 
 int launch_correlate(const CorrArgs &a, int fmt, cudaStream_t st) {

@@ -387,12 +387,14 @@ __device__ __forceinline__ float slogf(float v) { return copysignf(log1pf(fabsf(
 
 // Learned-flagger input features of one beam (one CTA per beam) from the
 // statistics pass: the plain flagger's four channel test statistics and its
-// time-series statistic, each scaled so that the plain rule fires at 1,
-// plus the downsampled spectrogram.  F[b][h][c][8], log-compressed by
-// slog(v) = sign(v) log(1 + |v|):
+// time-series statistic z, each scaled so that the plain rule fires at
+// |z| = 1 (z > 1 for the one-sided pp and time-series rules), given as
+// margins 10 (|z| - 1), plus the downsampled spectrogram.  F[b][h][c][8],
+// log-compressed by slog(v) = sign(v) log(1 + |v|):
 //   f0 (pixel mean - mu) / sigma * sqrt(tds)   f1 (pixel max - mu) / sigma
-//   f2 max over the pixel's samples of z_ts    f3 z_spec   f4 z_var
-//   f5 z_max   f6 z_pp   f7 mean over the pixel's samples of z_ts
+//   f2 10 (max over the pixel's samples of z_ts - 1)
+//   f3 10 (|z_spec| - 1)   f4 10 (|z_var| - 1)   f5 10 (|z_max| - 1)
+//   f6 10 (z_pp - 1)       f7 mean over the pixel's samples of z_ts
 // mu, sigma: mean and standard deviation of the beam's samples (from the
 // per-channel mean and variance).
 __global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(FlagArgs a, float *F,
@@ -480,6 +482,7 @@ __global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(Fla
   }
   __syncthreads();
   const float mu = mu_sd[0], inv = 1.0f / mu_sd[1], kpix = sqrtf((float)tds);
+  constexpr float kMargin = 10.0f;   // margins scaled so the rule's edge is steep
   float4 *Fb = F ? reinterpret_cast<float4 *>(F + (int64_t)b * H * C * 8) : nullptr;
   const float *ps = a.pix_sum + (int64_t)b * H * C;
   const float *pm = a.pix_max + (int64_t)b * H * C;
@@ -488,11 +491,11 @@ __global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(Fla
     float4 f, g;
     f.x = slogf((ps[i] / tds - mu) * inv * kpix);
     f.y = slogf((pm[i] - mu) * inv);
-    f.z = slogf(rmax[h]);
-    f.w = slogf(z[c]);
-    g.x = slogf(z[C + c]);
-    g.y = slogf(z[2 * C + c]);
-    g.z = slogf(z[3 * C + c]);
+    f.z = slogf(kMargin * (rmax[h] - 1.0f));
+    f.w = slogf(kMargin * (fabsf(z[c]) - 1.0f));
+    g.x = slogf(kMargin * (fabsf(z[C + c]) - 1.0f));
+    g.y = slogf(kMargin * (fabsf(z[2 * C + c]) - 1.0f));
+    g.z = slogf(kMargin * (z[3 * C + c] - 1.0f));
     g.w = slogf(rmean[h]);
     if (F) {
       Fb[2 * i] = f;

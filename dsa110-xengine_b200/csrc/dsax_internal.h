@@ -95,5 +95,7 @@ namespace dsax {
 // Channel-major corner turn: [nchan][npkt][64][4 B] (internal layout).
 int launch_reorder_chanmajor(const uint8_t *in, uint8_t *out, int npkt, int nant_in, int nchan,
                              cudaStream_t st);
-int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st);
+// bulk_fed: the operand feed is one cp.async.bulk per 64-packet stage (true)
+// or direct coalesced loads into registers (false).
+int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, bool bulk_fed);
 }  // namespace dsax

@@ -42,13 +42,13 @@ extern "C" int dsax_autotune(dsax_ctx *c, int reps, float *times_ms, int ntimes,
   float *vis = reinterpret_cast<float *>(blk + ((nin + 255) & ~(size_t)255));
   fill_pattern<<<1024, 256, 0, c->stream>>>(blk, nin, 12345u);
   const int saved = c->cfg.corr_path;
-  const int paths[3] = {1, 2, 3};
+  const int paths[4] = {1, 2, 3, 4};
   float best = 1e30f;
-  int bestp = 3;
+  int bestp = 4;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < 4; ++k) {
     c->cfg.corr_path = paths[k];
     for (int w = 0; w < 2; ++w)
       if ((rc = dsax_correlate_fmt(c, DSAX_FMT_CAPTURED, blk, vis, DSAX_MEM_DEVICE, 0)) != DSAX_OK)

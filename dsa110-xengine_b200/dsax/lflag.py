@@ -29,7 +29,7 @@ def pixel_labels(cm, tm, B, T, C, tds, guard):
     return cm[:, None, :] | (ts[:, :, None] & inside[None, None, :])
 
 
-def train(ctx, blocks, steps: int = 600, beams_per_step: int = 16, tds: int = 32,
+def train(ctx, blocks, steps: int = 1000, beams_per_step: int = 16, tds: int = 32,
           lr: float = 3e-3, pos_weight: float = 3.0, seed: int = 0, log=None):
     """blocks: list of device filterbanks [B][T][C] (torch float32).  Labels
     come from the GPU plain flagger on each whole block.  Adam with a cosine

@@ -69,11 +69,13 @@ typedef struct dsax_config {
     int bf_pkt_per_out;  /* packets per Stokes-I output sample (16 = 32 times)    */
     float bf_scale;      /* fixed scale before the uint8 quantisation             */
     unsigned long long wait_limit_ns; /* bound on device waits (0 = 1 s)          */
-    int corr_path;       /* captured-block correlation: 0 = default (= 3),
+    int corr_path;       /* captured-block correlation: 0 = default (= 4),
                             1 = one fused kernel reading the captured layout,
                             2 = corner turn to the REORDER layout + correlate,
-                            3 = corner turn to channel-major streams + bulk-
-                                copy-fed correlate                              */
+                            3 = corner turn to channel-major streams + correlate
+                                fed by direct coalesced loads,
+                            4 = as 3, fed by one bulk copy per 64-packet stage.
+                            3 and 4 also select the feed for DSAX_FMT_CHANMAJOR */
 } dsax_config;
 
 typedef struct dsax_ctx dsax_ctx;
@@ -121,9 +123,9 @@ int dsax_host_free(dsax_ctx *ctx, void *ptr);
 int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
 
 /* Autotuner: times the captured-block correlator variants (corr_path 1, 2,
- * 3) on a synthetic block of the context's geometry (reps launches each),
+ * 3, 4) on a synthetic block of the context's geometry (reps launches each),
  * sets the context's corr_path to the fastest, and returns the per-variant
- * milliseconds (times_ms[0..2] for paths 1..3, if given) and the choice. */
+ * milliseconds (times_ms[0..3] for paths 1..4, if given) and the choice. */
 int dsax_autotune(dsax_ctx *ctx, int reps, float *times_ms, int ntimes, int *best_path);
 
 /* massage() on the GPU (src/dsaX_reorder_raw.c:153-169): captured block ->

@@ -128,12 +128,17 @@ def test_statistics(x, p):
     return z, zt, spec, var
 
 
+MARGIN_SCALE = 10.0
+
+
 def features(x: np.ndarray, tds: int, p) -> np.ndarray:
     """x [B][T][C] -> [B][H = T/tds][C][8], slog(v) = sign(v) log(1 + |v|):
     f0 (pixel mean - mu) / sigma * sqrt(tds), f1 (pixel max - mu) / sigma,
-    f2 max and f7 mean over the pixel's samples of zt, f3..f6 the channel
-    statistics z (mean, variance, max, pp) of test_statistics; mu and sigma
-    are the beam's sample mean and standard deviation, from the per-channel
+    f2 = 10 (max over the pixel's samples of zt - 1), f3..f5 = 10 (|z| - 1)
+    for the mean, variance and max statistics, f6 = 10 (z_pp - 1), f7 the
+    mean over the pixel's samples of zt (z, zt from test_statistics; each
+    margin is positive exactly where the plain rule fires); mu and sigma are
+    the beam's sample mean and standard deviation, from the per-channel
     mean and variance.  p: the plain flagger's parameters (guard, filt,
     tbin, fbin, ts_base, tsflag, parity, thresh, var_add, ts_thresh)."""
     B, T, C = x.shape
@@ -151,11 +156,13 @@ def features(x: np.ndarray, tds: int, p) -> np.ndarray:
     ztp = zt[:, :H * tds].reshape(B, H, tds).astype(np.float64)
     ones_c = np.ones((1, 1, C))
     ones_h = np.ones((1, H, 1))
+    km = MARGIN_SCALE
     f[..., 0] = _slog((pm - m) / s * np.sqrt(tds))
     f[..., 1] = _slog((px - m) / s)
-    f[..., 2] = _slog(ztp.max(axis=2)[:, :, None] * ones_c)
-    for k in range(4):
-        f[..., 3 + k] = _slog(z[k].astype(np.float64)[:, None, :] * ones_h)
+    f[..., 2] = _slog(km * (ztp.max(axis=2)[:, :, None] * ones_c - 1.0))
+    for k in range(3):
+        f[..., 3 + k] = _slog(km * (np.abs(z[k].astype(np.float64))[:, None, :] * ones_h - 1.0))
+    f[..., 6] = _slog(km * (z[3].astype(np.float64)[:, None, :] * ones_h - 1.0))
     f[..., 7] = _slog(ztp.mean(axis=2)[:, :, None] * ones_c)
     return f
 

@@ -39,9 +39,9 @@ def test_oracle_gradients_finite_difference():
 
 
 def test_oracle_features_encode_plain_rule(oracle):
-    """The channel and time features are the plain flagger's own test
-    statistics: thresholding them at 1 (slog: log 2) reproduces the C
-    oracle's masks exactly, so a net can reach F1 = 1 from them."""
+    """The channel and time features are margins of the plain flagger's own
+    test statistics: "any margin > 0" reproduces the C oracle's masks
+    exactly, so a net can reach F1 = 1 from them."""
     from types import SimpleNamespace
     B, T, C, tds = 12, 4096, 48, 32
     x, _ = oracle.gen_filterbank(1000, nbeam=B)
@@ -52,9 +52,7 @@ def test_oracle_features_encode_plain_rule(oracle):
     cm, tm, _, _, _ = oracle.plain_flag(x, po, None)
     f = LO.features(x, tds, p)
     y = LO.labels(cm, tm, tds, 6)
-    t = np.log(2.0)
-    pred = ((np.abs(f[..., 3]) > t) | (np.abs(f[..., 4]) > t) | (np.abs(f[..., 5]) > t)
-            | (f[..., 6] > t) | (f[..., 2] > t))
+    pred = (f[..., 2] > 0) | (f[..., 3] > 0) | (f[..., 4] > 0) | (f[..., 5] > 0) | (f[..., 6] > 0)
     pred[..., :6] = False
     pred[..., C - 6:] = False
     assert y.sum() > 0
@@ -184,7 +182,7 @@ def test_training_reaches_plain_flagger_masks(dsax, oracle):
     with dsax.Context(dsax.default_config(npkt=16, nchan=8)) as ctx:
         ctx.lf_init(7)
         untrained = [LO.prf1(*lflag.evaluate(ctx, xb, tds)) for xb in test_blocks]
-        losses = lflag.train(ctx, train_blocks, steps=600, beams_per_step=16, tds=tds)
+        losses = lflag.train(ctx, train_blocks, steps=1000, beams_per_step=16, tds=tds)
         print("loss first/last", losses[0], losses[-1])
         trained = [LO.prf1(*lflag.evaluate(ctx, xb, tds)) for xb in test_blocks]
         # threshold rule on one feature (no learning): best over features and cuts
@@ -209,4 +207,4 @@ def test_training_reaches_plain_flagger_masks(dsax, oracle):
     f1 = min(t[2] for t in trained)
     assert f1 > max(u[2] for u in untrained) + 0.2
     assert f1 > best_rule
-    assert f1 > 0.9
+    assert f1 >= 0.98
