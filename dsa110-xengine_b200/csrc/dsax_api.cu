@@ -160,6 +160,13 @@ void dsax_destroy(dsax_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   release_batch_plan(c);
   c->release_all();
+  for (auto &st : c->side)
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  for (auto &ev : c->pev)
+    if (ev) cudaEventDestroy(ev);
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -25,6 +25,7 @@ enum {
   AUX_BATCH_SCRATCH = 12,  // batch: corner-turned block, beam filterbank, flag statistics
   AUX_TUNE = 13,           // autotuner: synthetic block + visibilities
   AUX_LF_TCW = 14,         // learned flagger: BF16 weight images of the tensor-core path
+  AUX_PIPE = 15,           // correlate_many: double-buffered inputs, corner turns, visibilities
 };
 
 struct DevBuf {
@@ -68,6 +69,10 @@ struct dsax_ctx {
   int weights_ready = 0;
   int weights_nchan = 0;      // channels covered by the weight image
   void *batch_plan = nullptr; // captured batch graph (dsax_batch.cu)
+  // correlate_many pipeline: side streams (copy in, corner turn, copy out)
+  // and per-buffer events, created on first use
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t pev[9] = {};
   dsax::LfNet lf_storage;
   dsax::LfNet *lf = &lf_storage;
   char errmsg[512] = {0};

@@ -148,6 +148,7 @@ def _bind_optional(L):
         "dsax_flag": ([P, ctypes.POINTER(FlagParams), P, P, P, P, P, P, I], I),
         "dsax_reorder": ([P, P, P, I], I),
         "dsax_corner_turn": ([P, P, P, I, I], I),
+        "dsax_correlate_many": ([P, P, P, I, I], I),
         "dsax_lf_nparams": ([], I),
         "dsax_lf_init": ([P, ctypes.c_ulonglong], I),
         "dsax_lf_set_params": ([P, P, I], I),
@@ -253,6 +254,16 @@ class Context:
                   accumulate: bool = False):
         rc = lib().dsax_correlate_fmt(self._h, fmt, _ptr(blk), _ptr(vis), mem, int(accumulate))
         self._check(rc, "dsax_correlate_fmt")
+
+    def correlate_many(self, blocks, vis, mem: int = MEM_DEVICE):
+        """blocks, vis: equal-length lists of buffers (device tensors or host
+        arrays); stages of consecutive blocks overlap on side streams."""
+        n = len(blocks)
+        if n != len(vis) or n == 0:
+            raise ValueError("blocks and vis must be non-empty and of equal length")
+        pb = (ctypes.c_void_p * n)(*[_ptr(b) for b in blocks])
+        pv = (ctypes.c_void_p * n)(*[_ptr(v) for v in vis])
+        self._check(lib().dsax_correlate_many(self._h, pb, pv, n, mem), "dsax_correlate_many")
 
     def reorder(self, captured, reordered, mem: int = MEM_DEVICE):
         """massage() on the GPU: captured -> REORDER-key layout."""

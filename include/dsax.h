@@ -122,6 +122,18 @@ int dsax_host_free(dsax_ctx *ctx, void *ptr);
  * overwrite. */
 int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
 
+/* nblk CAPTURED blocks -> nblk xGPU triangular visibility buffers, with the
+ * stages of consecutive blocks overlapped: block i+1's corner turn runs on a
+ * side stream while block i is correlated, and with mem = DSAX_MEM_HOST the
+ * copies in and out overlap both (pinned host buffers give asynchronous
+ * DMA).  Replaces the per-block loop of src/dsaX_xgpu.cu:300-357 (H2D,
+ * promoter, xgpuCudaXengine, matrix copy-out, one block at a time).  Device
+ * mode enqueues (ordered on the context stream); host mode returns when all
+ * visibilities are in the host buffers.  Output always overwrites.  Uses
+ * the channel-major path (corr_path 3 or 4 selects the correlator feed). */
+int dsax_correlate_many(dsax_ctx *ctx, const void *const *blocks, void *const *vis, int nblk,
+                        int mem);
+
 /* Autotuner: times the captured-block correlator variants (corr_path 1, 2,
  * 3, 4) on a synthetic block of the context's geometry (reps launches each),
  * sets the context's corr_path to the fastest, and returns the per-variant
