@@ -183,6 +183,22 @@ int dsax_sync(dsax_ctx *c) {
   return check_device_error(c);
 }
 
+int dsax_register_host(dsax_ctx *c, void *p, size_t n) {
+  if (!c || !p || n == 0) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  cudaError_t e = cudaHostRegister(p, n, cudaHostRegisterPortable);
+  if (e != cudaSuccess) return cuda_check(c, e, "cudaHostRegister");
+  return DSAX_OK;
+}
+
+int dsax_unregister_host(dsax_ctx *c, void *p) {
+  if (!c || !p) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  cudaError_t e = cudaHostUnregister(p);
+  if (e != cudaSuccess) return cuda_check(c, e, "cudaHostUnregister");
+  return DSAX_OK;
+}
+
 int dsax_host_alloc(dsax_ctx *c, size_t n, void **p) {
   if (!c || !p || n == 0) return DSAX_ERR_ARG;
   DeviceGuard g(c->device);

@@ -217,6 +217,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
     const int span = kN / nsub;                      // columns per output (>= 64)
     const int pgs_per_out = a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    float bpow = 0.f;   // this CTA's share of the beam's total power (AGC)
     for (int u = u_lo, i = 0; u < u_hi; ++u, ++i) {
       const int b = i & 1;
       const uint32_t ph = (uint32_t)(i >> 1) & 1u;
@@ -275,15 +276,20 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
             if (a.out_f32) a.out_f32[o] = P;
             if (a.out_fb) a.out_fb[((int64_t)beam * (a.npkt / a.ppo) + to) * ngrp + g] = P;
             if (a.out_u8) {
-              int v = __float2int_rn(P * a.scale);
+              // AGC: rint(P * bp) / 2 as src/dsaX_beamformer.cu adder (:150-156),
+              // saturated instead of wrapped
+              int v = a.agc_scale ? __float2int_rn(P * __ldg(a.agc_scale + beam)) / 2
+                                  : __float2int_rn(P * a.scale);
               a.out_u8[o] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
             }
+            bpow += P;
           }
         }
         named_bar(1, 128);
         acc[0] = acc[1] = acc[2] = acc[3] = 0.f;
       }
     }
+    if (a.beam_power && m < 64 && bpow != 0.f) atomicAdd(a.beam_power + 64 * bt + m, bpow);
   } else {
     // ------------------------------------------------------------ weights + UMMA
     if (lane == 0) {

@@ -75,6 +75,41 @@ int dsax_set_weights(dsax_ctx *c, const double *wre, const double *wim) {
   return DSAX_OK;
 }
 
+// Geometric (fan-beam) weights in FP64, restating calc_weights
+// (src/dsaX_beamformer.cu:421-449) with the calibration normalisation of
+// init_weights (:559-602): for channel group g (centre frequency
+// fch1 - (8g + 4) x 250/8192 MHz), pol p, beam b (offset theta_b =
+// sep x (127 - b) arcmin) and antenna a (easting pos_a),
+//   w = exp(i afac pos_a) x cal / |cal|^2,  afac = -2 pi nu theta_b / c,
+// zero for flagged antennas; then the BF16 operand image as dsax_set_weights.
+int dsax_set_geometric_weights(dsax_ctx *c, const double *antpos, const double *cal,
+                               const int *flagged, double fch1_mhz, double sep_arcmin) {
+  if (!c || !antpos || !cal) return DSAX_ERR_ARG;
+  const int ngrp = c->cfg.nchan / 8, nbeam = c->cfg.nbeam;
+  if (c->cfg.nchan % 8 || nbeam < 64 || nbeam % 64)
+    return set_error(c, DSAX_ERR_ARG, "beamformer needs nchan %% 8 == 0 and nbeam %% 64 == 0");
+  const double kPi = 3.14159265358979323846, kC = 299792458.0;
+  std::vector<double> wre((size_t)ngrp * 2 * nbeam * 64), wim(wre.size());
+  for (int g = 0; g < ngrp; ++g)
+    for (int pol = 0; pol < 2; ++pol)
+      for (int b = 0; b < nbeam; ++b)
+        for (int a = 0; a < 64; ++a) {
+          const double *cc = cal + (((size_t)a * ngrp + g) * 2 + pol) * 2;
+          double cr = cc[0], ci = cc[1];
+          const double n2 = cr * cr + ci * ci;
+          if (n2 != 0.0) { cr /= n2; ci /= n2; }
+          if (flagged && flagged[a]) { cr = 0.0; ci = 0.0; }
+          const double nu = (fch1_mhz - (8.0 * g + 4.0) * 250.0 / 8192.0) * 1e6;
+          const double theta = sep_arcmin * (127.0 - b) * kPi / 10800.0;
+          const double ph = -2.0 * kPi * nu * theta / kC * antpos[a];
+          const double tr = cos(ph), ti = sin(ph);
+          const size_t o = (((size_t)g * 2 + pol) * nbeam + b) * 64 + a;
+          wre[o] = tr * cr - ti * ci;
+          wim[o] = ti * cr + tr * ci;
+        }
+  return dsax_set_weights(c, wre.data(), wim.data());
+}
+
 int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int mem) {
   if (!c || !blk || (!out_u8 && !out_f32)) return DSAX_ERR_ARG;
   if (!c->weights_ready) return set_error(c, DSAX_ERR_ARG, "dsax_set_weights not called");
@@ -99,12 +134,20 @@ int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int
   a.ppo = ppo;
   a.scale = cf.bf_scale;
   a.wait_limit_ns = cf.wait_limit_ns;
+  if (c->agc_on) {   // per-beam scale from the previous blocks; this block's power for the next
+    a.agc_scale = agc_scale_ptr(c->aux[AUX_AGC].ptr, cf.nbeam);
+    a.beam_power = agc_power_ptr(c->aux[AUX_AGC].ptr, cf.nbeam);
+  }
+  auto agc_after = [&]() -> bool {
+    return !c->agc_on ||
+           launch_agc_update(c->aux[AUX_AGC].ptr, cf.nbeam, cf.nchan / 8, cf.npkt / 16, c->stream) == 0;
+  };
   if (mem == DSAX_MEM_DEVICE) {
     if (!aligned16(blk)) return set_error(c, DSAX_ERR_ARG, "block must be 16-byte aligned");
     a.in = static_cast<const uint8_t *>(blk);
     a.out_u8 = static_cast<uint8_t *>(out_u8);
     a.out_f32 = static_cast<float *>(out_f32);
-    if (launch_beamform(a, c->num_sms, c->stream) != 0)
+    if (launch_beamform(a, c->num_sms, c->stream) != 0 || !agc_after())
       return cuda_check(c, cudaGetLastError(), "beamformer launch");
     return DSAX_OK;
   }
@@ -118,7 +161,7 @@ int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int
   a.in = static_cast<const uint8_t *>(c->in_buf.ptr);
   a.out_u8 = out_u8 ? static_cast<uint8_t *>(c->aux[AUX_BEAM_U8].ptr) : nullptr;
   a.out_f32 = out_f32 ? static_cast<float *>(c->aux[AUX_BEAM_F32].ptr) : nullptr;
-  if (launch_beamform(a, c->num_sms, c->stream) != 0)
+  if (launch_beamform(a, c->num_sms, c->stream) != 0 || !agc_after())
     return cuda_check(c, cudaGetLastError(), "beamformer launch");
   if (out_u8 && (e = cudaMemcpyAsync(out_u8, a.out_u8, nout, cudaMemcpyDeviceToHost, c->stream)) !=
                     cudaSuccess)

@@ -26,6 +26,8 @@ enum {
   AUX_TUNE = 13,           // autotuner: synthetic block + visibilities
   AUX_LF_TCW = 14,         // learned flagger: BF16 weight images of the tensor-core path
   AUX_PIPE = 15,           // correlate_many: double-buffered inputs, corner turns, visibilities
+  AUX_AGC = 16,            // beamformer AGC: bandpass history, scales, per-beam power
+  AUX_COUNT = 20
 };
 
 struct DevBuf {
@@ -65,7 +67,8 @@ struct dsax_ctx {
   int *h_err = nullptr;   // pinned readback slot
   dsax::DevBuf in_buf;    // host-mode staging: input block
   dsax::DevBuf vis_buf;   // host-mode staging: visibilities
-  dsax::DevBuf aux[16];   // per-stage buffers, indexed by dsax::AUX_*
+  dsax::DevBuf aux[dsax::AUX_COUNT];   // per-stage buffers, indexed by dsax::AUX_*
+  int agc_on = 0;         // beamformer uses (and updates) the AGC bandpass state
   int weights_ready = 0;
   int weights_nchan = 0;      // channels covered by the weight image
   void *batch_plan = nullptr; // captured batch graph (dsax_batch.cu)

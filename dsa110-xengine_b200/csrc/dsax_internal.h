@@ -45,6 +45,8 @@ struct BfArgs {
   uint8_t *out_u8;         // [npkt/ppo][nbeam][nchan/8] Stokes-I uint8 (or null)
   float *out_f32;          // same layout, FP32 power before scaling (or null)
   float *out_fb;           // [nbeam][npkt/ppo][nchan/8] FP32 power (filterbank order, or null)
+  const float *agc_scale;  // per-beam AGC scale: u8 = rint(P * s) / 2 (or null: fixed scale)
+  float *beam_power;       // per-beam total power of the block, accumulated (or null)
   int *err;
   int npkt, nant_in, nchan, nbeam, ppo;
   float scale;
@@ -52,6 +54,14 @@ struct BfArgs {
 };
 
 int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st);
+
+// AGC bandpass state (dsax_agc.cu): per-beam scale for the next block from
+// this block's per-beam power.
+constexpr int kAgcNbp = 8;   // blocks averaged once the history is full
+int launch_agc_update(void *state, int nbeam, int ngrp, int nints, cudaStream_t st);
+size_t agc_state_bytes(int nbeam);
+float *agc_scale_ptr(void *state, int nbeam);
+float *agc_power_ptr(void *state, int nbeam);
 
 }  // namespace dsax
 

@@ -8,7 +8,8 @@
 //   warps 0-3 : producers.  Thread m gathers pixel m's eight 16-byte K
 //               chunks of a 64-wide K block straight into the 128-byte-
 //               swizzled A stage with cp.async (zero fill at the image
-//               border); it keeps four stages of copies in flight and
+//               border); it keeps all but two of the stages (6 to 12, as
+//               shared memory allows beside the weights) in flight and
 //               marks a stage full once its own copies have landed.
 //   warps 4-7 : epilogue: TMEM -> + bias -> ReLU -> BF16 NHWC activations,
 //               or for the third layer the 9 per-tap projections onto the
@@ -29,9 +30,14 @@ namespace dsax {
 
 namespace lftc {
 constexpr int kThreads = 288;
-constexpr int kStages = 6;
-constexpr int kAhead = 4;               // cp.async groups in flight per producer thread
 constexpr int kABytes = 128 * 128;      // A stage: 128 pixels x 64 bf16 (one K block)
+// As many A stages as fit beside the resident weight image (<= 200 KB of
+// shared memory); the producers keep all but two of them in flight.
+template <int CIN, int COUT> constexpr int stages() {
+  return (200 * 1024 - ((9 * CIN + 63) / 64) * COUT * 128) / kABytes < 12
+             ? (200 * 1024 - ((9 * CIN + 63) / 64) * COUT * 128) / kABytes
+             : 12;
+}
 }  // namespace lftc
 
 struct LfTcArgs {
@@ -59,6 +65,8 @@ __global__ void __launch_bounds__(lftc::kThreads, 1) lf_conv_tc_kernel(LfTcArgs 
   constexpr int WBYTES = KB * COUT * 128;
   constexpr uint32_t IDESC = umma_idesc(/*F32*/ 1, /*BF16*/ 1, /*BF16*/ 1, 128, COUT);
   constexpr uint32_t TCOLS = 2 * COUT;   // 64 or 128: a power of two >= 32
+  constexpr int kStages = stages<CIN, COUT>();
+  constexpr int kAhead = kStages - 2;      // cp.async groups in flight per producer thread
   static_assert(CIN % 8 == 0 && (COUT == 32 || COUT == 64), "layer shape");
 
   extern __shared__ uint8_t smem_raw[];
@@ -70,9 +78,15 @@ __global__ void __launch_bounds__(lftc::kThreads, 1) lf_conv_tc_kernel(LfTcArgs 
   __shared__ __align__(8) uint64_t final_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
+  // epilogue constants: bias, and the last layer's weights for the projection
+  __shared__ __align__(16) float s_bias[COUT];
+  __shared__ __align__(16) float s_w4[PROJ ? 9 * COUT : 4];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  for (int i = tid; i < COUT; i += blockDim.x) s_bias[i] = a.bias[i];
+  if (PROJ)
+    for (int i = tid; i < 9 * COUT; i += blockDim.x) s_w4[i] = a.w4[i];
   const uint32_t wsm = base;
   const uint32_t asm_base = base + WBYTES;
 
@@ -173,14 +187,26 @@ __global__ void __launch_bounds__(lftc::kThreads, 1) lf_conv_tc_kernel(LfTcArgs 
       const int p = ((int)blockIdx.x + i * (int)gridDim.x) * 128 + m;
       if (!ok || p >= npx) continue;
 #pragma unroll
-      for (int c = 0; c < COUT; ++c) v[c] = fmaxf(v[c] + __ldg(a.bias + c), 0.0f);
+      for (int c = 0; c < COUT; c += 4) {
+        const float4 bb = *reinterpret_cast<const float4 *>(s_bias + c);
+        v[c] = fmaxf(v[c] + bb.x, 0.0f);
+        v[c + 1] = fmaxf(v[c + 1] + bb.y, 0.0f);
+        v[c + 2] = fmaxf(v[c + 2] + bb.z, 0.0f);
+        v[c + 3] = fmaxf(v[c + 3] + bb.w, 0.0f);
+      }
       if (PROJ) {
 #pragma unroll
         for (int tap = 0; tap < 9; ++tap) {
-          float z = 0.0f;
+          float z0 = 0.0f, z1 = 0.0f;   // two chains
 #pragma unroll
-          for (int c = 0; c < COUT; ++c) z = fmaf(__ldg(a.w4 + tap * COUT + c), v[c], z);
-          a.z9[(int64_t)tap * npx + p] = z;
+          for (int c = 0; c < COUT; c += 4) {
+            const float4 ww = *reinterpret_cast<const float4 *>(s_w4 + tap * COUT + c);
+            z0 = fmaf(ww.x, v[c], z0);
+            z1 = fmaf(ww.y, v[c + 1], z1);
+            z0 = fmaf(ww.z, v[c + 2], z0);
+            z1 = fmaf(ww.w, v[c + 3], z1);
+          }
+          a.z9[(int64_t)tap * npx + p] = z0 + z1;
         }
       } else {
         uint4 *dst = reinterpret_cast<uint4 *>(a.out + (int64_t)p * COUT);
@@ -286,7 +312,7 @@ namespace {
 template <int CIN, int COUT, bool PROJ>
 int conv_tc_launch(const LfTcArgs &a, int num_sms, cudaStream_t st) {
   constexpr int KB = (9 * CIN + 63) / 64;
-  constexpr int smem = 1024 + KB * COUT * 128 + lftc::kStages * lftc::kABytes;
+  constexpr int smem = 1024 + KB * COUT * 128 + lftc::stages<CIN, COUT>() * lftc::kABytes;
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(lf_conv_tc_kernel<CIN, COUT, PROJ>,

@@ -149,6 +149,9 @@ def _bind_optional(L):
         "dsax_reorder": ([P, P, P, I], I),
         "dsax_corner_turn": ([P, P, P, I, I], I),
         "dsax_correlate_many": ([P, P, P, I, I], I),
+        "dsax_agc_enable": ([P, I], I),
+        "dsax_set_geometric_weights": ([P, P, P, P, ctypes.c_double, ctypes.c_double], I),
+        "dsax_agc_state": ([P, P, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "dsax_lf_nparams": ([], I),
         "dsax_lf_init": ([P, ctypes.c_ulonglong], I),
         "dsax_lf_set_params": ([P, P, I], I),
@@ -281,6 +284,30 @@ class Context:
         wre = np.ascontiguousarray(wre, dtype=np.float64)
         wim = np.ascontiguousarray(wim, dtype=np.float64)
         self._check(lib().dsax_set_weights(self._h, _ptr(wre), _ptr(wim)), "dsax_set_weights")
+
+    def set_geometric_weights(self, antpos, cal, flagged=None, fch1_mhz: float = 1530.0,
+                              sep_arcmin: float = 1.0):
+        """antpos[64] (m), cal[64][nchan/8][2][2] (re, im), flagged[64] or None."""
+        import numpy as np
+        antpos = np.ascontiguousarray(antpos, dtype=np.float64)
+        cal = np.ascontiguousarray(cal, dtype=np.float64)
+        fl = None if flagged is None else np.ascontiguousarray(flagged, dtype=np.int32)
+        self._check(lib().dsax_set_geometric_weights(self._h, _ptr(antpos), _ptr(cal), _ptr(fl),
+                                                     float(fch1_mhz), float(sep_arcmin)),
+                    "dsax_set_geometric_weights")
+
+    def agc_enable(self, mode: int = 1):
+        """1 adaptive, 2 frozen at the first block's median, 0 off."""
+        self._check(lib().dsax_agc_enable(self._h, mode), "dsax_agc_enable")
+
+    def agc_state(self):
+        """Returns (scale [nbeam] numpy, started, blocks)."""
+        import numpy as np
+        sc = np.zeros(self.cfg.nbeam, np.float32)
+        st, nb = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().dsax_agc_state(self._h, _ptr(sc), ctypes.byref(st), ctypes.byref(nb)),
+                    "dsax_agc_state")
+        return sc, st.value, nb.value
 
     def beamform(self, blk, out_u8=None, out_f32=None, mem: int = MEM_DEVICE):
         rc = lib().dsax_beamform(self._h, _ptr(blk), _ptr(out_u8), _ptr(out_f32), mem)

@@ -104,6 +104,12 @@ void *dsax_stream(dsax_ctx *ctx);
  * check (and clears it). */
 int dsax_sync(dsax_ctx *ctx);
 
+/* Pins caller-owned host memory (e.g. a shared-memory ring buffer) for
+ * asynchronous DMA, as src/dsaX_bfCorr.cu:86-114 does with
+ * cudaHostRegister; undo with dsax_unregister_host before freeing it. */
+int dsax_register_host(dsax_ctx *ctx, void *p, size_t n);
+int dsax_unregister_host(dsax_ctx *ctx, void *p);
+
 /* Pinned host memory for fast transfers (cudaHostAlloc / cudaFreeHost). */
 int dsax_host_alloc(dsax_ctx *ctx, size_t nbytes, void **ptr);
 int dsax_host_free(dsax_ctx *ctx, void *ptr);
@@ -170,8 +176,34 @@ int dsax_correlate_fmt(dsax_ctx *ctx, int fmt, const void *in, void *vis, int me
  *   out_f32 : P itself (FP32), or NULL.  At least one must be given.
  *   Requires nchan % 8 == 0, nbeam % 64 == 0, npkt % 16 == 0 and
  *   bf_pkt_per_out in {4, 8, 16, 32, ...} dividing npkt. */
+
+/* Geometric fan-beam weights computed in FP64 from the array description
+ * (src/dsaX_beamformer.cu calc_weights :421-449, init_weights :559-602):
+ * antpos[64] antenna eastings (m), cal[64][nchan/8][2 pol][re, im]
+ * calibration gains (weights use cal / |cal|^2), flagged[64] (nonzero:
+ * antenna zeroed; may be NULL), fch1_mhz (first channel), sep_arcmin (beam
+ * separation; beam b points at sep x (127 - b)).  Group g's frequency is
+ * fch1 - (8g + 4) x 250/8192 MHz.  Replaces dsax_set_weights' input. */
+int dsax_set_geometric_weights(dsax_ctx *ctx, const double *antpos, const double *cal,
+                               const int *flagged, double fch1_mhz, double sep_arcmin);
 int dsax_set_weights(dsax_ctx *ctx, const double *wre, const double *wim);
 int dsax_beamform(dsax_ctx *ctx, const void *blk, void *out_u8, void *out_f32, int mem);
+
+/* Automatic gain control of the uint8 beams (src/dsaX_beamformer.cu badder
+ * :79-112, calc_allbp :482-494, ret_med_bp :506-513, ret_many_bp :515-530,
+ * per-block update :1017-1062).  mode 1: adaptive (the default of the
+ * reference), 2: frozen at the first block's median (-g), 0: off (fixed
+ * bf_scale).  Enabling resets the state.  While on, every dsax_beamform
+ * quantises u8 = rint(P * bp[beam]) / 2 (saturated) with bp from the
+ * previous blocks (0 for the first block, whose beams are zero) and then
+ * updates bp on the GPU from this block's per-beam power: median over beams
+ * for the first 8 blocks, then the mean of the last 8 with beams more than
+ * 10 % off the first median reset to it; bp = 2.5 * 128 / (power / (nchan/8
+ * x npkt/16)). */
+int dsax_agc_enable(dsax_ctx *ctx, int mode);
+/* Current per-beam scale [nbeam] (may be NULL), state (0 before the first
+ * block, 1 median phase, 2 history phase) and blocks seen; synchronises. */
+int dsax_agc_state(dsax_ctx *ctx, float *scale, int *started, int *blocks);
 
 /* ---- plain RFI flagger ----
  * Replaces src/gpu_flagger.cu: the statistics kernels (:175-494) and the

@@ -182,6 +182,65 @@ def quantize_u8(power: np.ndarray, scale: float) -> np.ndarray:
     return np.clip(np.rint(power * scale), 0, 255).astype(np.uint8)
 
 
+def quantize_u8_agc(power: np.ndarray, bp: np.ndarray) -> np.ndarray:
+    """AGC requantisation of src/dsaX_beamformer.cu adder (:150-156):
+    rint(P * bp[beam]) / 2 (integer division), saturated to [0, 255]
+    (the reference wraps).  power [t][beam][g], bp [beam]."""
+    v = np.rint(power * bp[None, :, None].astype(np.float64)).astype(np.int64)
+    v = np.where(v >= 0, v // 2, -((-v) // 2))   # C division truncates toward zero
+    return np.clip(v, 0, 255).astype(np.uint8)
+
+
+class AgcOracle:
+    """Beamformer automatic gain control, restated from the host code of
+    src/dsaX_beamformer.cu: per-block per-beam power (badder :79-112 summed
+    over channels by calc_allbp :482-494) enters a history of NBP = 8 blocks
+    (:1022-1024); for the first 8 blocks every beam gets the median over
+    beams, 0.5 (sorted[n/2-1] + sorted[n/2]) (ret_med_bp :506-513), and the
+    first block's median is frozen as medbp (:1030-1036); afterwards the
+    mean over the history, with beams more than 10 % off medbp reset to it
+    (ret_many_bp :515-530); AGC off uses medbp throughout (:1055-1056);
+    bp = 2.5 * 128 / (bp / (48 * nints)) (:1057-1062).  float32 arithmetic
+    where the reference uses float, double where it promotes."""
+    NBP = 8
+
+    def __init__(self, nbeam: int, ngrp: int, nints: int, agc: bool = True):
+        self.nbeam, self.ngrp, self.nints, self.agc = nbeam, ngrp, nints, agc
+        self.started, self.bpctr = 0, 0
+        self.medbp = np.float32(0.0)
+        self.hist = np.zeros((self.NBP, nbeam), np.float32)
+        self.scale = np.zeros(nbeam, np.float32)
+
+    def update(self, power: np.ndarray) -> np.ndarray:
+        p = np.asarray(power, np.float32)
+        self.hist[self.bpctr % self.NBP] = p
+        f32 = np.float32
+        if self.started == 0 or self.bpctr < self.NBP:
+            srt = np.sort(p)
+            med = f32(f32(0.5) * f32(srt[self.nbeam // 2 - 1] + srt[self.nbeam // 2]))
+            if self.started == 0:
+                self.medbp = med
+            bp = np.full(self.nbeam, med, np.float32)
+            self.started = max(self.started, 1)
+        else:
+            acc = np.zeros(self.nbeam, np.float32)
+            for j in range(self.NBP):
+                acc = (acc + self.hist[j]).astype(np.float32)
+            bp = (acc.astype(np.float64) / self.NBP).astype(np.float32)
+            off = np.abs((bp - self.medbp).astype(np.float32)).astype(np.float64) / float(self.medbp) > 0.1
+            bp[off] = self.medbp
+            self.started = 2
+        if not self.agc:
+            bp = np.full(self.nbeam, self.medbp, np.float32)
+        out = np.zeros(self.nbeam, np.float32)
+        nz = bp != 0
+        v = (bp[nz].astype(np.float64) / (float(self.ngrp) * self.nints)).astype(np.float32)
+        out[nz] = (2.5 * 128.0 / v.astype(np.float64)).astype(np.float32)
+        self.scale = out
+        self.bpctr += 1
+        return out
+
+
 # --------------------------------------------------------------------------
 # plain flagger
 # --------------------------------------------------------------------------

@@ -13,7 +13,7 @@ REL_TOL = 5e-3
 MEAN_TOL = 1e-3
 
 
-def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None):
+def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None, set_w=True):
     import torch
     npkt, nant, nchan = blk.shape[:3]
     cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
@@ -21,7 +21,8 @@ def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None):
     own = ctx is None
     ctx = ctx or dsax.Context(cfg)
     try:
-        ctx.set_weights(wre, wim)
+        if set_w:
+            ctx.set_weights(wre, wim)
         d_in = torch.from_numpy(blk.reshape(-1)).cuda()
         nout = (npkt // ppo) * nbeam * (nchan // 8)
         u8 = torch.zeros(nout, dtype=torch.uint8, device="cuda")
@@ -84,6 +85,14 @@ def test_beamformer_geometric_weights(dsax, oracle):
     scale = 128.0 / float(np.median(ref))
     u8, f32 = _beamform(dsax, blk, wre, wim, 256, 16, scale)
     _check(oracle, blk, wre, wim, u8, f32, 16, scale)
+    # the library's own FP64 weight generation gives the same beams
+    cfg = dsax.default_config(npkt=64, nant_in=63, nchan=16, nbeam=256, bf_pkt_per_out=16,
+                              bf_scale=scale)
+    with dsax.Context(cfg) as ctx:
+        ctx.set_geometric_weights(pos, cal, flagged)
+        u8b, f32b = _beamform(dsax, blk, wre, wim, 256, 16, scale, ctx=ctx, set_w=False)
+    np.testing.assert_array_equal(f32b, f32)
+    np.testing.assert_array_equal(u8b, u8)
 
 
 def test_beamformer_single_antenna_tone(dsax, oracle):
@@ -99,3 +108,41 @@ def test_beamformer_single_antenna_tone(dsax, oracle):
     want = 13.0 * 16 * 16 * 2
     np.testing.assert_allclose(f32, want, rtol=REL_TOL)
     assert (u8 == 255).all()   # saturates instead of wrapping
+
+
+def test_agc_bandpass_sequence(dsax, oracle):
+    """Eleven blocks through the AGC: the per-beam scales after every block
+    against the oracle's restatement (median phase, then the 8-block mean
+    with the 10 % clamp -- block 9 at twice the amplitude drives beams into
+    the clamp), and the uint8 beams of each block quantised with the
+    previous scale (zeros for the first block) within 1 LSB."""
+    import torch
+    npkt, nant, nchan, nbeam, ppo = 64, 63, 16, 256, 16
+    wre, wim = oracle.random_phase_weights(77, nchan // 8, nbeam)
+    cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
+                              bf_pkt_per_out=ppo)
+    ref = oracle.AgcOracle(nbeam, nchan // 8, npkt // 16)
+    clamped = 0
+    with dsax.Context(cfg) as ctx:
+        ctx.set_weights(wre, wim)
+        ctx.agc_enable(1)
+        for k in range(11):
+            blk = oracle.gen_block(900 + k, npkt, nant, nchan, "gauss", sigma=5.0 if k == 9 else 2.5)
+            d_in = torch.from_numpy(blk.reshape(-1)).cuda()
+            u8 = torch.zeros((npkt // ppo) * nbeam * (nchan // 8), dtype=torch.uint8, device="cuda")
+            torch.cuda.synchronize()
+            prev = ref.scale.copy()
+            ctx.beamform(d_in, u8)
+            scale, started, nblk = ctx.agc_state()
+            pw = oracle.beamform_power(blk, wre, wim, pkt_per_out=ppo)
+            want_u8 = oracle.quantize_u8_agc(pw, prev)
+            got_u8 = u8.cpu().numpy().reshape(want_u8.shape)
+            assert np.abs(got_u8.astype(int) - want_u8.astype(int)).max() <= 1
+            if k == 0:
+                assert got_u8.max() == 0
+            want = ref.update(pw.sum(axis=(0, 2)))
+            assert nblk == k + 1 and started == ref.started
+            np.testing.assert_allclose(scale, want, rtol=2e-3)
+            if k >= 8:
+                clamped += int(np.sum(np.abs(ref.hist.mean(axis=0) - ref.medbp) / ref.medbp > 0.1))
+    assert clamped > 0
