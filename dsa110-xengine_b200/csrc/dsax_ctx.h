@@ -27,6 +27,7 @@ enum {
   AUX_LF_TCW = 14,         // learned flagger: BF16 weight images of the tensor-core path
   AUX_PIPE = 15,           // correlate_many: double-buffered inputs, corner turns, visibilities
   AUX_AGC = 16,            // beamformer AGC: bandpass history, scales, per-beam power
+  AUX_EXTRACT = 17,        // correlate_extract: device visibilities, input, product
   AUX_COUNT = 20
 };
 

@@ -150,6 +150,10 @@ def _bind_optional(L):
         "dsax_corner_turn": ([P, P, P, I, I], I),
         "dsax_correlate_many": ([P, P, P, I, I], I),
         "dsax_agc_enable": ([P, I], I),
+        "dsax_extract": ([P, P, P, I], I),
+        "dsax_place_packets": ([P, P, I, I, I, P, I, ctypes.c_ulonglong, ctypes.c_ulonglong, I, P, P,
+                                P], I),
+        "dsax_correlate_extract": ([P, P, P, I], I),
         "dsax_set_geometric_weights": ([P, P, P, P, ctypes.c_double, ctypes.c_double], I),
         "dsax_agc_state": ([P, P, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "dsax_lf_nparams": ([], I),
@@ -295,6 +299,22 @@ class Context:
         self._check(lib().dsax_set_geometric_weights(self._h, _ptr(antpos), _ptr(cal), _ptr(fl),
                                                      float(fch1_mhz), float(sep_arcmin)),
                     "dsax_set_geometric_weights")
+
+    def place_packets(self, pkts, npk, stride, payload, ant_lookup, act0, nslots, slots_per_seq,
+                      block, counts, next_block=None):
+        """Device tensors: pkts (bytes), ant_lookup (int32), block, counts (int64[4])."""
+        rc = lib().dsax_place_packets(self._h, _ptr(pkts), npk, stride, payload, _ptr(ant_lookup),
+                                      int(ant_lookup.numel()), act0, nslots, slots_per_seq,
+                                      _ptr(block), _ptr(next_block), _ptr(counts))
+        self._check(rc, "dsax_place_packets")
+
+    def extract(self, vis, out, mem: int = MEM_DEVICE):
+        """simple_extract: XX/YY averaged over the two time slots."""
+        self._check(lib().dsax_extract(self._h, _ptr(vis), _ptr(out), mem), "dsax_extract")
+
+    def correlate_extract(self, blk, out, mem: int = MEM_DEVICE):
+        self._check(lib().dsax_correlate_extract(self._h, _ptr(blk), _ptr(out), mem),
+                    "dsax_correlate_extract")
 
     def agc_enable(self, mode: int = 1):
         """1 adaptive, 2 frozen at the first block's median, 0 off."""

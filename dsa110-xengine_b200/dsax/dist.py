@@ -1,8 +1,10 @@
-"""Multi-GPU plumbing for the benchmark: one process per GPU, blocks shard
-over ranks with no collective on the data path (each rank correlates its
-own blocks), and timings reduce as the max over ranks.  torch.distributed
-is used only for the barrier and that reduction (NCCL on GPUs, gloo in the
-CPU tests)."""
+"""Multi-GPU plumbing: one process per GPU.  For the correlator, blocks
+shard over ranks with no collective on the data path (each rank correlates
+its own blocks) and timings reduce as the max over ranks.  The one real
+exchange of the pipeline is the beam corner turn (corner_turn_beams): every
+rank beamforms its own subband, then an all-to-all gives each rank a group
+of beams across all subbands for the search stage.  torch.distributed
+carries it (NCCL over NVLink on GPUs, gloo in the CPU tests)."""
 from __future__ import annotations
 
 import datetime
@@ -36,3 +38,27 @@ def max_over_ranks(value: float, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def corner_turn_beams(local, group=None):
+    """Beam corner turn of the dsaX_dbnic -> dsaX_nicdb stage
+    (src/dsaX_dbnic.c:84-152, src/dsaX_nicdb.c:180-196) as one all-to-all.
+
+    local: this rank's beamformer output for its subband, a tensor
+    [T][NB][C] (time, beam, channel; uint8 or float) with NB divisible by the
+    world size W.  Returns [NB/W][T][W*C]: beams NB/W*r .. NB/W*(r+1)-1 of
+    rank r, with the channel axis ordered by source rank (subband), i.e. the
+    filterbank the flagger of that beam group reads."""
+    import torch
+    import torch.distributed as dist
+    W = dist.get_world_size(group)
+    T, NB, C = local.shape
+    if NB % W:
+        raise ValueError("beam count must divide by the world size")
+    nb = NB // W
+    # [W dest][nb][T][C], contiguous per destination
+    send = local.reshape(T, W, nb, C).permute(1, 2, 0, 3).contiguous()
+    recv = torch.empty_like(send)
+    dist.all_to_all_single(recv.view(-1), send.view(-1), group=group)
+    # recv[src][nb][T][C] -> [nb][T][src][C] -> [nb][T][W*C]
+    return recv.permute(1, 2, 0, 3).reshape(nb, T, W * C)

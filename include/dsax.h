@@ -140,6 +140,31 @@ int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
 int dsax_correlate_many(dsax_ctx *ctx, const void *const *blocks, void *const *vis, int nblk,
                         int mem);
 
+/* Packet capture -> block assembly (src/dsaX_capture.c receive_obs
+ * :870-960) for npk packets in device memory, `stride` bytes apart: an
+ * 8-byte header (35-bit sequence number in bytes 0-4, 16-bit antenna id in
+ * bytes 6-7, big-endian) and `payload` bytes (multiple of 8) at offset 8.
+ * Slot act = seq * slots_per_seq + ant_lookup[ant_id] (ant_lookup: device
+ * int[nlookup], -1 = unknown) goes to block slot act - act0 when below
+ * nslots, else to next_block (may be NULL) when below 2 nslots; earlier
+ * slots are late.  counts (device, 4 x uint64, accumulated): placed,
+ * placed in the next block, late, dropped (beyond / unknown antenna).
+ * Enqueued on the context stream. */
+int dsax_place_packets(dsax_ctx *ctx, const void *pkts, int npk, int stride, int payload,
+                       const int *ant_lookup, int nlookup, unsigned long long act0,
+                       unsigned long long nslots, int slots_per_seq, void *block, void *next_block,
+                       unsigned long long *counts);
+
+/* simple_extract of src/dsaX_writevis.c:55-74 on the GPU: XX and YY
+ * (pol-products 0 and 3) averaged over the two time slots of each channel,
+ * xGPU triangular visibilities -> [2080 baselines][nchan][2 pol][re, im]
+ * float (dsax_extract_bytes).  dsax_correlate_extract correlates a
+ * CAPTURED block and extracts on the device, so only the product is copied
+ * out in host mode. */
+size_t dsax_extract_bytes(const dsax_config *cfg);
+int dsax_extract(dsax_ctx *ctx, const void *vis, void *out, int mem);
+int dsax_correlate_extract(dsax_ctx *ctx, const void *in, void *out, int mem);
+
 /* Autotuner: times the captured-block correlator variants (corr_path 1, 2,
  * 3, 4) on a synthetic block of the context's geometry (reps launches each),
  * sets the context's corr_path to the fastest, and returns the per-variant

@@ -242,6 +242,56 @@ class AgcOracle:
 
 
 # --------------------------------------------------------------------------
+# packet capture -> block assembly
+# --------------------------------------------------------------------------
+def packet_header(seq: int, ch_id: int, ant_id: int) -> bytes:
+    """8-byte header as decoded by src/dsaX_capture.c:872-891: 35-bit seq in
+    bytes 0-4 (its low 3 bits in the top of byte 4), 13-bit ch_id in the low
+    5 bits of byte 4 and byte 5, 16-bit ant_id in bytes 6-7 (big-endian)."""
+    h = bytearray(8)
+    h[0] = (seq >> 27) & 0xFF
+    h[1] = (seq >> 19) & 0xFF
+    h[2] = (seq >> 11) & 0xFF
+    h[3] = (seq >> 3) & 0xFF
+    h[4] = ((seq & 7) << 5) | ((ch_id >> 8) & 0x1F)
+    h[5] = ch_id & 0xFF
+    h[6] = (ant_id >> 8) & 0xFF
+    h[7] = ant_id & 0xFF
+    return bytes(h)
+
+
+def place_packets(pkts: bytes, stride: int, payload: int, ant_lookup, act0: int, nslots: int,
+                  slots_per_seq: int, with_next: bool = True):
+    """Placement of receive_obs (src/dsaX_capture.c:870-960): returns
+    (block, next_block, counts[placed, next, late, dropped])."""
+    block = bytearray(nslots * payload)
+    nxt = bytearray(nslots * payload)
+    counts = [0, 0, 0, 0]
+    for k in range(len(pkts) // stride):
+        p = pkts[k * stride:(k + 1) * stride]
+        seq = ((p[4] & 0xE0) >> 5) | (p[3] << 3) | (p[2] << 11) | (p[1] << 19) | (p[0] << 27)
+        ant_id = (p[6] << 8) | p[7]
+        aid = ant_lookup[ant_id] if ant_id < len(ant_lookup) else -1
+        if aid < 0:
+            counts[3] += 1
+            continue
+        act = seq * slots_per_seq + aid
+        if act < act0:
+            counts[2] += 1
+        elif act - act0 < nslots:
+            o = (act - act0) * payload
+            block[o:o + payload] = p[8:8 + payload]
+            counts[0] += 1
+        elif with_next and act - act0 < 2 * nslots:
+            o = (act - act0 - nslots) * payload
+            nxt[o:o + payload] = p[8:8 + payload]
+            counts[1] += 1
+        else:
+            counts[3] += 1
+    return bytes(block), bytes(nxt), counts
+
+
+# --------------------------------------------------------------------------
 # plain flagger
 # --------------------------------------------------------------------------
 class FlagParams(ctypes.Structure):

@@ -51,3 +51,51 @@ def test_shard_and_max_over_ranks_gloo(nblocks):
         flat = sorted(i for part in gathered for i in part)
         assert flat == list(range(nblocks))
         assert abs(len(gathered[0]) - len(gathered[1])) <= 1
+
+
+def _ct_worker(rank, world_size, port, out):
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                    "dsa110-xengine_b200"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world_size), LOCAL_RANK=str(rank))
+    import numpy as np
+    import torch
+    from dsax import dist as D
+    d = D.init("gloo", timeout_s=60)
+    T, NB, C = 6, 8, 3
+    # subband `rank`: value encodes (t, beam, global channel)
+    loc = np.zeros((T, NB, C), np.int64)
+    for t in range(T):
+        for b in range(NB):
+            for c in range(C):
+                loc[t, b, c] = (t * 1000 + b) * 100 + rank * C + c
+    got = D.corner_turn_beams(torch.from_numpy(loc))
+    d.barrier()
+    d.destroy_process_group()
+    out.put((rank, got.numpy()))
+
+
+def test_beam_corner_turn_all_to_all_gloo():
+    """World size 2: each rank ends with its half of the beams, all times,
+    and the channels of both subbands in rank order."""
+    import numpy as np
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ct_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    T, NB, C, W = 6, 8, 3, 2
+    for r in range(W):
+        got = res[r]
+        assert got.shape == (NB // W, T, W * C)
+        for bl in range(NB // W):
+            for t in range(T):
+                for ch in range(W * C):
+                    assert got[bl, t, ch] == (t * 1000 + r * (NB // W) + bl) * 100 + ch
