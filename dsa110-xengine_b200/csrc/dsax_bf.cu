@@ -42,19 +42,47 @@ namespace dsax {
 namespace bf {
 constexpr int kPktPerStage = 16;                      // N = 16 packets x 16 chunnels = 256
 constexpr int kN = 256;
-constexpr int kKBlockBytes = 128;                     // 64 bf16 = 32 antennas x {re,im}
+constexpr int kKBlockBytes = 128;                     // one 128-byte K block per row
 constexpr int kWTileBytes = 128 * kKBlockBytes;       // 128 rows x 128 B = 16 KB
-constexpr int kWBytes = 2 /*pol*/ * 2 /*kb*/ * kWTileBytes;  // 64 KB per (g, bt)
 constexpr int kDTileBytes = kN * kKBlockBytes;        // 256 rows x 128 B = 32 KB
-constexpr int kStageBytes = 2 /*kb*/ * kDTileBytes;   // 64 KB
-constexpr int kStages = 2;
 constexpr int kProducers = 256;                       // 8 producer warps
 constexpr int kRawRowBytes = kProducers * 16;         // one 16 B load per producer thread
 constexpr int kRawBytes = 8 * kRawRowBytes;           // 32 KB: one packet group, both pols
-constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
 constexpr int kThreads = kProducers + 128 + 32;       // + 4 epilogue warps + UMMA warp
-constexpr uint32_t kIdesc = umma_idesc(/*F32*/ 1, /*BF16*/ 1, /*BF16*/ 1, 128, kN);
+// Operand type: BF16 (K = 64 antennas x {re, im} = 128 elements in two
+// 128-byte K blocks) or FP8 E4M3 (the same K in one 128-byte K block).
+template <bool kFp8> struct T {
+  static constexpr int kKB = kFp8 ? 1 : 2;            // K blocks per operand row
+  static constexpr int kWBytes = 2 /*pol*/ * kKB * kWTileBytes;   // per (g, bt)
+  static constexpr int kStageBytes = kKB * kDTileBytes;
+  static constexpr int kStages = kFp8 ? 3 : 2;
+  static constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
+  // f8f6f4: E4M3 = 0 for A and B; f16: BF16 = 1
+  static constexpr uint32_t kIdesc = kFp8 ? umma_idesc(1, 0, 0, 128, kN) : umma_idesc(1, 1, 1, 128, kN);
+};
 }  // namespace bf
+
+// PTX prmt in its default mode: selector nibble bit 3 replicates the msb of
+// the chosen byte over the result byte (CUDA's __byte_perm drops that bit).
+__device__ __forceinline__ uint32_t prmt_sx(uint32_t a, uint32_t b, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+  return d;
+}
+
+// Two packed complex 4-bit samples (the low 16 bits of s: nibbles re0, im0,
+// re1, im1, two's complement) -> their 4 E4M3 codes [re0 im0 re1 im1].  The
+// nibbles are the PRMT selectors themselves.  A = table of e4m3(0..7)
+// indexed by the nibble: negative nibbles (bit 3 set) replicate the msb of a
+// positive code, 0.  B = table of |e4m3(-8..-1)| indexed by the nibble ^ 8:
+// now the non-negative nibbles have bit 3 set and give 0.  B is nonzero
+// exactly for the negative values, whose sign bit is then added.  Exact for
+// all 16 values.
+__device__ __forceinline__ uint32_t nib2_to_e4m3x4(uint32_t s) {
+  const uint32_t A = prmt_sx(0x44403800u, 0x4e4c4a48u, s);            // 0 .. 7
+  const uint32_t B = prmt_sx(0x4a4c4e50u, 0x38404448u, s ^ 0x8888u);  // |-8| .. |-1|
+  return A | B | ((B + 0x7F7F7F7Fu) & 0x80808080u);
+}
 
 // Unit u of a CTA's range: r = u / 2 enumerates (channel group g, packet
 // group pg) as g * npg + pg; pol = u % 2.  The beam tile is fixed per CTA.
@@ -65,8 +93,11 @@ __device__ __forceinline__ void bf_decode(int u, int npg, int &g, int &pg, int &
   g = r / npg;
 }
 
+template <bool kFp8>
 __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   using namespace bf;
+  using TT = T<kFp8>;
+  constexpr int kWBytes = TT::kWBytes, kStageBytes = TT::kStageBytes, kStages = TT::kStages;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kStages];
   __shared__ __align__(8) uint64_t empty_bar[kStages];
@@ -83,7 +114,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   const uint32_t wsm = base;                  // weights [pol][kb][128 x 128 B]
   const uint32_t dsm = base + kWBytes;        // data stages [s][kb][256 x 128 B]
-  const uint32_t raw = dsm + kStages * kStageBytes;   // producer staging [16][128][16 B]
+  const uint32_t raw = dsm + kStages * kStageBytes;   // producer staging [8][256][16 B]
 
   // Work split: the nbt CTAs of a slot (consecutive blockIdx) own the same
   // (g, pg) range, one beam tile each, and run it in lockstep, so each
@@ -130,9 +161,12 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
     // 32 kb + 4j .. +3.  The 16 B loads of a (g, pg) carry both pols: they
     // are issued once, one packet group ahead (while the previous group's
     // two pol stages are built), and reused for the pol-1 stage.
-    const int j = tid & 7;
-    const int q = (tid >> 3) & 15;                   // packet within the stage
-    const int kb = tid >> 7;
+    // FP8: thread (q, j, kh): antennas 8j .. 8j+7 (one 16-byte K chunk of
+    // the single K block), channels 4kh .. 4kh+3 of the group.
+    const int j = kFp8 ? (tid >> 1) & 7 : tid & 7;
+    const int q = kFp8 ? tid >> 4 : (tid >> 3) & 15;   // packet within the stage
+    const int kb = kFp8 ? 0 : tid >> 7;
+    const int kh = kFp8 ? tid & 1 : 0;
     const int64_t ant_stride = (int64_t)a.nchan * 4;
     const int64_t pkt_stride = (int64_t)a.nant_in * ant_stride;
     // Each thread stages its own 8 loads of the next packet group in a
@@ -146,19 +180,18 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       const int g = r / npg, pg = r % npg;
       const int p = pg * kPktPerStage + q;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii) {
-          const int ant = 32 * kb + 4 * j + ii;
-          const bool ok = ant < a.nant_in && p < a.npkt;
-          const uint8_t *src = a.in + (ok ? p * pkt_stride + ant * ant_stride + (int64_t)(8 * g) * 4 +
-                                                16 * h
-                                          : 0);
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
-                           myraw + (uint32_t)(4 * h + ii) * (kRawRowBytes)),
-                       "l"(src), "r"(ok ? 16 : 0)
-                       : "memory");
-        }
+      for (int k8 = 0; k8 < 8; ++k8) {
+        // BF16: k8 = (channel half h, antenna ii); FP8: k8 = antenna 8j + k8, half kh
+        const int h = kFp8 ? kh : k8 >> 2;
+        const int ant = kFp8 ? 8 * j + k8 : 32 * kb + 4 * j + (k8 & 3);
+        const bool ok = ant < a.nant_in && p < a.npkt;
+        const uint8_t *src = a.in + (ok ? p * pkt_stride + ant * ant_stride + (int64_t)(8 * g) * 4 +
+                                              16 * h
+                                        : 0);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                         myraw + (uint32_t)k8 * (kRawRowBytes)),
+                     "l"(src), "r"(ok ? 16 : 0)
+                     : "memory");
       }
       asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -183,6 +216,33 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
         break;
       const uint32_t sel = (uint32_t)pol | ((4u + pol) << 4) | ((2u + pol) << 8) | ((6u + pol) << 12);
       const uint32_t tile = dsm + (uint32_t)s * kStageBytes + (uint32_t)kb * kDTileBytes;
+      if constexpr (kFp8) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {                   // channel 4kh + w of the group
+          // t[ag][pair]: antennas 8j + 4ag + 2pair, +1 at time 0 (bits 0-15)
+          // and time 1 (bits 16-31)
+          uint32_t t[2][2];
+#pragma unroll
+          for (int ag = 0; ag < 2; ++ag) {
+            const uint4 *U = Ucur + 4 * ag;
+            const uint32_t u0 = w == 0 ? U[0].x : w == 1 ? U[0].y : w == 2 ? U[0].z : U[0].w;
+            const uint32_t u1 = w == 0 ? U[1].x : w == 1 ? U[1].y : w == 2 ? U[1].z : U[1].w;
+            const uint32_t u2 = w == 0 ? U[2].x : w == 1 ? U[2].y : w == 2 ? U[2].z : U[2].w;
+            const uint32_t u3 = w == 0 ? U[3].x : w == 1 ? U[3].y : w == 2 ? U[3].z : U[3].w;
+            t[ag][0] = __byte_perm(u0, u1, sel);
+            t[ag][1] = __byte_perm(u2, u3, sel);
+          }
+#pragma unroll
+          for (int odd = 0; odd < 2; ++odd) {
+            uint32_t o[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) o[e] = nib2_to_e4m3x4(t[e >> 1][e & 1] >> (16 * odd));
+            const int k = 8 * kh + 2 * w + odd;       // chunnel = 2*chan + time
+            st_shared_v4(tile + sw128_offset((uint32_t)(16 * q + k), (uint32_t)j), o[0], o[1], o[2],
+                         o[3]);
+          }
+        }
+      } else {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
 #pragma unroll
@@ -204,6 +264,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
             st_shared_v4(tile + sw128_offset(row, (uint32_t)j), o[0], o[1], o[2], o[3]);
           }
         }
+      }
       }
       fence_proxy_async_smem();
       mbar_arrive(&full_bar[s]);
@@ -270,7 +331,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
 #pragma unroll
           for (int sI = 0; sI < 4; ++sI) {
             if (sI >= nsub) break;
-            const float P = acc[sI] + red[sI][m];
+            const float P = (acc[sI] + red[sI][m]) * a.pscale;
             const int to = a.ppo <= kPktPerStage ? pg * nsub + sI : pg / pgs_per_out;
             const int64_t o = ((int64_t)to * a.nbeam + beam) * ngrp + g;
             if (a.out_f32) a.out_f32[o] = P;
@@ -327,14 +388,17 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
                                DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
           break;
         tc_fence_after();
-        const uint32_t wpol = wsm + (uint32_t)pol * (2 * kWTileBytes);
+        const uint32_t wpol = wsm + (uint32_t)pol * (TT::kKB * kWTileBytes);
         const uint32_t stage = dsm + (uint32_t)s * kStageBytes;
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {   // K = 128 bf16 = 8 x 16
+        for (int kk = 0; kk < 4 * TT::kKB; ++kk) {   // 32-byte K steps (16 bf16 / 32 e4m3)
           const uint32_t kb = kk >> 2, koff = 32u * (kk & 3);
           const uint64_t ad = umma_desc_sw128(wpol + kb * kWTileBytes + koff, 1024u);
           const uint64_t bd = umma_desc_sw128(stage + kb * kDTileBytes + koff, 1024u);
-          umma_f16(tmem + (uint32_t)b * 256u, ad, bd, kIdesc, kk > 0);
+          if constexpr (kFp8)
+            umma_f8(tmem + (uint32_t)b * 256u, ad, bd, TT::kIdesc, kk > 0);
+          else
+            umma_f16(tmem + (uint32_t)b * 256u, ad, bd, TT::kIdesc, kk > 0);
         }
         umma_commit(&empty_bar[s]);
         umma_commit(&tfull_bar[b]);
@@ -357,11 +421,12 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   }
 }
 
-int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
+template <bool kFp8>
+static int launch_bf(const BfArgs &a, int num_sms, cudaStream_t st) {
   static bool attr_done = false;
   if (!attr_done) {
-    if (cudaFuncSetAttribute(bf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bf::kSmemBytes) != cudaSuccess)
+    if (cudaFuncSetAttribute(bf_kernel<kFp8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bf::T<kFp8>::kSmemBytes) != cudaSuccess)
       return -2;
     attr_done = true;
   }
@@ -373,10 +438,14 @@ int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
   if (nslots > nchunks) nslots = nchunks;
   const int grid = nslots * nbt;
   void *args[] = {(void *)&a};
-  return cudaLaunchKernel((const void *)bf_kernel, dim3(grid), dim3(bf::kThreads), args,
-                          bf::kSmemBytes, st) == cudaSuccess
+  return cudaLaunchKernel((const void *)bf_kernel<kFp8>, dim3(grid), dim3(bf::kThreads), args,
+                          bf::T<kFp8>::kSmemBytes, st) == cudaSuccess
              ? 0
              : -2;
+}
+
+int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
+  return a.fp8 ? launch_bf<true>(a, num_sms, st) : launch_bf<false>(a, num_sms, st);
 }
 
 }  // namespace dsax

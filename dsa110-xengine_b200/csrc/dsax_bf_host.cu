@@ -1,5 +1,6 @@
 // dsax_bf_host.cu -- beamformer entry points of the C-ABI and the host-side
 // conversion of FP64 weights to the BF16 UMMA operand image.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -31,6 +32,31 @@ uint32_t sw128_off(uint32_t row, uint32_t chunk) {
 
 constexpr size_t kWTile = 16384;  // 128 rows x 128 B
 constexpr size_t kWPerGB = 4 * kWTile;  // [2 pol][2 kb] per (group, beam tile)
+constexpr size_t kWPerGB8 = 2 * kWTile;  // FP8: [2 pol][1 kb] per (group, beam tile)
+
+// FP32 -> E4M3 (1 sign, 4 exponent bits with bias 7, 3 mantissa bits; no
+// infinities, 0x7F/0xFF are NaN), round to nearest even, saturating at 448.
+uint8_t f32_to_e4m3_rne(float f) {
+  const uint8_t sign = std::signbit(f) ? 0x80 : 0x00;
+  double a = std::fabs((double)f);
+  if (std::isnan(f)) return 0x7F;
+  if (a == 0.0) return sign;
+  if (a >= 448.0) return sign | 0x7E;
+  int e = (int)std::floor(std::log2(a));
+  if (e < -6) {   // subnormal: units of 2^-9
+    const double m = std::nearbyint(std::ldexp(a, 9));
+    return sign | (uint8_t)m;   // m == 8 is the smallest normal, 0x08
+  }
+  if (std::ldexp(1.0, e) > a) --e;          // guard against log2 rounding
+  if (std::ldexp(1.0, e + 1) <= a) ++e;
+  double m = std::nearbyint((a / std::ldexp(1.0, e) - 1.0) * 8.0);
+  if (m >= 8.0) {
+    m = 0.0;
+    ++e;
+  }
+  if (e > 8 || (e == 8 && m > 6.0)) return sign | 0x7E;
+  return sign | (uint8_t)(((e + 7) << 3) | (int)m);
+}
 
 }  // namespace
 
@@ -70,6 +96,40 @@ int dsax_set_weights(dsax_ctx *c, const double *wre, const double *wim) {
                                   cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "upload weights");
+  // FP8 E4M3 image with one power-of-two scale: q = e4m3(2^s w), s chosen
+  // so that the largest |coefficient| lands in [128, 256) (E4M3 tops out at
+  // 448).  E4M3's relative precision does not depend on the magnitude, so
+  // one scale serves every antenna whose weights lie within 2^13 of the
+  // largest; the epilogue multiplies the power by 2^-2s.
+  {
+    double mx = 0.0;
+    for (size_t i = 0; i < (size_t)ngrp * 2 * nbeam * 64; ++i)
+      mx = std::max(mx, std::max(std::fabs(wre[i]), std::fabs(wim[i])));
+    const int es = mx > 0.0 ? std::min(60, std::max(-60, 7 - (int)std::floor(std::log2(mx)))) : 0;
+    const size_t nb8 = (size_t)ngrp * nbt * kWPerGB8;
+    std::vector<uint8_t> img8(nb8, 0);
+    for (int g = 0; g < ngrp; ++g)
+      for (int bt = 0; bt < nbt; ++bt)
+        for (int pol = 0; pol < 2; ++pol)
+          for (int m = 0; m < 128; ++m)
+            for (int ant = 0; ant < 64; ++ant) {
+              const int beam = 64 * bt + (m & 63);
+              const size_t wi_ = (((size_t)g * 2 + pol) * nbeam + beam) * 64 + ant;
+              const double wr = wre[wi_], wi = wim[wi_];
+              const double sc = std::ldexp(1.0, es);
+              const double c0 = (m < 64 ? wr : wi) * sc, c1 = (m < 64 ? -wi : wr) * sc;
+              const size_t off = (((size_t)(g * nbt + bt) * 2 + pol)) * kWTile +
+                                 sw128_off((uint32_t)m, (uint32_t)(ant / 8)) + 2 * (ant % 8);
+              img8[off] = f32_to_e4m3_rne((float)c0);
+              img8[off + 1] = f32_to_e4m3_rne((float)c1);
+            }
+    if ((rc = ensure_buffer(c, c->aux[AUX_WIMG_FP8], nb8, "FP8 beamformer weights")) != DSAX_OK)
+      return rc;
+    e = cudaMemcpyAsync(c->aux[AUX_WIMG_FP8].ptr, img8.data(), nb8, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "upload FP8 weights");
+    c->fp8_pscale = (float)std::ldexp(1.0, -2 * es);
+  }
   c->weights_ready = 1;
   c->weights_nchan = c->cfg.nchan;
   return DSAX_OK;
@@ -134,6 +194,12 @@ int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int
   a.ppo = ppo;
   a.scale = cf.bf_scale;
   a.wait_limit_ns = cf.wait_limit_ns;
+  a.pscale = 1.0f;
+  if (cf.bf_fp8) {   // E4M3 operands: weights scaled by 2^s, power by 2^-2s
+    a.fp8 = 1;
+    a.wimg = static_cast<const uint8_t *>(c->aux[AUX_WIMG_FP8].ptr);
+    a.pscale = c->fp8_pscale;
+  }
   if (c->agc_on) {   // per-beam scale from the previous blocks; this block's power for the next
     a.agc_scale = agc_scale_ptr(c->aux[AUX_AGC].ptr, cf.nbeam);
     a.beam_power = agc_power_ptr(c->aux[AUX_AGC].ptr, cf.nbeam);

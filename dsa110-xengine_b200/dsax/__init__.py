@@ -52,6 +52,7 @@ class Config(ctypes.Structure):
         ("bf_scale", ctypes.c_float),
         ("wait_limit_ns", ctypes.c_ulonglong),
         ("corr_path", ctypes.c_int),
+        ("bf_fp8", ctypes.c_int),
     ]
 
 

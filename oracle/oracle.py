@@ -182,6 +182,30 @@ def quantize_u8(power: np.ndarray, scale: float) -> np.ndarray:
     return np.clip(np.rint(power * scale), 0, 255).astype(np.uint8)
 
 
+def e4m3(x: np.ndarray) -> np.ndarray:
+    """Values of FP32(x) rounded to FP8 E4M3 (3 mantissa bits, exponent
+    -6..8, subnormal step 2^-9, round to nearest even, saturating at 448)."""
+    x32 = np.asarray(x, np.float32).astype(np.float64)
+    a = np.abs(x32)
+    out = np.zeros_like(a)
+    nz = a > 0
+    e = np.maximum(np.floor(np.log2(a[nz])), -6.0)
+    step = np.ldexp(1.0, (e - 3).astype(np.int64))
+    out[nz] = np.minimum(np.rint(a[nz] / step) * step, 448.0)
+    return np.copysign(out, x32)
+
+
+def fp8_weights(wre: np.ndarray, wim: np.ndarray):
+    """The FP8 beamformer's effective weights: one power-of-two scale 2^s
+    with the largest |coefficient| times 2^s in [128, 256), and
+    w = 2^-s e4m3(2^s w).  wre, wim: [ngrp][2][nbeam][64].  Returns
+    (wre_q, wim_q, s)."""
+    mx = max(float(np.abs(wre).max()), float(np.abs(wim).max()))
+    s = int(np.clip(7 - np.floor(np.log2(mx)), -60, 60)) if mx > 0 else 0
+    sc = np.ldexp(1.0, s)
+    return e4m3(wre * sc) / sc, e4m3(wim * sc) / sc, s
+
+
 def quantize_u8_agc(power: np.ndarray, bp: np.ndarray) -> np.ndarray:
     """AGC requantisation of src/dsaX_beamformer.cu adder (:150-156):
     rint(P * bp[beam]) / 2 (integer division), saturated to [0, 255]

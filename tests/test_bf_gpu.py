@@ -146,3 +146,48 @@ def test_agc_bandpass_sequence(dsax, oracle):
             if k >= 8:
                 clamped += int(np.sum(np.abs(ref.hist.mean(axis=0) - ref.medbp) / ref.medbp > 0.1))
     assert clamped > 0
+
+
+@pytest.mark.parametrize("weights", ["unit", "calibrated"])
+def test_beamformer_fp8(dsax, oracle, weights):
+    """FP8 E4M3 operands (kind::f8f6f4) with one power-of-two weight scale
+    (calibrated: gains spread over e^6 between antennas): against the FP64
+    oracle run with the same E4M3-rounded
+    weights the FP32 power agrees to 1e-4 (the data are exact in E4M3 and
+    the products exact in FP32); against the unrounded FP64 weights the
+    error is the weight rounding (3 mantissa bits), reported and bounded."""
+    import torch
+    npkt, nant, nchan, nbeam, ppo = 64, 63, 16, 256, 16
+    if weights == "unit":
+        wre, wim = oracle.random_phase_weights(51, nchan // 8, nbeam)
+    else:
+        rng = np.random.default_rng(8)
+        cal = rng.normal(size=(64, nchan // 8, 2, 2)) * np.exp(rng.uniform(-3, 3, 64))[:, None, None, None]
+        wre, wim = oracle.geometric_weights(rng.uniform(-600, 600, 64), cal, np.zeros(64, np.int32),
+                                            nchan // 8, nbeam)
+    qre, qim, _ = oracle.fp8_weights(wre, wim)
+    if weights == "calibrated":
+        amax = np.maximum(np.abs(wre), np.abs(wim)).max(axis=(0, 1, 2))
+        assert amax.max() / amax.min() > 64
+    # uniform data: every 4-bit value, -8 included, in every nibble position
+    blk = oracle.gen_block(61, npkt, nant, nchan, "uniform" if weights == "unit" else "gauss")
+    ref_q = oracle.beamform_power(blk, qre, qim, pkt_per_out=ppo)
+    ref = oracle.beamform_power(blk, wre, wim, pkt_per_out=ppo)
+    scale = 128.0 / float(np.median(ref))
+    cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
+                              bf_pkt_per_out=ppo, bf_scale=scale, bf_fp8=1)
+    with dsax.Context(cfg) as ctx:
+        ctx.set_weights(wre, wim)
+        d_in = torch.from_numpy(blk.reshape(-1)).cuda()
+        n = ref.size
+        u8 = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        f32 = torch.zeros(n, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.beamform(d_in, u8, f32)
+        ctx.sync()
+        got = f32.cpu().numpy().reshape(ref.shape).astype(np.float64)
+    rel_q = np.abs(got - ref_q) / np.maximum(ref_q, 1e-30)
+    assert rel_q.max() < 1e-4, rel_q.max()
+    rel = np.abs(got - ref) / np.maximum(ref, 1e-30)
+    print(f"FP8 vs FP64 weights: mean rel {rel.mean():.2e}, max rel {rel.max():.2e}")
+    assert rel.mean() < 2e-2
