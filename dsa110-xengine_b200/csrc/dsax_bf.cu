@@ -84,6 +84,21 @@ __device__ __forceinline__ uint32_t nib2_to_e4m3x4(uint32_t s) {
   return A | B | ((B + 0x7F7F7F7Fu) & 0x80808080u);
 }
 
+// As nib2_to_e4m3x4, each value times 2^d of its antenna: `add` holds 8d
+// mod 128 per output byte ([d_a, d_a, d_b, d_b]), d in [-6, 5].  The
+// exponent field of every nonzero code moves by d (the magnitude codes of
+// 1..8 have exponents 7..10, so the result stays normal and below 0x7F);
+// zero stays zero.  m + add stays below 0x100 in every byte, so no carry
+// crosses bytes; the mask to 7 bits drops the mod-128 wrap of negative d.
+__device__ __forceinline__ uint32_t nib2_to_e4m3x4_shift(uint32_t s, uint32_t add) {
+  const uint32_t A = prmt_sx(0x44403800u, 0x4e4c4a48u, s);
+  const uint32_t B = prmt_sx(0x4a4c4e50u, 0x38404448u, s ^ 0x8888u);
+  const uint32_t m = A | B;                                        // |code|, 0 for 0
+  const uint32_t nz = prmt_sx(m + 0x7F7F7F7Fu, 0u, 0xBA98u);        // 0xFF where nonzero
+  const uint32_t r = m + (add & nz);
+  return (r & 0x7F7F7F7Fu) | ((B + 0x7F7F7F7Fu) & 0x80808080u);
+}
+
 // Unit u of a CTA's range: r = u / 2 enumerates (channel group g, packet
 // group pg) as g * npg + pg; pol = u % 2.  The beam tile is fixed per CTA.
 __device__ __forceinline__ void bf_decode(int u, int npg, int &g, int &pg, int &pol) {
@@ -176,6 +191,17 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
     // group's copies.
     const uint32_t myraw = raw + 16u * (uint32_t)tid;
     uint4 Ucur[8];
+    // FP8: exponent offsets 8d of this thread's 8 antennas, one byte per
+    // E4M3 output byte ([re, im] per antenna, two antennas per word)
+    uint32_t shift_add[4] = {0u, 0u, 0u, 0u};
+    if (kFp8 && a.e4m3_add) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t a0 = (uint32_t)a.e4m3_add[8 * j + 2 * e] & 0x7Fu;
+        const uint32_t a1 = (uint32_t)a.e4m3_add[8 * j + 2 * e + 1] & 0x7Fu;
+        shift_add[e] = a0 | (a0 << 8) | (a1 << 16) | (a1 << 24);
+      }
+    }
     auto stage_group = [&](int r) {
       const int g = r / npg, pg = r % npg;
       const int p = pg * kPktPerStage + q;
@@ -236,7 +262,12 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
           for (int odd = 0; odd < 2; ++odd) {
             uint32_t o[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) o[e] = nib2_to_e4m3x4(t[e >> 1][e & 1] >> (16 * odd));
+            for (int e = 0; e < 4; ++e) {
+              const uint32_t sel2 = t[e >> 1][e & 1] >> (16 * odd);
+              // per-antenna power-of-two scale only where the weights need it
+              // (uniform branch)
+              o[e] = a.e4m3_add ? nib2_to_e4m3x4_shift(sel2, shift_add[e]) : nib2_to_e4m3x4(sel2);
+            }
             const int k = 8 * kh + 2 * w + odd;       // chunnel = 2*chan + time
             st_shared_v4(tile + sw128_offset((uint32_t)(16 * q + k), (uint32_t)j), o[0], o[1], o[2],
                          o[3]);

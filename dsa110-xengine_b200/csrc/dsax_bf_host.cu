@@ -96,16 +96,45 @@ int dsax_set_weights(dsax_ctx *c, const double *wre, const double *wim) {
                                   cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "upload weights");
-  // FP8 E4M3 image with one power-of-two scale: q = e4m3(2^s w), s chosen
-  // so that the largest |coefficient| lands in [128, 256) (E4M3 tops out at
-  // 448).  E4M3's relative precision does not depend on the magnitude, so
-  // one scale serves every antenna whose weights lie within 2^13 of the
-  // largest; the epilogue multiplies the power by 2^-2s.
+  // FP8 E4M3 image with a per-antenna power-of-two scale.  Antenna a's
+  // ideal exponent e_a puts its largest |coefficient| times 2^e_a in
+  // [128, 256) (E4M3 tops out at 448).  The data of antenna a are scaled by
+  // 2^d_a (an exponent shift in the kernel, exact for 4-bit integers while
+  // d_a is in [-6, 5]) and its weights stored as q = e4m3(2^(E - d_a) w), so
+  // every product carries the common factor 2^E, which the epilogue removes
+  // from the power (2^-2E).  E = max(min e, max e - 6), at most min e + 5,
+  // keeps d_a = E - e_a in range for spreads up to 11 octaves; beyond that
+  // the antennas with the smallest weights are clamped (scaled by less than
+  // their ideal 2^e_a, so they lose precision but never saturate).  Equal
+  // exponents (for instance unit-magnitude weights) need no shift at all.
   {
-    double mx = 0.0;
-    for (size_t i = 0; i < (size_t)ngrp * 2 * nbeam * 64; ++i)
-      mx = std::max(mx, std::max(std::fabs(wre[i]), std::fabs(wim[i])));
-    const int es = mx > 0.0 ? std::min(60, std::max(-60, 7 - (int)std::floor(std::log2(mx)))) : 0;
+    int ea[64];
+    bool live[64];
+    int emin = 1 << 20, emax = -(1 << 20);
+    for (int ant = 0; ant < 64; ++ant) {
+      double mx = 0.0;
+      for (int g = 0; g < ngrp; ++g)
+        for (int pol = 0; pol < 2; ++pol)
+          for (int b = 0; b < nbeam; ++b) {
+            const size_t wi_ = (((size_t)g * 2 + pol) * nbeam + b) * 64 + ant;
+            mx = std::max(mx, std::max(std::fabs(wre[wi_]), std::fabs(wim[wi_])));
+          }
+      live[ant] = mx > 0.0;
+      ea[ant] = live[ant] ? std::min(50, std::max(-50, 7 - (int)std::floor(std::log2(mx)))) : 0;
+      if (live[ant]) {
+        emin = std::min(emin, ea[ant]);
+        emax = std::max(emax, ea[ant]);
+      }
+    }
+    const int E = emin <= emax ? std::min(emin + 5, std::max(emin, emax - 6)) : 0;
+    int d[64];
+    signed char add[64];
+    bool any = false;
+    for (int ant = 0; ant < 64; ++ant) {
+      d[ant] = live[ant] ? std::min(5, std::max(-6, E - ea[ant])) : 0;
+      add[ant] = (signed char)(d[ant] * 8);
+      any |= d[ant] != 0;
+    }
     const size_t nb8 = (size_t)ngrp * nbt * kWPerGB8;
     std::vector<uint8_t> img8(nb8, 0);
     for (int g = 0; g < ngrp; ++g)
@@ -116,19 +145,23 @@ int dsax_set_weights(dsax_ctx *c, const double *wre, const double *wim) {
               const int beam = 64 * bt + (m & 63);
               const size_t wi_ = (((size_t)g * 2 + pol) * nbeam + beam) * 64 + ant;
               const double wr = wre[wi_], wi = wim[wi_];
-              const double sc = std::ldexp(1.0, es);
+              const double sc = std::ldexp(1.0, E - d[ant]);
               const double c0 = (m < 64 ? wr : wi) * sc, c1 = (m < 64 ? -wi : wr) * sc;
               const size_t off = (((size_t)(g * nbt + bt) * 2 + pol)) * kWTile +
                                  sw128_off((uint32_t)m, (uint32_t)(ant / 8)) + 2 * (ant % 8);
               img8[off] = f32_to_e4m3_rne((float)c0);
               img8[off + 1] = f32_to_e4m3_rne((float)c1);
             }
-    if ((rc = ensure_buffer(c, c->aux[AUX_WIMG_FP8], nb8, "FP8 beamformer weights")) != DSAX_OK)
+    if ((rc = ensure_buffer(c, c->aux[AUX_WIMG_FP8], nb8 + 256, "FP8 beamformer weights")) != DSAX_OK)
       return rc;
-    e = cudaMemcpyAsync(c->aux[AUX_WIMG_FP8].ptr, img8.data(), nb8, cudaMemcpyHostToDevice, c->stream);
+    uint8_t *d8 = static_cast<uint8_t *>(c->aux[AUX_WIMG_FP8].ptr);
+    e = cudaMemcpyAsync(d8, img8.data(), nb8, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d8 + nb8, add, 64, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "upload FP8 weights");
-    c->fp8_pscale = (float)std::ldexp(1.0, -2 * es);
+    c->fp8_pscale = (float)std::ldexp(1.0, -2 * E);
+    c->fp8_shift = any ? 1 : 0;
+    c->fp8_img_bytes = nb8;
   }
   c->weights_ready = 1;
   c->weights_nchan = c->cfg.nchan;
@@ -195,10 +228,13 @@ int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int
   a.scale = cf.bf_scale;
   a.wait_limit_ns = cf.wait_limit_ns;
   a.pscale = 1.0f;
-  if (cf.bf_fp8) {   // E4M3 operands: weights scaled by 2^s, power by 2^-2s
+  if (cf.bf_fp8) {   // E4M3 operands, per-antenna data exponents, power by 2^-2E
     a.fp8 = 1;
     a.wimg = static_cast<const uint8_t *>(c->aux[AUX_WIMG_FP8].ptr);
     a.pscale = c->fp8_pscale;
+    a.e4m3_add = c->fp8_shift
+                     ? reinterpret_cast<const signed char *>(a.wimg + c->fp8_img_bytes)
+                     : nullptr;
   }
   if (c->agc_on) {   // per-beam scale from the previous blocks; this block's power for the next
     a.agc_scale = agc_scale_ptr(c->aux[AUX_AGC].ptr, cf.nbeam);

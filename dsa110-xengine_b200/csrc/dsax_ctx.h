@@ -70,7 +70,9 @@ struct dsax_ctx {
   dsax::DevBuf vis_buf;   // host-mode staging: visibilities
   dsax::DevBuf aux[dsax::AUX_COUNT];   // per-stage buffers, indexed by dsax::AUX_*
   int agc_on = 0;         // beamformer uses (and updates) the AGC bandpass state
-  float fp8_pscale = 1.0f;   // 2^-2s for FP8 weights stored as e4m3(2^s w)
+  float fp8_pscale = 1.0f;   // 2^-2E: FP8 operands carry 2^E in every product
+  int fp8_shift = 0;         // FP8 data get a nonzero per-antenna exponent
+  size_t fp8_img_bytes = 0;  // FP8 weight image; the 64 exponent bytes follow it
   int weights_ready = 0;
   int weights_nchan = 0;      // channels covered by the weight image
   void *batch_plan = nullptr; // captured batch graph (dsax_batch.cu)

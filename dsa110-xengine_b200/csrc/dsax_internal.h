@@ -45,7 +45,8 @@ struct BfArgs {
   uint8_t *out_u8;         // [npkt/ppo][nbeam][nchan/8] Stokes-I uint8 (or null)
   float *out_f32;          // same layout, FP32 power before scaling (or null)
   float *out_fb;           // [nbeam][npkt/ppo][nchan/8] FP32 power (filterbank order, or null)
-  float pscale = 1.0f;     // power scale: 1 (BF16); FP8 2^-2s undoes the weights' 2^s
+  float pscale = 1.0f;     // power scale: 1 (BF16); FP8 2^-2E undoes the operands' 2^E
+  const signed char *e4m3_add;  // FP8: per-antenna data exponent 8d (64 entries) or null
   int fp8;                 // operands: 0 BF16 (kind::f16), 1 FP8 E4M3 (kind::f8f6f4)
   const float *agc_scale;  // per-beam AGC scale: u8 = rint(P * s) / 2 (or null: fixed scale)
   float *beam_power;       // per-beam total power of the block, accumulated (or null)

@@ -77,9 +77,9 @@ typedef struct dsax_config {
                             4 = as 3, fed by one bulk copy per 64-packet stage.
                             3 and 4 also select the feed for DSAX_FMT_CHANMAJOR */
     int bf_fp8;          /* beamformer operands: 0 BF16 (tcgen05 kind::f16), 1 FP8
-                            E4M3 weights e4m3(2^s w) with one power-of-two
-                            scale, undone on the power (kind::f8f6f4; the
-                            4-bit data are exact in E4M3) */
+                            E4M3 with a per-antenna power-of-two scale
+                            (kind::f8f6f4; the 4-bit data, shifted by the
+                            antenna's exponent, are exact in E4M3) */
 } dsax_config;
 
 typedef struct dsax_ctx dsax_ctx;

@@ -196,14 +196,21 @@ def e4m3(x: np.ndarray) -> np.ndarray:
 
 
 def fp8_weights(wre: np.ndarray, wim: np.ndarray):
-    """The FP8 beamformer's effective weights: one power-of-two scale 2^s
-    with the largest |coefficient| times 2^s in [128, 256), and
-    w = 2^-s e4m3(2^s w).  wre, wim: [ngrp][2][nbeam][64].  Returns
-    (wre_q, wim_q, s)."""
-    mx = max(float(np.abs(wre).max()), float(np.abs(wim).max()))
-    s = int(np.clip(7 - np.floor(np.log2(mx)), -60, 60)) if mx > 0 else 0
-    sc = np.ldexp(1.0, s)
-    return e4m3(wre * sc) / sc, e4m3(wim * sc) / sc, s
+    """The FP8 beamformer's effective weights with a per-antenna
+    power-of-two scale.  Antenna a's ideal exponent e_a puts its largest
+    |coefficient| times 2^e_a in [128, 256); E = max(min e, max e - 6),
+    at most min e + 5; the
+    data shift d_a = clip(E - e_a, -6, 5); the stored weight is
+    q = e4m3(2^(E - d_a) w), so the effective weight is 2^-(E - d_a) q.
+    wre, wim: [ngrp][2][nbeam][64].  Returns (wre_q, wim_q, d, E)."""
+    mx = np.maximum(np.abs(wre), np.abs(wim)).max(axis=(0, 1, 2))
+    live = mx > 0
+    ea = np.zeros(64, np.int64)
+    ea[live] = np.clip(7 - np.floor(np.log2(mx[live])), -50, 50).astype(np.int64)
+    E = int(min(ea[live].min() + 5, max(ea[live].min(), ea[live].max() - 6))) if live.any() else 0
+    d = np.where(live, np.clip(E - ea, -6, 5), 0)
+    sc = np.ldexp(1.0, E - d)
+    return e4m3(wre * sc) / sc, e4m3(wim * sc) / sc, d, E
 
 
 def quantize_u8_agc(power: np.ndarray, bp: np.ndarray) -> np.ndarray:
