@@ -448,7 +448,11 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
             const int P = 2 * (int)c + e + 8 * q;
             w[e][q] = P < pvalid ? rw[P * 64 + ant] : 0u;
           }
-        mbar_arrive(&rempty_bar[r]);   // raw stage consumed (generic-proxy reads only)
+        // The next bulk copy (async proxy) overwrites this stage: order these
+        // generic-proxy reads before it, or under load the copy can land
+        // first (a write-after-read race across proxies).
+        fence_proxy_async_smem();
+        mbar_arrive(&rempty_bar[r]);
         if (!unpack_store(ks, w)) break;
       }
     } else {
