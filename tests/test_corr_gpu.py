@@ -214,6 +214,31 @@ def test_correlate_many_device_pipelined(dsax, oracle, corr_path):
                                           oracle.correlate(b))
 
 
+def test_correlate_many_full_blocks_match_single_calls(dsax, oracle):
+    """Three full-size blocks [2048][63][384][2][2] through the pipelined
+    correlator (corner turn of block i+1 overlapped with the correlation of
+    block i) equal, bit for bit, one dsax_correlate call per block; one
+    channel per block also against the oracle."""
+    import torch
+    cfg = dsax.default_config()
+    blks = [oracle.gen_block(900 + k, 2048, 63, 384, "gauss") for k in range(3)]
+    n = 768 * 2080 * 8
+    with dsax.Context(cfg) as ctx:
+        d_in = [torch.from_numpy(b.reshape(-1)).cuda() for b in blks]
+        many = [torch.full((n,), -1.0, dtype=torch.float32, device="cuda") for _ in blks]
+        one = torch.zeros(n, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.correlate_many(d_in, many)
+        ctx.sync()
+        for k, (b, d, v) in enumerate(zip(blks, d_in, many)):
+            ctx.correlate(d, one, dsax.MEM_DEVICE)
+            ctx.sync()
+            assert torch.equal(v, one), k
+            c = 97 * k + 5
+            got = v.cpu().numpy().reshape(768, 2080, 4, 2)[2 * c:2 * c + 2]
+            np.testing.assert_array_equal(got, oracle.correlate(b, ch0=c, nch=1))
+
+
 def test_correlate_many_host_pipelined(dsax, oracle):
     """Host buffers in and out (copies overlapped with the device stages)."""
     cfg = dsax.default_config(npkt=128, nant_in=63, nchan=32)
