@@ -142,14 +142,16 @@ def test_ramp_block(dsax, oracle):
     np.testing.assert_array_equal(_run(dsax, blk), oracle.correlate(blk))
 
 
-def test_accumulate_integrates_blocks(dsax, oracle):
-    """accumulate=1 adds into vis like xGPU's device integration buffer."""
+@pytest.mark.parametrize("corr_path,nchan", [(0, 16), (3, 16), (0, 160)])
+def test_accumulate_integrates_blocks(dsax, oracle, corr_path, nchan):
+    """accumulate=1 adds into vis like xGPU's device integration buffer (160
+    channels: more CTAs than SMs)."""
     import torch
-    b1 = oracle.gen_block(1, 128, 63, 16, "gauss")
-    b2 = oracle.gen_block(2, 128, 63, 16, "gauss")
-    cfg = dsax.default_config(npkt=128, nant_in=63, nchan=16)
+    b1 = oracle.gen_block(1, 128, 63, nchan, "gauss")
+    b2 = oracle.gen_block(2, 128, 63, nchan, "gauss")
+    cfg = dsax.default_config(npkt=128, nant_in=63, nchan=nchan, corr_path=corr_path)
     with dsax.Context(cfg) as ctx:
-        vis = torch.zeros(32 * 2080 * 8, dtype=torch.float32, device="cuda")
+        vis = torch.zeros(2 * nchan * 2080 * 8, dtype=torch.float32, device="cuda")
         _run(dsax, b1, ctx=ctx, vis=vis, accumulate=True)
         got = _run(dsax, b2, ctx=ctx, vis=vis, accumulate=True)
     np.testing.assert_array_equal(got, oracle.correlate(b1) + oracle.correlate(b2))
