@@ -28,6 +28,7 @@ enum {
   AUX_PIPE = 15,           // correlate_many: double-buffered inputs, corner turns, visibilities
   AUX_AGC = 16,            // beamformer AGC: bandpass history, scales, per-beam power
   AUX_EXTRACT = 17,        // correlate_extract: device visibilities, input, product
+  AUX_LF_PAD = 18,         // learned flagger: two zero-bordered activation grids
   AUX_COUNT = 20
 };
 

@@ -49,14 +49,22 @@ size_t lf_part_floats(int B, int H);   // partial-gradient scratch size
 // Tensor-core inference (dsax_lflag_tc.cu).
 struct LfTcBuffers {
   const uint16_t *feat_bf16 = nullptr;  // [npx][8] BF16 features
-  uint16_t *act1 = nullptr;             // [npx][32] BF16
-  uint16_t *act2 = nullptr;             // [npx][64] BF16
+  uint16_t *act1p = nullptr;            // padded grid [B][H+2][W+2][64] BF16 (layer-1 output)
+  uint16_t *act2p = nullptr;            // padded grid [B][H+2][W+2][64] BF16 (layer-2 output)
   float *z9 = nullptr;                  // [9][npx] last-layer tap projections
   float *logit = nullptr;               // [npx] (may be null)
   uint8_t *mask = nullptr;              // [npx]
   const uint8_t *wimg = nullptr;        // weight images of layers 0..2 (lf_tc_wimg_bytes)
 };
 size_t lf_tc_wimg_bytes();
+// Padded-grid layers (dsax_lflag_tma.cu).
+size_t lf_pad_bytes(int B, int H, int W);   // one padded activation grid
+size_t lf_tma_wimg_bytes();
+int lf_tma_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st);
+int lf_pad_borders(uint16_t *act, int B, int H, int W, cudaStream_t st);
+int lf_tma_layers23(const LfNet &net, const uint8_t *wimg, const uint16_t *act1p, uint16_t *act2p,
+                    float *z9, int B, int H, int W, int num_sms, int *err, uint64_t wait_limit_ns,
+                    cudaStream_t st);
 int lf_tc_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st);
 int lf_tc_forward(const LfNet &net, const LfTcBuffers &bufs, int B, int H, int W, int guard,
                   const LfPerm &perm, int num_sms, int *err, uint64_t wait_limit_ns,

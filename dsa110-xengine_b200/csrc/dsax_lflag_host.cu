@@ -250,11 +250,15 @@ int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, in
   if ((rc = ensure_buffer(c, c->aux[AUX_LF_TCW], lf_tc_wimg_bytes(), "learned-flagger weight images")) !=
       DSAX_OK)
     return rc;
+  const size_t npad = lf_pad_bytes(B, H, W);
+  if ((rc = ensure_buffer(c, c->aux[AUX_LF_PAD], 2 * npad, "learned-flagger padded activations")) !=
+      DSAX_OK)
+    return rc;
   LfTcBuffers tb;
   uint16_t *fbf = reinterpret_cast<uint16_t *>(s.F);
   tb.feat_bf16 = fbf;
-  tb.act1 = reinterpret_cast<uint16_t *>(s.a1);
-  tb.act2 = reinterpret_cast<uint16_t *>(s.a2);
+  tb.act1p = static_cast<uint16_t *>(c->aux[AUX_LF_PAD].ptr);
+  tb.act2p = reinterpret_cast<uint16_t *>(static_cast<uint8_t *>(c->aux[AUX_LF_PAD].ptr) + npad);
   tb.z9 = s.a3;
   tb.logit = s.z;
   tb.mask = mem == DSAX_MEM_DEVICE ? mask : s.L;

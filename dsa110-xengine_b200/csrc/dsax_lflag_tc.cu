@@ -1,20 +1,22 @@
-// dsax_lflag_tc.cu -- learned-flagger inference on sm_100a tensor cores.
+// dsax_lflag_tc.cu -- learned-flagger inference on sm_100a tensor cores:
+// the first 3x3 layer (8 -> 32 channels), the 64 -> 1 tap sum and the mask;
+// the 64-channel layers are TMA-fed (dsax_lflag_tma.cu).
 //
-// Each 3x3 layer is an implicit GEMM: D[128 pixels x Cout] = A B^T with
+// The first layer is an implicit GEMM: D[128 pixels x Cout] = A B^T with
 // A row m = the pixel's 3x3 neighbourhood, K = 9 taps x Cin (k = tap * Cin
 // + ci, tap = 3 ky + kx, zero outside the image), and B = the layer's
 // weights W[co][tap][ci] in the same K order.  BF16 operands, FP32
-// accumulation in TMEM (tcgen05.mma kind::f16, M=128, N=Cout).
+// accumulation in TMEM (tcgen05.mma kind::f16, M=128, N=Cout).  With 8
+// input channels a tap is 16 bytes, too narrow for a swizzled TMA box, so
 //   warps 0-3 : producers.  Thread m gathers pixel m's eight 16-byte K
 //               chunks of a 64-wide K block straight into the 128-byte-
 //               swizzled A stage with cp.async (zero fill at the image
-//               border); it keeps all but two of the stages (6 to 12, as
-//               shared memory allows beside the weights) in flight and
+//               border); it keeps all but two of the stages in flight and
 //               marks a stage full once its own copies have landed.
-//   warps 4-7 : epilogue: TMEM -> + bias -> ReLU -> BF16 NHWC activations,
-//               or for the third layer the 9 per-tap projections onto the
-//               last layer's weights (the 64 -> 1 layer then only sums 9
-//               shifted values per pixel, lf_tapsum_kernel).
+//   warps 4-7 : epilogue: TMEM -> + bias -> ReLU -> BF16 activations, written
+//               into the zero-bordered 64-channel grid the next layer reads
+//               (pad_out), or, for a projection layer, the 9 per-tap
+//               projections onto the last layer's weights.
 //   warp  8   : TMEM allocation, weight image load (bulk copy, resident),
 //               single-thread UMMA issue.
 // Persistent CTAs walk 128-pixel tiles; TMEM holds two accumulators so the
@@ -50,6 +52,7 @@ struct LfTcArgs {
   int *err;
   int B, H, W;
   uint64_t wait_limit_ns;
+  int pad_out;          // 1: write the padded grid [B][H+2][W+2][64] (channels >= COUT zero)
 };
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
@@ -209,7 +212,15 @@ __global__ void __launch_bounds__(lftc::kThreads, 1) lf_conv_tc_kernel(LfTcArgs 
           a.z9[(int64_t)tap * npx + p] = z0 + z1;
         }
       } else {
-        uint4 *dst = reinterpret_cast<uint4 *>(a.out + (int64_t)p * COUT);
+        uint4 *dst;
+        if (a.pad_out) {   // padded grid: pixel (b, h + 1, w + 1) of [B][H+2][W+2][64]
+          const int w = p % a.W, h = (p / a.W) % a.H, b = p / (a.W * a.H);
+          dst = reinterpret_cast<uint4 *>(a.out + (((int64_t)b * (a.H + 2) + h + 1) * (a.W + 2) + w + 1) * 64);
+#pragma unroll
+          for (int c = COUT / 8; c < 8; ++c) dst[c] = make_uint4(0u, 0u, 0u, 0u);
+        } else {
+          dst = reinterpret_cast<uint4 *>(a.out + (int64_t)p * COUT);
+        }
 #pragma unroll
         for (int c = 0; c < COUT / 8; ++c)
           dst[c] = make_uint4(pack_bf16x2(v[8 * c], v[8 * c + 1]), pack_bf16x2(v[8 * c + 2], v[8 * c + 3]),
@@ -330,39 +341,37 @@ int conv_tc_launch(const LfTcArgs &a, int num_sms, cudaStream_t st) {
 
 }  // namespace
 
-size_t lf_tc_wimg_bytes() {
-  size_t n = 0;
-  for (int l = 0; l < 3; ++l) n += (size_t)((9 * kLfCin[l] + 63) / 64) * kLfCout[l] * 128;
-  return n;
-}
+// Weight images: layer 0 in the gather layout (K = 9 taps x 8 channels in
+// 64-wide blocks), then layers 1 and 2 in the padded-grid layout
+// (dsax_lflag_tma.cu).
+static size_t lf_l0_wimg_bytes() { return (size_t)((9 * kLfCin[0] + 63) / 64) * kLfCout[0] * 128; }
+
+size_t lf_tc_wimg_bytes() { return lf_l0_wimg_bytes() + lf_tma_wimg_bytes(); }
 
 int lf_tc_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st) {
-  size_t o = 0;
-  for (int l = 0; l < 3; ++l) {
-    const int nkb = (9 * kLfCin[l] + 63) / 64;
-    lf_tc_wimg_kernel<<<64, 256, 0, st>>>(net.w[l], wimg + o, kLfCin[l], kLfCout[l], nkb);
-    o += (size_t)nkb * kLfCout[l] * 128;
-  }
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+  lf_tc_wimg_kernel<<<64, 256, 0, st>>>(net.w[0], wimg, kLfCin[0], kLfCout[0],
+                                        (9 * kLfCin[0] + 63) / 64);
+  if (cudaGetLastError() != cudaSuccess) return -2;
+  return lf_tma_prepare(net, wimg + lf_l0_wimg_bytes(), st);
 }
 
+// Forward pass: layer 1 (8 -> 32, per-pixel gather) into the padded grid
+// act1p, layers 2 and 3 TMA-fed from the padded grids (dsax_lflag_tma.cu),
+// then the 64 -> 1 tap sum and the mask.
 int lf_tc_forward(const LfNet &net, const LfTcBuffers &bufs, int B, int H, int W, int guard,
                   const LfPerm &perm, int num_sms, int *err, uint64_t wait_limit_ns,
                   cudaStream_t st) {
-  static_assert(kLfCin[0] == 8 && kLfCout[0] == 32 && kLfCin[1] == 32 && kLfCout[1] == 64 &&
-                    kLfCin[2] == 64 && kLfCout[2] == 64 && kLfCin[3] == 64 && kLfCout[3] == 1,
+  static_assert(kLfCin[0] == 8 && kLfCout[0] == 32 && kLfCin[3] == 64 && kLfCout[3] == 1,
                 "tensor-core path is written for the 8-32-64-64-1 net");
-  const size_t o1 = (size_t)((9 * 8 + 63) / 64) * 32 * 128;
-  const size_t o2 = o1 + (size_t)((9 * 32 + 63) / 64) * 64 * 128;
   LfTcArgs a{};
   a.B = B; a.H = H; a.W = W; a.err = err; a.wait_limit_ns = wait_limit_ns;
-  a.in = bufs.feat_bf16; a.wimg = bufs.wimg; a.bias = net.b[0]; a.out = bufs.act1;
-  int e = conv_tc_launch<8, 32, false>(a, num_sms, st);
-  a.in = bufs.act1; a.wimg = bufs.wimg + o1; a.bias = net.b[1]; a.out = bufs.act2;
-  e |= conv_tc_launch<32, 64, false>(a, num_sms, st);
-  a.in = bufs.act2; a.wimg = bufs.wimg + o2; a.bias = net.b[2]; a.out = nullptr;
-  a.w4 = net.w[3]; a.z9 = bufs.z9;
-  e |= conv_tc_launch<64, 64, true>(a, num_sms, st);
+  a.in = bufs.feat_bf16; a.wimg = bufs.wimg; a.bias = net.b[0]; a.out = bufs.act1p;
+  a.pad_out = 1;
+  int e = lf_pad_borders(bufs.act1p, B, H, W, st);
+  e |= lf_pad_borders(bufs.act2p, B, H, W, st);
+  e |= conv_tc_launch<8, 32, false>(a, num_sms, st);
+  e |= lf_tma_layers23(net, bufs.wimg + lf_l0_wimg_bytes(), bufs.act1p, bufs.act2p, bufs.z9, B, H, W,
+                       num_sms, err, wait_limit_ns, st);
   lf_tapsum_kernel<<<1024, 256, 0, st>>>(bufs.z9, net.b[3], bufs.logit, bufs.mask, B, H, W, guard,
                                          0.0f, perm);
   if (cudaGetLastError() != cudaSuccess) e = -2;

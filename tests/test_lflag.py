@@ -95,13 +95,15 @@ def test_features_match_oracle(dsax, oracle):
 
 
 @pytest.mark.gpu
-def test_tensor_core_inference_matches_oracle(dsax, oracle):
-    """dsax_flag_learned (tcgen05 BF16 implicit-GEMM convolutions) against
-    the oracle's restatement of the same arithmetic (BF16 operands, wide
-    accumulation): logits within 5e-3 of their scale, the mask identical
-    away from the decision boundary."""
+@pytest.mark.parametrize("B", [6, 40])
+def test_tensor_core_inference_matches_oracle(dsax, oracle, B):
+    """dsax_flag_learned (tcgen05 BF16 implicit-GEMM convolutions, the
+    64-channel layers TMA-fed from zero-bordered grids) against the oracle's
+    restatement of the same arithmetic (BF16 operands, wide accumulation):
+    logits within 5e-3 of their scale, the mask identical away from the
+    decision boundary.  40 beams: several 128-pixel tiles per CTA."""
     import torch
-    B, T, C, tds = 6, 1024, 48, 32
+    T, C, tds = 1024, 48, 32
     x, _ = oracle.gen_filterbank(21, nbeam=B, ntime=T, nchan=C)
     p = dsax.flag_params(B, T, C)
     rng = np.random.default_rng(9)
