@@ -507,7 +507,8 @@ __global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(Fla
       asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.y) : "f"(f.w), "f"(f.z));
       asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.z) : "f"(g.y), "f"(g.x));
       asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.w) : "f"(g.w), "f"(g.z));
-      reinterpret_cast<uint4 *>(Fbf)[(int64_t)b * H * C + i] = o;
+      // zero-bordered grid [B][H+2][C+2][8] read by the first conv layer
+      reinterpret_cast<uint4 *>(Fbf)[((int64_t)b * (H + 2) + h + 1) * (C + 2) + c + 1] = o;
     }
   }
 }

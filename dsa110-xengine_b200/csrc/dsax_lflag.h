@@ -48,7 +48,7 @@ size_t lf_part_floats(int B, int H);   // partial-gradient scratch size
 
 // Tensor-core inference (dsax_lflag_tc.cu).
 struct LfTcBuffers {
-  const uint16_t *feat_bf16 = nullptr;  // [npx][8] BF16 features
+  uint16_t *featp = nullptr;            // padded grid [B][H+2][W+2][8] BF16 features
   uint16_t *act1p = nullptr;            // padded grid [B][H+2][W+2][64] BF16 (layer-1 output)
   uint16_t *act2p = nullptr;            // padded grid [B][H+2][W+2][64] BF16 (layer-2 output)
   float *z9 = nullptr;                  // [9][npx] last-layer tap projections
@@ -61,7 +61,11 @@ size_t lf_tc_wimg_bytes();
 size_t lf_pad_bytes(int B, int H, int W);   // one padded activation grid
 size_t lf_tma_wimg_bytes();
 int lf_tma_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st);
-int lf_pad_borders(uint16_t *act, int B, int H, int W, cudaStream_t st);
+size_t lf_feat_pad_bytes(int B, int H, int W);   // the padded feature grid
+int lf_pad_borders(uint16_t *grid, int B, int H, int W, int chunks, cudaStream_t st);
+int lf_tma_layer1(const LfNet &net, const uint8_t *wimg, const uint16_t *featp, uint16_t *act1p,
+                  int B, int H, int W, int num_sms, int *err, uint64_t wait_limit_ns,
+                  cudaStream_t st);
 int lf_tma_layers23(const LfNet &net, const uint8_t *wimg, const uint16_t *act1p, uint16_t *act2p,
                     float *z9, int B, int H, int W, int num_sms, int *err, uint64_t wait_limit_ns,
                     cudaStream_t st);

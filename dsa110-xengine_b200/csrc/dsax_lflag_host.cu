@@ -250,15 +250,24 @@ int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, in
   if ((rc = ensure_buffer(c, c->aux[AUX_LF_TCW], lf_tc_wimg_bytes(), "learned-flagger weight images")) !=
       DSAX_OK)
     return rc;
-  const size_t npad = lf_pad_bytes(B, H, W);
-  if ((rc = ensure_buffer(c, c->aux[AUX_LF_PAD], 2 * npad, "learned-flagger padded activations")) !=
-      DSAX_OK)
+  // zero-bordered grids: layer-1 output, layer-2 output, features
+  const size_t npad = lf_pad_bytes(B, H, W), nfeat = lf_feat_pad_bytes(B, H, W);
+  void *const prev_pad = c->aux[AUX_LF_PAD].ptr;
+  if ((rc = ensure_buffer(c, c->aux[AUX_LF_PAD], 2 * npad + nfeat,
+                          "learned-flagger padded activations")) != DSAX_OK)
     return rc;
+  uint8_t *const padb = static_cast<uint8_t *>(c->aux[AUX_LF_PAD].ptr);
+  // Channels 32-63 of the layer-1 grid are never written: zero them with the
+  // new allocation (the interior of each call's grid is then fully defined).
+  if (c->aux[AUX_LF_PAD].ptr != prev_pad) {
+    cudaError_t ce = cudaMemsetAsync(padb, 0, npad, c->stream);
+    if (ce != cudaSuccess) return cuda_check(c, ce, "padded grid clear");
+  }
   LfTcBuffers tb;
-  uint16_t *fbf = reinterpret_cast<uint16_t *>(s.F);
-  tb.feat_bf16 = fbf;
-  tb.act1p = static_cast<uint16_t *>(c->aux[AUX_LF_PAD].ptr);
-  tb.act2p = reinterpret_cast<uint16_t *>(static_cast<uint8_t *>(c->aux[AUX_LF_PAD].ptr) + npad);
+  uint16_t *fbf = reinterpret_cast<uint16_t *>(padb + 2 * npad);
+  tb.featp = fbf;
+  tb.act1p = reinterpret_cast<uint16_t *>(padb);
+  tb.act2p = reinterpret_cast<uint16_t *>(padb + npad);
   tb.z9 = s.a3;
   tb.logit = s.z;
   tb.mask = mem == DSAX_MEM_DEVICE ? mask : s.L;

@@ -319,22 +319,266 @@ __global__ void lf_tma_wimg_kernel(const float *w, uint8_t *img, int cin, int co
   }
 }
 
-// Zeroes the border pixels (all 64 channels) of a padded activation grid.
-__global__ void lf_pad_border_kernel(uint16_t *act, int B, int H, int W) {
+// Zeroes the border pixels of a padded grid of `chunks` 16-byte chunks per
+// pixel (8 for 64 BF16 channels, 1 for the 8 BF16 features).
+__global__ void lf_pad_border_kernel(uint16_t *act, int B, int H, int W, int chunks) {
   const int Hp = H + 2, Wp = W + 2;
   const int per = 2 * Wp + 2 * H;   // border pixels per image
-  const int64_t n = (int64_t)B * per * 8;   // 16-byte chunks
+  const int64_t n = (int64_t)B * per * chunks;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int chunk = (int)(i & 7);
-    const int64_t q = i >> 3;
+    const int chunk = (int)(i % chunks);
+    const int64_t q = i / chunks;
     const int b = (int)(q / per), k = (int)(q % per);
     int hq, wq;
     if (k < Wp) { hq = 0; wq = k; }
     else if (k < 2 * Wp) { hq = Hp - 1; wq = k - Wp; }
     else { const int k2 = k - 2 * Wp; hq = 1 + (k2 >> 1); wq = (k2 & 1) ? Wp - 1 : 0; }
     const int64_t pp = ((int64_t)b * Hp + hq) * Wp + wq;
-    reinterpret_cast<uint4 *>(act + pp * lftma::kC)[chunk] = make_uint4(0u, 0u, 0u, 0u);
+    reinterpret_cast<uint4 *>(act)[pp * chunks + chunk] = make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// First layer (8 -> 32 channels) from the zero-bordered feature grid
+// [B][H+2][W+2][8] BF16.  A tap is 16 bytes, too narrow for a swizzled box,
+// so per tile three unswizzled TMA boxes of 130 pixels x 16 B (one per
+// kernel row) land in a band slot, and four builder warps copy each pixel's
+// nine taps into the K-major 128-byte-swizzled A tile (K = 72 in two 64-wide
+// blocks, k = 8 tap + ci; the rest of the second block stays zero), then
+// 8 MMAs of N = 32.  The epilogue writes channels 0-31 of the interior
+// pixels of the 64-channel grid the next layer reads (channels 32-63 are
+// zero there).
+//   warps 0-3 : A-tile builders      warps 4-7 : epilogue
+//   warp  8   : TMA producer         warp  9   : TMEM, weights, UMMA issue
+namespace lf1 {
+constexpr int kThreads = 320;
+constexpr int kBandPix = 130;
+constexpr int kBandBytes = kBandPix * 16;           // 2,080
+constexpr int kBandStride = 2176;                   // 128-byte aligned band offset
+constexpr int kSlotBytes = 3 * kBandStride;         // 6,528
+constexpr int kSlotStride = 6656;                   // 128-byte aligned slot
+constexpr int kSlots = 8;
+constexpr int kABytes = 2 * 16384;                  // two K blocks of 128 x 128 B
+constexpr int kAStages = 4;
+constexpr int kCout = 32;
+constexpr int kWBytes = 2 * kCout * 128;            // B operand: two K blocks
+constexpr int kSmemBytes = 1024 + kWBytes + kAStages * kABytes + kSlots * kSlotStride;
+static_assert(kSmemBytes <= 227 * 1024, "shared memory budget");
+}  // namespace lf1
+
+struct Lf1Args {
+  const uint8_t *wimg;   // [2 K blocks][32 rows x 128 B], 128-byte swizzle
+  const float *bias;     // [32]
+  uint16_t *out;         // padded BF16 [npp][64]: channels 0-31 written
+  int *err;
+  int B, H, W;
+  uint64_t wait_limit_ns;
+};
+
+__global__ void __launch_bounds__(lf1::kThreads, 1)
+    lf_conv1_tma_kernel(const __grid_constant__ CUtensorMap tfeat, Lf1Args a) {
+  using namespace lf1;
+  constexpr uint32_t IDESC = umma_idesc(/*F32*/ 1, /*BF16*/ 1, /*BF16*/ 1, 128, kCout);
+  constexpr uint32_t TCOLS = 2 * kCout;   // 64
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bfull_bar[kSlots];
+  __shared__ __align__(8) uint64_t bempty_bar[kSlots];
+  __shared__ __align__(8) uint64_t afull_bar[kAStages];
+  __shared__ __align__(8) uint64_t aempty_bar[kAStages];
+  __shared__ __align__(8) uint64_t tfull_bar[2];
+  __shared__ __align__(8) uint64_t tempty_bar[2];
+  __shared__ __align__(8) uint64_t w_bar;
+  __shared__ __align__(8) uint64_t final_bar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+  __shared__ __align__(16) float s_bias[kCout];
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  uint8_t *const gbase = smem_raw + (base - smem_u32(smem_raw));
+  const uint32_t wsm = base;
+  const uint32_t a_base = base + kWBytes;                    // 1024-aligned (kWBytes = 8 KB)
+  const uint32_t b_base = a_base + kAStages * kABytes;
+  for (int i = tid; i < kCout; i += blockDim.x) s_bias[i] = a.bias[i];
+  // chunks 1-7 of every A stage's second K block are never written again
+  for (int i = tid; i < kAStages * 128 * 7; i += blockDim.x) {
+    const int st = i / (128 * 7), r = (i / 7) % 128, ch = 1 + i % 7;
+    *reinterpret_cast<uint4 *>(gbase + kWBytes + st * kABytes + 16384 + sw128_offset(r, ch)) =
+        make_uint4(0u, 0u, 0u, 0u);
+  }
+  fence_proxy_async_smem();
+
+  const int Hp = a.H + 2, Wp = a.W + 2;
+  const int npp = a.B * Hp * Wp;
+  const int ntiles = (npp + 127) / 128;
+  const int nmine = ntiles > (int)blockIdx.x ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+  if (tid == 0) {
+    for (int r = 0; r < kSlots; ++r) {
+      mbar_init(&bfull_bar[r], 1);
+      mbar_init(&bempty_bar[r], 128);
+    }
+    for (int s2 = 0; s2 < kAStages; ++s2) {
+      mbar_init(&afull_bar[s2], 128);
+      mbar_init(&aempty_bar[s2], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], 128);
+    }
+    mbar_init(&w_bar, 1);
+    mbar_init(&final_bar, 1);
+    abort_sh = 0;
+    mbar_fence_init();
+  }
+  if (warp == 9) {
+    tmem_alloc(&tmem_base_sh, TCOLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+
+  if (warp < 4) {
+    // ------------------------------------------------------------ A builders
+    const int m = tid;
+    for (int i = 0; i < nmine && !abort_sh; ++i) {
+      const int r = i % kSlots, s2 = i % kAStages;
+      if (!mbar_wait_bounded(&bfull_bar[r], (uint32_t)(i / kSlots) & 1u, &abort_sh, a.err,
+                             DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+        break;
+      uint4 t[9];
+      const uint8_t *slot = gbase + kWBytes + kAStages * kABytes + r * kSlotStride;
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap)
+        t[tap] = *reinterpret_cast<const uint4 *>(slot + (tap / 3) * kBandStride + (m + tap % 3) * 16);
+      // the next TMA load (async proxy) overwrites this slot: order the reads
+      fence_proxy_async_smem();
+      mbar_arrive(&bempty_bar[r]);
+      if (!mbar_wait_bounded(&aempty_bar[s2], ((uint32_t)(i / kAStages) & 1u) ^ 1u, &abort_sh, a.err,
+                             DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+        break;
+      uint8_t *as = gbase + kWBytes + s2 * kABytes;
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap)
+        *reinterpret_cast<uint4 *>(as + (tap / 8) * 16384 + sw128_offset((uint32_t)m, (uint32_t)(tap % 8))) =
+            t[tap];
+      fence_proxy_async_smem();
+      mbar_arrive(&afull_bar[s2]);
+    }
+  } else if (warp < 8) {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;
+    const int m = 32 * q + lane;
+    const bool small = npp < (1 << 24);
+    const float iWp = 1.0f / (float)Wp, iHp = 1.0f / (float)Hp;
+    for (int i = 0; i < nmine; ++i) {
+      const int bf = i & 1;
+      bool ok = mbar_wait_bounded(&tfull_bar[bf], (uint32_t)(i >> 1) & 1u, &abort_sh, a.err,
+                                  DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+      tc_fence_after();
+      ok = __all_sync(0xffffffffu, ok && !abort_sh);
+      float v[kCout];
+      if (ok) {
+        uint32_t rr[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(bf * kCout), rr);
+        tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 32; ++e) v[e] = __uint_as_float(rr[e]);
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty_bar[bf]);
+      const int pp = ((int)blockIdx.x + i * (int)gridDim.x) * 128 + m;
+      if (!ok || pp >= npp) continue;
+      const int r = small ? div_small(pp, Wp, iWp) : pp / Wp;
+      const int wq = pp - r * Wp;
+      const int b = small ? div_small(r, Hp, iHp) : r / Hp;
+      const int hq = r - b * Hp;
+      if (wq < 1 || wq > a.W || hq < 1 || hq > a.H) continue;
+#pragma unroll
+      for (int c = 0; c < kCout; ++c) v[c] = fmaxf(v[c] + s_bias[c], 0.0f);
+      uint4 *dst = reinterpret_cast<uint4 *>(a.out + (int64_t)pp * lftma::kC);
+#pragma unroll
+      for (int c = 0; c < kCout / 8; ++c)
+        dst[c] = make_uint4(tma_pack_bf16x2(v[8 * c], v[8 * c + 1]),
+                            tma_pack_bf16x2(v[8 * c + 2], v[8 * c + 3]),
+                            tma_pack_bf16x2(v[8 * c + 4], v[8 * c + 5]),
+                            tma_pack_bf16x2(v[8 * c + 6], v[8 * c + 7]));
+    }
+  } else if (warp == 8) {
+    // ------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tfeat)) : "memory");
+      int i = 0;
+      for (; i < nmine && !abort_sh; ++i) {
+        const int r = i % kSlots;
+        if (!mbar_wait_bounded(&bempty_bar[r], ((uint32_t)(i / kSlots) & 1u) ^ 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+          break;
+        const int p0 = ((int)blockIdx.x + i * (int)gridDim.x) * 128;
+        mbar_arrive_expect_tx(&bfull_bar[r], (uint32_t)(3 * kBandBytes));
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy)
+          tma_load_2d(b_base + (uint32_t)(r * kSlotStride + dy * kBandStride), &tfeat, 0,
+                      p0 + (dy - 1) * Wp - 1, &bfull_bar[r]);
+      }
+      // loads still landing after an abort: wait (bounded) before exiting
+      volatile int no_abort = 0;
+      for (int i2 = i - kSlots; i2 < i; ++i2)
+        if (i2 >= 0)
+          mbar_wait_bounded(&bfull_bar[i2 % kSlots], (uint32_t)(i2 / kSlots) & 1u, &no_abort, a.err,
+                            DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ weights + UMMA
+    if (lane == 0) {
+      mbar_arrive_expect_tx(&w_bar, (uint32_t)kWBytes);
+      bulk_g2s(wsm, a.wimg, (uint32_t)kWBytes, &w_bar);
+      const uint64_t adesc0 = umma_desc_sw128(a_base, 1024u);
+      const uint64_t bdesc0 = umma_desc_sw128(wsm, 1024u);
+      bool ok = mbar_wait_bounded(&w_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+      if (!ok) {   // the weight copy may still be landing
+        volatile int no_abort = 0;
+        mbar_wait_bounded(&w_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+      }
+      for (int i = 0; i < nmine && ok && !abort_sh; ++i) {
+        const int bf = i & 1, s2 = i % kAStages;
+        if (!mbar_wait_bounded(&tempty_bar[bf], ((uint32_t)(i >> 1) & 1u) ^ 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+          break;
+        if (!mbar_wait_bounded(&afull_bar[s2], (uint32_t)(i / kAStages) & 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+          break;
+        tc_fence_after();
+        const uint64_t ab = adesc0 + (uint64_t)(((uint32_t)s2 * kABytes) >> 4);
+        const uint32_t dcol = tmem + (uint32_t)(bf * kCout);
+#pragma unroll
+        for (int kb = 0; kb < 2; ++kb)
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk)
+            umma_f16(dcol, ab + (uint64_t)((kb * 16384 + 32 * kk) >> 4),
+                     bdesc0 + (uint64_t)((kb * kCout * 128 + 32 * kk) >> 4), IDESC, (kb | kk) != 0);
+        umma_commit(&aempty_bar[s2]);
+        umma_commit(&tfull_bar[bf]);
+      }
+      umma_commit(&final_bar);
+    }
+    __syncwarp();
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 9) {
+    if (lane == 0) {
+      volatile int no_abort = 0;
+      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+    }
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, TCOLS);
   }
 }
 
@@ -357,19 +601,20 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// Tensor map over a padded activation grid [npp][64] BF16: 130-pixel x
-// 128-byte boxes, 128-byte swizzle, zero fill out of bounds.
-int encode_act_map(CUtensorMap *map, const uint16_t *act, int64_t npp) {
+// Tensor map over a padded grid [npp][ch] BF16 with 130-pixel boxes: ch =
+// 64 (128-byte rows, 128-byte swizzle) or 8 (16-byte rows, no swizzle);
+// zero fill out of bounds.
+int encode_grid_map(CUtensorMap *map, const uint16_t *grid, int64_t npp, int ch) {
   EncodeTiledFn fn = encode_fn();
-  if (!fn || npp < 1 || npp > (int64_t)0x7fffffff) return -1;
-  const cuuint64_t dims[2] = {(cuuint64_t)lftma::kC, (cuuint64_t)npp};
-  const cuuint64_t strides[1] = {(cuuint64_t)lftma::kC * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)lftma::kC, (cuuint32_t)lftma::kBandRows};
+  if (!fn || npp < 1 || npp > (int64_t)0x7fffffff || (ch != 64 && ch != 8)) return -1;
+  const cuuint64_t dims[2] = {(cuuint64_t)ch, (cuuint64_t)npp};
+  const cuuint64_t strides[1] = {(cuuint64_t)ch * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)ch, (cuuint32_t)lftma::kBandRows};
   const cuuint32_t estr[2] = {1u, 1u};
-  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t *>(act), dims,
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t *>(grid), dims,
                         strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                        ch == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? 0 : -1;
 }
 
@@ -406,8 +651,36 @@ int lf_tma_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-int lf_pad_borders(uint16_t *act, int B, int H, int W, cudaStream_t st) {
-  lf_pad_border_kernel<<<256, 256, 0, st>>>(act, B, H, W);
+int lf_pad_borders(uint16_t *grid, int B, int H, int W, int chunks, cudaStream_t st) {
+  lf_pad_border_kernel<<<256, 256, 0, st>>>(grid, B, H, W, chunks);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+size_t lf_feat_pad_bytes(int B, int H, int W) { return (size_t)B * (H + 2) * (W + 2) * 16; }
+
+// Layer 1 (8 -> 32) from the padded feature grid featp into channels 0-31 of
+// the padded grid act1p.
+int lf_tma_layer1(const LfNet &net, const uint8_t *wimg, const uint16_t *featp, uint16_t *act1p,
+                  int B, int H, int W, int num_sms, int *err, uint64_t wait_limit_ns,
+                  cudaStream_t st) {
+  static_assert(kLfCin[0] == 8 && kLfCout[0] == lf1::kCout, "layer 1 is 8 -> 32");
+  const int64_t npp = (int64_t)B * (H + 2) * (W + 2);
+  CUtensorMap mf;
+  if (encode_grid_map(&mf, featp, npp, 8) != 0) return -1;
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(lf_conv1_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             lf1::kSmemBytes) != cudaSuccess)
+      return -2;
+    attr = true;
+  }
+  Lf1Args a{};
+  a.wimg = wimg; a.bias = net.b[0]; a.out = act1p; a.err = err;
+  a.B = B; a.H = H; a.W = W; a.wait_limit_ns = wait_limit_ns;
+  const int ntiles = (int)((npp + 127) / 128);
+  const int grid = ntiles < num_sms ? ntiles : num_sms;
+  if (grid < 1) return 0;
+  lf_conv1_tma_kernel<<<grid, lf1::kThreads, lf1::kSmemBytes, st>>>(mf, a);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -420,7 +693,7 @@ int lf_tma_layers23(const LfNet &net, const uint8_t *wimg, const uint16_t *act1p
                 "padded layers are written for 32 -> 64 -> 64");
   const int64_t npp = (int64_t)B * (H + 2) * (W + 2);
   CUtensorMap m1, m2;
-  if (encode_act_map(&m1, act1p, npp) != 0 || encode_act_map(&m2, act2p, npp) != 0) return -1;
+  if (encode_grid_map(&m1, act1p, npp, 64) != 0 || encode_grid_map(&m2, act2p, npp, 64) != 0) return -1;
   LfTmaArgs a{};
   a.err = err;
   a.B = B; a.H = H; a.W = W;
