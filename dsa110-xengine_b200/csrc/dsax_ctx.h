@@ -82,6 +82,8 @@ struct dsax_ctx {
   cudaStream_t side[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t pev[9] = {};
   dsax::LfNet lf_storage;
+  unsigned lf_wimg_version = ~0u;   // parameter version the inference weight images hold
+  int lf_pad_geom[3] = {0, 0, 0};   // (B, H, W) whose grid borders are zero
   dsax::LfNet *lf = &lf_storage;
   char errmsg[512] = {0};
 

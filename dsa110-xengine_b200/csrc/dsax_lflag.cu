@@ -348,6 +348,7 @@ int lf_bce(const float *z, const uint8_t *L, float *dz, double *loss_acc, int B,
 
 int lf_adam(LfNet &net, float lr, cudaStream_t st) {
   net.step += 1;
+  net.version += 1;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.f - powf(b1, (float)net.step), c2 = 1.f - powf(b2, (float)net.step);
   lf_adam_kernel<<<128, 256, 0, st>>>(net.params, net.grads, net.m, net.v, lf_nparams(), lr, b1, b2,

@@ -25,6 +25,7 @@ struct LfNet {
   float *gw[kLfLayers] = {}, *gb[kLfLayers] = {};    // views into grads
   float *wt[kLfLayers] = {}, *wf[kLfLayers] = {};    // forward / data-gradient layouts
   int step = 0;
+  unsigned version = 0;   // bumped whenever the parameters change
 };
 
 // Permanently flagged channels of the plain flagger's configuration.
@@ -71,7 +72,7 @@ int lf_tma_layers23(const LfNet &net, const uint8_t *wimg, const uint16_t *act1p
                     cudaStream_t st);
 int lf_tc_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st);
 int lf_tc_forward(const LfNet &net, const LfTcBuffers &bufs, int B, int H, int W, int guard,
-                  const LfPerm &perm, int num_sms, int *err, uint64_t wait_limit_ns,
-                  cudaStream_t st);
+                  const LfPerm &perm, bool zero_borders, int num_sms, int *err,
+                  uint64_t wait_limit_ns, cudaStream_t st);
 
 }  // namespace dsax

@@ -159,6 +159,7 @@ int dsax_lf_set_params(dsax_ctx *c, const float *params, int n) {
   if (e != cudaSuccess) return cuda_check(c, e, "upload parameters");
   cudaMemsetAsync(net.m, 0, sizeof(float) * 2 * n, c->stream);  // m and v
   net.step = 0;
+  net.version += 1;
   return dsax_sync(c);
 }
 
@@ -247,9 +248,11 @@ int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, in
   }
   // Inference on the tensor cores: BF16 features and activations in the
   // FP32 training buffers' space, FP32 accumulation.
+  void *const prev_w = c->aux[AUX_LF_TCW].ptr;
   if ((rc = ensure_buffer(c, c->aux[AUX_LF_TCW], lf_tc_wimg_bytes(), "learned-flagger weight images")) !=
       DSAX_OK)
     return rc;
+  if (c->aux[AUX_LF_TCW].ptr != prev_w) c->lf_wimg_version = ~0u;
   // zero-bordered grids: layer-1 output, layer-2 output, features
   const size_t npad = lf_pad_bytes(B, H, W), nfeat = lf_feat_pad_bytes(B, H, W);
   void *const prev_pad = c->aux[AUX_LF_PAD].ptr;
@@ -257,9 +260,12 @@ int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, in
                           "learned-flagger padded activations")) != DSAX_OK)
     return rc;
   uint8_t *const padb = static_cast<uint8_t *>(c->aux[AUX_LF_PAD].ptr);
-  // Channels 32-63 of the layer-1 grid are never written: zero them with the
-  // new allocation (the interior of each call's grid is then fully defined).
-  if (c->aux[AUX_LF_PAD].ptr != prev_pad) {
+  // No kernel writes a border pixel or channels 32-63 of the layer-1 grid, so
+  // they stay zero until the geometry (or the allocation) changes; then the
+  // layer-1 grid is cleared and the other grids' borders zeroed.
+  if (c->aux[AUX_LF_PAD].ptr != prev_pad) c->lf_pad_geom[0] = 0;
+  const bool zero_borders = c->lf_pad_geom[0] != B || c->lf_pad_geom[1] != H || c->lf_pad_geom[2] != W;
+  if (zero_borders) {
     cudaError_t ce = cudaMemsetAsync(padb, 0, npad, c->stream);
     if (ce != cudaSuccess) return cuda_check(c, ce, "padded grid clear");
   }
@@ -277,10 +283,18 @@ int dsax_flag_learned(dsax_ctx *c, const float *x, const dsax_flag_params *p, in
   for (int k = 0; k < p->nperm; ++k) perm.ch[k] = p->perm[k];
   int e = 0;
   e |= lf_make_features(p, xd, tds, s, nullptr, fbf, c->stream);
-  e |= lf_tc_prepare(net, static_cast<uint8_t *>(c->aux[AUX_LF_TCW].ptr), c->stream);
-  e |= lf_tc_forward(net, tb, B, H, W, p->guard, perm, c->num_sms, c->d_err, c->cfg.wait_limit_ns,
-                     c->stream);
+  if (c->lf_wimg_version != net.version) {   // weight images of the current parameters
+    e |= lf_tc_prepare(net, static_cast<uint8_t *>(c->aux[AUX_LF_TCW].ptr), c->stream);
+    if (!e) c->lf_wimg_version = net.version;
+  }
+  e |= lf_tc_forward(net, tb, B, H, W, p->guard, perm, zero_borders, c->num_sms, c->d_err,
+                     c->cfg.wait_limit_ns, c->stream);
   if (e) return cuda_check(c, cudaGetLastError(), "learned flagger launch");
+  if (zero_borders) {
+    c->lf_pad_geom[0] = B;
+    c->lf_pad_geom[1] = H;
+    c->lf_pad_geom[2] = W;
+  }
   if (mem == DSAX_MEM_DEVICE) {
     if (logits)
       cudaMemcpyAsync(logits, s.z, px * 4, cudaMemcpyDeviceToDevice, c->stream);

@@ -68,12 +68,15 @@ int lf_tc_prepare(const LfNet &net, uint8_t *wimg, cudaStream_t st) {
 // feature grid into act1p, layers 2 and 3 from act1p / act2p to the tap
 // projections (dsax_lflag_tma.cu), then the 64 -> 1 tap sum and the mask.
 int lf_tc_forward(const LfNet &net, const LfTcBuffers &bufs, int B, int H, int W, int guard,
-                  const LfPerm &perm, int num_sms, int *err, uint64_t wait_limit_ns,
-                  cudaStream_t st) {
+                  const LfPerm &perm, bool zero_borders, int num_sms, int *err,
+                  uint64_t wait_limit_ns, cudaStream_t st) {
   static_assert(kLfCin[3] == 64 && kLfCout[3] == 1, "64 -> 1 last layer");
-  int e = lf_pad_borders(bufs.featp, B, H, W, 1, st);
-  e |= lf_pad_borders(bufs.act1p, B, H, W, 8, st);
-  e |= lf_pad_borders(bufs.act2p, B, H, W, 8, st);
+  int e = 0;
+  if (zero_borders) {   // the grids' borders, once per geometry
+    e |= lf_pad_borders(bufs.featp, B, H, W, 1, st);
+    e |= lf_pad_borders(bufs.act1p, B, H, W, 8, st);
+    e |= lf_pad_borders(bufs.act2p, B, H, W, 8, st);
+  }
   e |= lf_tma_layer1(net, bufs.wimg, bufs.featp, bufs.act1p, B, H, W, num_sms, err, wait_limit_ns, st);
   e |= lf_tma_layers23(net, bufs.wimg + lf_l0_wimg_bytes(), bufs.act1p, bufs.act2p, bufs.z9, B, H, W,
                        num_sms, err, wait_limit_ns, st);

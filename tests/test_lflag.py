@@ -170,6 +170,37 @@ def test_gradients_match_oracle(dsax, oracle):
 
 
 @pytest.mark.gpu
+def test_inference_context_reuse(dsax, oracle):
+    """One context, calls with new parameters and changing geometry (40
+    beams, then 6, then 40 again inside the same allocation): the cached
+    weight images follow the parameters and the zero-bordered grids follow
+    the geometry; each call matches the oracle."""
+    import torch
+    T, C, tds = 1024, 48, 32
+    rng = np.random.default_rng(17)
+    nets = []
+    for k in range(2):
+        params = LO.init_params(40 + k)
+        nets.append([(w, rng.normal(scale=0.1, size=b.shape)) for w, b in params])
+    with dsax.Context(dsax.default_config(npkt=16, nchan=8)) as ctx:
+        for B, k in ((40, 0), (6, 1), (40, 1)):
+            x, _ = oracle.gen_filterbank(50 + B + k, nbeam=B, ntime=T, nchan=C)
+            p = dsax.flag_params(B, T, C)
+            ctx.lf_set_params(_flat(nets[k]))
+            H = T // tds
+            xd = torch.from_numpy(x).cuda()
+            mask = torch.zeros(B * H * C, dtype=torch.uint8, device="cuda")
+            logit = torch.zeros(B * H * C, dtype=torch.float32, device="cuda")
+            torch.cuda.synchronize()
+            ctx.flag_learned(p, xd, mask, logits=logit, tds=tds)
+            ctx.sync()
+            got = logit.cpu().numpy().reshape(B, H, C)
+            want = LO.forward_bf16(_unflat(_flat(nets[k])), LO.features(x, tds, p))
+            scale = np.abs(want).max()
+            assert np.abs(got - want).max() < 5e-3 * scale, (B, k)
+
+
+@pytest.mark.gpu
 def test_training_reaches_plain_flagger_masks(dsax, oracle):
     """Train on 4 synthetic blocks labelled by the GPU plain flagger, test on
     2 held-out blocks: report P/R/F1 per block; the trained net must beat
