@@ -397,7 +397,7 @@ __device__ __forceinline__ float slogf(float v) { return copysignf(log1pf(fabsf(
 //   f6 10 (z_pp - 1)       f7 mean over the pixel's samples of z_ts
 // mu, sigma: mean and standard deviation of the beam's samples (from the
 // per-channel mean and variance).
-__global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(FlagArgs a, float *F,
+__global__ void __launch_bounds__(2 * flag::kDecThreads) lf_stat_features_kernel(FlagArgs a, float *F,
                                                                             uint16_t *Fbf) {
   const int b = blockIdx.x;
   const int C = a.nchan, G = a.guard, T = a.ntime, n = C - 2 * G, tds = a.tds, H = T / tds;
@@ -458,16 +458,23 @@ __global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(Fla
       zt[t] = a.tsflag ? zz : 0.0f;
     }
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {   // beam mean and variance over channels, one warp
     double s = 0.0, q = 0.0;
-    for (int c = 0; c < C; ++c) {
+    for (int c = threadIdx.x; c < C; c += 32) {
       const double m = a.spec[b * C + c];
       s += m;
       q += (double)a.var[b * C + c] + m * m;
     }
-    const double mu = s / C;
-    mu_sd[0] = (float)mu;
-    mu_sd[1] = (float)sqrt(fmax(q / C - mu * mu, 1e-30));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+      q += __shfl_xor_sync(0xffffffffu, q, o);
+    }
+    if (threadIdx.x == 0) {
+      const double mu = s / C;
+      mu_sd[0] = (float)mu;
+      mu_sd[1] = (float)sqrt(fmax(q / C - mu * mu, 1e-30));
+    }
   }
   __syncthreads();
   for (int h = threadIdx.x; h < H; h += blockDim.x) {
@@ -483,20 +490,48 @@ __global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(Fla
   __syncthreads();
   const float mu = mu_sd[0], inv = 1.0f / mu_sd[1], kpix = sqrtf((float)tds);
   constexpr float kMargin = 10.0f;   // margins scaled so the rule's edge is steep
+  // features that depend only on the channel (f3..f6) or only on the row
+  // (f2, f7): once each, in place
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    z[c] = slogf(kMargin * (fabsf(z[c]) - 1.0f));
+    z[C + c] = slogf(kMargin * (fabsf(z[C + c]) - 1.0f));
+    z[2 * C + c] = slogf(kMargin * (fabsf(z[2 * C + c]) - 1.0f));
+    z[3 * C + c] = slogf(kMargin * (z[3 * C + c] - 1.0f));
+  }
+  for (int h = threadIdx.x; h < H; h += blockDim.x) {
+    rmax[h] = slogf(kMargin * (rmax[h] - 1.0f));
+    rmean[h] = slogf(rmean[h]);
+  }
+  __syncthreads();
   float4 *Fb = F ? reinterpret_cast<float4 *>(F + (int64_t)b * H * C * 8) : nullptr;
   const float *ps = a.pix_sum + (int64_t)b * H * C;
   const float *pm = a.pix_max + (int64_t)b * H * C;
-  for (int i = threadIdx.x; i < H * C; i += blockDim.x) {
-    const int h = i / C, c = i - h * C;
+  const float invC = 1.0f / (float)C, invT = 1.0f / (float)tds;
+  constexpr int kBatch = 4;   // pixel loads issued together
+  for (int i0 = threadIdx.x; i0 < H * C; i0 += kBatch * blockDim.x) {
+    float pv[kBatch], mv[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const int i = i0 + k * blockDim.x;
+      pv[k] = i < H * C ? ps[i] : 0.0f;
+      mv[k] = i < H * C ? pm[i] : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+    const int i = i0 + k * blockDim.x;
+    if (i >= H * C) break;
+    int h = __float2int_rz((float)i * invC);   // i / C, corrected (i < 2^24)
+    h += (i - h * C >= C) - (i - h * C < 0);
+    const int c = i - h * C;
     float4 f, g;
-    f.x = slogf((ps[i] / tds - mu) * inv * kpix);
-    f.y = slogf((pm[i] - mu) * inv);
-    f.z = slogf(kMargin * (rmax[h] - 1.0f));
-    f.w = slogf(kMargin * (fabsf(z[c]) - 1.0f));
-    g.x = slogf(kMargin * (fabsf(z[C + c]) - 1.0f));
-    g.y = slogf(kMargin * (fabsf(z[2 * C + c]) - 1.0f));
-    g.z = slogf(kMargin * (z[3 * C + c] - 1.0f));
-    g.w = slogf(rmean[h]);
+    f.x = slogf((pv[k] * invT - mu) * inv * kpix);
+    f.y = slogf((mv[k] - mu) * inv);
+    f.z = rmax[h];
+    f.w = z[c];
+    g.x = z[C + c];
+    g.y = z[2 * C + c];
+    g.z = z[3 * C + c];
+    g.w = rmean[h];
     if (F) {
       Fb[2 * i] = f;
       Fb[2 * i + 1] = g;
@@ -509,6 +544,7 @@ __global__ void __launch_bounds__(flag::kDecThreads) lf_stat_features_kernel(Fla
       asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(o.w) : "f"(g.w), "f"(g.z));
       // zero-bordered grid [B][H+2][C+2][8] read by the first conv layer
       reinterpret_cast<uint4 *>(Fbf)[((int64_t)b * (H + 2) + h + 1) * (C + 2) + c + 1] = o;
+    }
     }
   }
 }
@@ -525,7 +561,7 @@ int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStre
                          200 * 1024);
     attr = true;
   }
-  lf_stat_features_kernel<<<a.nbeam, flag::kDecThreads, sh, st>>>(a, F, Fbf);
+  lf_stat_features_kernel<<<a.nbeam, 2 * flag::kDecThreads, sh, st>>>(a, F, Fbf);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
