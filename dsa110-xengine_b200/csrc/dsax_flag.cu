@@ -346,24 +346,6 @@ __device__ void window_detrend(const float *sb, const FlagArgs &a, float *corr) 
   __syncthreads();
 }
 
-// channflag() on one statistic of one beam: forward median detrend over
-// `filt` channels (the last windows clamped at C-G-filt), median and MAD
-// over the guard-banded channels, flag |x| > thr*MAD.
-__device__ void channflag_dev(const float *sb, float thr, const FlagArgs &a, uint8_t *mask,
-                              float *corr, float *tmp, float *slot) {
-  const int C = a.nchan, G = a.guard, n = C - 2 * G;
-  window_detrend(sb, a, corr);
-  const float med = block_lower_median(corr, n, slot);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = fabsf(corr[i] - med);
-  __syncthreads();
-  const float mad = block_lower_median(tmp, n, slot);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const float v = corr[i];
-    if (v > thr * mad || v < -thr * mad) mask[G + i] = 1;
-  }
-  __syncthreads();
-}
-
 // channflag()'s test statistic as a number: corr[j] / (thr * MAD), so the
 // channel is flagged exactly when |z| > 1 (z = +-1e6 when the MAD is 0 and
 // corr is not; 0 in the guard band).  Used as a learned-flagger feature.
@@ -565,83 +547,176 @@ int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStre
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-__global__ void __launch_bounds__(flag::kDecThreads) flag_decide_kernel(FlagArgs a) {
-  const int b = blockIdx.x;
+// Group versions of the median and detrend: `gsize` threads (whole warps)
+// with group-local index gtid synchronise on named barrier `bid`.
+__device__ float grp_lower_median(const float *v, int n, float *result_slot, int gtid, int gsize,
+                                  int bid) {
+  const int k = (n + 1) / 2 - 1;
+  int gs = 1;
+  while (gs < 32 && gs * 2 * n <= gsize) gs *= 2;
+  const int sub = gtid & (gs - 1);
+  const int per = (n + gs - 1) / gs;
+  const int rounds = (n * gs + gsize - 1) / gsize;   // uniform trip count
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int i = (rd * gsize + gtid) / gs;
+    const bool live = i < n;
+    const float x = live ? v[i] : 0.0f;
+    int r = 0;
+    if (live) {
+      const int j0 = sub * per, j1 = min(n, j0 + per);
+#pragma unroll 8
+      for (int j = j0; j < j1; ++j) {
+        const float y = v[j];
+        r += (y < x) || (y == x && j < i);
+      }
+    }
+    for (int o = gs >> 1; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (live && sub == 0 && r == k) *result_slot = x;
+  }
+  named_bar(bid, gsize);
+  const float med = *result_slot;
+  named_bar(bid, gsize);
+  return med;
+}
+
+__device__ void grp_channflag(const float *sb, float thr, const FlagArgs &a, uint8_t *mask,
+                              float *corr, float *tmp, float *slot, int gtid, int gsize, int bid) {
+  const int C = a.nchan, G = a.guard, F = a.filt, n = C - 2 * G;
+  const int kf = (F + 1) / 2 - 1;
+  for (int idx = gtid; idx < n * F; idx += gsize) {   // forward median detrend
+    const int jj = idx / F, i = idx - jj * F;
+    const int j = G + jj;
+    const int w0 = (C - G - j >= F) ? j : C - G - F;
+    const float x = sb[w0 + i];
+    int r = 0;
+    for (int q = 0; q < F; ++q) {
+      const float y = sb[w0 + q];
+      r += (y < x) || (y == x && q < i);
+    }
+    if (r == kf) corr[jj] = sb[j] - x;
+  }
+  named_bar(bid, gsize);
+  const float med = grp_lower_median(corr, n, slot, gtid, gsize, bid);
+  for (int i = gtid; i < n; i += gsize) tmp[i] = fabsf(corr[i] - med);
+  named_bar(bid, gsize);
+  const float mad = grp_lower_median(tmp, n, slot, gtid, gsize, bid);
+  for (int i = gtid; i < n; i += gsize) {
+    const float v = corr[i];
+    if (v > thr * mad || v < -thr * mad) mask[G + i] = 1;
+  }
+}
+
+// The decisions of one beam (one CTA): the four channel tests and the
+// time-series test are independent, so five thread groups run them at once
+// (the reference runs them in sequence, src/gpu_flagger.cu:1340-1398; the
+// flags are the same):
+//   group 0-2 (64 threads each): channflag(spec - oldspec, Thr),
+//             channflag(var, Thr + 0.5), channflag(max, Thr)
+//   group 3   (64 threads): simple_channflag(pp, Thr / sqrt(FBIN)), one-sided
+//   group 4   (128 threads): simple_tsflag(ts, TsThr) over the first ts_base
+// The channel groups OR their flags into one shared mask.
+namespace flag {
+constexpr int kDecideThreads = 384;
+}
+
+__global__ void __launch_bounds__(flag::kDecideThreads) flag_decide_kernel(FlagArgs a) {
+  const int b = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
   const int C = a.nchan, G = a.guard, T = a.ntime, n = C - 2 * G;
-  extern __shared__ float dsh[];
-  float *spec = dsh;                    // C
-  float *corr = spec + C;               // C
-  float *tmp = corr + C;                // max(C, ts_base)
-  float *tsb = tmp + (a.ts_base > C ? a.ts_base : C);  // ts_base
-  __shared__ uint8_t cmask[flag::kMaxChan * 2];
-  __shared__ float slot;
+  extern __shared__ float dsh[];          // [4 groups][3][C], then ts: [2][ts_base]
+  __shared__ uint8_t cmask[flag::kMaxChan];
+  __shared__ float slots[5];
 
-  for (int c = threadIdx.x; c < C; c += blockDim.x) cmask[c] = 0;
+  for (int c = tid; c < C; c += blockDim.x) cmask[c] = 0;
   __syncthreads();
-
-  // 1) channflag(spec - oldspec, Thr)
-  for (int c = threadIdx.x; c < C; c += blockDim.x)
-    spec[c] = a.spec[b * C + c] - (a.oldspec ? a.oldspec[b * C + c] : 0.0f);
-  __syncthreads();
-  channflag_dev(spec, a.thresh, a, cmask, corr, tmp, &slot);
-  // 2) channflag(var, Thr + 0.5)
-  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.var[b * C + c];
-  __syncthreads();
-  channflag_dev(spec, a.thresh + a.var_add, a, cmask, corr, tmp, &slot);
-  // 3) channflag(max, Thr)
-  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.maxs[b * C + c];
-  __syncthreads();
-  channflag_dev(spec, a.thresh, a, cmask, corr, tmp, &slot);
-  // 4) simple_channflag(pp, Thr): one-sided, Thr/sqrt(FBIN)
-  for (int c = threadIdx.x; c < C; c += blockDim.x) spec[c] = a.pp[b * C + c];
-  __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) corr[i] = spec[G + i];
-  __syncthreads();
-  {
-    const float med = block_lower_median(corr, n, &slot);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) tmp[i] = fabsf(corr[i] - med);
-    __syncthreads();
-    const float mad = block_lower_median(tmp, n, &slot);
-    const float mythr = a.thresh / sqrtf((float)a.fbin);
-    for (int j = G + threadIdx.x; j < C - G - a.fbin; j += blockDim.x) {
-      float vv = 0.0f;
-      for (int k = 0; k < a.fbin; ++k) vv += a.parity ? spec[j] : spec[j + k];
-      vv = vv / (float)a.fbin - med;
-      if (vv > mythr * mad) cmask[j] = 1;
+  const int g = warp < 8 ? warp >> 1 : 4;
+  const int gsize = g < 4 ? 64 : 128, gtid = g < 4 ? tid - 64 * g : tid - 256, bid = 1 + g;
+  if (g < 4) {
+    float *sb = dsh + g * 3 * C, *corr = sb + C, *tmp = corr + C;
+    const float *src = g == 0 ? a.spec : g == 1 ? a.var : g == 2 ? a.maxs : a.pp;
+    for (int c = gtid; c < C; c += gsize)
+      sb[c] = src[b * C + c] - ((g == 0 && a.oldspec) ? a.oldspec[b * C + c] : 0.0f);
+    named_bar(bid, gsize);
+    if (g < 3) {
+      const float thr = g == 1 ? a.thresh + a.var_add : a.thresh;
+      grp_channflag(sb, thr, a, cmask, corr, tmp, &slots[g], gtid, gsize, bid);
+    } else {
+      for (int i = gtid; i < n; i += gsize) corr[i] = sb[G + i];
+      named_bar(bid, gsize);
+      const float med = grp_lower_median(corr, n, &slots[g], gtid, gsize, bid);
+      for (int i = gtid; i < n; i += gsize) tmp[i] = fabsf(corr[i] - med);
+      named_bar(bid, gsize);
+      const float mad = grp_lower_median(tmp, n, &slots[g], gtid, gsize, bid);
+      const float mythr = a.thresh / sqrtf((float)a.fbin);
+      for (int j = G + gtid; j < C - G - a.fbin; j += gsize) {
+        float vv = 0.0f;
+        for (int k = 0; k < a.fbin; ++k) vv += a.parity ? sb[j] : sb[j + k];
+        vv = vv / (float)a.fbin - med;
+        if (vv > mythr * mad) cmask[j] = 1;
+      }
+    }
+  } else {
+    const float *tb = a.ts + (int64_t)b * T;
+    if (a.tsflag) {
+      float *tsb = dsh + 12 * C, *tmp = tsb + a.ts_base;
+      for (int i = gtid; i < a.ts_base; i += gsize) tsb[i] = tb[i];
+      named_bar(bid, gsize);
+      const float med = grp_lower_median(tsb, a.ts_base, &slots[4], gtid, gsize, bid);
+      for (int i = gtid; i < a.ts_base; i += gsize) tmp[i] = fabsf(tsb[i] - med);
+      named_bar(bid, gsize);
+      const float mad = grp_lower_median(tmp, a.ts_base, &slots[4], gtid, gsize, bid);
+      const float lim = a.ts_thresh * mad;
+      int nts = 0;
+      uint8_t *mb = a.tsmask + (int64_t)b * T;
+      if ((T & 3) == 0 && (reinterpret_cast<uintptr_t>(tb) & 15u) == 0 &&
+          (reinterpret_cast<uintptr_t>(mb) & 3u) == 0) {
+        // four samples per load and one 32-bit mask word per store; all of a
+        // thread's loads (read-only path) are issued before its stores, which
+        // as byte stores could otherwise alias them
+        const float4 *t4 = reinterpret_cast<const float4 *>(tb);
+        uint32_t *m4 = reinterpret_cast<uint32_t *>(mb);
+        constexpr int kU = 8;
+        for (int i0 = gtid; i0 < T / 4; i0 += kU * gsize) {
+          float4 v[kU];
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            const int i = i0 + u * gsize;
+            v[u] = i < T / 4 ? __ldg(t4 + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            const int i = i0 + u * gsize;
+            if (i >= T / 4) break;
+            const uint32_t f0 = (v[u].x - med) > lim, f1 = (v[u].y - med) > lim;
+            const uint32_t f2 = (v[u].z - med) > lim, f3 = (v[u].w - med) > lim;
+            m4[i] = f0 | (f1 << 8) | (f2 << 16) | (f3 << 24);
+            nts += (int)(f0 + f1 + f2 + f3);
+          }
+        }
+      } else {
+        for (int t = gtid; t < T; t += gsize) {
+          const uint8_t f = (__ldg(tb + t) - med) > lim ? 1 : 0;
+          mb[t] = f;
+          nts += f;
+        }
+      }
+      if (nts) atomicAdd(a.counts + 1, nts);
+    } else {
+      for (int t = gtid; t < T; t += gsize) a.tsmask[(int64_t)b * T + t] = 0;
     }
   }
   __syncthreads();
-  for (int k = 0; k < a.nperm; ++k) {
-    const int j = a.perm[k];
-    if (threadIdx.x == 0 && j >= G && j < C - G) cmask[j] = 1;
-  }
+  if (tid == 0)
+    for (int k = 0; k < a.nperm; ++k) {
+      const int j = a.perm[k];
+      if (j >= G && j < C - G) cmask[j] = 1;
+    }
   __syncthreads();
   int nflag = 0;
-  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+  for (int c = tid; c < C; c += blockDim.x) {
     a.chanmask[b * C + c] = cmask[c];
     nflag += cmask[c];
   }
   if (nflag) atomicAdd(a.counts, nflag);
-
-  // 5) simple_tsflag(ts, TsThr): median/MAD over the first ts_base samples
-  const float *tb = a.ts + (int64_t)b * T;
-  if (a.tsflag) {
-    for (int i = threadIdx.x; i < a.ts_base; i += blockDim.x) tsb[i] = tb[i];
-    __syncthreads();
-    const float med = block_lower_median(tsb, a.ts_base, &slot);
-    for (int i = threadIdx.x; i < a.ts_base; i += blockDim.x) tmp[i] = fabsf(tsb[i] - med);
-    __syncthreads();
-    const float mad = block_lower_median(tmp, a.ts_base, &slot);
-    int nts = 0;
-    for (int t = threadIdx.x; t < T; t += blockDim.x) {
-      const uint8_t f = (tb[t] - med) > a.ts_thresh * mad ? 1 : 0;
-      a.tsmask[(int64_t)b * T + t] = f;
-      nts += f;
-    }
-    if (nts) atomicAdd(a.counts + 1, nts);
-  } else {
-    for (int t = threadIdx.x; t < T; t += blockDim.x) a.tsmask[(int64_t)b * T + t] = 0;
-  }
 }
 
 int launch_flag_stats(const FlagArgs &a, cudaStream_t st) {
@@ -671,9 +746,8 @@ int launch_flag(const FlagArgs &a, cudaStream_t st) {
   if (a.nchan > flag::kMaxChan || a.ts_base > 4096) return -1;
   const int rc = launch_flag_stats(a, st);
   if (rc != 0) return rc;
-  const int tmpn = a.ts_base > a.nchan ? a.ts_base : a.nchan;
-  const size_t sh = sizeof(float) * (2 * a.nchan + tmpn + a.ts_base);
-  flag_decide_kernel<<<a.nbeam, flag::kDecThreads, sh, st>>>(a);
+  const size_t sh = sizeof(float) * (12 * (size_t)a.nchan + 2 * (size_t)a.ts_base);
+  flag_decide_kernel<<<a.nbeam, flag::kDecideThreads, sh, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
