@@ -579,6 +579,61 @@ __device__ float grp_lower_median(const float *v, int n, float *result_slot, int
   return med;
 }
 
+// The k-th smallest of v[0..n) (0-based; the value rank counting with
+// ties by index returns) by a four-pass MSB-first radix select over
+// order-preserving 32-bit keys: per pass a 256-bin shared histogram of the
+// candidates that still match the selected prefix, then one warp finds the
+// bin holding rank k.  O(n) work instead of O(n^2); finite inputs.
+__device__ __forceinline__ uint32_t ordered_key(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ float grp_radix_select(const float *v, int n, int k, uint32_t *hist, uint32_t *sel,
+                                  int gtid, int gsize, int bid) {
+  uint32_t prefix = 0u, pmask = 0u;
+  int kk = k;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = gtid; i < 256; i += gsize) hist[i] = 0u;
+    named_bar(bid, gsize);
+    for (int i = gtid; i < n; i += gsize) {
+      const uint32_t u = ordered_key(v[i]);
+      if ((u & pmask) == prefix) atomicAdd(&hist[(u >> shift) & 255u], 1u);
+    }
+    named_bar(bid, gsize);
+    if (gtid < 32) {   // the first warp: bin holding rank kk
+      uint32_t c[8], tot = 0u;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) { c[e] = hist[8 * gtid + e]; tot += c[e]; }
+      uint32_t incl = tot;   // inclusive scan over lanes
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (gtid >= o) incl += y;
+      }
+      const uint32_t excl = incl - tot;
+      if (excl <= (uint32_t)kk && (uint32_t)kk < incl) {
+        uint32_t run = excl;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          if ((uint32_t)kk < run + c[e]) {
+            sel[0] = (uint32_t)(8 * gtid + e);
+            sel[1] = (uint32_t)kk - run;
+            break;
+          }
+          run += c[e];
+        }
+      }
+    }
+    named_bar(bid, gsize);
+    prefix |= sel[0] << shift;
+    pmask |= 0xFFu << shift;
+    kk = (int)sel[1];
+    named_bar(bid, gsize);
+  }
+  const uint32_t u = (prefix & 0x80000000u) ? (prefix & 0x7FFFFFFFu) : ~prefix;
+  return __uint_as_float(u);
+}
+
 __device__ void grp_channflag(const float *sb, float thr, const FlagArgs &a, uint8_t *mask,
                               float *corr, float *tmp, float *slot, int gtid, int gsize, int bid) {
   const int C = a.nchan, G = a.guard, F = a.filt, n = C - 2 * G;
@@ -625,6 +680,7 @@ __global__ void __launch_bounds__(flag::kDecideThreads) flag_decide_kernel(FlagA
   extern __shared__ float dsh[];          // [4 groups][3][C], then ts: [2][ts_base]
   __shared__ uint8_t cmask[flag::kMaxChan];
   __shared__ float slots[5];
+  __shared__ uint32_t ts_hist[256], ts_sel[2];   // radix select of the time-series group
 
   for (int c = tid; c < C; c += blockDim.x) cmask[c] = 0;
   __syncthreads();
@@ -660,10 +716,11 @@ __global__ void __launch_bounds__(flag::kDecideThreads) flag_decide_kernel(FlagA
       float *tsb = dsh + 12 * C, *tmp = tsb + a.ts_base;
       for (int i = gtid; i < a.ts_base; i += gsize) tsb[i] = tb[i];
       named_bar(bid, gsize);
-      const float med = grp_lower_median(tsb, a.ts_base, &slots[4], gtid, gsize, bid);
+      const int kmed = (a.ts_base + 1) / 2 - 1;   // lower median
+      const float med = grp_radix_select(tsb, a.ts_base, kmed, ts_hist, ts_sel, gtid, gsize, bid);
       for (int i = gtid; i < a.ts_base; i += gsize) tmp[i] = fabsf(tsb[i] - med);
       named_bar(bid, gsize);
-      const float mad = grp_lower_median(tmp, a.ts_base, &slots[4], gtid, gsize, bid);
+      const float mad = grp_radix_select(tmp, a.ts_base, kmed, ts_hist, ts_sel, gtid, gsize, bid);
       const float lim = a.ts_thresh * mad;
       int nts = 0;
       uint8_t *mb = a.tsmask + (int64_t)b * T;
