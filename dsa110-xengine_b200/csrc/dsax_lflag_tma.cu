@@ -356,7 +356,6 @@ constexpr int kThreads = 320;
 constexpr int kBandPix = 130;
 constexpr int kBandBytes = kBandPix * 16;           // 2,080
 constexpr int kBandStride = 2176;                   // 128-byte aligned band offset
-constexpr int kSlotBytes = 3 * kBandStride;         // 6,528
 constexpr int kSlotStride = 6656;                   // 128-byte aligned slot
 constexpr int kSlots = 8;
 constexpr int kABytes = 2 * 16384;                  // two K blocks of 128 x 128 B
