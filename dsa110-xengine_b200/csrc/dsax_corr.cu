@@ -498,26 +498,20 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
           break;
         tc_fence_after();
         const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
-        // Re (K = 128 bytes = 4 x 32) and C = I R^T (K = 64 bytes = 2 x 32)
-        // of both time slots: four accumulators, issued interleaved so that
-        // consecutive MMAs never accumulate into the same TMEM columns
-        // (order Re0 Re1 C0 | Re0 Re1 C1' | Re0 Re1 C0 | Re0 Re1 C1', with
-        // slot t's C steps spread over the stage).
 #pragma unroll
-        for (int n = 0; n < 12; ++n) {
-          const int kk = n / 3, j = n % 3;                 // group kk: Re(t=0), Re(t=1), one C
-          const bool is_c = j == 2;
-          const int t = is_c ? (kk & 1) : j;
-          const int ck = kk >> 1;                          // C K step of slot t
+        for (int t = 0; t < 2; ++t) {
           const uint32_t tile = stage + (uint32_t)t * kTile;
-          const uint32_t dre = tmem + (uint32_t)t * 256u;
-          if (!is_c) {
+          const uint32_t dre = tmem + (uint32_t)t * 256u, dc = dre + 128u;
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {   // Re: K = 128 bytes = 4 x 32
             const uint64_t d = umma_desc_sw128(tile + 32u * kk, 1024u);
             umma_i8(dre, d, d, kIdescN128, (ks | kk) != 0);
-          } else {
-            const uint64_t di = umma_desc_sw128(tile + 64u + 32u * ck, 1024u);
-            const uint64_t dr = umma_desc_sw128(tile + 32u * ck, 1024u);
-            umma_i8(dre + 128u, di, dr, kIdescN128, (ks | ck) != 0);
+          }
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk) {   // C = I R^T: K = 64 bytes = 2 x 32
+            const uint64_t di = umma_desc_sw128(tile + 64u + 32u * kk, 1024u);
+            const uint64_t dr = umma_desc_sw128(tile + 32u * kk, 1024u);
+            umma_i8(dc, di, dr, kIdescN128, (ks | kk) != 0);
           }
         }
         umma_commit(&empty_bar[s]);
