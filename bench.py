@@ -187,7 +187,7 @@ def cpu_baseline_sample(budget_s: float = 12.0):
             "sample": f"{done} of 384 channels of one full block ({t_total:.1f} s), scaled"}
 
 
-BF_FLOPS = 8 * 256 * 64 * 2 * 384 * 4096      # config 3 beamformer, per block
+BF_FLOPS = 8 * 256 * 64 * 2 * 384 * 4096      # 256-beam beamformer, FLOP per full block
 
 
 def _bf16_peak():
@@ -215,7 +215,7 @@ def _time_loop(stream, fn, steps, warm=3):
 
 
 def bench_beamformer(dsax, synth, dev, blk_dev, steps):
-    """Config 3: 256 beams, 32 t x 8 ch Stokes-I from a full block (BF16)."""
+    """Beamformer workload: 256 beams, 32 t x 8 ch Stokes-I from a full block (BF16)."""
     import torch
     cfg = dsax.default_config(bf_scale=128.0 / (512 * 64 * 2 * 6.25))
     with dsax.Context(cfg, device=dev) as ctx:
@@ -247,7 +247,7 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps):
 
 
 def bench_flaggers(dsax, synth, dev, steps, train_steps=1000):
-    """Config 4: plain vs learned flagger on [256][4096][48] FP32 (chi2(2)+RFI).
+    """Flagger workload: plain vs learned flagger on [256][4096][48] FP32 (chi2(2)+RFI).
     The learned net is trained here first (outside the timed regions)."""
     import torch
     from dsax import lflag
@@ -285,7 +285,7 @@ def bench_flaggers(dsax, synth, dev, steps, train_steps=1000):
 
 
 def bench_batch(dsax, synth, dev, steps):
-    """Config 5: 16 blocks, widths from {192, 384, 768}, corner turn +
+    """Batch workload: 16 blocks, widths from {192, 384, 768}, corner turn +
     correlate + beamform + flag each, one CUDA graph vs per-block launches."""
     import torch
     rng = np.random.default_rng(55)

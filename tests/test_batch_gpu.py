@@ -1,4 +1,4 @@
-"""Batches of blocks with mixed subband widths (BASELINE config 5 shape):
+"""Batches of blocks with mixed subband widths (16 blocks of 192 / 384 / 768 channels):
 the batch API, with and without graph capture, must reproduce the per-block
 entry points exactly, and the beam flags must equal the plain flagger run
 on the beamformer's FP32 filterbank."""

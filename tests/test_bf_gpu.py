@@ -51,7 +51,7 @@ def _check(oracle, blk, wre, wim, u8, f32, ppo, scale, g0=0, ng=None):
 
 
 def test_beamformer_config3_subset(dsax, oracle):
-    """BASELINE shape: 64 ants (63 populated) x 2 pols x 384 ch x 4096 t,
+    """Full-size block: 64 ants (63 populated) x 2 pols x 384 ch x 4096 t,
     256 beams, unit-magnitude random-phase weights, 32 t x 8 ch sums."""
     blk = oracle.gen_block(303, 2048, 63, 384, "gauss")
     wre, wim = oracle.random_phase_weights(9, 48, 256)
