@@ -3,8 +3,8 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA library
  * is compared against.  Nothing in the product path (libdsax.so, the C-ABI,
- * the driver) links, loads or calls it; only tests/, __graft_entry__.smoke()
- * and bench.py's CPU-baseline leg do.
+ * the dsax_xengine host program) links, loads or calls it; only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg do.
  *
  * Parity status (which outputs are pinned by what):
  *  - 4-bit decode: pinned by the reference's own decoder (utils/gen_packet.py
