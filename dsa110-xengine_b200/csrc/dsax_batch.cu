@@ -72,6 +72,9 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     f.counts = reinterpret_cast<int *>(fstats + 4 * nbc + (size_t)cf.nbeam * nout);
     f.chanmask = d.chanmask;
     f.tsmask = d.tsmask ? d.tsmask : reinterpret_cast<uint8_t *>(f.counts + 2);
+    // the flag counters accumulate with atomics: clear them per block (inside
+    // the graph too, so every replay starts from zero)
+    if (cudaMemsetAsync(f.counts, 0, 2 * sizeof(int), c->stream) != cudaSuccess) return -2;
     if (launch_flag(f, c->stream) != 0) return -2;
   }
   return 0;

@@ -483,13 +483,8 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
 
 template <bool kFp8>
 static int launch_bf(const BfArgs &a, int num_sms, cudaStream_t st) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    if (cudaFuncSetAttribute(bf_kernel<kFp8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bf::T<kFp8>::kSmemBytes) != cudaSuccess)
-      return -2;
-    attr_done = true;
-  }
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, bf_kernel<kFp8>, bf::T<kFp8>::kSmemBytes) != cudaSuccess) return -2;
   const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / bf::kPktPerStage;
   const int align = 2 * (a.ppo > bf::kPktPerStage ? a.ppo / bf::kPktPerStage : 1);
   const int nchunks = ngrp * npg * 2 / align;

@@ -590,13 +590,9 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
 
 template <bool kBulk>
 static int launch_cm(const CorrArgs &a, cudaStream_t st) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    if (cudaFuncSetAttribute(corr_cm_kernel<kBulk>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             corrcm::smem_bytes<kBulk>()) != cudaSuccess)
-      return -2;
-    attr_done = true;
-  }
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, corr_cm_kernel<kBulk>, corrcm::smem_bytes<kBulk>()) != cudaSuccess)
+    return -2;
   void *args[] = {(void *)&a};
   return cudaLaunchKernel((const void *)corr_cm_kernel<kBulk>, dim3(a.nchan),
                           dim3(corrcm::threads<kBulk>()), args, corrcm::smem_bytes<kBulk>(),
@@ -610,17 +606,12 @@ int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, bool bulk_fed
 }
 
 int launch_correlate(const CorrArgs &a, int fmt, cudaStream_t st) {
-  static bool attr_done[3] = {false, false, false};
+  static SmemAttrOnce attr[3];
   const void *fn = fmt == FMT_CAPTURED    ? (const void *)corr_kernel<FMT_CAPTURED>
                    : fmt == FMT_REORDERED ? (const void *)corr_kernel<FMT_REORDERED>
                                           : (const void *)corr_kernel<FMT_XGPU_INT8>;
   if (fmt < 0 || fmt > 2) return -1;
-  if (!attr_done[fmt]) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         corr::kSmemBytes);
-    if (e != cudaSuccess) return -2;
-    attr_done[fmt] = true;
-  }
+  if (smem_attr_once(attr[fmt], fn, corr::kSmemBytes) != cudaSuccess) return -2;
   dim3 grid(a.nchan), block(corr::kThreads);
   void *args[] = {(void *)&a};
   cudaError_t e = cudaLaunchKernel(fn, grid, block, args, corr::kSmemBytes, st);

@@ -537,12 +537,8 @@ int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStre
   const size_t sh = sizeof(float) * (2 * a.nchan + (a.ts_base > a.nchan ? a.ts_base : a.nchan) +
                                      4 * a.nchan + a.ntime + 2 * H);
   if (sh > 200 * 1024) return -1;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(lf_stat_features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-    attr = true;
-  }
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, lf_stat_features_kernel, 200 * 1024) != cudaSuccess) return -2;
   lf_stat_features_kernel<<<a.nbeam, 2 * flag::kDecThreads, sh, st>>>(a, F, Fbf);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
@@ -779,21 +775,15 @@ __global__ void __launch_bounds__(flag::kDecideThreads) flag_decide_kernel(FlagA
 int launch_flag_stats(const FlagArgs &a, cudaStream_t st) {
   if (a.nchan > flag::kMaxChan) return -1;
   if (flag_stats_staged_ok(a)) {
-    static bool attr2 = false;
-    if (!attr2) {
-      const int mx = flag::kFastStages * flag::kFastStageMax + 48 * 1024;
-      cudaFuncSetAttribute(flag_stats_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      attr2 = true;
-    }
+    static SmemAttrOnce attr2;
+    const int mx = flag::kFastStages * flag::kFastStageMax + 48 * 1024;
+    if (smem_attr_once(attr2, flag_stats_staged_kernel, mx) != cudaSuccess) return -2;
     flag_stats_staged_kernel<<<a.nbeam, flag::kFastThreads, staged_stats_smem(a), st>>>(a);
   } else {
     if (a.pix_sum) return -1;
-    static bool attr = false;
+    static SmemAttrOnce attr;
     const size_t ssh = 16 * flag::kMaxChan * (4 * sizeof(double) + sizeof(float));
-    if (!attr) {
-      cudaFuncSetAttribute(flag_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssh);
-      attr = true;
-    }
+    if (smem_attr_once(attr, flag_stats_kernel, (int)ssh) != cudaSuccess) return -2;
     flag_stats_kernel<<<a.nbeam, flag::kStatThreads, ssh, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
@@ -825,19 +815,24 @@ static __device__ __align__(256) float g_flag_scratch[kNoAllocScratchFloats];
 
 namespace {
 constexpr int kMaxDevices = 64;
-float *g_scratch_addr[kMaxDevices] = {};   // device address per device, set up once
+// device address of the array per device, looked up once; atomic because
+// host threads may make their first call on a device concurrently (they
+// store the same value)
+std::atomic<float *> g_scratch_addr[kMaxDevices] = {};
 }  // namespace
 
-// Resolves the array's device address on the current device (once per
+// Resolves the array's device address on the current device `dev` (once per
 // device).  Returns nullptr on failure.
 static float *noalloc_scratch(int dev) {
   if (dev < 0 || dev >= kMaxDevices) return nullptr;
-  if (!g_scratch_addr[dev]) {
+  float *s = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!s) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_flag_scratch) != cudaSuccess) return nullptr;
-    g_scratch_addr[dev] = static_cast<float *>(p);
+    s = static_cast<float *>(p);
+    g_scratch_addr[dev].store(s, std::memory_order_release);
   }
-  return g_scratch_addr[dev];
+  return s;
 }
 
 }  // namespace dsax

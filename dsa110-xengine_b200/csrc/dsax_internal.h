@@ -1,10 +1,33 @@
 // dsax_internal.h -- launch-argument structs shared between the kernels and
 // the C-ABI layer (not installed; the public interface is include/dsax.h).
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace dsax {
+
+// Per-device "max dynamic shared memory" attribute of one kernel.
+// cudaFuncSetAttribute applies to the current device only, so the set-once
+// state is one bit per device (devices 0..63; higher ordinals set it on
+// every launch), kept in an atomic so that host threads driving different
+// contexts may launch concurrently.  Two threads racing on a device's first
+// launch both set the same value, which is harmless.
+struct SmemAttrOnce {
+  std::atomic<unsigned long long> done{0ull};
+};
+template <typename Kernel>
+inline cudaError_t smem_attr_once(SmemAttrOnce &once, Kernel kernel, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < 64) ? 1ull << dev : 0ull;
+  if (bit && (once.done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(reinterpret_cast<const void *>(kernel),
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && bit) once.done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
 
 // ---- error codes written to the device error word (bit flags) ----
 enum : int {

@@ -254,12 +254,9 @@ template <int CIN, int COUT, int CO_T, bool RELU>
 int conv_launch(const float *in, const float *gate, const float *wt, const float *bias, float *out,
                 int B, int H, int W, cudaStream_t st) {
   const size_t sh = (size_t)6 * (W + 2) * CIN * sizeof(float);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(conv3x3_kernel<CIN, COUT, CO_T, RELU>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, conv3x3_kernel<CIN, COUT, CO_T, RELU>, 200 * 1024) != cudaSuccess)
+    return -2;
   const int grid = B * ((H + 3) / 4);
   conv3x3_kernel<CIN, COUT, CO_T, RELU><<<grid, 256, sh, st>>>(in, gate, wt, bias, out, B, H, W);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
@@ -269,12 +266,8 @@ template <int CIN, int CO_T>
 int wgrad_launch(const float *in, const float *dz, const float *gate, int cout, float *part, int B,
                  int H, int W, int rpc, cudaStream_t st) {
   const size_t sh = ((size_t)(rpc + 2) * (W + 2) * CIN + (size_t)rpc * W * CO_T) * sizeof(float);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(conv3x3_wgrad_kernel<CIN, CO_T>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, conv3x3_wgrad_kernel<CIN, CO_T>, 200 * 1024) != cudaSuccess) return -2;
   dim3 grid(B * ((H + rpc - 1) / rpc), cout / CO_T);
   conv3x3_wgrad_kernel<CIN, CO_T><<<grid, 256, sh, st>>>(in, dz, gate, cout, part, B, H, W, rpc);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;

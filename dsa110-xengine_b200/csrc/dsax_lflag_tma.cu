@@ -620,13 +620,8 @@ int encode_grid_map(CUtensorMap *map, const uint16_t *grid, int64_t npp, int ch)
 template <int COUT, bool PROJ>
 int conv_tma_launch(const CUtensorMap &map, const LfTmaArgs &a, int num_sms, cudaStream_t st) {
   constexpr int smem = 1024 + lftma::kTaps * COUT * 128 + lftma::stages<COUT>() * lftma::kABytes;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(lf_conv_tma_kernel<COUT, PROJ>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-      return -2;
-    attr = true;
-  }
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, lf_conv_tma_kernel<COUT, PROJ>, smem) != cudaSuccess) return -2;
   const int64_t npp = (int64_t)a.B * (a.H + 2) * (a.W + 2);
   const int ntiles = (int)((npp + 127) / 128);
   const int grid = ntiles < num_sms ? ntiles : num_sms;
@@ -666,13 +661,8 @@ int lf_tma_layer1(const LfNet &net, const uint8_t *wimg, const uint16_t *featp, 
   const int64_t npp = (int64_t)B * (H + 2) * (W + 2);
   CUtensorMap mf;
   if (encode_grid_map(&mf, featp, npp, 8) != 0) return -1;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(lf_conv1_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             lf1::kSmemBytes) != cudaSuccess)
-      return -2;
-    attr = true;
-  }
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, lf_conv1_tma_kernel, lf1::kSmemBytes) != cudaSuccess) return -2;
   Lf1Args a{};
   a.wimg = wimg; a.bias = net.b[0]; a.out = act1p; a.err = err;
   a.B = B; a.H = H; a.W = W; a.wait_limit_ns = wait_limit_ns;

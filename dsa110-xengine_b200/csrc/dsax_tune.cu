@@ -1,11 +1,10 @@
 // dsax_tune.cu -- autotuner: times the interchangeable kernel variants of
 // a stage on the context's own geometry and device, keeps the fastest in
 // the context, and reports every timing.  Candidates for the captured-block
-// correlator: (1) one fused kernel on the captured layout, (2) corner turn
-// to the REORDER layout + row-load correlator, (3) corner turn to channel-
-// major streams + bulk-copy-fed correlator (two kinds of operand staging
-// and tile shape: 64-packet stages of [re,im | -im,re] vs 128-packet R/I
-// stages).
+// correlator (corr_path): (1) one fused kernel on the captured layout,
+// (2) corner turn to the REORDER layout + row-load correlator, (3) corner
+// turn to channel-major streams + correlator fed by direct coalesced loads,
+// (4) the same correlator fed by one bulk copy per 64-packet stage.
 #include <cstring>
 #include <cuda_runtime.h>
 
