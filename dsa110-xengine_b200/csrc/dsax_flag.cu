@@ -1,15 +1,24 @@
-// dsax_flag.cu -- the plain RFI flagger on the GPU: one HBM pass for all
-// per-(beam, channel) and per-(beam, time) statistics, then the
-// median/MAD decisions on the device (the reference does them on the host).
+// dsax_flag.cu -- the plain RFI flagger on the GPU, statistics and data path.
 //
-// Replaces src/gpu_flagger.cu: calc_spectrum (:175-223), calc_varspec
-// (:229-278), calc_maxspec (:283-319; the reference calls calc_spectrum in
-// its place at :1334 -- parity mode keeps that), calc_ppspec (:324-376),
-// make_ts (:414-453), and the host decisions medval/channflag/
-// simple_channflag/simple_tsflag (:534-720) run in the order of
-// :1340-1398.  The shapes the reference hard-codes ([64][16384][1024],
-// ZeroChannels 128, nFiltSize 21, TBIN 128, FBIN 8, T/16) are parameters.
+// Replaces src/gpu_flagger.cu, per block in the order of its main loop
+// (:1290-1410):
+//   scaley (:382-394, once a baseline exists)        -> fused into the
+//   calc_spectrum / calc_varspec / calc_maxspec /       statistics pass
+//   calc_ppspec (:175-376; the reference calls           (one HBM read)
+//   calc_spectrum in calc_maxspec's place at :1334 -- parity mode keeps that)
+//   total-power modulation check (:1313-1330)        -> flag_chan_kernel
+//   channflag x3, simple_channflag (:1340-1347),        (decisions on the
+//   calc_bpwr (:759-769), gather_mask                   GPU, per beam)
+//   flag (:459-474), then make_ts (:414-453)         -> flag_apply_kernel
+//                                                       (reads only the
+//                                                       flagged columns)
+//   simple_tsflag (:612-653), flagts (:479-494)      -> flag_ts_kernel
+// and fix_zspec (:114-170) + median_calc (:771-798) for the scaley
+// baseline.  The shapes the reference hard-codes ([64][16384][1024] uint8,
+// ZeroChannels 128, nFiltSize 21, TBIN 128, FBIN 8, T/16) are parameters;
+// the filterbank may be uint8 (the reference's type) or FP32.
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "dsax_internal.h"
@@ -19,107 +28,16 @@
 namespace dsax {
 
 namespace flag {
-constexpr int kStatThreads = 512;   // 16 warps per beam
-constexpr int kMaxChan = 128;       // four channels per lane
+constexpr int kStatThreads = 256;
+constexpr int kStages = 3;
+constexpr int kStageTarget = 24576;   // bytes per pipeline stage (upper bound)
+constexpr int kMaxChan = 1024;
+constexpr int kChanThreads = 256;     // four decision groups of 64 threads
+constexpr int kApplyRows = 256;       // rows per apply CTA (one per thread)
+constexpr int kTsThreads = 256;
+constexpr int kMaxTsBase = 4096;
+constexpr int kLfMaxChan = 128;       // learned-flagger features: channels per beam
 constexpr int kDecThreads = 256;
-}  // namespace flag
-
-// ---------------------------------------------------------------- stats
-// One CTA per beam.  Warp w owns the TBIN-sample bins w, w+16, ...; lane l
-// owns channels l, l+32, l+64, l+96.  Sums are FP64 in sample order within a
-// bin (the oracle's order), max/bin extremes exact.
-__global__ void __launch_bounds__(flag::kStatThreads) flag_stats_kernel(FlagArgs a) {
-  constexpr int NL = flag::kMaxChan / 32;   // channels per lane
-  const int b = blockIdx.x;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nw = blockDim.x >> 5;
-  const int T = a.ntime, C = a.nchan, TB = a.tbin;
-  const int nbins = T / TB;
-  const float *xb = a.x + (int64_t)b * T * C;
-
-  double s[NL], q[NL], bmax[NL], bmin[NL], bs[NL];
-  float m[NL];
-#pragma unroll
-  for (int k = 0; k < NL; ++k) {
-    s[k] = 0.0; q[k] = 0.0; bmax[k] = -1e300; bmin[k] = 1e300; m[k] = -INFINITY;
-  }
-  auto row = [&](int t, bool bin) {
-    const float *rp = xb + (int64_t)t * C;
-    double r = 0.0;
-#pragma unroll
-    for (int k = 0; k < NL; ++k) {
-      const int c = lane + 32 * k;
-      const float v = c < C ? __ldg(rp + c) : 0.0f;
-      if (bin) bs[k] += v; else s[k] += v;
-      q[k] += (double)v * v;
-      if (c < C) m[k] = fmaxf(m[k], v);
-      r += v;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-    if (lane == 0) a.ts[(int64_t)b * T + t] = (float)(r / C);
-  };
-  for (int bin = warp; bin < nbins; bin += nw) {
-#pragma unroll
-    for (int k = 0; k < NL; ++k) bs[k] = 0.0;
-    for (int t = bin * TB; t < (bin + 1) * TB; ++t) row(t, true);
-#pragma unroll
-    for (int k = 0; k < NL; ++k) {
-      s[k] += bs[k];
-      const double mb = bs[k] / TB;
-      bmax[k] = fmax(bmax[k], mb);
-      bmin[k] = fmin(bmin[k], mb);
-    }
-  }
-  // samples beyond the last whole bin (T % TB): sums and max only
-  for (int t = nbins * TB + warp; t < T; t += nw) row(t, false);
-
-  extern __shared__ double fsh[];
-  double *sh_s = fsh, *sh_q = sh_s + 16 * flag::kMaxChan;
-  double *sh_bmax = sh_q + 16 * flag::kMaxChan, *sh_bmin = sh_bmax + 16 * flag::kMaxChan;
-  float *sh_m = reinterpret_cast<float *>(sh_bmin + 16 * flag::kMaxChan);
-#pragma unroll
-  for (int k = 0; k < NL; ++k) {
-    const int c = lane + 32 * k;
-    sh_s[warp * flag::kMaxChan + c] = s[k];
-    sh_q[warp * flag::kMaxChan + c] = q[k];
-    sh_m[warp * flag::kMaxChan + c] = m[k];
-    sh_bmax[warp * flag::kMaxChan + c] = bmax[k];
-    sh_bmin[warp * flag::kMaxChan + c] = bmin[k];
-  }
-  __syncthreads();
-  if (threadIdx.x < C) {
-    const int c = threadIdx.x;
-    double ss = 0.0, qq = 0.0, bx = -1e300, bn = 1e300;
-    float mm = -INFINITY;
-    for (int w = 0; w < nw; ++w) {
-      ss += sh_s[w * flag::kMaxChan + c]; qq += sh_q[w * flag::kMaxChan + c];
-      mm = fmaxf(mm, sh_m[w * flag::kMaxChan + c]);
-      bx = fmax(bx, sh_bmax[w * flag::kMaxChan + c]); bn = fmin(bn, sh_bmin[w * flag::kMaxChan + c]);
-    }
-    const double mean = ss / T;
-    const double var = fmax(qq / T - mean * mean, 0.0);
-    const int o = b * C + c;
-    a.spec[o] = (float)mean;
-    a.var[o] = (float)var;
-    a.maxs[o] = a.parity ? (float)mean : mm;
-    a.pp[o] = nbins > 0 ? (float)(bx - bn) : 0.0f;
-  }
-}
-
-// ---------------------------------------------------------------- stats, staged
-// Same statistics as flag_stats_kernel for the common shapes (nchan a
-// multiple of 4, one TBIN-sample bin <= 32 KB): one CTA per beam streams the
-// beam's bins through a 3-stage cp.async ring in shared memory (each bin is
-// one contiguous TB x C x 4-byte run of the [T][C] filterbank), so the HBM
-// reads stay in flight while the previous bin is reduced.  Thread (p, c4)
-// owns channels 4c4..4c4+3 and rows p, p+P, ... of every bin; per-row sums
-// (the time series) and per-bin sums are finished in shared memory in a
-// fixed order, so results do not depend on scheduling.
-namespace flag {
-constexpr int kFastThreads = 256;
-constexpr int kFastStages = 3;
-constexpr int kFastStageMax = 32768;
 }  // namespace flag
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
@@ -131,122 +49,226 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-__global__ void __launch_bounds__(flag::kFastThreads, 2) flag_stats_staged_kernel(FlagArgs a) {
-  constexpr int S = flag::kFastStages;
-  const int b = blockIdx.x, tid = threadIdx.x;
-  const int T = a.ntime, C = a.nchan, TB = a.tbin;
-  const int C4 = C >> 2, P = flag::kFastThreads / C4;
-  const int p = tid / C4, c4 = tid - p * C4;
+// ---------------------------------------------------------------- elements
+// Four consecutive channels of one row: FP32 (16 bytes) or uint8 (4 bytes).
+template <typename E>
+__device__ __forceinline__ void ld4(const void *p, float (&v)[4]) {
+  if constexpr (std::is_same<E, float>::value) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else {
+    const uint32_t w = *reinterpret_cast<const uint32_t *>(p);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) v[j] = (float)((w >> (8 * j)) & 255u);
+  }
+}
+template <typename E>
+__device__ __forceinline__ void st4(void *p, const float (&v)[4]) {
+  if constexpr (std::is_same<E, float>::value) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {   // values are already integers in [0, 255]
+    *reinterpret_cast<uint32_t *>(p) = (uint32_t)v[0] | ((uint32_t)v[1] << 8) |
+                                       ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
+  }
+}
+template <typename E>
+__device__ __forceinline__ const E *elem_in(const FlagArgs &a) {
+  if constexpr (std::is_same<E, float>::value) return a.x; else return a.xu8;
+}
+template <typename E>
+__device__ __forceinline__ E *elem_out(const FlagArgs &a) {
+  if constexpr (std::is_same<E, float>::value) return a.xw; else return a.xw8;
+}
+
+// scaley (src/gpu_flagger.cu:382-394): (x - spec0) * (SIG / sqrtf(var0)) + MN,
+// with the reference's mixed float / double evaluation; uint8 data are
+// requantised as (unsigned char)(__float2uint_rn(2 val) / 2), which wraps
+// modulo 256 above 255.
+template <typename E>
+__device__ __forceinline__ float scaley1(float x, float s0, double k, float mn) {
+  const float val = (float)((double)(x - s0) * k + (double)mn);
+  if constexpr (std::is_same<E, float>::value) {
+    return val;
+  } else {
+    return (float)((__float2uint_rn(2.0f * val) / 2u) & 255u);
+  }
+}
+
+// The replacement level MN * bpwr as the element type: uint8 is the C
+// conversion of `data[idx] = MN * bpwr[bm]` (:473): truncation toward zero,
+// clamped to [0, 255] by the device conversion.
+template <typename E>
+__device__ __forceinline__ E repl_elem(float r) {
+  if constexpr (std::is_same<E, float>::value) {
+    return r;
+  } else {
+    return (uint8_t)__float2uint_rz(fminf(r, 255.0f));
+  }
+}
+
+// ---------------------------------------------------------------- statistics
+// One CTA per (channel slab of up to kFlagSlab channels, beam).  The slab's
+// rows stream through a three-stage cp.async ring of `rs` rows each (rs
+// divides TBIN).  Thread (p, g) owns channels 4g..4g+3 of the slab and rows
+// p, p + P, ... of every stage; sums are FP64 and finished in shared memory
+// in a fixed order, so results do not depend on scheduling.  With a scaley
+// baseline the stage is normalised in shared memory first and written back
+// (the statistics then describe the normalised block, as in the reference).
+// Per row the slab's raw sum goes to rowsum (or to ts when there is one
+// slab); flag_apply_kernel turns it into the channel-mean series after the
+// flagged columns are replaced.
+template <typename E>
+__global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagArgs a) {
+  constexpr int S = flag::kStages;
+  constexpr int ES = (int)sizeof(E);
+  const int slab = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+  const int T = a.ntime, C = a.nchan, TB = a.tbin, RS = a.rs;
+  const int c0 = slab * kFlagSlab;
+  const int cs = min(kFlagSlab, C - c0);
+  const int G4 = cs >> 2, P = flag::kStatThreads / G4;
+  const int p = tid / G4, g = tid - p * G4;
   const bool active = p < P;
-  const int nbins = T / TB;
-  const int stage_f4 = TB * C4;                     // float4 per bin
-  const int stage_bytes = (stage_f4 * 16 + 127) & ~127;
-  const float4 *xb = reinterpret_cast<const float4 *>(a.x + (int64_t)b * T * C);
+  const int nbins = T / TB, spb = TB / RS, nst = nbins * spb;
+  const int rb = cs * ES;                        // bytes of one slab row (multiple of 16)
+  const int ck = rb >> 4;                        // 16-byte chunks per row
+  const int stage_bytes = (RS * rb + 127) & ~127;
+  const int64_t rstride = (int64_t)C * ES;
+  const uint8_t *xb =
+      reinterpret_cast<const uint8_t *>(elem_in<E>(a) + (int64_t)b * T * C + c0);
+  E *xw = elem_out<E>(a);
+  const bool scale = a.spec0 != nullptr;
 
   extern __shared__ __align__(16) uint8_t fs_raw[];
   const uint32_t sbase = smem_u32(fs_raw);
-  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * stage_bytes);   // [TB][C4]
-  double *sm_bp = sm_rs + TB * C4;                                         // [P][C]
+  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * stage_bytes);   // [RS][G4]
+  double *sm_bp = sm_rs + RS * G4;                                         // [P][cs]
+  double *sm_k = sm_bp + P * cs;                                           // [cs]
+  float *sm_s0 = reinterpret_cast<float *>(sm_k + cs);                     // [cs]
 
-  auto issue = [&](int bin) {
-    if (bin < nbins) {
-      const float4 *src = xb + (int64_t)bin * stage_f4;
-      const uint32_t dst = sbase + (uint32_t)(bin % S) * stage_bytes;
-      for (int i = tid; i < stage_f4; i += flag::kFastThreads) cp_async16(dst + 16u * i, src + i);
+  if (scale)
+    for (int c = tid; c < cs; c += flag::kStatThreads) {
+      sm_s0[c] = a.spec0[b * C + c0 + c];
+      sm_k[c] = (double)a.sig / (double)sqrtf(a.var0[b * C + c0 + c]);
+    }
+  __syncthreads();
+
+  auto issue = [&](int st) {
+    if (st < nst) {
+      const uint8_t *src = xb + (int64_t)st * RS * rstride;
+      const uint32_t dst = sbase + (uint32_t)(st % S) * stage_bytes;
+      for (int i = tid; i < RS * ck; i += flag::kStatThreads) {
+        const int r = i / ck, k = i - r * ck;
+        cp_async16(dst + r * rb + 16 * k, src + r * rstride + 16 * k);
+      }
     }
     cp_async_commit();
   };
-
-  double s[4], q[4];
+  auto put_row = [&](int t, double r) {
+    if (a.nslab == 1)
+      a.ts[(int64_t)b * T + t] = a.ts_mean ? (float)(r / C) : (float)r;
+    else
+      a.rowsum[((int64_t)b * a.nslab + slab) * T + t] = (float)r;
+  };
+  // normalise (if scaling) and accumulate the four channels of one row
+  double s[4], q[4], bs[4];
   float m[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) { s[j] = 0.0; q[j] = 0.0; m[j] = -INFINITY; }
-  double bmax = -1e300, bmin = 1e300;   // owned by thread tid < C (channel tid)
+  for (int j = 0; j < 4; ++j) { s[j] = 0.0; q[j] = 0.0; bs[j] = 0.0; m[j] = -INFINITY; }
+  auto take = [&](float (&v)[4], int t, bool bin) -> double {
+    if (scale) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[j] = scaley1<E>(v[j], sm_s0[4 * g + j], sm_k[4 * g + j], a.mn);
+      if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
+    }
+    double r = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (bin) bs[j] += v[j]; else s[j] += v[j];
+      q[j] += (double)v[j] * v[j];
+      m[j] = fmaxf(m[j], v[j]);
+      r += v[j];
+    }
+    return r;
+  };
+  double bmax = -1e300, bmin = 1e300;   // owned by thread tid < cs (channel tid)
 
 #pragma unroll
   for (int i = 0; i < S - 1; ++i) issue(i);
-  for (int bin = 0; bin < nbins; ++bin) {
-    issue(bin + S - 1);
+  for (int st = 0; st < nst; ++st) {
+    issue(st + S - 1);
     cp_async_wait<S - 1>();
     __syncthreads();
+    uint8_t *sp = fs_raw + (st % S) * stage_bytes;
+    const int t0 = st * RS;
     if (active) {
-      const float4 *st = reinterpret_cast<const float4 *>(fs_raw + (bin % S) * stage_bytes);
-      double bs[4] = {0.0, 0.0, 0.0, 0.0};
-      for (int t = p; t < TB; t += P) {
-        const float4 v4 = st[t * C4 + c4];
-        const float v[4] = {v4.x, v4.y, v4.z, v4.w};
-        double r = 0.0;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          bs[j] += v[j];
-          q[j] += (double)v[j] * v[j];
-          m[j] = fmaxf(m[j], v[j]);
-          r += v[j];
-        }
-        sm_rs[t * C4 + c4] = r;
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        s[j] += bs[j];
-        sm_bp[p * C + 4 * c4 + j] = bs[j];
+      for (int r = p; r < RS; r += P) {
+        float v[4];
+        ld4<E>(sp + r * rb + 4 * g * ES, v);
+        const double rr = take(v, t0 + r, true);
+        if (a.pix_sum && scale) st4<E>(sp + r * rb + 4 * g * ES, v);
+        sm_rs[r * G4 + g] = rr;
       }
     }
-    if (a.pix_sum) {   // downsampled spectrogram: tbin / tds whole pixel rows per bin
-      const float *sf = reinterpret_cast<const float *>(fs_raw + (bin % S) * stage_bytes);
-      const int npr = TB / a.tds, H = T / a.tds;
-      for (int i = tid; i < npr * C; i += flag::kFastThreads) {
-        const int pr = i / C, c = i - pr * C;
+    if (a.pix_sum) {   // downsampled spectrogram: rs / tds whole pixel rows per stage
+      __syncthreads();
+      const float *sf = reinterpret_cast<const float *>(sp);
+      const int npr = RS / a.tds, H = T / a.tds;
+      for (int i = tid; i < npr * cs; i += flag::kStatThreads) {
+        const int pr = i / cs, c = i - pr * cs;
         float sum = 0.f, mx = -INFINITY;
         for (int r = 0; r < a.tds; ++r) {
-          const float v = sf[(pr * a.tds + r) * C + c];
+          const float v = sf[(pr * a.tds + r) * cs + c];
           sum += v;
           mx = fmaxf(mx, v);
         }
-        const int64_t o = ((int64_t)b * H + bin * npr + pr) * C + c;
+        const int64_t o = ((int64_t)b * H + t0 / a.tds + pr) * C + c0 + c;
         a.pix_sum[o] = sum;
         a.pix_max[o] = mx;
       }
     }
     __syncthreads();
-    if (tid < TB) {
+    if (tid < RS) {
       double r = 0.0;
-      for (int k = 0; k < C4; ++k) r += sm_rs[tid * C4 + k];
-      a.ts[(int64_t)b * T + (int64_t)bin * TB + tid] = (float)(r / C);
+      for (int k = 0; k < G4; ++k) r += sm_rs[tid * G4 + k];
+      put_row(t0 + tid, r);
     }
-    if (tid < C) {
-      double bsum = 0.0;
-      for (int k = 0; k < P; ++k) bsum += sm_bp[k * C + tid];
-      const double mb = bsum / TB;
-      bmax = fmax(bmax, mb);
-      bmin = fmin(bmin, mb);
+    if ((st + 1) % spb == 0) {   // the last stage of a TBIN bin: bin means per channel
+      if (active) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          sm_bp[p * cs + 4 * g + j] = bs[j];
+          s[j] += bs[j];
+          bs[j] = 0.0;
+        }
+      }
+      __syncthreads();
+      if (tid < cs) {
+        double bsum = 0.0;
+        for (int k = 0; k < P; ++k) bsum += sm_bp[k * cs + tid];
+        const double mb = bsum / TB;
+        bmax = fmax(bmax, mb);
+        bmin = fmin(bmin, mb);
+      }
     }
   }
   cp_async_wait<0>();
-  // rows beyond the last whole bin (T % TB): sums, squares, max and the
-  // time series, read directly
-  for (int t0 = nbins * TB; t0 < T; t0 += TB) {
+  // rows beyond the last whole bin (T % TB): sums, squares, max and row
+  // sums, read directly
+  for (int t0 = nbins * TB; t0 < T; t0 += RS) {
     __syncthreads();
-    const int rows = min(TB, T - t0);
+    const int rows = min(RS, T - t0);
     if (active) {
-      for (int t = p; t < rows; t += P) {
-        const float4 v4 = __ldg(xb + (int64_t)(t0 + t) * C4 + c4);
-        const float v[4] = {v4.x, v4.y, v4.z, v4.w};
-        double r = 0.0;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          s[j] += v[j];
-          q[j] += (double)v[j] * v[j];
-          m[j] = fmaxf(m[j], v[j]);
-          r += v[j];
-        }
-        sm_rs[t * C4 + c4] = r;
+      for (int r = p; r < rows; r += P) {
+        float v[4];
+        ld4<E>(xb + (int64_t)(t0 + r) * rstride + 4 * g * ES, v);
+        sm_rs[r * G4 + g] = take(v, t0 + r, false);
       }
     }
     __syncthreads();
     if (tid < rows) {
       double r = 0.0;
-      for (int k = 0; k < C4; ++k) r += sm_rs[tid * C4 + k];
-      a.ts[(int64_t)b * T + t0 + tid] = (float)(r / C);
+      for (int k = 0; k < G4; ++k) r += sm_rs[tid * G4 + k];
+      put_row(t0 + tid, r);
     }
   }
   // per-channel totals over the P row phases, in phase order
@@ -257,20 +279,20 @@ __global__ void __launch_bounds__(flag::kFastThreads, 2) flag_stats_staged_kerne
     if (active) {
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        sm_bp[p * C + 4 * c4 + j] = pass == 0 ? s[j] : pass == 1 ? q[j] : (double)m[j];
+        sm_bp[p * cs + 4 * g + j] = pass == 0 ? s[j] : pass == 1 ? q[j] : (double)m[j];
     }
     __syncthreads();
-    if (tid < C) {
+    if (tid < cs) {
       for (int k = 0; k < P; ++k) {
-        const double v = sm_bp[k * C + tid];
+        const double v = sm_bp[k * cs + tid];
         tot[pass] = pass < 2 ? tot[pass] + v : fmax(tot[pass], v);
       }
     }
   }
-  if (tid < C) {
+  if (tid < cs) {
     const double mean = tot[0] / T;
     const double var = fmax(tot[1] / T - mean * mean, 0.0);
-    const int o = b * C + tid;
+    const int o = b * C + c0 + tid;
     a.spec[o] = (float)mean;
     a.var[o] = (float)var;
     a.maxs[o] = a.parity ? (float)mean : (float)tot[2];
@@ -278,19 +300,436 @@ __global__ void __launch_bounds__(flag::kFastThreads, 2) flag_stats_staged_kerne
   }
 }
 
-bool flag_stats_staged_ok(const FlagArgs &a) {
-  const bool pix_ok = !a.pix_sum || (a.tds > 0 && a.tbin % a.tds == 0 && a.ntime % a.tbin == 0);
-  return a.nchan % 4 == 0 && (reinterpret_cast<uintptr_t>(a.x) & 15u) == 0 &&
-         (int64_t)a.tbin * a.nchan * 4 <= flag::kFastStageMax && a.tbin <= flag::kFastThreads &&
-         pix_ok;
+// ---------------------------------------------------------------- decisions
+// (the order-statistic helpers: radix select below, the rank-count medians
+// and the learned-flagger feature kernel)
+// The k-th smallest of v[0..n) (0-based; the value rank counting with
+// ties by index returns) by a four-pass MSB-first radix select over
+// order-preserving 32-bit keys: per pass a 256-bin shared histogram of the
+// candidates that still match the selected prefix, then one warp finds the
+// bin holding rank k.  O(n) work instead of O(n^2); finite inputs.
+__device__ __forceinline__ uint32_t ordered_key(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ float grp_radix_select(const float *v, int n, int k, uint32_t *hist, uint32_t *sel,
+                                  int gtid, int gsize, int bid) {
+  uint32_t prefix = 0u, pmask = 0u;
+  int kk = k;
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    for (int i = gtid; i < 256; i += gsize) hist[i] = 0u;
+    named_bar(bid, gsize);
+    for (int i = gtid; i < n; i += gsize) {
+      const uint32_t u = ordered_key(v[i]);
+      if ((u & pmask) == prefix) atomicAdd(&hist[(u >> shift) & 255u], 1u);
+    }
+    named_bar(bid, gsize);
+    if (gtid < 32) {   // the first warp: bin holding rank kk
+      uint32_t c[8], tot = 0u;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) { c[e] = hist[8 * gtid + e]; tot += c[e]; }
+      uint32_t incl = tot;   // inclusive scan over lanes
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (gtid >= o) incl += y;
+      }
+      const uint32_t excl = incl - tot;
+      if (excl <= (uint32_t)kk && (uint32_t)kk < incl) {
+        uint32_t run = excl;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          if ((uint32_t)kk < run + c[e]) {
+            sel[0] = (uint32_t)(8 * gtid + e);
+            sel[1] = (uint32_t)kk - run;
+            break;
+          }
+          run += c[e];
+        }
+      }
+    }
+    named_bar(bid, gsize);
+    prefix |= sel[0] << shift;
+    pmask |= 0xFFu << shift;
+    kk = (int)sel[1];
+    named_bar(bid, gsize);
+  }
+  const uint32_t u = (prefix & 0x80000000u) ? (prefix & 0x7FFFFFFFu) : ~prefix;
+  return __uint_as_float(u);
 }
 
-static size_t staged_stats_smem(const FlagArgs &a) {
-  const int C4 = a.nchan / 4, P = flag::kFastThreads / C4;
-  const size_t stage = ((size_t)a.tbin * a.nchan * 4 + 127) & ~(size_t)127;
-  return flag::kFastStages * stage + sizeof(double) * ((size_t)a.tbin * C4 + (size_t)P * a.nchan);
+// channflag (src/gpu_flagger.cu:655-720) for one beam in a group of `gsize`
+// threads: forward nFiltSize-channel median detrend, then |x| > Thr * MAD
+// of the detrended spectrum inside the guard band (compared against 0, as
+// the reference does).  Medians are lower medians (medval, :534-556).
+__device__ void grp_channflag(const float *sb, float thr, const FlagArgs &a, uint8_t *mask,
+                              float *corr, float *tmp, uint32_t *hist, uint32_t *sel, int gtid,
+                              int gsize, int bid) {
+  const int C = a.nchan, G = a.guard, F = a.filt, n = C - 2 * G;
+  const int kf = (F + 1) / 2 - 1;
+  for (int idx = gtid; idx < n * F; idx += gsize) {   // forward median detrend
+    const int jj = idx / F, i = idx - jj * F;
+    const int j = G + jj;
+    const int w0 = (C - G - j >= F) ? j : C - G - F;
+    const float x = sb[w0 + i];
+    int r = 0;
+    for (int q = 0; q < F; ++q) {
+      const float y = sb[w0 + q];
+      r += (y < x) || (y == x && q < i);
+    }
+    if (r == kf) corr[jj] = sb[j] - x;
+  }
+  named_bar(bid, gsize);
+  const int k = (n + 1) / 2 - 1;
+  const float med = grp_radix_select(corr, n, k, hist, sel, gtid, gsize, bid);
+  for (int i = gtid; i < n; i += gsize) tmp[i] = fabsf(corr[i] - med);
+  named_bar(bid, gsize);
+  const float mad = grp_radix_select(tmp, n, k, hist, sel, gtid, gsize, bid);
+  for (int i = gtid; i < n; i += gsize) {
+    const float v = corr[i];
+    if (v > thr * mad || v < -thr * mad) mask[G + i] = 1;
+  }
 }
 
+// The channel decisions of one beam (one CTA), after the block-level steps:
+//  - total power of the block (sum of every beam's spectrum, FP64, the same
+//    order in every CTA) and, with modcheck, the modulation test against
+//    the previous flagged block (:1313-1330): at or above mod_thresh the
+//    block is replaced by noise and nothing else is flagged;
+//  - calc_bpwr (:759-769) when pwr is set: the beam's replacement level;
+//  - the four channel tests, concurrently in four groups of 64 threads:
+//    channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
+//    channflag(max, Thr), simple_channflag(pp, Thr / sqrt(FBIN)) (one-sided
+//    FBIN-channel mean; parity mode keeps the reference's spec[j] sum,
+//    :594), ORed into one mask, plus the permanent flag channels.
+__global__ void __launch_bounds__(flag::kChanThreads) flag_chan_kernel(FlagArgs a) {
+  const int b = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
+  const int C = a.nchan, G = a.guard, n = C - 2 * G, BC = a.nbeam * C;
+  extern __shared__ float dsh[];                          // [4 groups][3][C]
+  uint8_t *cmask = reinterpret_cast<uint8_t *>(dsh + 12 * C);   // [C]
+  __shared__ uint32_t hist[4][256], sel[4][2];
+  __shared__ double red[flag::kChanThreads];
+  __shared__ int replaced_sh;
+
+  if (a.modcheck || a.tpwr_out) {
+    double acc = 0.0;
+    for (int i = tid; i < BC; i += flag::kChanThreads) acc += a.spec[i];
+    red[tid] = acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int rep = 0;
+    if (a.modcheck || a.tpwr_out) {
+      double tp = 0.0;
+      for (int k = 0; k < flag::kChanThreads; ++k) tp += red[k];
+      if (a.modcheck) {
+        const double prev = *a.prev_tpwr;
+        if (prev > 0.0 && fabs(tp - prev) / prev >= (double)a.mod_thresh) rep = 1;
+      }
+      if (b == 0 && a.tpwr_out) *a.tpwr_out = tp;
+    }
+    if (b == 0 && a.status) a.status[0] = rep;
+    replaced_sh = rep;
+    if (!rep && a.pwr && a.bpwr) {   // calc_bpwr: float sum over every channel, in order
+      float acc = 0.0f;
+      for (int c = 0; c < C; ++c) acc += a.spec[b * C + c];
+      a.bpwr[b] = (float)(((double)acc / (double)(C - 2 * G)) / (double)a.mn);
+    }
+  }
+  for (int c = tid; c < C; c += flag::kChanThreads) cmask[c] = 0;
+  __syncthreads();
+  if (!replaced_sh) {
+    const int g = warp >> 1, gsize = 64, gtid = tid - 64 * g, bid = 1 + g;
+    float *sb = dsh + g * 3 * C, *corr = sb + C, *tmp = corr + C;
+    const float *src = g == 0 ? a.spec : g == 1 ? a.var : g == 2 ? a.maxs : a.pp;
+    for (int c = gtid; c < C; c += gsize)
+      sb[c] = src[b * C + c] - ((g == 0 && a.oldspec) ? a.oldspec[b * C + c] : 0.0f);
+    named_bar(bid, gsize);
+    if (g < 3) {
+      const float thr = g == 1 ? a.thresh + a.var_add : a.thresh;
+      grp_channflag(sb, thr, a, cmask, corr, tmp, hist[g], sel[g], gtid, gsize, bid);
+    } else {   // simple_channflag (:559-610)
+      for (int i = gtid; i < n; i += gsize) corr[i] = sb[G + i];
+      named_bar(bid, gsize);
+      const int k = (n + 1) / 2 - 1;
+      const float med = grp_radix_select(corr, n, k, hist[g], sel[g], gtid, gsize, bid);
+      for (int i = gtid; i < n; i += gsize) tmp[i] = fabsf(corr[i] - med);
+      named_bar(bid, gsize);
+      const float mad = grp_radix_select(tmp, n, k, hist[g], sel[g], gtid, gsize, bid);
+      const float mythr = (float)((double)a.thresh / sqrt((double)a.fbin));
+      for (int j = G + gtid; j < C - G - a.fbin; j += gsize) {
+        float vv = 0.0f;
+        for (int q = 0; q < a.fbin; ++q) vv += a.parity ? sb[j] : sb[j + q];
+        vv = vv / (float)a.fbin - med;
+        if (vv > mythr * mad) cmask[j] = 1;
+      }
+    }
+    __syncthreads();
+    if (tid == 0)
+      for (int q = 0; q < a.nperm; ++q) {
+        const int j = a.perm[q];
+        if (j >= G && j < C - G) cmask[j] = 1;
+      }
+  }
+  __syncthreads();
+  int nflag = 0;
+  for (int c = tid; c < C; c += flag::kChanThreads) {
+    a.chanmask[b * C + c] = cmask[c];
+    nflag += cmask[c];
+  }
+  if (nflag && a.counts) atomicAdd(a.counts, nflag);
+}
+
+// flag (:459-474) followed by make_ts (:414-453): the flagged columns of a
+// beam are replaced by MN * bpwr[beam] (clean mode) and the channel-mean
+// time series is formed from the replaced data.  Only the flagged columns
+// are read: ts = (row sum from the statistics pass + sum over flagged
+// channels of (level - x)) / nchan.  For uint8 every term is an exact
+// integer, so ts equals the reference's float tree sum / NCHAN_P bit for
+// bit.  When the modulation check replaced the block, clean mode writes the
+// noise block into every beam (:1323-1324) and the series is that of the
+// noise.  One thread per row, grid (row chunks, beams).
+template <typename E>
+__global__ void __launch_bounds__(flag::kApplyRows) flag_apply_kernel(FlagArgs a) {
+  const int b = blockIdx.y, tid = threadIdx.x;
+  const int T = a.ntime, C = a.nchan;
+  const int t0 = blockIdx.x * flag::kApplyRows, t = t0 + tid;
+  __shared__ short fl[flag::kMaxChan];
+  __shared__ int nf_sh;
+  const bool replaced = a.status && a.status[0];
+  const E *xin = (a.spec0 && elem_out<E>(a)) ? elem_out<E>(a) : elem_in<E>(a);
+  E *xw = a.clean ? elem_out<E>(a) : nullptr;
+  if (replaced) {
+    const E *nz = static_cast<const E *>(a.noise);
+    const int rows = min(flag::kApplyRows, T - t0);
+    if (xw && nz)
+      for (int i = tid; i < rows * C; i += flag::kApplyRows)
+        xw[((int64_t)b * T + t0) * C + i] = nz[(int64_t)t0 * C + i];
+    if (t < T && nz) {
+      double r = 0.0;
+      for (int c = 0; c < C; ++c) r += (float)nz[(int64_t)t * C + c];
+      a.ts[(int64_t)b * T + t] = (float)(r / C);
+    }
+    return;
+  }
+  if (tid == 0) {
+    int k = 0;
+    for (int c = 0; c < C; ++c)
+      if (a.chanmask[b * C + c]) fl[k++] = (short)c;
+    nf_sh = k;
+  }
+  __syncthreads();
+  if (t >= T) return;
+  const int nf = nf_sh;
+  const E re = repl_elem<E>(a.mn * (a.bpwr ? a.bpwr[b] : 1.0f));
+  const float rf = (float)re;
+  double corr = 0.0;
+  if (nf) {
+    const E *row = xin + ((int64_t)b * T + t) * C;
+    E *wrow = xw ? xw + ((int64_t)b * T + t) * C : nullptr;
+    for (int k = 0; k < nf; ++k) {
+      const int c = fl[k];
+      corr += (double)(rf - (float)row[c]);
+      if (wrow) wrow[c] = re;
+    }
+  }
+  double rsum;
+  if (a.nslab == 1) {
+    rsum = a.ts[(int64_t)b * T + t];
+  } else {
+    rsum = 0.0;
+    for (int s = 0; s < a.nslab; ++s) rsum += a.rowsum[((int64_t)b * a.nslab + s) * T + t];
+  }
+  a.ts[(int64_t)b * T + t] = (float)((rsum + corr) / C);
+}
+
+// simple_tsflag (:612-653) and flagts (:479-494) for one beam: median and
+// MAD (lower medians, by radix select) of the first ts_base samples of the
+// series, rows with ts - med > TsThr * MAD flagged (one-sided); clean mode
+// then sets channels [guard, nchan - guard) of every flagged row to the
+// beam's level.
+template <typename E>
+__global__ void __launch_bounds__(flag::kTsThreads) flag_ts_kernel(FlagArgs a) {
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const int T = a.ntime, C = a.nchan, G = a.guard;
+  uint8_t *mb = a.tsmask + (int64_t)b * T;
+  const bool replaced = a.status && a.status[0];
+  if (!a.tsflag || replaced) {
+    for (int t = tid; t < T; t += flag::kTsThreads) mb[t] = 0;
+    return;
+  }
+  extern __shared__ float tsh[];   // [2][ts_base]
+  __shared__ uint32_t hist[256], sel[2];
+  const float *tb = a.ts + (int64_t)b * T;
+  float *tsb = tsh, *tmp = tsh + a.ts_base;
+  for (int i = tid; i < a.ts_base; i += flag::kTsThreads) tsb[i] = tb[i];
+  __syncthreads();
+  const int kmed = (a.ts_base + 1) / 2 - 1;   // lower median
+  const float med = grp_radix_select(tsb, a.ts_base, kmed, hist, sel, tid, flag::kTsThreads, 1);
+  for (int i = tid; i < a.ts_base; i += flag::kTsThreads) tmp[i] = fabsf(tsb[i] - med);
+  __syncthreads();
+  const float mad = grp_radix_select(tmp, a.ts_base, kmed, hist, sel, tid, flag::kTsThreads, 1);
+  const float lim = a.ts_thresh * mad;
+  int nts = 0;
+  for (int t = tid; t < T; t += flag::kTsThreads) {
+    const uint8_t f = (tb[t] - med) > lim ? 1 : 0;
+    mb[t] = f;
+    nts += f;
+  }
+  if (nts && a.counts) atomicAdd(a.counts + 1, nts);
+  E *xw = a.clean ? elem_out<E>(a) : nullptr;
+  if (!xw) return;
+  __syncthreads();   // the row flags written above are read back by other threads
+  const E re = repl_elem<E>(a.mn * (a.bpwr ? a.bpwr[b] : 1.0f));
+  const int warp = tid >> 5, lane = tid & 31, nw = flag::kTsThreads / 32;
+  for (int t = warp; t < T; t += nw) {
+    if (!mb[t]) continue;
+    E *row = xw + ((int64_t)b * T + t) * C;
+    for (int c = G + lane; c < C - G; c += 32) row[c] = re;
+  }
+}
+
+// fix_zspec (:114-170) over naver blocks of history: per (beam, channel),
+// the value whose count of other values <= it equals naver / 2 (ties
+// resolve to one value); if no value has that count the first block's is
+// kept, as the kernel leaves s0[block_id] unwritten then.
+__global__ void flag_zspec_kernel(const float *hs, const float *hv, int naver, int bc, float *s0,
+                                  float *v0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= bc) return;
+  const int place = naver / 2;
+  for (int which = 0; which < 2; ++which) {
+    const float *h = which ? hv : hs;
+    float out = h[i];
+    for (int k = 0; k < naver; ++k) {
+      const float x = h[(int64_t)k * bc + i];
+      int ct = 0;
+      for (int j = 0; j < naver; ++j)
+        if (j != k && h[(int64_t)j * bc + i] <= x) ++ct;
+      if (ct == place) out = x;
+    }
+    (which ? v0 : s0)[i] = out;
+  }
+}
+
+// median_calc (:771-798): per channel the lower median over beams
+// (sorted[(nbeam + 1) / 2 - 1]; beam 31 of 64 in the reference), then
+// broadcast to every beam.  One thread per channel.
+__global__ void flag_medcalc_kernel(float *arr0, float *arr1, int nbeam, int nchan) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchan) return;
+  const int k = (nbeam + 1) / 2 - 1;
+  for (int which = 0; which < 2; ++which) {
+    float *arr = which ? arr1 : arr0;
+    float med = arr[c];
+    for (int i = 0; i < nbeam; ++i) {
+      const float x = arr[(int64_t)i * nchan + c];
+      int r = 0;
+      for (int j = 0; j < nbeam; ++j) {
+        const float y = arr[(int64_t)j * nchan + c];
+        r += (y < x) || (y == x && j < i);
+      }
+      if (r == k) med = x;
+    }
+    for (int i = 0; i < nbeam; ++i) arr[(int64_t)i * nchan + c] = med;
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+static int stage_rows(const FlagArgs &a, int es) {
+  const int cs = a.nchan < kFlagSlab ? a.nchan : kFlagSlab;
+  int lim = flag::kStageTarget / (cs * es);
+  if (lim > flag::kStatThreads) lim = flag::kStatThreads;
+  if (lim > a.tbin) lim = a.tbin;
+  for (int d = lim; d >= 1; --d)
+    if (a.tbin % d == 0 && (!a.pix_sum || d % a.tds == 0)) return d;
+  return 0;
+}
+
+bool flag_shape_ok(const FlagArgs &a) {
+  const bool u8 = a.xu8 != nullptr;
+  const int es = u8 ? 1 : 4;
+  const void *x = u8 ? (const void *)a.xu8 : (const void *)a.x;
+  if (!x || a.nchan < 4 || a.nchan > flag::kMaxChan || a.tbin < 1 || a.ntime < 1) return false;
+  if ((a.nchan * es) % 16 || (reinterpret_cast<uintptr_t>(x) & 15u)) return false;
+  if (a.pix_sum && (u8 || a.nchan > kFlagSlab || a.tds < 1 || a.tbin % a.tds ||
+                    a.ntime % a.tbin))
+    return false;
+  FlagArgs t = a;
+  return stage_rows(t, es) > 0;
+}
+
+// Upper bounds over every slab of the launch (a narrower last slab has
+// fewer column groups and at most 4 x kStatThreads bin partials).
+static size_t stats_smem(const FlagArgs &a, int es) {
+  const int cs = a.nchan < kFlagSlab ? a.nchan : kFlagSlab;
+  const size_t stage = ((size_t)a.rs * cs * es + 127) & ~(size_t)127;
+  return flag::kStages * stage +
+         sizeof(double) * ((size_t)a.rs * (kFlagSlab / 4) + 4 * flag::kStatThreads + kFlagSlab) +
+         sizeof(float) * kFlagSlab;
+}
+
+int launch_flag_stats(FlagArgs a, cudaStream_t st) {
+  if (!flag_shape_ok(a)) return -1;
+  const bool u8 = a.xu8 != nullptr;
+  const int es = u8 ? 1 : 4;
+  a.rs = stage_rows(a, es);
+  a.nslab = (a.nchan + kFlagSlab - 1) / kFlagSlab;
+  if (a.nslab > 1 && !a.rowsum) return -1;
+  const size_t sh = stats_smem(a, es);
+  const dim3 grid(a.nslab, a.nbeam);
+  if (u8) {
+    static SmemAttrOnce attr;
+    if (smem_attr_once(attr, flag_stats_kernel<uint8_t>, 160 * 1024) != cudaSuccess) return -2;
+    flag_stats_kernel<uint8_t><<<grid, flag::kStatThreads, sh, st>>>(a);
+  } else {
+    static SmemAttrOnce attr;
+    if (smem_attr_once(attr, flag_stats_kernel<float>, 160 * 1024) != cudaSuccess) return -2;
+    flag_stats_kernel<float><<<grid, flag::kStatThreads, sh, st>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// Statistics, channel decisions, column replacement + time series, time
+// series decisions (+ row replacement): four launches on one stream.
+int launch_flag(const FlagArgs &a0, cudaStream_t st) {
+  FlagArgs a = a0;
+  if (a.nchan > flag::kMaxChan || a.ts_base < 1 || a.ts_base > flag::kMaxTsBase ||
+      a.ts_base > a.ntime)
+    return -1;
+  a.ts_mean = 0;
+  a.nslab = (a.nchan + kFlagSlab - 1) / kFlagSlab;
+  int rc = launch_flag_stats(a, st);
+  if (rc != 0) return rc;
+  const bool u8 = a.xu8 != nullptr;
+  a.rs = stage_rows(a, u8 ? 1 : 4);
+  const size_t sh_chan = sizeof(float) * 12 * (size_t)a.nchan + a.nchan;
+  static SmemAttrOnce attr_chan;
+  if (smem_attr_once(attr_chan, flag_chan_kernel, 64 * 1024) != cudaSuccess) return -2;
+  flag_chan_kernel<<<a.nbeam, flag::kChanThreads, sh_chan, st>>>(a);
+  const dim3 agrid((a.ntime + flag::kApplyRows - 1) / flag::kApplyRows, a.nbeam);
+  const size_t sh_ts = sizeof(float) * 2 * (size_t)a.ts_base;
+  if (u8) {
+    flag_apply_kernel<uint8_t><<<agrid, flag::kApplyRows, 0, st>>>(a);
+    flag_ts_kernel<uint8_t><<<a.nbeam, flag::kTsThreads, sh_ts, st>>>(a);
+  } else {
+    flag_apply_kernel<float><<<agrid, flag::kApplyRows, 0, st>>>(a);
+    flag_ts_kernel<float><<<a.nbeam, flag::kTsThreads, sh_ts, st>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int launch_flag_baseline(const float *hist_spec, const float *hist_var, int naver, int nbeam,
+                         int nchan, float *spec0, float *var0, cudaStream_t st) {
+  const int bc = nbeam * nchan;
+  flag_zspec_kernel<<<(bc + 255) / 256, 256, 0, st>>>(hist_spec, hist_var, naver, bc, spec0, var0);
+  flag_medcalc_kernel<<<(nchan + 127) / 128, 128, 0, st>>>(spec0, var0, nbeam, nchan);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+}  // namespace dsax
+
+namespace dsax {
 // ---------------------------------------------------------------- decisions
 // Lower median sorted[(n+1)/2 - 1] of v[0..n) in shared memory, by rank
 // counting with ties broken by index (the element a stable sort would put
@@ -532,7 +971,7 @@ __global__ void __launch_bounds__(2 * flag::kDecThreads) lf_stat_features_kernel
 }
 
 int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStream_t st) {
-  if (!a.pix_sum || a.tds < 1 || a.ntime % a.tds || a.nchan > flag::kMaxChan) return -1;
+  if (!a.pix_sum || a.tds < 1 || a.ntime % a.tds || a.nchan > flag::kLfMaxChan) return -1;
   const int H = a.ntime / a.tds;
   const size_t sh = sizeof(float) * (2 * a.nchan + (a.ts_base > a.nchan ? a.ts_base : a.nchan) +
                                      4 * a.nchan + a.ntime + 2 * H);
@@ -540,261 +979,6 @@ int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStre
   static SmemAttrOnce attr;
   if (smem_attr_once(attr, lf_stat_features_kernel, 200 * 1024) != cudaSuccess) return -2;
   lf_stat_features_kernel<<<a.nbeam, 2 * flag::kDecThreads, sh, st>>>(a, F, Fbf);
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
-}
-
-// Group versions of the median and detrend: `gsize` threads (whole warps)
-// with group-local index gtid synchronise on named barrier `bid`.
-__device__ float grp_lower_median(const float *v, int n, float *result_slot, int gtid, int gsize,
-                                  int bid) {
-  const int k = (n + 1) / 2 - 1;
-  int gs = 1;
-  while (gs < 32 && gs * 2 * n <= gsize) gs *= 2;
-  const int sub = gtid & (gs - 1);
-  const int per = (n + gs - 1) / gs;
-  const int rounds = (n * gs + gsize - 1) / gsize;   // uniform trip count
-  for (int rd = 0; rd < rounds; ++rd) {
-    const int i = (rd * gsize + gtid) / gs;
-    const bool live = i < n;
-    const float x = live ? v[i] : 0.0f;
-    int r = 0;
-    if (live) {
-      const int j0 = sub * per, j1 = min(n, j0 + per);
-#pragma unroll 8
-      for (int j = j0; j < j1; ++j) {
-        const float y = v[j];
-        r += (y < x) || (y == x && j < i);
-      }
-    }
-    for (int o = gs >> 1; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-    if (live && sub == 0 && r == k) *result_slot = x;
-  }
-  named_bar(bid, gsize);
-  const float med = *result_slot;
-  named_bar(bid, gsize);
-  return med;
-}
-
-// The k-th smallest of v[0..n) (0-based; the value rank counting with
-// ties by index returns) by a four-pass MSB-first radix select over
-// order-preserving 32-bit keys: per pass a 256-bin shared histogram of the
-// candidates that still match the selected prefix, then one warp finds the
-// bin holding rank k.  O(n) work instead of O(n^2); finite inputs.
-__device__ __forceinline__ uint32_t ordered_key(float f) {
-  const uint32_t u = __float_as_uint(f);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ float grp_radix_select(const float *v, int n, int k, uint32_t *hist, uint32_t *sel,
-                                  int gtid, int gsize, int bid) {
-  uint32_t prefix = 0u, pmask = 0u;
-  int kk = k;
-  for (int shift = 24; shift >= 0; shift -= 8) {
-    for (int i = gtid; i < 256; i += gsize) hist[i] = 0u;
-    named_bar(bid, gsize);
-    for (int i = gtid; i < n; i += gsize) {
-      const uint32_t u = ordered_key(v[i]);
-      if ((u & pmask) == prefix) atomicAdd(&hist[(u >> shift) & 255u], 1u);
-    }
-    named_bar(bid, gsize);
-    if (gtid < 32) {   // the first warp: bin holding rank kk
-      uint32_t c[8], tot = 0u;
-#pragma unroll
-      for (int e = 0; e < 8; ++e) { c[e] = hist[8 * gtid + e]; tot += c[e]; }
-      uint32_t incl = tot;   // inclusive scan over lanes
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (gtid >= o) incl += y;
-      }
-      const uint32_t excl = incl - tot;
-      if (excl <= (uint32_t)kk && (uint32_t)kk < incl) {
-        uint32_t run = excl;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          if ((uint32_t)kk < run + c[e]) {
-            sel[0] = (uint32_t)(8 * gtid + e);
-            sel[1] = (uint32_t)kk - run;
-            break;
-          }
-          run += c[e];
-        }
-      }
-    }
-    named_bar(bid, gsize);
-    prefix |= sel[0] << shift;
-    pmask |= 0xFFu << shift;
-    kk = (int)sel[1];
-    named_bar(bid, gsize);
-  }
-  const uint32_t u = (prefix & 0x80000000u) ? (prefix & 0x7FFFFFFFu) : ~prefix;
-  return __uint_as_float(u);
-}
-
-__device__ void grp_channflag(const float *sb, float thr, const FlagArgs &a, uint8_t *mask,
-                              float *corr, float *tmp, float *slot, int gtid, int gsize, int bid) {
-  const int C = a.nchan, G = a.guard, F = a.filt, n = C - 2 * G;
-  const int kf = (F + 1) / 2 - 1;
-  for (int idx = gtid; idx < n * F; idx += gsize) {   // forward median detrend
-    const int jj = idx / F, i = idx - jj * F;
-    const int j = G + jj;
-    const int w0 = (C - G - j >= F) ? j : C - G - F;
-    const float x = sb[w0 + i];
-    int r = 0;
-    for (int q = 0; q < F; ++q) {
-      const float y = sb[w0 + q];
-      r += (y < x) || (y == x && q < i);
-    }
-    if (r == kf) corr[jj] = sb[j] - x;
-  }
-  named_bar(bid, gsize);
-  const float med = grp_lower_median(corr, n, slot, gtid, gsize, bid);
-  for (int i = gtid; i < n; i += gsize) tmp[i] = fabsf(corr[i] - med);
-  named_bar(bid, gsize);
-  const float mad = grp_lower_median(tmp, n, slot, gtid, gsize, bid);
-  for (int i = gtid; i < n; i += gsize) {
-    const float v = corr[i];
-    if (v > thr * mad || v < -thr * mad) mask[G + i] = 1;
-  }
-}
-
-// The decisions of one beam (one CTA): the four channel tests and the
-// time-series test are independent, so five thread groups run them at once
-// (the reference runs them in sequence, src/gpu_flagger.cu:1340-1398; the
-// flags are the same):
-//   group 0-2 (64 threads each): channflag(spec - oldspec, Thr),
-//             channflag(var, Thr + 0.5), channflag(max, Thr)
-//   group 3   (64 threads): simple_channflag(pp, Thr / sqrt(FBIN)), one-sided
-//   group 4   (128 threads): simple_tsflag(ts, TsThr) over the first ts_base
-// The channel groups OR their flags into one shared mask.
-namespace flag {
-constexpr int kDecideThreads = 384;
-}
-
-__global__ void __launch_bounds__(flag::kDecideThreads) flag_decide_kernel(FlagArgs a) {
-  const int b = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
-  const int C = a.nchan, G = a.guard, T = a.ntime, n = C - 2 * G;
-  extern __shared__ float dsh[];          // [4 groups][3][C], then ts: [2][ts_base]
-  __shared__ uint8_t cmask[flag::kMaxChan];
-  __shared__ float slots[5];
-  __shared__ uint32_t ts_hist[256], ts_sel[2];   // radix select of the time-series group
-
-  for (int c = tid; c < C; c += blockDim.x) cmask[c] = 0;
-  __syncthreads();
-  const int g = warp < 8 ? warp >> 1 : 4;
-  const int gsize = g < 4 ? 64 : 128, gtid = g < 4 ? tid - 64 * g : tid - 256, bid = 1 + g;
-  if (g < 4) {
-    float *sb = dsh + g * 3 * C, *corr = sb + C, *tmp = corr + C;
-    const float *src = g == 0 ? a.spec : g == 1 ? a.var : g == 2 ? a.maxs : a.pp;
-    for (int c = gtid; c < C; c += gsize)
-      sb[c] = src[b * C + c] - ((g == 0 && a.oldspec) ? a.oldspec[b * C + c] : 0.0f);
-    named_bar(bid, gsize);
-    if (g < 3) {
-      const float thr = g == 1 ? a.thresh + a.var_add : a.thresh;
-      grp_channflag(sb, thr, a, cmask, corr, tmp, &slots[g], gtid, gsize, bid);
-    } else {
-      for (int i = gtid; i < n; i += gsize) corr[i] = sb[G + i];
-      named_bar(bid, gsize);
-      const float med = grp_lower_median(corr, n, &slots[g], gtid, gsize, bid);
-      for (int i = gtid; i < n; i += gsize) tmp[i] = fabsf(corr[i] - med);
-      named_bar(bid, gsize);
-      const float mad = grp_lower_median(tmp, n, &slots[g], gtid, gsize, bid);
-      const float mythr = a.thresh / sqrtf((float)a.fbin);
-      for (int j = G + gtid; j < C - G - a.fbin; j += gsize) {
-        float vv = 0.0f;
-        for (int k = 0; k < a.fbin; ++k) vv += a.parity ? sb[j] : sb[j + k];
-        vv = vv / (float)a.fbin - med;
-        if (vv > mythr * mad) cmask[j] = 1;
-      }
-    }
-  } else {
-    const float *tb = a.ts + (int64_t)b * T;
-    if (a.tsflag) {
-      float *tsb = dsh + 12 * C, *tmp = tsb + a.ts_base;
-      for (int i = gtid; i < a.ts_base; i += gsize) tsb[i] = tb[i];
-      named_bar(bid, gsize);
-      const int kmed = (a.ts_base + 1) / 2 - 1;   // lower median
-      const float med = grp_radix_select(tsb, a.ts_base, kmed, ts_hist, ts_sel, gtid, gsize, bid);
-      for (int i = gtid; i < a.ts_base; i += gsize) tmp[i] = fabsf(tsb[i] - med);
-      named_bar(bid, gsize);
-      const float mad = grp_radix_select(tmp, a.ts_base, kmed, ts_hist, ts_sel, gtid, gsize, bid);
-      const float lim = a.ts_thresh * mad;
-      int nts = 0;
-      uint8_t *mb = a.tsmask + (int64_t)b * T;
-      if ((T & 3) == 0 && (reinterpret_cast<uintptr_t>(tb) & 15u) == 0 &&
-          (reinterpret_cast<uintptr_t>(mb) & 3u) == 0) {
-        // four samples per load and one 32-bit mask word per store; all of a
-        // thread's loads (read-only path) are issued before its stores, which
-        // as byte stores could otherwise alias them
-        const float4 *t4 = reinterpret_cast<const float4 *>(tb);
-        uint32_t *m4 = reinterpret_cast<uint32_t *>(mb);
-        constexpr int kU = 8;
-        for (int i0 = gtid; i0 < T / 4; i0 += kU * gsize) {
-          float4 v[kU];
-#pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            const int i = i0 + u * gsize;
-            v[u] = i < T / 4 ? __ldg(t4 + i) : make_float4(0.f, 0.f, 0.f, 0.f);
-          }
-#pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            const int i = i0 + u * gsize;
-            if (i >= T / 4) break;
-            const uint32_t f0 = (v[u].x - med) > lim, f1 = (v[u].y - med) > lim;
-            const uint32_t f2 = (v[u].z - med) > lim, f3 = (v[u].w - med) > lim;
-            m4[i] = f0 | (f1 << 8) | (f2 << 16) | (f3 << 24);
-            nts += (int)(f0 + f1 + f2 + f3);
-          }
-        }
-      } else {
-        for (int t = gtid; t < T; t += gsize) {
-          const uint8_t f = (__ldg(tb + t) - med) > lim ? 1 : 0;
-          mb[t] = f;
-          nts += f;
-        }
-      }
-      if (nts) atomicAdd(a.counts + 1, nts);
-    } else {
-      for (int t = gtid; t < T; t += gsize) a.tsmask[(int64_t)b * T + t] = 0;
-    }
-  }
-  __syncthreads();
-  if (tid == 0)
-    for (int k = 0; k < a.nperm; ++k) {
-      const int j = a.perm[k];
-      if (j >= G && j < C - G) cmask[j] = 1;
-    }
-  __syncthreads();
-  int nflag = 0;
-  for (int c = tid; c < C; c += blockDim.x) {
-    a.chanmask[b * C + c] = cmask[c];
-    nflag += cmask[c];
-  }
-  if (nflag) atomicAdd(a.counts, nflag);
-}
-
-int launch_flag_stats(const FlagArgs &a, cudaStream_t st) {
-  if (a.nchan > flag::kMaxChan) return -1;
-  if (flag_stats_staged_ok(a)) {
-    static SmemAttrOnce attr2;
-    const int mx = flag::kFastStages * flag::kFastStageMax + 48 * 1024;
-    if (smem_attr_once(attr2, flag_stats_staged_kernel, mx) != cudaSuccess) return -2;
-    flag_stats_staged_kernel<<<a.nbeam, flag::kFastThreads, staged_stats_smem(a), st>>>(a);
-  } else {
-    if (a.pix_sum) return -1;
-    static SmemAttrOnce attr;
-    const size_t ssh = 16 * flag::kMaxChan * (4 * sizeof(double) + sizeof(float));
-    if (smem_attr_once(attr, flag_stats_kernel, (int)ssh) != cudaSuccess) return -2;
-    flag_stats_kernel<<<a.nbeam, flag::kStatThreads, ssh, st>>>(a);
-  }
-  return cudaGetLastError() == cudaSuccess ? 0 : -2;
-}
-
-int launch_flag(const FlagArgs &a, cudaStream_t st) {
-  if (a.nchan > flag::kMaxChan || a.ts_base > 4096) return -1;
-  const int rc = launch_flag_stats(a, st);
-  if (rc != 0) return rc;
-  const size_t sh = sizeof(float) * (12 * (size_t)a.nchan + 2 * (size_t)a.ts_base);
-  flag_decide_kernel<<<a.nbeam, flag::kDecideThreads, sh, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

@@ -94,31 +94,61 @@ float *agc_power_ptr(void *state, int nbeam);
 namespace dsax {
 
 struct FlagArgs {
-  const float *x;          // filterbank [nbeam][ntime][nchan] FP32 (device)
-  const float *oldspec;    // previous block's spec [nbeam][nchan] or null
-  float *spec, *var, *maxs, *pp, *ts;   // statistics (device)
-  uint8_t *chanmask;       // [nbeam][nchan]
-  uint8_t *tsmask;         // [nbeam][ntime]
-  int *counts;             // [2]: flagged (beam, chan) columns, (beam, t) rows
-  int nbeam, ntime, nchan, guard, filt, tbin, fbin, ts_base, tsflag, parity;
-  float thresh, var_add, ts_thresh;
-  int nperm;
-  int perm[8];
-  // optional downsampled spectrogram (staged statistics kernel only; needs
+  const float *x = nullptr;      // filterbank [nbeam][ntime][nchan] FP32 (device), or
+  const uint8_t *xu8 = nullptr;  // the same as uint8 (the reference's type)
+  float *xw = nullptr;           // where scaled / replaced FP32 data go (clean mode; may be x)
+  uint8_t *xw8 = nullptr;        // the same for uint8
+  const float *oldspec = nullptr;  // previous block's spec [nbeam][nchan] or null
+  float *spec = nullptr, *var = nullptr, *maxs = nullptr, *pp = nullptr;  // [nbeam][nchan]
+  float *ts = nullptr;           // [nbeam][ntime] channel-mean series (after replacement)
+  float *rowsum = nullptr;       // [nbeam][nslab][ntime] raw row sums when nslab > 1
+  uint8_t *chanmask = nullptr;   // [nbeam][nchan]
+  uint8_t *tsmask = nullptr;     // [nbeam][ntime]
+  int *counts = nullptr;         // [2]: flagged (beam, chan) columns, (beam, t) rows
+  int nbeam = 0, ntime = 0, nchan = 0, guard = 0, filt = 0, tbin = 0, fbin = 0, ts_base = 0;
+  int tsflag = 0, parity = 0;
+  float thresh = 0.f, var_add = 0.f, ts_thresh = 0.f;
+  int nperm = 0;
+  int perm[8] = {};
+  // optional downsampled spectrogram (FP32, one channel slab; needs
   // tbin % tds == 0): per (beam, pixel row of tds samples, chan) sum and max
   float *pix_sum = nullptr, *pix_max = nullptr;
   int tds = 0;
+  // statistics-pass geometry, set by the launcher
+  int nslab = 1;                 // channel slabs of kFlagSlab channels (CTAs per beam)
+  int rs = 0;                    // rows per pipeline stage (divides tbin)
+  int ts_mean = 0;               // 1: the statistics pass writes ts = row mean (no apply pass)
+  // data path (src/gpu_flagger.cu:1290-1410)
+  int clean = 0;                 // 1: replace flagged columns / rows in xw / xw8
+  float mn = 48.0f;              // MN: replacement level (x bpwr[beam])
+  float sig = 6.0f;              // SIG: scaley target standard deviation
+  const float *spec0 = nullptr, *var0 = nullptr;  // scaley baseline [nbeam][nchan] (null: none)
+  float *bpwr = nullptr;         // per-beam level [nbeam] (null: 1)
+  int pwr = 0;                   // 1: bpwr from this block's spectrum (calc_bpwr)
+  int modcheck = 0;              // 1: total-power modulation check against *prev_tpwr
+  float mod_thresh = 0.0005f;
+  const double *prev_tpwr = nullptr;  // previous flagged block's total power (0: none)
+  double *tpwr_out = nullptr;    // this block's total power
+  int *status = nullptr;         // [0] = 1 when the block was replaced by noise
+  const void *noise = nullptr;   // replacement block [ntime][nchan] (element type of x)
 };
 
+constexpr int kFlagSlab = 128;   // channels per statistics CTA
+
 int launch_flag(const FlagArgs &a, cudaStream_t st);
-// Statistics pass only (spec, var, max, pp, ts and the optional pixel sums);
-// returns -1 when the staged kernel cannot take the shape.
-int launch_flag_stats(const FlagArgs &a, cudaStream_t st);
-bool flag_stats_staged_ok(const FlagArgs &a);
+// Statistics pass only (spec, var, max, pp, ts and the optional pixel sums).
+// With a.ts_mean the series is the plain row mean.  Returns -1 when the
+// shape is not supported.
+int launch_flag_stats(FlagArgs a, cudaStream_t st);
+bool flag_shape_ok(const FlagArgs &a);
 // Learned-flagger features F[B][T/tds][C][8] from a finished statistics pass
 // (spec, var, maxs, pp, ts, pix_sum, pix_max of `a`).
 // F (FP32, may be null) and / or Fbf (BF16, may be null).
 int launch_lf_stat_features(const FlagArgs &a, float *F, uint16_t *Fbf, cudaStream_t st);
+// Scaley baseline from naver blocks of history (fix_zspec, then median_calc
+// across beams): hist_spec / hist_var [naver][nbeam][nchan] -> spec0 / var0.
+int launch_flag_baseline(const float *hist_spec, const float *hist_var, int naver, int nbeam,
+                         int nchan, float *spec0, float *var0, cudaStream_t st);
 
 }  // namespace dsax
 

@@ -121,7 +121,8 @@ int lf_make_features(const dsax_flag_params *p, const float *x, int tds, const L
   a.pix_sum = s.pix;
   a.pix_max = s.pix + (size_t)B * H * C;
   a.tds = tds;
-  if (!flag_stats_staged_ok(a)) return -1;
+  a.ts_mean = 1;
+  if (!flag_shape_ok(a)) return -1;
   int rc = launch_flag_stats(a, st);
   if (rc != 0) return rc;
   return launch_lf_stat_features(a, F, Fbf, st);

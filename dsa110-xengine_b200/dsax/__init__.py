@@ -65,6 +65,31 @@ class FlagParams(ctypes.Structure):
                 ("nperm", ctypes.c_int), ("perm", ctypes.c_int * 8)]
 
 
+class FlagCleanParams(ctypes.Structure):
+    _fields_ = [("mn", ctypes.c_float), ("sig", ctypes.c_float), ("mod_thresh", ctypes.c_float),
+                ("naver", ctypes.c_int), ("scale", ctypes.c_int), ("pwr", ctypes.c_int),
+                ("modcheck", ctypes.c_int), ("seed", ctypes.c_ulonglong)]
+
+
+class FlagBlockInfo(ctypes.Structure):
+    _fields_ = [("blocks", ctypes.c_int), ("started", ctypes.c_int), ("flagged", ctypes.c_int),
+                ("replaced", ctypes.c_int), ("nchan_flagged", ctypes.c_int),
+                ("nts_flagged", ctypes.c_int), ("tpwr", ctypes.c_double),
+                ("prev_tpwr", ctypes.c_double)]
+
+
+DTYPE_F32 = 0
+DTYPE_U8 = 1
+
+
+def flag_clean_params(**kw) -> FlagCleanParams:
+    cp = FlagCleanParams()
+    lib().dsax_default_flag_clean_params(ctypes.byref(cp))
+    for k, v in kw.items():
+        setattr(cp, k, v)
+    return cp
+
+
 class BlockDesc(ctypes.Structure):
     _fields_ = [("blk", ctypes.c_void_p), ("nchan", ctypes.c_int), ("vis", ctypes.c_void_p),
                 ("beams", ctypes.c_void_p), ("chanmask", ctypes.c_void_p),
@@ -166,6 +191,15 @@ def _bind_optional(L):
                                 ctypes.c_float, I, P, P], I),
         "dsax_flag_learned": ([P, P, ctypes.POINTER(FlagParams), I, P, P, I], I),
         "dsax_run_batch": ([P, ctypes.POINTER(BlockDesc), I, I], I),
+        "dsax_default_flag_clean_params": ([ctypes.POINTER(FlagCleanParams)], None),
+        "dsax_flag_state_create": ([P, ctypes.POINTER(FlagParams), ctypes.POINTER(FlagCleanParams),
+                                    I, ctypes.POINTER(P)], I),
+        "dsax_flag_state_destroy": ([P], None),
+        "dsax_flag_clean": ([P, P, P, P, P, I], I),
+        "dsax_flag_state_info": ([P, P, ctypes.POINTER(FlagBlockInfo)], I),
+        "dsax_flag_state_get_baseline": ([P, P, P, P], I),
+        "dsax_flag_state_set_baseline": ([P, P, P, P], I),
+        "dsax_flag_state_noise": ([P, P, P], I),
         "dsax_autotune": ([P, I, P, I, P], I),
     }
     for name, (args, res) in table.items():
@@ -341,6 +375,10 @@ class Context:
                              _ptr(chanmask), _ptr(tsmask), _ptr(stats), _ptr(counts), mem)
         self._check(rc, "dsax_flag")
 
+    def flag_state(self, params: FlagParams, clean: FlagCleanParams | None = None,
+                   dtype: int = DTYPE_F32) -> "FlagState":
+        return FlagState(self, params, clean if clean is not None else flag_clean_params(), dtype)
+
     # -- learned flagger ---------------------------------------------------
     def lf_init(self, seed: int = 0):
         self._check(lib().dsax_lf_init(self._h, seed), "dsax_lf_init")
@@ -403,3 +441,70 @@ class Context:
             arr[i].tsmask = _ptr(d.get("tsmask"))
         self._check(lib().dsax_run_batch(self._h, arr, len(descs), int(use_graph)),
                     "dsax_run_batch")
+
+
+class FlagState:
+    """The plain flagger's per-block data path (dsax_flag_clean) and its
+    state: baseline, previous spectrum and total power, noise block."""
+
+    def __init__(self, ctx: Context, params: FlagParams, clean: FlagCleanParams, dtype: int):
+        self.ctx = ctx
+        self.params = params
+        self.clean_params = clean
+        self.dtype = dtype
+        self._h = ctypes.c_void_p()
+        ctx._check(lib().dsax_flag_state_create(ctx.handle, ctypes.byref(params),
+                                                ctypes.byref(clean), dtype, ctypes.byref(self._h)),
+                   "dsax_flag_state_create")
+
+    def close(self):
+        if self._h:
+            lib().dsax_flag_state_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def clean(self, data, chanmask=None, tsmask=None, mem: int = MEM_DEVICE):
+        """One block, cleaned in place."""
+        self.ctx._check(lib().dsax_flag_clean(self.ctx.handle, self._h, _ptr(data), _ptr(chanmask),
+                                              _ptr(tsmask), mem), "dsax_flag_clean")
+
+    def info(self) -> FlagBlockInfo:
+        inf = FlagBlockInfo()
+        self.ctx._check(lib().dsax_flag_state_info(self.ctx.handle, self._h, ctypes.byref(inf)),
+                        "dsax_flag_state_info")
+        return inf
+
+    def baseline(self):
+        import numpy as np
+        n = self.params.nbeam * self.params.nchan
+        s0, v0 = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self.ctx._check(lib().dsax_flag_state_get_baseline(self.ctx.handle, self._h, _ptr(s0),
+                                                           _ptr(v0)), "dsax_flag_state_get_baseline")
+        shape = (self.params.nbeam, self.params.nchan)
+        return s0.reshape(shape), v0.reshape(shape)
+
+    def set_baseline(self, spec0, var0):
+        import numpy as np
+        s0 = np.ascontiguousarray(spec0, dtype=np.float32)
+        v0 = np.ascontiguousarray(var0, dtype=np.float32)
+        self.ctx._check(lib().dsax_flag_state_set_baseline(self.ctx.handle, self._h, _ptr(s0),
+                                                           _ptr(v0)), "dsax_flag_state_set_baseline")
+
+    def noise(self):
+        import numpy as np
+        dt = np.uint8 if self.dtype == DTYPE_U8 else np.float32
+        out = np.zeros((self.params.ntime, self.params.nchan), dt)
+        self.ctx._check(lib().dsax_flag_state_noise(self.ctx.handle, self._h, _ptr(out)),
+                        "dsax_flag_state_noise")
+        return out

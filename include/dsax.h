@@ -243,7 +243,8 @@ int dsax_agc_state(dsax_ctx *ctx, float *scale, int *started, int *blocks);
  * :534-556) and MADs -- on the GPU.  The shapes the reference hard-codes
  * are parameters here. */
 typedef struct dsax_flag_params {
-    int nbeam, ntime, nchan; /* filterbank [nbeam][ntime][nchan], nchan <= 128     */
+    int nbeam, ntime, nchan; /* filterbank [nbeam][ntime][nchan], 4 <= nchan <= 1024;
+                                nchan a multiple of 4 (FP32) or 16 (uint8)        */
     int guard;     /* ZeroChannels guard band at each edge (128 of 1024)           */
     int filt;      /* nFiltSize forward median window (21)                          */
     int tbin;      /* TBIN samples per peak-to-peak bin (128)                       */
@@ -266,9 +267,84 @@ void dsax_default_flag_params(dsax_flag_params *p, int nbeam, int ntime, int nch
  * [nbeam][nchan] and tsmask [nbeam][ntime] (0/1 bytes); stats (optional)
  * [spec | var | max | pp] each [nbeam][nchan] then ts [nbeam][ntime];
  * counts (optional) = {flagged (beam, chan) columns, flagged (beam, t) rows}.
+ * The time series is the channel mean after the flagged columns are set to
+ * MN = 48 (the reference replaces them before make_ts, :1379-1386); x itself
+ * is not modified.  ts_base <= 4096.
  * With DSAX_MEM_DEVICE every pointer is device memory. */
 int dsax_flag(dsax_ctx *ctx, const dsax_flag_params *p, const float *x, const float *oldspec,
               uint8_t *chanmask, uint8_t *tsmask, float *stats, int *counts, int mem);
+
+/* ---- plain flagger, data path ----
+ * The per-block processing of src/gpu_flagger.cu's main loop (:1260-1487)
+ * on a filterbank block that is cleaned in place: once a baseline exists,
+ * scaley (:1296-1297) normalises the block with the baseline spectrum and
+ * variance; the total-power modulation check (:1313-1330) replaces the whole
+ * block with a fixed noise block when the summed spectrum changed by
+ * mod_thresh or more since the previous flagged block; otherwise the
+ * channel tests run, flagged columns are set to MN x bpwr[beam] (flag,
+ * :459-474), the time series is formed from that data and flagged rows are
+ * set to the same level inside the guard band (flagts, :479-494).  The first
+ * naver blocks are only measured (no flagging, data unchanged): their
+ * spectra and variances give the baseline by a per-(beam, channel) median
+ * over the naver blocks (fix_zspec, :114-170) and then the median over
+ * beams broadcast to every beam (median_calc, :771-798) -- the state that
+ * the reference also reloads from specvar0.dat.
+ * Deviations: the reference compares its first flagged block with a
+ * pre-start noise block (:1276-1282), which in practice replaces it; here
+ * the first flagged block has no previous total power and is not checked.
+ * The noise block is a seeded Box-Muller block [ntime][nchan] (uniforms
+ * from SplitMix64 quantised to 1/16384 as genrand does, :500-516, with u1 in
+ * (0, 1] so that no sample is infinite), the same for every beam as in
+ * :1323-1324. */
+typedef struct dsax_flag_clean_params {
+    float mn;           /* MN, replacement level (48)                                */
+    float sig;          /* SIG, scaley target standard deviation (6)                 */
+    float mod_thresh;   /* -q, total-power modulation threshold (0.0005)             */
+    int naver;          /* blocks in the baseline median (5)                         */
+    int scale;          /* 1: scaley once the baseline exists (the reference: always) */
+    int pwr;            /* 1: level from this block's spectrum (calc_bpwr, -p); 0: 1  */
+    int modcheck;       /* 1: total-power modulation check (the reference: always)   */
+    unsigned long long seed; /* noise block                                         */
+} dsax_flag_clean_params;
+
+#define DSAX_DTYPE_F32 0
+#define DSAX_DTYPE_U8 1
+
+typedef struct dsax_flag_block_info {
+    int blocks;          /* blocks processed by this state                             */
+    int started;         /* 1 once the baseline exists (flagging on)                   */
+    int flagged;         /* the last block went through the flagging branch            */
+    int replaced;        /* the last block was replaced by noise (modulation check)    */
+    int nchan_flagged;   /* flagged (beam, channel) columns of the last block          */
+    int nts_flagged;     /* flagged (beam, time) rows of the last block                */
+    double tpwr;         /* the last flagged block's total power (sum of spec)         */
+    double prev_tpwr;    /* the total power it was compared with (0: none)             */
+} dsax_flag_block_info;
+
+typedef struct dsax_flag_state dsax_flag_state;
+
+void dsax_default_flag_clean_params(dsax_flag_clean_params *cp);
+/* A state for blocks of p's shape and element type dtype (DSAX_DTYPE_F32
+ * or DSAX_DTYPE_U8) on the context's device; p and cp are copied. */
+int dsax_flag_state_create(dsax_ctx *ctx, const dsax_flag_params *p,
+                           const dsax_flag_clean_params *cp, int dtype, dsax_flag_state **st);
+void dsax_flag_state_destroy(dsax_flag_state *st);
+/* One block: data [nbeam][ntime][nchan] of the state's type, cleaned in
+ * place; chanmask [nbeam][nchan], tsmask [nbeam][ntime] (0/1; NULL to skip
+ * in host mode).  mem = DSAX_MEM_DEVICE enqueues on the context stream.
+ * Calls on one state are serialised by the caller. */
+int dsax_flag_clean(dsax_ctx *ctx, dsax_flag_state *st, void *data, uint8_t *chanmask,
+                    uint8_t *tsmask, int mem);
+/* Waits for the context stream and reports the last block. */
+int dsax_flag_state_info(dsax_ctx *ctx, dsax_flag_state *st, dsax_flag_block_info *info);
+/* The baseline spectrum and variance [nbeam][nchan] (host memory; either may
+ * be NULL); get waits for the stream.  set loads a saved baseline and turns
+ * flagging on (the reference's specvar0.dat, :1430-1441). */
+int dsax_flag_state_get_baseline(dsax_ctx *ctx, dsax_flag_state *st, float *spec0, float *var0);
+int dsax_flag_state_set_baseline(dsax_ctx *ctx, dsax_flag_state *st, const float *spec0,
+                                 const float *var0);
+/* The noise block [ntime][nchan] of the state's type (host memory). */
+int dsax_flag_state_noise(dsax_ctx *ctx, dsax_flag_state *st, void *noise);
 
 /* Allocation-free plain flagger.  No counterpart in the reference: it is for
  * callers that cannot call cudaMalloc -- a process whose device memory is

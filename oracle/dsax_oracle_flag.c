@@ -144,13 +144,14 @@ void oracle_channflag(const float *spec, float thr,
 }
 
 /* simple_channflag (src/gpu_flagger.cu:562-610): one-sided,
- * Thr/sqrt(FBIN), over channels [G, C-G-FBIN). */
+ * Thr/sqrt(FBIN) (evaluated in double and stored float, as there), over
+ * channels [G, C-G-FBIN). */
 void oracle_simple_channflag(const float *spec, float thr,
                              const oracle_flag_params *P, int *mask,
                              float *margin) {
     const int B = P->nbeam, C = P->nchan, G = P->guard, FB = P->fbin;
     const int n = C - 2 * G;
-    const float mythr = thr / sqrtf((float)FB);
+    const float mythr = (float)((double)thr / sqrt((double)FB));
 #pragma omp parallel for schedule(static)
     for (int b = 0; b < B; b++) {
         float *tmp = (float *)malloc(sizeof(float) * C);
@@ -199,23 +200,33 @@ void oracle_simple_tsflag(const float *ts, float thr,
     }
 }
 
-/* The per-block decision chain of src/gpu_flagger.cu:1340-1398:
- * channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
- * channflag(max, Thr), simple_channflag(pp, Thr), and (if enabled)
- * simple_tsflag(ts, TsThr).  oldspec may be NULL (first block: zeros).
- * chanmask [B][C] and tsmask [B][T] are overwritten (0/1).  Returns the
- * number of flagged (beam, chan) columns. */
-int oracle_plain_flag(const float *x, const oracle_flag_params *P,
-                      const float *oldspec, int *chanmask, int *tsmask,
-                      float *chan_margin, float *ts_margin, float *stats_out) {
+/* The channel-mean time series after flag() (:459-474) has set the flagged
+ * columns of each beam to level[beam] (make_ts, :414-453, runs on the
+ * replaced data at :1384): accumulated in double, stored float. */
+void oracle_ts_replaced(const float *x, const oracle_flag_params *P, const int *chanmask,
+                        const float *level, float *ts) {
     const int B = P->nbeam, T = P->ntime, C = P->nchan;
-    float *spec = (float *)malloc(sizeof(float) * B * C);
-    float *var = (float *)malloc(sizeof(float) * B * C);
-    float *mx = (float *)malloc(sizeof(float) * B * C);
-    float *pp = (float *)malloc(sizeof(float) * B * C);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < B; b++) {
+        const float *xb = x + (int64_t)b * T * C;
+        const int *mb = chanmask + (int64_t)b * C;
+        for (int t = 0; t < T; t++) {
+            double s = 0.0;
+            for (int c = 0; c < C; c++) s += mb[c] ? (double)level[b] : (double)xb[(int64_t)t * C + c];
+            ts[(int64_t)b * T + t] = (float)(s / C);
+        }
+    }
+}
+
+/* The channel decisions of :1340-1347 on given statistics:
+ * channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
+ * channflag(max, Thr), simple_channflag(pp, Thr), plus the permanent flag
+ * channels.  chanmask is overwritten (0/1). */
+void oracle_chan_flags(const float *spec, const float *var, const float *mx, const float *pp,
+                       const float *oldspec, const oracle_flag_params *P, int *chanmask,
+                       float *chan_margin) {
+    const int B = P->nbeam, C = P->nchan;
     float *sub = (float *)malloc(sizeof(float) * B * C);
-    float *ts = (float *)malloc(sizeof(float) * (int64_t)B * T);
-    oracle_flag_stats(x, P, spec, var, mx, pp, ts);
     for (int i = 0; i < B * C; i++) {
         chanmask[i] = 0;
         sub[i] = spec[i] - (oldspec ? oldspec[i] : 0.0f);
@@ -225,6 +236,34 @@ int oracle_plain_flag(const float *x, const oracle_flag_params *P,
     oracle_channflag(var, P->thresh + P->var_add, P, chanmask, chan_margin);
     oracle_channflag(mx, P->thresh, P, chanmask, chan_margin);
     oracle_simple_channflag(pp, P->thresh, P, chanmask, chan_margin);
+    free(sub);
+}
+
+/* The per-block decision chain of src/gpu_flagger.cu:1340-1398:
+ * channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
+ * channflag(max, Thr), simple_channflag(pp, Thr), then (if enabled)
+ * simple_tsflag(ts, TsThr) on the time series of the data with the flagged
+ * columns set to `level` (MN x bpwr, the same for every beam here).
+ * oldspec may be NULL (first block: zeros).  chanmask [B][C] and tsmask
+ * [B][T] are overwritten (0/1).  Returns the number of flagged (beam, chan)
+ * columns. */
+int oracle_plain_flag(const float *x, const oracle_flag_params *P,
+                      const float *oldspec, int *chanmask, int *tsmask,
+                      float *chan_margin, float *ts_margin, float *stats_out, float level) {
+    const int B = P->nbeam, T = P->ntime, C = P->nchan;
+    float *spec = (float *)malloc(sizeof(float) * B * C);
+    float *var = (float *)malloc(sizeof(float) * B * C);
+    float *mx = (float *)malloc(sizeof(float) * B * C);
+    float *pp = (float *)malloc(sizeof(float) * B * C);
+    float *sub = (float *)malloc(sizeof(float) * B * C);
+    float *ts = (float *)malloc(sizeof(float) * (int64_t)B * T);
+    oracle_flag_stats(x, P, spec, var, mx, pp, ts);
+    for (int i = 0; i < B * C; i++) sub[i] = spec[i] - (oldspec ? oldspec[i] : 0.0f);
+    oracle_chan_flags(spec, var, mx, pp, oldspec, P, chanmask, chan_margin);
+    float *lev = (float *)malloc(sizeof(float) * B);
+    for (int b = 0; b < B; b++) lev[b] = level;
+    oracle_ts_replaced(x, P, chanmask, lev, ts);
+    free(lev);
     for (int64_t i = 0; i < (int64_t)B * T; i++) {
         tsmask[i] = 0;
         if (ts_margin) ts_margin[i] = INFINITY;

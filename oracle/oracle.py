@@ -55,8 +55,20 @@ def lib():
         L.oracle_beamform.argtypes = [P, i32, i32, i32, P, P, i32, i32, i32, i32, P]
         L.oracle_beamform.restype = i32
         L.oracle_geometric_weights.argtypes = [P, P, P, i32, i32, f64, f64, P, P]
-        L.oracle_plain_flag.argtypes = [P, P, P, P, P, P, P, P]
+        L.oracle_plain_flag.argtypes = [P, P, P, P, P, P, P, P, f32]
         L.oracle_plain_flag.restype = i32
+        L.oracle_flag_stats.argtypes = [P, P, P, P, P, P, P]
+        L.oracle_flag_stats.restype = None
+        L.oracle_chan_flags.argtypes = [P, P, P, P, P, P, P, P]
+        L.oracle_chan_flags.restype = None
+        L.oracle_simple_tsflag.argtypes = [P, f32, P, P, P]
+        L.oracle_simple_tsflag.restype = None
+        L.oracle_channflag.argtypes = [P, f32, P, P, P]
+        L.oracle_channflag.restype = None
+        L.oracle_simple_channflag.argtypes = [P, f32, P, P, P]
+        L.oracle_simple_channflag.restype = None
+        L.oracle_ts_replaced.argtypes = [P, P, P, P, P]
+        L.oracle_ts_replaced.restype = None
         L.oracle_nthreads.restype = i32
         _lib = L
     return _lib
@@ -142,6 +154,32 @@ def simple_extract(vis: np.ndarray) -> np.ndarray:
     out = np.empty((NBL, nchan, 2, 2), dtype=np.float32)
     lib().oracle_simple_extract(_ptr(np.ascontiguousarray(vis)), nchan, _ptr(out))
     return out
+
+
+def auto_extract(extracted: np.ndarray, specs: np.ndarray | None = None,
+                 nant: int = 63) -> np.ndarray:
+    """auto_extract (src/dsaX_wrangle.c:47-70): adds the real parts of both
+    polarisations of every autocorrelation (baseline i(i+1)/2 + i, i < nant)
+    of a simple_extract product [2080][nchan][2][2] into specs[nant][nchan]."""
+    nchan = extracted.shape[1]
+    if specs is None:
+        specs = np.zeros((nant, nchan), np.float32)
+    for i in range(nant):
+        bl = i * (i + 1) // 2 + i
+        specs[i] = (specs[i] + extracted[bl, :, 0, 0]).astype(np.float32)
+        specs[i] = (specs[i] + extracted[bl, :, 1, 0]).astype(np.float32)
+    return specs
+
+
+def greg_order() -> np.ndarray:
+    """gen_lookup (src/dsaX_wrangleAndWrite.c:46-80): for each baseline of
+    the "Greg" order -- antenna pairs (i, j >= i), i major -- its index in
+    xGPU's triangular order (pair (j, i) with j <= i at i(i+1)/2 + j)."""
+    idx = []
+    for i in range(NST):
+        for j in range(i, NST):
+            idx.append(j * (j + 1) // 2 + i)
+    return np.asarray(idx, np.int32)
 
 
 # --------------------------------------------------------------------------
@@ -350,9 +388,10 @@ def flag_params(nbeam, ntime, nchan, guard=None, filt=21, tbin=128, fbin=8,
     return p
 
 
-def plain_flag(x: np.ndarray, params: FlagParams, oldspec=None):
+def plain_flag(x: np.ndarray, params: FlagParams, oldspec=None, level: float = 48.0):
     """Returns (chanmask[B][C] int32, tsmask[B][T] int32, chan_margin,
-    ts_margin, stats) for a float32 filterbank x[B][T][C]."""
+    ts_margin, stats) for a float32 filterbank x[B][T][C].  The time series
+    is formed after the flagged columns are set to `level` (MN)."""
     B, T, C = x.shape
     x = np.ascontiguousarray(x, dtype=np.float32)
     cm = np.zeros((B, C), np.int32)
@@ -363,7 +402,7 @@ def plain_flag(x: np.ndarray, params: FlagParams, oldspec=None):
     old = None if oldspec is None else np.ascontiguousarray(oldspec, dtype=np.float32)
     lib().oracle_plain_flag(_ptr(x), ctypes.byref(params),
                             None if old is None else _ptr(old),
-                            _ptr(cm), _ptr(tm), _ptr(cmg), _ptr(tmg), _ptr(st))
+                            _ptr(cm), _ptr(tm), _ptr(cmg), _ptr(tmg), _ptr(st), float(level))
     stats = {
         "spec": st[0:B * C].reshape(B, C), "var": st[B * C:2 * B * C].reshape(B, C),
         "max": st[2 * B * C:3 * B * C].reshape(B, C), "pp": st[3 * B * C:4 * B * C].reshape(B, C),
@@ -372,3 +411,258 @@ def plain_flag(x: np.ndarray, params: FlagParams, oldspec=None):
     return cm, tm, cmg, tmg, stats
 
 
+
+
+# --------------------------------------------------------------------------
+# plain flagger: the per-block data path of src/gpu_flagger.cu:1260-1487
+# --------------------------------------------------------------------------
+def flag_stats(x: np.ndarray, params: FlagParams):
+    """spec, var, max, pp [B][C] (float32) of a filterbank (any real dtype,
+    converted to float32 exactly for uint8)."""
+    B, T, C = x.shape
+    xf = np.ascontiguousarray(x, dtype=np.float32)
+    out = [np.zeros((B, C), np.float32) for _ in range(4)]
+    ts = np.zeros((B, T), np.float32)
+    lib().oracle_flag_stats(_ptr(xf), ctypes.byref(params), *[_ptr(o) for o in out], _ptr(ts))
+    return out
+
+
+def chan_flags(spec, var, mx, pp, params: FlagParams, oldspec=None):
+    """chanmask [B][C] int32 and its decision margins (channflag x3 +
+    simple_channflag + permanent channels, :1340-1347)."""
+    B, C = spec.shape
+    cm = np.zeros((B, C), np.int32)
+    mg = np.zeros((B, C), np.float32)
+    arr = [np.ascontiguousarray(a, dtype=np.float32) for a in (spec, var, mx, pp)]
+    old = None if oldspec is None else np.ascontiguousarray(oldspec, dtype=np.float32)
+    lib().oracle_chan_flags(*[_ptr(a) for a in arr], None if old is None else _ptr(old),
+                            ctypes.byref(params), _ptr(cm), _ptr(mg))
+    return cm, mg
+
+
+def ts_flags(ts, params: FlagParams):
+    """simple_tsflag (:612-653): tsmask [B][T] int32 and margins."""
+    B, T = ts.shape
+    tm = np.zeros((B, T), np.int32)
+    mg = np.full((B, T), np.inf, np.float32)
+    t = np.ascontiguousarray(ts, dtype=np.float32)
+    lib().oracle_simple_tsflag(_ptr(t), float(params.ts_thresh), ctypes.byref(params), _ptr(tm),
+                               _ptr(mg))
+    return tm, mg
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser of x + golden gamma (uint64 arrays)."""
+    with np.errstate(over="ignore"):
+        z = (x + np.uint64(0x9E3779B97F4A7C15)).astype(np.uint64)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def noise_block(seed: int, ntime: int, nchan: int, sig: float = 6.0, mn: float = 48.0,
+                dtype=np.float32) -> np.ndarray:
+    """The replacement noise block [ntime][nchan]: genrand's Box-Muller
+    (src/gpu_flagger.cu:500-516) on uniforms quantised to 1/16384 (RMAX),
+    drawn from SplitMix64 with u1 in (0, 1]; uint8 requantised as
+    (unsigned char)(rint(2 v) / 2)."""
+    n = ntime * nchan
+    i = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        base = np.uint64(seed) * np.uint64(0x100000001B3)
+        r1 = splitmix64(base + np.uint64(2) * i)
+        r2 = splitmix64(base + np.uint64(2) * i + np.uint64(1))
+    u1 = ((r1 % np.uint64(16384)).astype(np.float64) + 1.0) / 16384.0
+    u2 = (r2 % np.uint64(16384)).astype(np.float64) / 16384.0
+    va = np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+    v = (va * float(sig) + float(mn)).astype(np.float32)
+    if dtype == np.uint8:
+        w = np.rint(2.0 * v.astype(np.float64))
+        u = np.clip(w, 0, 4294967295).astype(np.uint64)
+        return ((u // np.uint64(2)) & np.uint64(255)).astype(np.uint8).reshape(ntime, nchan)
+    return v.reshape(ntime, nchan)
+
+
+def scaley(x: np.ndarray, spec0: np.ndarray, var0: np.ndarray, sig: float = 6.0,
+           mn: float = 48.0) -> np.ndarray:
+    """scaley (:382-394): (x - spec0) * (SIG / sqrtf(var0)) + MN with the
+    reference's float / double evaluation; uint8 requantised as
+    (unsigned char)(__float2uint_rn(2 val) / 2) (wraps modulo 256)."""
+    B, T, C = x.shape
+    xf = x.astype(np.float32)
+    d = (xf - spec0.astype(np.float32)[:, None, :]).astype(np.float32)
+    k = np.float64(sig) / np.sqrt(var0.astype(np.float32)).astype(np.float64)
+    val = (d.astype(np.float64) * k[:, None, :] + np.float64(mn)).astype(np.float32)
+    if x.dtype == np.uint8:
+        w = np.rint(2.0 * val.astype(np.float64))
+        w = np.where(np.isnan(w), 0.0, w)
+        u = np.clip(w, 0, 4294967295).astype(np.uint64)
+        return ((u // np.uint64(2)) & np.uint64(255)).astype(np.uint8)
+    return val
+
+
+def calc_bpwr(spec: np.ndarray, guard: int, mn: float = 48.0) -> np.ndarray:
+    """calc_bpwr (:759-769): float sum of every channel in order, divided by
+    the channels inside the guard band, then by MN."""
+    B, C = spec.shape
+    acc = np.zeros(B, np.float32)
+    for c in range(C):
+        acc = (acc + spec[:, c].astype(np.float32)).astype(np.float32)
+    return ((acc.astype(np.float64) / float(C - 2 * guard)) / float(mn)).astype(np.float32)
+
+
+def zspec_median(hist: np.ndarray) -> np.ndarray:
+    """fix_zspec (:114-170) over hist[naver][...]: the value whose count of
+    other values <= it is naver // 2; the first block's value if none."""
+    n = hist.shape[0]
+    out = hist[0].copy()
+    for k in range(n):
+        ct = np.zeros(hist.shape[1:], np.int64)
+        for j in range(n):
+            if j != k:
+                ct += hist[j] <= hist[k]
+        out = np.where(ct == n // 2, hist[k], out)
+    return out
+
+
+def median_calc(arr: np.ndarray) -> np.ndarray:
+    """median_calc (:771-798): per channel the lower median over beams,
+    broadcast to every beam."""
+    B = arr.shape[0]
+    med = np.sort(arr, axis=0)[(B + 1) // 2 - 1]
+    return np.broadcast_to(med, arr.shape).astype(np.float32).copy()
+
+
+def repl_level(level: np.ndarray, dtype) -> np.ndarray:
+    """MN x bpwr as the element type: uint8 truncates toward zero, clamped."""
+    if dtype == np.uint8:
+        return np.clip(np.trunc(np.minimum(level, 255.0)), 0, 255).astype(np.uint8)
+    return level.astype(np.float32)
+
+
+class CleanOracle:
+    """The per-block data path of dsax_flag_clean, restated: measure the
+    first naver blocks, then scaley + modulation check + channel flags +
+    column replacement + time-series flags + row replacement per block."""
+
+    def __init__(self, params: FlagParams, dtype=np.float32, mn=48.0, sig=6.0, mod_thresh=5e-4,
+                 naver=5, scale=True, pwr=False, modcheck=True, seed=1):
+        self.p = params
+        self.dtype = np.dtype(dtype).type
+        self.mn, self.sig, self.mod_thresh = mn, sig, mod_thresh
+        self.naver, self.scale, self.pwr, self.modcheck = naver, scale, pwr, modcheck
+        B, T, C = params.nbeam, params.ntime, params.nchan
+        self.noise = noise_block(seed, T, C, sig, mn, self.dtype)
+        self.hist = []
+        self.started = False
+        self.spec0 = self.var0 = None
+        self.oldspec = np.zeros((B, C), np.float32)
+        self.prev_tpwr = 0.0
+        self.bpwr = np.ones(B, np.float32)
+
+    def step(self, data: np.ndarray):
+        """Returns (cleaned data, chanmask, tsmask, info dict, margins)."""
+        p = self.p
+        B, T, C, G = p.nbeam, p.ntime, p.nchan, p.guard
+        x = np.array(data, copy=True)
+        cm = np.zeros((B, C), np.uint8)
+        tm = np.zeros((B, T), np.uint8)
+        info = {"flagged": False, "replaced": False, "tpwr": 0.0, "prev_tpwr": 0.0}
+        cmg = np.full((B, C), np.inf, np.float32)
+        tmg = np.full((B, T), np.inf, np.float32)
+        if not self.started:
+            spec, var, mx, pp = flag_stats(x, p)
+            self.hist.append((spec, var))
+            if len(self.hist) >= self.naver:
+                hs = np.stack([h[0] for h in self.hist])
+                hv = np.stack([h[1] for h in self.hist])
+                self.spec0 = median_calc(zspec_median(hs))
+                self.var0 = median_calc(zspec_median(hv))
+                self.started = True
+        else:
+            if self.scale:
+                x = scaley(x, self.spec0, self.var0, self.sig, self.mn)
+            spec, var, mx, pp = flag_stats(x, p)
+            tpwr = float(np.sum(spec.astype(np.float64)))
+            info.update(flagged=True, tpwr=tpwr, prev_tpwr=self.prev_tpwr)
+            replaced = (self.modcheck and self.prev_tpwr > 0 and
+                        abs(tpwr - self.prev_tpwr) / self.prev_tpwr >= self.mod_thresh)
+            info["mod_index"] = (abs(tpwr - self.prev_tpwr) / self.prev_tpwr
+                                 if self.prev_tpwr > 0 else None)
+            if replaced:
+                x[:] = self.noise[None, :, :]
+                info["replaced"] = True
+            else:
+                cmi, cmg = chan_flags(spec, var, mx, pp, p, self.oldspec)
+                cm = cmi.astype(np.uint8)
+                if self.pwr:
+                    self.bpwr = calc_bpwr(spec, G, self.mn)
+                lev = repl_level(self.mn * self.bpwr.astype(np.float32), self.dtype)
+                for b in range(B):
+                    cols = np.nonzero(cm[b])[0]
+                    if cols.size:
+                        x[b][:, cols] = lev[b]
+                ts = (x.astype(np.float64).sum(axis=2) / C).astype(np.float32)
+                if p.tsflag:
+                    tmi, tmg = ts_flags(ts, p)
+                    tm = tmi.astype(np.uint8)
+                    for b in range(B):
+                        rows = np.nonzero(tm[b])[0]
+                        if rows.size:
+                            x[b][rows, G:C - G] = lev[b]
+                info["ts"] = ts
+            self.prev_tpwr = tpwr
+        self.oldspec = spec
+        info["spec"] = spec
+        return x, cm, tm, info, (cmg, tmg)
+
+
+# --------------------------------------------------------------------------
+# oracle/_ref: the reference's own functions (built by make_ref.py)
+# --------------------------------------------------------------------------
+_ref_libs = {}
+
+
+def ref_lib(small: bool = False):
+    """oracle/_ref/libref.so (or the 64-packet build), built from the
+    reference tree when missing.  Raises FileNotFoundError when neither the
+    library nor the reference tree is present."""
+    key = "small" if small else "full"
+    if key in _ref_libs:
+        return _ref_libs[key]
+    path = os.path.join(_HERE, "_ref", "libref_small.so" if small else "libref.so")
+    if not os.path.exists(path):
+        import make_ref  # noqa: E402  (oracle/ is on sys.path)
+        make_ref.build()
+    L = ctypes.CDLL(path)
+    P, i32, f32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.ref_flag_shape.argtypes = [P, P, P]
+    L.ref_medval.argtypes = [P, i32]
+    L.ref_medval.restype = f32
+    for n in ("ref_channflag", "ref_simple_channflag", "ref_simple_tsflag"):
+        getattr(L, n).argtypes = [P, f32, P]
+    for n in ("ref_gather_mask", "ref_gather_tsmask"):
+        getattr(L, n).argtypes = [P, P, P]
+    L.ref_calc_bpwr.argtypes = [P, P]
+    L.ref_median_calc.argtypes = [P]
+    L.ref_scaley.argtypes = [P, P, P]
+    L.ref_flag.argtypes = [P, P, i32, P]
+    L.ref_flagts.argtypes = [P, P, i32, P]
+    L.ref_auto_extract.argtypes = [P, P]
+    L.ref_simple_extract.argtypes = [P, P]
+    L.ref_gen_lookup.argtypes = [P]
+    L.ref_reorder_gh.argtypes = [P, P, P]
+    L.ref_massage_raw.argtypes = [P, P, i32]
+    L.ref_massage_raw.restype = i32
+    L.ref_massage_bak.argtypes = [P, P, i32]
+    L.ref_massage_bak.restype = i32
+    L.ref_npackets.restype = i32
+    L.ref_nants.restype = i32
+    _ref_libs[key] = L
+    return L
+
+
+def ref_available() -> bool:
+    if os.path.exists(os.path.join(_HERE, "_ref", "libref.so")):
+        return True
+    return os.path.isdir(os.environ.get("DSAX_REFERENCE", "/root/reference"))
