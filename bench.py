@@ -72,56 +72,76 @@ def _traffic_from_profiles(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """SM clocks and clock-event reasons sampled DURING the timed region.
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NVML is read (never set) from a thread every ~2 ms, so even a timed
+    region of a few milliseconds gets samples; nvidia-smi at 100 ms is the
+    fallback when the NVML bindings are missing."""
+
+    NAMES = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+             ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+             ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+             ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.f = None
+        self.rows = []
+        self.smax = None
+        self._stop = threading.Event()
+        self._thr = None
+        self._nv = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _run(self, nv, h):
+        bits = [(name, getattr(nv, const, 0)) for name, const in self.NAMES]
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((sm, [n for n, b in bits if b and (r & b)]))
+            except Exception:
+                break
+            time.sleep(0.002)
 
     def __enter__(self):
         try:
-            self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._nv = nv
+            self._thr = threading.Thread(target=self._run, args=(nv, h), daemon=True)
+            self._thr.start()
         except Exception:
-            self.proc = None
+            self._thr = None
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+        self._stop.set()
+        if self._thr is not None:
+            self._thr.join(timeout=5)
+        if self._nv is not None:
             try:
-                self.proc.wait(timeout=5)
+                self._nv.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
-        if self.proc is None or self.f is None:
-            return None
-        self.f.flush()
-        rows = []
-        with open(self.f.name) as fh:
-            for line in fh:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.f.name)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        if self._thr is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no NVML"], "samples": 0}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["no samples"], "samples": 0}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({n for r in self.rows for n in r[1]})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.smax, "reasons": reasons,
+                "samples": len(self.rows), "source": "NVML, ~2 ms period"}
 
 
 def _dist():
@@ -131,40 +151,113 @@ def _dist():
     return ws, rank, local
 
 
+def _has_avx512bw() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            return " avx512bw" in f.read()
+    except Exception:
+        return False
+
+
+def _time_reorders(oracle, blk, nthr: int):
+    """The reference's own CPU corner turns on one full block, from
+    oracle/_ref (lifted from the reference tree): massage()
+    (src/dsaX_reorder_raw.c:153-169, byte reorder) and the AVX-512 fluff +
+    transpose (src/dsaX_reorder_raw.c.bak:184-258), at 1 and nthr threads.
+    Returns {name: seconds per block} or {"unavailable": why}."""
+    import ctypes
+    try:
+        ref = oracle.ref_lib()
+    except Exception as exc:
+        return {"unavailable": f"oracle/_ref: {type(exc).__name__}: {exc}"}
+    src = np.ascontiguousarray(blk)
+    out = {}
+    nts = sorted({1, max(1, min(16, nthr))})
+    for name, fn, nbytes in (("massage", ref.ref_massage_raw, 2048 * 768 * 64 * 2),
+                             ("fluff_avx512", ref.ref_massage_bak, 2048 * 768 * 64 * 4)):
+        if name == "fluff_avx512" and not _has_avx512bw():
+            out[name] = "host CPU has no AVX-512BW"
+            continue
+        buf = np.zeros(nbytes, np.uint8)
+        for nt in nts:
+            while 2048 % nt:
+                nt -= 1
+            fn(src.ctypes.data_as(ctypes.c_void_p), buf.ctypes.data_as(ctypes.c_void_p), nt)
+            t0 = time.perf_counter()
+            fn(src.ctypes.data_as(ctypes.c_void_p), buf.ctypes.data_as(ctypes.c_void_p), nt)
+            out[f"{name}_{nt}t_s"] = time.perf_counter() - t0
+    return out
+
+
 def run_reference(args):
+    """The reference's CPU path for one full block on the host cores: its
+    own massage() corner turn (oracle/_ref, all threads up to its 16-thread
+    limit) plus the CPU X-engine of the oracle port (xGPU, whose CPU
+    X-engine the reference calls xgpuOmpXengine, is not in the reference
+    tree), every step a whole block unless --steps would take too long."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    import numpy as np
+    import ctypes
     import oracle
     oracle.build()
     nthr = oracle.nthreads()
     blk = oracle.gen_block(12345, 2048, 63, 384, "gauss")
-    # bounded sample: `nch` channels of the full block per step, scaled
-    nch = max(1, min(384, args.ref_channels))
+    try:
+        ref = oracle.ref_lib()
+        mthr = max(1, min(16, nthr))
+        while 2048 % mthr:
+            mthr -= 1
+        reo = np.zeros(2048 * 768 * 64 * 2, np.uint8)
+
+        def massage():
+            ref.ref_massage_raw(blk.ctypes.data_as(ctypes.c_void_p),
+                                reo.ctypes.data_as(ctypes.c_void_p), mthr)
+        kind = "reference"
+    except Exception:
+        massage, mthr = (lambda: oracle.massage(blk)), nthr
+        kind = "port"
+    t0 = time.perf_counter()
+    massage()
+    oracle.correlate(blk)
+    full_s = time.perf_counter() - t0
+    # a whole block per step when the run stays within ~3 minutes, else a
+    # channel sample of the X-engine per step, scaled to a block
+    nch = 384 if (args.steps + 1) * full_s <= 180 else \
+        max(8, int(384 * 180 / ((args.steps + 1) * full_s)))
     for _ in range(max(0, min(args.warmup, 1))):
+        massage()
         oracle.correlate(blk, ch0=0, nch=nch)
     times = []
     for s in range(args.steps):
         ch0 = (s * nch) % (384 - nch + 1)
         t0 = time.perf_counter()
+        massage()
+        t1 = time.perf_counter()
         oracle.correlate(blk, ch0=ch0, nch=nch)
-        times.append(time.perf_counter() - t0)
-    per_block = statistics.mean(times) * 384.0 / nch
+        t2 = time.perf_counter()
+        times.append((t1 - t0) + (t2 - t1) * 384.0 / nch)
+    per_block = statistics.mean(times)
     v = 1.0 / per_block
+    sample = ("one full block per step" if nch == 384 else
+              f"massage on the full block + X-engine on {nch} of 384 channels per step, scaled")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_block * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic seeded Gaussian sigma 2.5, 4+4-bit",
         "config": {"workload": "full-size correlator block [2048][63][384][2][2] -> 768x2080x4 vis",
-                   "sample": f"{nch} of 384 channels per step, scaled to a block"},
+                   "sample": sample},
+        "same_config": nch == 384,
         "realtime_factor": v * REALTIME_S,
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthr, "kind": "port",
-                         "sample": f"{nch} channels x 2048 packets x 63 antennas per step"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthr, "kind": kind,
+                         "sample": sample,
+                         "parts": f"massage() from the reference source ({mthr} threads) + "
+                                  f"oracle X-engine ({nthr} threads)"},
+        "reorders_s_per_block": _time_reorders(oracle, blk, nthr),
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference C/CUDA sources need psrdada and the un-vendored xGPU; the "
-                "oracle/ port of the xGPU CPU X-engine (OpenMP) is timed instead",
+        "note": "the reference's X-engine is the un-vendored xGPU library; its CPU arithmetic "
+                "is the oracle port (OpenMP); the corner turn is the reference's own code",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -214,42 +307,109 @@ def _time_loop(stream, fn, steps, warm=3):
     return e0.elapsed_time(e1) / steps
 
 
-def bench_beamformer(dsax, synth, dev, blk_dev, steps):
-    """Beamformer workload: 256 beams, 32 t x 8 ch Stokes-I from a full block (BF16)."""
+def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
+    """Beamformer workload: 256 beams, 32 t x 8 ch Stokes-I from a full block
+    (BF16, and FP8 E4M3): device-timed, end to end with host buffers, error
+    of every output of two channel groups against the FP64 oracle, and the
+    oracle's FP64 beamformer on the host cores as the CPU baseline."""
+    import ctypes
     import torch
-    cfg = dsax.default_config(bf_scale=128.0 / (512 * 64 * 2 * 6.25))
+    import oracle
+    scale = 128.0 / (512 * 64 * 2 * 6.25)
+    cfg = dsax.default_config(bf_scale=scale)
+    wre, wim = synth.random_phase_weights(9, 48, 256)
+    blk_host = synth.gen_block(4242, 2048, 63, 384, "gauss")
+    nout = 128 * 256 * 48
     with dsax.Context(cfg, device=dev) as ctx:
-        wre, wim = synth.random_phase_weights(9, 48, 256)
         ctx.set_weights(wre, wim)
-        out = torch.empty(128 * 256 * 48, dtype=torch.uint8, device=f"cuda:{dev}")
+        out = torch.empty(nout, dtype=torch.uint8, device=f"cuda:{dev}")
+        f32 = torch.empty(nout, dtype=torch.float32, device=f"cuda:{dev}")
         st = torch.cuda.ExternalStream(ctx.stream)
         ms = _time_loop(st, lambda i: ctx.beamform(blk_dev[i % len(blk_dev)], out), steps)
+        # error against FP64 on two channel groups of the first block
+        ctx.beamform(blk_dev[0], out, f32)
         ctx.sync()
-    # the same block with FP8 E4M3 operands (per-antenna power-of-two weight scale)
-    cfg8 = dsax.default_config(bf_scale=128.0 / (512 * 64 * 2 * 6.25), bf_fp8=1)
+        got = f32.cpu().numpy().reshape(128, 256, 48).astype(np.float64)
+        gu8 = out.cpu().numpy().reshape(128, 256, 48)
+        # end to end: pinned host block in, uint8 beams out, every step
+        lib = dsax.lib()
+        p_in, p_out = ctypes.c_void_p(), ctypes.c_void_p()
+        assert lib.dsax_host_alloc(ctx.handle, BLOCK_IN, ctypes.byref(p_in)) == 0
+        assert lib.dsax_host_alloc(ctx.handle, nout, ctypes.byref(p_out)) == 0
+        ctypes.memmove(p_in.value, blk_host.ctypes.data, BLOCK_IN)
+        for _ in range(2):
+            ctx.beamform(p_in.value, p_out.value, None, dsax.MEM_HOST)
+        e_steps = 10
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            ctx.beamform(p_in.value, p_out.value, None, dsax.MEM_HOST)
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / e_steps
+        lib.dsax_host_free(ctx.handle, p_in)
+        lib.dsax_host_free(ctx.handle, p_out)
+    # the FP8 E4M3 operands (per-antenna power-of-two weight scale)
+    cfg8 = dsax.default_config(bf_scale=scale, bf_fp8=1)
     with dsax.Context(cfg8, device=dev) as ctx:
         ctx.set_weights(wre, wim)
         st = torch.cuda.ExternalStream(ctx.stream)
         ms8 = _time_loop(st, lambda i: ctx.beamform(blk_dev[i % len(blk_dev)], out), steps)
         ctx.sync()
+    # per-output error on groups 0 and 47 against the oracle on the same block
+    blk0 = blk_dev[0].cpu().numpy().reshape(2048, 63, 384, 2, 2)
+    err = {}
+    rel_all, lsb_all = [], []
+    for g in (0, 47):
+        ref = oracle.beamform_power(blk0, wre, wim, 16, g0=g, ng=1)[:, :, 0]
+        rel = np.abs(got[:, :, g] - ref) / np.maximum(ref, 1e-30)
+        lsb = np.abs(gu8[:, :, g].astype(int) - oracle.quantize_u8(ref, scale).astype(int))
+        rel_all.append(rel.reshape(-1))
+        lsb_all.append(lsb.reshape(-1))
+    rel_all = np.concatenate(rel_all)
+    lsb_all = np.concatenate(lsb_all)
+    err = {"outputs_checked": int(rel_all.size), "groups": [0, 47],
+           "fp32_rel_max": float(rel_all.max()), "fp32_rel_mean": float(rel_all.mean()),
+           "u8_max_lsb": int(lsb_all.max()), "u8_frac_off_by_1": float((lsb_all == 1).mean())}
+    # CPU baseline: the oracle's FP64 beamformer on the host cores, a sample
+    # of channel groups scaled to the block
+    t0 = time.perf_counter()
+    ng = 0
+    while ng < 48 and time.perf_counter() - t0 < 8.0:
+        oracle.beamform_power(blk_host, wre, wim, 16, g0=ng, ng=2)
+        ng += 2
+    cpu_s = (time.perf_counter() - t0) * 48.0 / ng
     burst, sust, kind = _bf16_peak()
     tf = BF_FLOPS / (ms * 1e-3) / 1e12
     tf8 = BF_FLOPS / (ms8 * 1e-3) / 1e12
-    return {"workload": "64 ant x 2 pol x 384 ch x 4096 t -> 128 x 256 x 48 uint8, 256 beams, BF16",
-            "blocks_per_s": 1e3 / ms, "ms_per_block": ms, "realtime_factor": 1e3 / ms * REALTIME_S,
-            "gpu_launches_per_block": 1,
-            "roofline": {"bound": "tensor", "kernel": "bf_kernel", "achieved": tf,
-                         "peak": burst, "unit": "TFLOP/s", "frac": tf / burst,
-                         "frac_of_sustained": tf / sust, "peak_kind": f"{kind} BF16 dense"},
-            "fp8": {"ms_per_block": ms8, "blocks_per_s": 1e3 / ms8, "achieved_tflops": tf8,
-                    "frac_of_2x_bf16_peak": tf8 / (2 * burst),
-                    "peak_kind": "E4M3 dense taken as 2x the measured BF16 burst (FP8 not measured)"}}
+    fp8_peak = (peaks or {}).get("fp8_tops")
+    res = {"workload": "64 ant x 2 pol x 384 ch x 4096 t -> 128 x 256 x 48 uint8, 256 beams, BF16",
+           "blocks_per_s": 1e3 / ms, "ms_per_block": ms, "realtime_factor": 1e3 / ms * REALTIME_S,
+           "gpu_launches_per_block": 1,
+           "roofline": {"bound": "tensor", "kernel": "bf_kernel", "achieved": tf,
+                        "peak": burst, "unit": "TFLOP/s", "frac": tf / burst,
+                        "frac_of_sustained": tf / sust, "peak_kind": f"{kind} BF16 dense (cuBLAS)"},
+           "error_vs_fp64": err,
+           "e2e": {"value": 1e3 / e2e_ms, "unit": "blocks/s", "ms_per_step": e2e_ms,
+                   "h2d_bytes_per_step": BLOCK_IN, "d2h_bytes_per_step": nout,
+                   "call": "dsax_beamform, DSAX_MEM_HOST (pinned)"},
+           "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "blocks/s", "kind": "port",
+                            "cores": oracle.nthreads(),
+                            "sample": f"FP64 oracle beamformer on {ng} of 48 channel groups of one "
+                                      f"block, scaled"},
+           "fp8": {"ms_per_block": ms8, "blocks_per_s": 1e3 / ms8, "achieved_tflops": tf8,
+                   "frac_of_2x_bf16_peak": tf8 / (2 * burst),
+                   "peak_kind": "E4M3 dense taken as 2x the measured BF16 burst"}}
+    if fp8_peak:
+        res["fp8"]["frac_of_probe"] = tf8 / fp8_peak
+        res["fp8"]["probe_tflops"] = fp8_peak
+    return res
 
 
 def bench_flaggers(dsax, synth, dev, steps, train_steps=1000):
-    """Flagger workload: plain vs learned flagger on [256][4096][48] FP32 (chi2(2)+RFI).
+    """Flagger workload: plain vs learned flagger on [256][4096][48] FP32
+    (chi2(2) + RFI), plus the plain flagger's data path (dsax_flag_clean) on
+    that block and on a reference-shaped uint8 block [64][16384][1024].
     The learned net is trained here first (outside the timed regions)."""
     import torch
+    import oracle
     from dsax import lflag
     x, _ = synth.gen_filterbank(4040)
     xd = torch.from_numpy(x).to(f"cuda:{dev}")
@@ -261,6 +421,30 @@ def bench_flaggers(dsax, synth, dev, steps, train_steps=1000):
         cm = torch.zeros(B * C, dtype=torch.uint8, device=xd.device)
         tm = torch.zeros(B * T, dtype=torch.uint8, device=xd.device)
         plain_ms = _time_loop(st, lambda i: ctx.flag(p, xd, cm, tm), steps)
+        # the data path: measured blocks build the baseline (naver = 1), then
+        # flagged + cleaned blocks in place (the modulation check on)
+        clean = {}
+        for name, arr, dt, fp in (
+                ("fp32_256x4096x48", x, dsax.DTYPE_F32, p),
+                ("u8_64x16384x1024", None, dsax.DTYPE_U8,
+                 dsax.flag_params(64, 16384, 1024, guard=128, ts_base=1024))):
+            if arr is None:
+                g = torch.Generator(device=xd.device)
+                g.manual_seed(9)
+                d = torch.randint(40, 80, (64 * 16384 * 1024,), dtype=torch.uint8,
+                                  device=xd.device, generator=g)
+            else:
+                d = torch.from_numpy(arr.copy()).to(xd.device).reshape(-1)
+            fs = ctx.flag_state(fp, dsax.flag_clean_params(naver=1, mod_thresh=1.0), dt)
+            fs.clean(d)
+            nbytes = d.numel() * d.element_size()
+            cms = _time_loop(st, lambda i: fs.clean(d), steps)
+            inf = fs.info()
+            fs.close()
+            clean[name] = {"ms_per_block": cms, "gbytes_per_s": nbytes / (cms * 1e-3) / 1e9,
+                           "block_bytes": nbytes, "flagged": bool(inf.flagged),
+                           "gpu_launches_per_block": 4}
+            del d
         train = [torch.from_numpy(synth.gen_filterbank(5000 + k, nbeam=64)[0]).to(xd.device)
                  for k in range(4)]
         ctx.lf_init(11)
@@ -274,14 +458,57 @@ def bench_flaggers(dsax, synth, dev, steps, train_steps=1000):
         pred, ref = lflag.evaluate(ctx, xd, tds)
     P, R, F1 = lflag.prf1(pred, ref)
     npx = B * T * C
+    peak, peak_kind = _peaks()
+    alg = npx * 4 + B * C + B * T          # filterbank read once, masks written
+    # CPU baseline: the oracle's plain flagger (statistics + decisions) on a
+    # sample of beams, scaled to the block
+    nb = 32
+    po = oracle.flag_params(nb, T, C)
+    xs = np.ascontiguousarray(x[:nb])
+    oracle.plain_flag(xs, po)
+    t0 = time.perf_counter()
+    reps = 0
+    while reps < 20 and (reps == 0 or time.perf_counter() - t0 < 6.0):
+        oracle.plain_flag(xs, po)
+        reps += 1
+    cpu_s = (time.perf_counter() - t0) / reps * B / nb
     return {"workload": "256 beams x 4096 t x 48 ch FP32 chi2(2) + tones/bursts/drifts",
             "plain": {"ms_per_block": plain_ms, "samples_per_s": npx / (plain_ms * 1e-3),
-                      "gpu_launches_per_block": 2},
+                      "gpu_launches_per_block": 4,
+                      "roofline": {"bound": "hbm", "kernel": "plain flagger (4 launches)",
+                                   "achieved": alg / (plain_ms * 1e-3) / 1e9, "peak": peak,
+                                   "unit": "GB/s", "frac": alg / (plain_ms * 1e-3) / 1e9 / peak,
+                                   "alg_bytes_per_block": alg,
+                                   "peak_kind": f"{peak_kind} (HBM copy bandwidth)"},
+                      "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "blocks/s", "kind": "port",
+                                       "cores": oracle.nthreads(),
+                                       "sample": f"oracle plain flagger on {nb} of {B} beams, "
+                                                 f"scaled"}},
+            "clean": clean,
             "learned": {"ms_per_block": learned_ms, "samples_per_s": npx / (learned_ms * 1e-3),
                         "precision": P, "recall": R, "f1": F1, "train_s": train_s,
                         "train_steps": train_steps, "params": dsax.lib().dsax_lf_nparams(),
                         "gpu_launches_per_block": 9},
             "learned_vs_plain_speed": plain_ms / learned_ms}
+
+
+def bench_config1(dsax, synth, dev, steps):
+    """The small correlator case: 64 antennas x 48 channels x 2048 packets,
+    samples uniform on [-8, 7] (bit-exact in the tests), device-timed."""
+    import torch
+    blk = synth.gen_block(101, 2048, 64, 48, "uniform")
+    cfg = dsax.default_config(npkt=2048, nant_in=64, nchan=48)
+    with dsax.Context(cfg, device=dev) as ctx:
+        d = torch.from_numpy(blk.reshape(-1)).to(f"cuda:{dev}")
+        vis = torch.empty(96 * 2080 * 8, dtype=torch.float32, device=f"cuda:{dev}")
+        st = torch.cuda.ExternalStream(ctx.stream)
+        ms = _time_loop(st, lambda i: ctx.correlate(d, vis), steps)
+        ctx.sync()
+    ops = 8 * 2080 * 4 * 96 * 2048
+    return {"workload": "64 ant x 48 ch x 2048 pkt x 2 t, uniform [-8, 7] -> 96 x 2080 x 4 vis",
+            "blocks_per_s": 1e3 / ms, "ms_per_block": ms,
+            "int8_alg_tops": ops / (ms * 1e-3) / 1e12, "gpu_launches_per_block": 2,
+            "note": "L2-resident (25 MB input); latency-bound at this size"}
 
 
 def bench_batch(dsax, synth, dev, steps):
@@ -322,10 +549,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="dsax", choices=["dsax", "reference"])
-    ap.add_argument("--ref-channels", type=int, default=24)
     ap.add_argument("--e2e-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["beamformer", "flagger", "batch"], default=None,
+    ap.add_argument("--only", choices=["beamformer", "flagger", "batch", "config1"], default=None,
                     help="run one side workload alone (profiling); prints its JSON")
     ap.add_argument("--serial", action="store_true",
                     help="one dsax_correlate call per block (no cross-block overlap)")
@@ -355,6 +581,8 @@ def main():
             blk = synth.gen_block(4242, 2048, 63, 384, "gauss")
             ins = [torch.from_numpy(blk.reshape(-1)).to(f"cuda:{local}")]
             res = bench_beamformer(dsax, synth, local, ins, args.steps)
+        elif args.only == "config1":
+            res = bench_config1(dsax, synth, local, args.steps)
         elif args.only == "flagger":
             res = bench_flaggers(dsax, synth, local, args.steps, args.lf_train_steps)
         else:
@@ -385,6 +613,17 @@ def main():
     for w in range(args.warmup):
         ctx.correlate(ins[w % nbuf], vis)
     ctx.sync()
+
+    # measured tensor-pipe peaks of this GPU (the pool measures HBM and
+    # cuBLAS BF16 only): int8, BF16 and FP8 E4M3 tcgen05.mma from shared memory
+    probes = {}
+    if rank == 0:
+        for kname, kind in (("int8_tops", 0), ("bf16_tflops", 1), ("fp8_tops", 2)):
+            try:
+                probes[kname] = ctx.probe_tensor_peak(kind, 3) / 1e12
+            except Exception as exc:
+                probes[kname] = None
+                probes[kname + "_error"] = str(exc)
 
     # ---------------------------------------------------------- device-timed
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -541,7 +780,17 @@ def main():
                          "peak_kind": f"{peak_kind} (HBM copy bandwidth)",
                          "alg_bytes_per_launch": alg,
                          "int8_alg_tops": ALG_OPS / (corr_ms * 1e-3) / 1e12,
-                         "int8_mma_tops": MMA_OPS / (corr_ms * 1e-3) / 1e12},
+                         "int8_mma_tops": MMA_OPS / (corr_ms * 1e-3) / 1e12,
+                         "int8_peak_probe_tops": probes.get("int8_tops"),
+                         "int8_alg_frac_of_probe": (ALG_OPS / (corr_ms * 1e-3) / 1e12 /
+                                                    probes["int8_tops"]
+                                                    if probes.get("int8_tops") else None),
+                         "int8_mma_frac_of_probe": (MMA_OPS / (corr_ms * 1e-3) / 1e12 /
+                                                    probes["int8_tops"]
+                                                    if probes.get("int8_tops") else None)},
+            "tensor_peaks_probe": dict(probes, how="dsax_probe_tensor_peak: every SM issues "
+                                       "back-to-back tcgen05.mma M128 N256 from shared memory "
+                                       "(builder-measured, not the pool's peak file)"),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": BLOCK_IN,
                     "d2h_bytes_per_step": VIS_OUT, "steps": e2e_steps,
                     "ms_per_step": ms_e2e / e2e_steps},
@@ -550,7 +799,9 @@ def main():
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline_sample()
         if not args.no_extras and ws == 1:
-            for key, fn in (("beamformer", lambda: bench_beamformer(dsax, synth, dev, ins, 20)),
+            for key, fn in (("config1", lambda: bench_config1(dsax, synth, dev, 50)),
+                            ("beamformer", lambda: bench_beamformer(dsax, synth, dev, ins, 20,
+                                                                    probes)),
                             ("flagger", lambda: bench_flaggers(dsax, synth, dev, 20,
                                                                args.lf_train_steps)),
                             ("batch", lambda: bench_batch(dsax, synth, dev, 5))):

@@ -434,8 +434,13 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
           for (int c = 0; c < kWBytes / 16384; ++c)
             bulk_g2s(wsm + 16384u * c, src + 16384 * c, 16384u, &wload_bar);
           if (!mbar_wait_bounded(&wload_bar, nload & 1u, &abort_sh, a.err, DEV_ERR_WAIT_FULL,
-                                 a.wait_limit_ns))
+                                 a.wait_limit_ns)) {
+            // the weight copies may still be landing: let them finish first
+            volatile int no_abort = 0;
+            mbar_wait_bounded(&wload_bar, nload & 1u, &no_abort, a.err, DEV_ERR_WAIT_FULL,
+                              drain_limit(a.wait_limit_ns));
             break;
+          }
           ++nload;
           cur_gb = gb;
         }
@@ -473,7 +478,8 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   if (warp == 12) {
     if (lane == 0) {
       volatile int no_abort = 0;
-      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM,
+                        drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
     tc_fence_after();

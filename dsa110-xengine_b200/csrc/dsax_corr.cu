@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
     // (bounded, and independent of the abort flag).
     if (lane == 0) {
       volatile int no_abort = 0;
-      mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+      mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
     tc_fence_after();
@@ -474,7 +474,8 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
   } else if (kBulk && warp == 9) {
     // ------------------------------------------------------------ bulk loader
     if (lane == 0) {
-      for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+      int ks = 0;
+      for (; ks < nks && !abort_sh; ++ks) {
         const int r = ks % kRawStages;
         if (!mbar_wait_bounded(&rempty_bar[r], ((uint32_t)(ks / kRawStages) & 1u) ^ 1u, &abort_sh,
                                a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
@@ -486,6 +487,14 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
                  a.in + (int64_t)ch * a.npkt * 256 + (int64_t)ks * kPktPerStage * 256, bytes,
                  &rfull_bar[r]);
       }
+      // copies still landing after an abort (their stages are never
+      // consumed): wait for the last one issued on each raw stage before the
+      // CTA exits; each stage has at most one copy outstanding
+      volatile int no_abort = 0;
+      for (int k2 = ks - kRawStages; k2 < ks; ++k2)
+        if (k2 >= 0)
+          mbar_wait_bounded(&rfull_bar[k2 % kRawStages], (uint32_t)(k2 / kRawStages) & 1u,
+                            &no_abort, a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
   } else {
@@ -580,7 +589,7 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
   if (warp == 8) {
     if (lane == 0) {
       volatile int no_abort = 0;
-      mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+      mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
     tc_fence_after();

@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(lftma::kThreads, 1)
       for (int g2 = g - kStages; g2 < g; ++g2)
         if (g2 >= 0)
           mbar_wait_bounded(&full_bar[g2 % kStages], (uint32_t)(g2 / kStages) & 1u, &no_abort,
-                            a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+                            a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
   } else {
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(lftma::kThreads, 1)
       bool ok = mbar_wait_bounded(&w_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns);
       if (!ok) {   // the weight copies may still be landing
         volatile int no_abort = 0;
-        mbar_wait_bounded(&w_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+        mbar_wait_bounded(&w_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
       }
       for (int i = 0; i < nmine && ok && !abort_sh; ++i) {
         const int bf = i & 1;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(lftma::kThreads, 1)
   if (warp == 9) {
     if (lane == 0) {
       volatile int no_abort = 0;
-      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
     tc_fence_after();
@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(lf1::kThreads, 1)
       for (int i2 = i - kSlots; i2 < i; ++i2)
         if (i2 >= 0)
           mbar_wait_bounded(&bfull_bar[i2 % kSlots], (uint32_t)(i2 / kSlots) & 1u, &no_abort, a.err,
-                            DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+                            DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
   } else {
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(lf1::kThreads, 1)
       bool ok = mbar_wait_bounded(&w_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns);
       if (!ok) {   // the weight copy may still be landing
         volatile int no_abort = 0;
-        mbar_wait_bounded(&w_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+        mbar_wait_bounded(&w_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
       }
       for (int i = 0; i < nmine && ok && !abort_sh; ++i) {
         const int bf = i & 1, s2 = i % kAStages;
@@ -573,7 +573,7 @@ __global__ void __launch_bounds__(lf1::kThreads, 1)
   if (warp == 9) {
     if (lane == 0) {
       volatile int no_abort = 0;
-      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, a.wait_limit_ns);
+      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
     tc_fence_after();

@@ -80,6 +80,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   }
 }
 
+// Bound on the waits that drain a CTA's own copies and MMAs in flight before
+// it frees TMEM and exits, also after an abort: at least 250 ms, so that a
+// short pipeline-wait limit never lets a CTA exit while its copies are still
+// landing in shared memory or its MMAs still reading it.
+__device__ __forceinline__ uint64_t drain_limit(uint64_t limit_ns) {
+  return limit_ns > 250000000ull ? limit_ns : 250000000ull;
+}
+
 // Generic-proxy shared-memory writes -> visible to the async proxy
 // (tensor-core operand reads).
 __device__ __forceinline__ void fence_proxy_async_smem() {

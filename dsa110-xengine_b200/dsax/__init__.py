@@ -180,6 +180,8 @@ def _bind_optional(L):
         "dsax_place_packets": ([P, P, I, I, I, P, I, ctypes.c_ulonglong, ctypes.c_ulonglong, I, P, P,
                                 P], I),
         "dsax_correlate_extract": ([P, P, P, I], I),
+        "dsax_extract_ex": ([P, P, P, I, P, I], I),
+        "dsax_correlate_extract_ex": ([P, P, P, I, P, I], I),
         "dsax_set_geometric_weights": ([P, P, P, P, ctypes.c_double, ctypes.c_double], I),
         "dsax_agc_state": ([P, P, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "dsax_lf_nparams": ([], I),
@@ -192,6 +194,7 @@ def _bind_optional(L):
         "dsax_flag_learned": ([P, P, ctypes.POINTER(FlagParams), I, P, P, I], I),
         "dsax_run_batch": ([P, ctypes.POINTER(BlockDesc), I, I], I),
         "dsax_default_flag_clean_params": ([ctypes.POINTER(FlagCleanParams)], None),
+        "dsax_probe_tensor_peak": ([P, I, I, ctypes.POINTER(ctypes.c_double)], I),
         "dsax_flag_state_create": ([P, ctypes.POINTER(FlagParams), ctypes.POINTER(FlagCleanParams),
                                     I, ctypes.POINTER(P)], I),
         "dsax_flag_state_destroy": ([P], None),
@@ -347,9 +350,15 @@ class Context:
         """simple_extract: XX/YY averaged over the two time slots."""
         self._check(lib().dsax_extract(self._h, _ptr(vis), _ptr(out), mem), "dsax_extract")
 
-    def correlate_extract(self, blk, out, mem: int = MEM_DEVICE):
-        self._check(lib().dsax_correlate_extract(self._h, _ptr(blk), _ptr(out), mem),
-                    "dsax_correlate_extract")
+    def correlate_extract(self, blk, out, mem: int = MEM_DEVICE, order: int = 0, autos=None):
+        """order 0: xGPU baselines, 1: "Greg" order; autos: spectra added to."""
+        self._check(lib().dsax_correlate_extract_ex(self._h, _ptr(blk), _ptr(out), order,
+                                                    _ptr(autos), mem),
+                    "dsax_correlate_extract_ex")
+
+    def extract_ex(self, vis, out, order: int = 0, autos=None, mem: int = MEM_DEVICE):
+        self._check(lib().dsax_extract_ex(self._h, _ptr(vis), _ptr(out), order, _ptr(autos), mem),
+                    "dsax_extract_ex")
 
     def agc_enable(self, mode: int = 1):
         """1 adaptive, 2 frozen at the first block's median, 0 off."""
@@ -415,6 +424,13 @@ class Context:
         rc = lib().dsax_flag_learned(self._h, _ptr(x), ctypes.byref(params), tds, _ptr(mask),
                                      _ptr(logits), mem)
         self._check(rc, "dsax_flag_learned")
+
+    def probe_tensor_peak(self, kind: int = 0, reps: int = 3) -> float:
+        """Measured dense tensor-core ops/s: kind 0 int8, 1 BF16, 2 FP8 E4M3."""
+        v = ctypes.c_double(0.0)
+        self._check(lib().dsax_probe_tensor_peak(self._h, kind, reps, ctypes.byref(v)),
+                    "dsax_probe_tensor_peak")
+        return v.value
 
     # -- autotuner ---------------------------------------------------------
     def autotune(self, reps: int = 10):

@@ -169,11 +169,34 @@ size_t dsax_extract_bytes(const dsax_config *cfg);
 int dsax_extract(dsax_ctx *ctx, const void *vis, void *out, int mem);
 int dsax_correlate_extract(dsax_ctx *ctx, const void *in, void *out, int mem);
 
+/* The same with the options of the visibility writers:
+ * order = DSAX_BL_XGPU keeps xGPU's baseline order; DSAX_BL_GREG writes the
+ *   baselines in the "Greg" order of src/dsaX_wrangleAndWrite.c gen_lookup /
+ *   reorder_gh (:46-93): antenna pairs (i, j >= i), i major, so output
+ *   baseline k holds xGPU baseline lookup[k].
+ * autos (may be NULL): [nant_in][nchan] float spectra to which auto_extract
+ *   (src/dsaX_wrangle.c:47-70) adds, per antenna and channel, the real part
+ *   of the time-slot-averaged XX and then YY autocorrelation (accumulated
+ *   across calls, as the reference sums N_INTS blocks before writing).
+ * out may be NULL when autos is given.  Pointers follow `mem`. */
+#define DSAX_BL_XGPU 0
+#define DSAX_BL_GREG 1
+int dsax_extract_ex(dsax_ctx *ctx, const void *vis, void *out, int order, float *autos, int mem);
+int dsax_correlate_extract_ex(dsax_ctx *ctx, const void *in, void *out, int order, float *autos,
+                              int mem);
+
 /* Autotuner: times the captured-block correlator variants (corr_path 1, 2,
  * 3, 4) on a synthetic block of the context's geometry (reps launches each),
  * sets the context's corr_path to the fastest, and returns the per-variant
  * milliseconds (times_ms[0..3] for paths 1..4, if given) and the choice. */
 int dsax_autotune(dsax_ctx *ctx, int reps, float *times_ms, int ntimes, int *best_path);
+
+/* Measured dense tensor-core throughput of the context's GPU (ops/s, best
+ * of reps): every SM issues back-to-back tcgen05.mma M=128 N=256 from shared
+ * memory.  kind 0: int8 (kind::i8, as the correlator), 1: BF16 (kind::f16,
+ * as the beamformer), 2: FP8 E4M3 (kind::f8f6f4).  No reference
+ * counterpart: the denominator for the int8 and FP8 roofline fractions. */
+int dsax_probe_tensor_peak(dsax_ctx *ctx, int kind, int reps, double *ops_per_s);
 
 /* massage() on the GPU (src/dsaX_reorder_raw.c:153-169): captured block ->
  * REORDER-key layout [pkt][2*nchan][64][2 pol] (4+4-bit kept packed, padded

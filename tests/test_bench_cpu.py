@@ -1,6 +1,7 @@
 """bench.py's reference arm on the host cores: one JSON line carrying the
 keys the benchmark contract names (metric, value, unit, cpu_baseline, e2e
-...), computed from a tiny channel sample.  Needs no GPU."""
+...), each step a whole block: the reference's own massage() (from
+oracle/_ref) plus the oracle X-engine.  Needs no GPU."""
 import json
 import os
 import subprocess
@@ -12,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_reference_arm_json_line():
     out = subprocess.run(
         [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
-         "--warmup", "1", "--ref-channels", "2"],
+         "--warmup", "1"],
         cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
@@ -26,7 +27,10 @@ def test_reference_arm_json_line():
     assert d["value"] > 0 and d["higher_is_better"] is True
     assert "workload" in d["config"]
     cb = d["cpu_baseline"]
-    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"]
+    assert d["same_config"] is True
+    ro = d["reorders_s_per_block"]
+    assert "unavailable" in ro or any(k.startswith("massage_") for k in ro)
     assert cb["unit"] == d["unit"] and cb["sample"]
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]

@@ -50,15 +50,16 @@ def _check(oracle, blk, wre, wim, u8, f32, ppo, scale, g0=0, ng=None):
     return rel, diff
 
 
-def test_beamformer_config3_subset(dsax, oracle):
+def test_beamformer_config3_full_block(dsax, oracle):
     """Full-size block: 64 ants (63 populated) x 2 pols x 384 ch x 4096 t,
-    256 beams, unit-magnitude random-phase weights, 32 t x 8 ch sums."""
+    256 beams, unit-magnitude random-phase weights, 32 t x 8 ch sums; every
+    one of the 128 x 256 x 48 outputs against the FP64 oracle."""
     blk = oracle.gen_block(303, 2048, 63, 384, "gauss")
     wre, wim = oracle.random_phase_weights(9, 48, 256)
     scale = 128.0 / (512 * 64 * 2 * 6.25)   # E[P] = 512 samples x 64 ants x E|x|^2
     u8, f32 = _beamform(dsax, blk, wre, wim, 256, 16, scale)
     assert f32.shape == (128, 256, 48)
-    rel, diff = _check(oracle, blk, wre, wim, u8, f32, 16, scale, g0=5, ng=3)
+    rel, diff = _check(oracle, blk, wre, wim, u8, f32, 16, scale)
     assert np.median(u8) > 60 and np.median(u8) < 200   # fixed scaling lands mid-range
 
 

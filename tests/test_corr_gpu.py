@@ -55,17 +55,25 @@ def test_reorder_matches_massage(dsax, oracle):
         np.testing.assert_array_equal(got, oracle.massage(blk))
 
 
+_FULL = {}
+
+
+def _full_block(oracle):
+    """The config-2 block and its oracle visibilities (computed once)."""
+    if not _FULL:
+        blk = oracle.gen_block(202, 2048, 63, 384, "gauss")
+        _FULL["blk"], _FULL["vis"] = blk, oracle.correlate(blk)
+    return _FULL["blk"], _FULL["vis"]
+
+
 @pytest.mark.parametrize("corr_path", [1, 2, 3, 4])
 def test_config2_full_block(dsax, oracle, corr_path):
     """Full block [2048][63->64][384][2][2], Gaussian sigma 2.5 clipped to
-    [-8, 7]: bit-exact on 24 channels checked by the oracle, plus
-    size-independent properties over all 768 frequencies."""
-    blk = oracle.gen_block(202, 2048, 63, 384, "gauss")
+    [-8, 7]: all 768 frequencies x 2080 baselines x 4 products bit-exact
+    against the oracle, plus size-independent properties."""
+    blk, want = _full_block(oracle)
     vis = _run(dsax, blk, corr_path=corr_path)
-    rng = np.random.default_rng(7)
-    chans = sorted(rng.choice(384, size=22, replace=False).tolist() + [0, 383])
-    for c in chans:
-        np.testing.assert_array_equal(vis[2 * c:2 * c + 2], oracle.correlate(blk, ch0=c, nch=1))
+    np.testing.assert_array_equal(vis, want)
     # autocorrelation power of every (freq, station, pol) equals sum |x|^2
     lre, lim = oracle.unpack4(np.arange(256, dtype=np.uint8))
     lut = (lre.astype(np.int16) ** 2 + lim.astype(np.int16) ** 2).astype(np.uint8)
@@ -270,3 +278,32 @@ def test_extract_and_correlate_extract(dsax, oracle):
         ctx.extract(vis, dout)
         ctx.sync()
         np.testing.assert_array_equal(dout.cpu().numpy().reshape(want.shape), want)
+
+
+def test_extract_greg_order_and_autos(dsax, oracle):
+    """The visibility writers' options on the GPU: the "Greg" baseline
+    order (gen_lookup / reorder_gh) and auto_extract accumulated over two
+    blocks, against the oracle restatements (themselves checked against the
+    reference's functions in tests/test_ref_pin.py); bit-exact."""
+    import torch
+    nchan = 40
+    cfg = dsax.default_config(npkt=128, nant_in=63, nchan=nchan)
+    blks = [oracle.gen_block(1310 + k, 128, 63, nchan, "gauss") for k in range(2)]
+    greg = oracle.greg_order()
+    specs = np.zeros((63, nchan), np.float32)
+    with dsax.Context(cfg) as ctx:
+        autos = np.zeros((63, nchan), np.float32)
+        dautos = torch.zeros(63 * nchan, dtype=torch.float32, device="cuda")
+        for blk in blks:
+            ex = oracle.simple_extract(oracle.correlate(blk))
+            specs = oracle.auto_extract(ex, specs)
+            out = np.zeros(ex.size, np.float32)
+            ctx.correlate_extract(np.ascontiguousarray(blk.reshape(-1)), out, mem=dsax.MEM_HOST,
+                                  order=1, autos=autos)
+            np.testing.assert_array_equal(out.reshape(ex.shape), ex[greg])
+            d = torch.from_numpy(np.ascontiguousarray(blk.reshape(-1))).cuda()
+            torch.cuda.synchronize()
+            ctx.correlate_extract(d, None, mem=dsax.MEM_DEVICE, autos=dautos)
+            ctx.sync()
+        np.testing.assert_array_equal(autos, specs)
+        np.testing.assert_array_equal(dautos.cpu().numpy().reshape(63, nchan), specs)
