@@ -203,6 +203,43 @@ int dsax_set_geometric_weights(dsax_ctx *c, const double *antpos, const double *
   return dsax_set_weights(c, wre.data(), wim.data());
 }
 
+int dsax_set_two_arm_weights(dsax_ctx *c, const double *antpos_e, const double *antpos_n,
+                             const int *arm, const double *cal, const int *flagged,
+                             double sfreq_mhz, double sep_arcmin, double dec_deg) {
+  if (!c || !antpos_e || !antpos_n || !arm || !cal) return DSAX_ERR_ARG;
+  const int ngrp = c->cfg.nchan / 8, nbeam = c->cfg.nbeam, nb_arm = nbeam / 2;
+  if (c->cfg.nchan % 8 || nbeam < 128 || nbeam % 128)
+    return set_error(c, DSAX_ERR_ARG, "two-arm weights need nchan %% 8 == 0, nbeam %% 128 == 0");
+  for (int a = 0; a < 64; ++a)
+    if (arm[a] != 0 && arm[a] != 1 && arm[a] != -1)
+      return set_error(c, DSAX_ERR_ARG, "arm[%d] must be 0 (E-W), 1 (N-S) or -1 (unused)", a);
+  const double kPi = 3.14159265358979323846, kC = 299792458.0;
+  std::vector<double> wre((size_t)ngrp * 2 * nbeam * 64, 0.0), wim(wre.size(), 0.0);
+  for (int g = 0; g < ngrp; ++g) {
+    const double nu = (sfreq_mhz - g * 250.0 / 1024.0) * 1e6;   // :1131
+    for (int pol = 0; pol < 2; ++pol)
+      for (int b = 0; b < nbeam; ++b) {
+        const int A = b / nb_arm, bb = b - A * nb_arm;
+        double theta = sep_arcmin * ((nb_arm / 2 - 1) - bb) * kPi / 10800.0;
+        if (A == 1) theta -= dec_deg * kPi / 180.0;
+        const double afac = -2.0 * kPi * nu * theta / kC;
+        for (int a = 0; a < 64; ++a) {
+          if (arm[a] != A || (flagged && flagged[a])) continue;
+          const double *cc = cal + (((size_t)a * ngrp + g) * 2 + pol) * 2;
+          double cr = cc[0], ci = cc[1];
+          const double n = std::sqrt(cr * cr + ci * ci);   // unit gain phase (:891-895)
+          if (n != 0.0) { cr /= n; ci /= n; }
+          const double ph = afac * (A == 0 ? antpos_e[a] : antpos_n[a]);
+          const double tr = std::cos(ph), ti = std::sin(ph);
+          const size_t o = (((size_t)g * 2 + pol) * nbeam + b) * 64 + a;
+          wre[o] = tr * cr - ti * ci;
+          wim[o] = ti * cr + tr * ci;
+        }
+      }
+  }
+  return dsax_set_weights(c, wre.data(), wim.data());
+}
+
 int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int mem) {
   if (!c || !blk || (!out_u8 && !out_f32)) return DSAX_ERR_ARG;
   if (!c->weights_ready) return set_error(c, DSAX_ERR_ARG, "dsax_set_weights not called");

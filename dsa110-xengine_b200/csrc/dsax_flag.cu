@@ -659,14 +659,19 @@ bool flag_shape_ok(const FlagArgs &a) {
   return stage_rows(t, es) > 0;
 }
 
-// Upper bounds over every slab of the launch (a narrower last slab has
-// fewer column groups and at most 4 x kStatThreads bin partials).
+// The largest layout over the launch's slabs: the full slab width cs and,
+// when nchan is not a multiple of it, the narrower last slab (whose P x cs
+// bin partials can exceed the full slab's).  Kept tight: at 48 channels two
+// CTAs must share an SM.
 static size_t stats_smem(const FlagArgs &a, int es) {
   const int cs = a.nchan < kFlagSlab ? a.nchan : kFlagSlab;
+  const int last = a.nchan > kFlagSlab ? a.nchan % kFlagSlab : 0;
+  auto bp = [](int w) { return (size_t)(flag::kStatThreads / (w / 4)) * w; };
+  size_t nbp = bp(cs);
+  if (last && bp(last) > nbp) nbp = bp(last);
   const size_t stage = ((size_t)a.rs * cs * es + 127) & ~(size_t)127;
-  return flag::kStages * stage +
-         sizeof(double) * ((size_t)a.rs * (kFlagSlab / 4) + 4 * flag::kStatThreads + kFlagSlab) +
-         sizeof(float) * kFlagSlab;
+  return flag::kStages * stage + sizeof(double) * ((size_t)a.rs * (cs / 4) + nbp + cs) +
+         sizeof(float) * cs;
 }
 
 int launch_flag_stats(FlagArgs a, cudaStream_t st) {

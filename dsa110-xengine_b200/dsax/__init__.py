@@ -183,6 +183,8 @@ def _bind_optional(L):
         "dsax_extract_ex": ([P, P, P, I, P, I], I),
         "dsax_correlate_extract_ex": ([P, P, P, I, P, I], I),
         "dsax_set_geometric_weights": ([P, P, P, P, ctypes.c_double, ctypes.c_double], I),
+        "dsax_set_two_arm_weights": ([P, P, P, P, P, P, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double], I),
         "dsax_agc_state": ([P, P, ctypes.POINTER(I), ctypes.POINTER(I)], I),
         "dsax_lf_nparams": ([], I),
         "dsax_lf_init": ([P, ctypes.c_ulonglong], I),
@@ -337,6 +339,21 @@ class Context:
         self._check(lib().dsax_set_geometric_weights(self._h, _ptr(antpos), _ptr(cal), _ptr(fl),
                                                      float(fch1_mhz), float(sep_arcmin)),
                     "dsax_set_geometric_weights")
+
+    def set_two_arm_weights(self, antpos_e, antpos_n, arm, cal, flagged=None,
+                            sfreq_mhz: float = 1498.75, sep_arcmin: float = 1.0,
+                            dec_deg: float = 0.0):
+        """Two-arm weights with the declination term (see include/dsax.h)."""
+        import numpy as np
+        ae = np.ascontiguousarray(antpos_e, dtype=np.float64)
+        an = np.ascontiguousarray(antpos_n, dtype=np.float64)
+        ar = np.ascontiguousarray(arm, dtype=np.int32)
+        cal = np.ascontiguousarray(cal, dtype=np.float64)
+        fl = None if flagged is None else np.ascontiguousarray(flagged, dtype=np.int32)
+        self._check(lib().dsax_set_two_arm_weights(self._h, _ptr(ae), _ptr(an), _ptr(ar), _ptr(cal),
+                                                   _ptr(fl), float(sfreq_mhz), float(sep_arcmin),
+                                                   float(dec_deg)),
+                    "dsax_set_two_arm_weights")
 
     def place_packets(self, pkts, npk, stride, payload, ant_lookup, act0, nslots, slots_per_seq,
                       block, counts, next_block=None):

@@ -239,6 +239,21 @@ int dsax_correlate_fmt(dsax_ctx *ctx, int fmt, const void *in, void *vis, int me
 int dsax_set_geometric_weights(dsax_ctx *ctx, const double *antpos, const double *cal,
                                const int *flagged, double fch1_mhz, double sep_arcmin);
 int dsax_set_weights(dsax_ctx *ctx, const double *wre, const double *wim);
+
+/* Two-arm weights with a declination term, the cuBLAS beamformer's
+ * populate_weights_matrix (src/dsaX_bfCorr.cu:815-863, calc_weights
+ * :869-928): beams [0, nbeam/2) are formed from the E-W arm (arm[a] == 0,
+ * phase from antpos_e), beams [nbeam/2, nbeam) from the N-S arm (arm[a] ==
+ * 1, phase from antpos_n, the beam angle offset by -dec_deg degrees; the
+ * reference passes 37.23 - its observation declination); an antenna only
+ * contributes to its own arm's beams (arm[a] = -1: to none).  Beam b of an
+ * arm points at sep x (nbeam/4 - 1 - b) arcmin (127 - b for 256 beams per
+ * arm); group g's frequency is sfreq - g x 250/1024 MHz (:1131); gains are
+ * cal / |cal| (:891-895), zero for flagged antennas.  Computed in FP64,
+ * then converted as dsax_set_weights.  Needs nbeam % 128 == 0. */
+int dsax_set_two_arm_weights(dsax_ctx *ctx, const double *antpos_e, const double *antpos_n,
+                             const int *arm, const double *cal, const int *flagged,
+                             double sfreq_mhz, double sep_arcmin, double dec_deg);
 int dsax_beamform(dsax_ctx *ctx, const void *blk, void *out_u8, void *out_f32, int mem);
 
 /* Automatic gain control of the uint8 beams (src/dsaX_beamformer.cu badder

@@ -23,6 +23,10 @@ generated file):
   src/dsaX_wrangle.c  auto_extract, simple_extract (:47-93);
   src/dsaX_wrangleAndWrite.c  gen_lookup, reorder_gh (:46-93, the "Greg"
                       baseline order);
+  src/dsaX_bfCorr.cu  populate_weights_matrix (:815-863), the two-arm
+                      weights with the declination term (an element kernel,
+                      run per (block, thread) on the host; half stored as
+                      float);
   src/dsaX_reorder_raw.c      massage (:98-219, the byte reorder);
   src/dsaX_reorder_raw.c.bak  massage (:98-266, AVX-512 fluff + transpose).
 
@@ -34,7 +38,10 @@ Shapes (the reference's compile-time constants, set with -D):
            baseline is NTIMES_P/16 = 128 samples), NPERMFLAGS 1,
            flagchannels {10}, MN 48, SIG 6, FBIN 8, TBIN 128;
   reorder  NANTS 63 (README.md:34; dsaX_def.h's 96 belongs to the bfCorr
-           variant), NPACKETS 2048 and a 64-packet build for quick tests.
+           variant), NPACKETS 2048 and a 64-packet build for quick tests;
+  weights  NANTS 96 (48 per arm), NBEAMS 512, NCHAN_PER_PACKET 16 (two
+           frequency groups instead of 48, to keep the host run short),
+           sep 1.0 arcmin, PI and CVAC as dsaX_def.h:28-29.
 
 Usage:  python oracle/make_ref.py [--reference DIR]
 """
@@ -78,6 +85,7 @@ int massage_run_@TAG@(const char *in, char *out, int nthreads) {
 '''
 
 FLAG_SHAPE = {"NBEAMS_P": 64, "NTIMES_P": 2048, "NCHAN_P": 1024}
+BFCORR_SHAPE = ["-DNCHAN_PER_PACKET=16", "-DNBEAMS=512"]
 
 
 def _strip_spans(src: str) -> list[tuple[int, int]]:
@@ -169,7 +177,12 @@ def generate(ref: str) -> list[str]:
     wpieces += [(ww, *extract(ww, n)) for n in GH_FUNCS]
     # dsaX_wrangleAndWrite.c:40 declares the baseline count these use
     wr_src = _unit('#include "ref_stubs.h"\nstatic const int nbl = 2080;\n', wpieces)
-    units = {"ref_flagger.cpp": flag_src, "ref_wrangle.c": wr_src}
+    bc = os.path.join(ref, "src", "dsaX_bfCorr.cu")
+    bc_src = _unit('#include "ref_stubs.h"\n#include <cmath>\ntypedef float half;\n'
+                   '#define __float2half(x) (x)\n#define sep 1.0\n#define PI 3.14159265359\n'
+                   '#define CVAC 299792458.0\n',
+                   [(bc, *extract(bc, "populate_weights_matrix"))])
+    units = {"ref_flagger.cpp": flag_src, "ref_wrangle.c": wr_src, "ref_bfcorr.cpp": bc_src}
     for tag, fname in (("raw", "dsaX_reorder_raw.c"), ("bak", "dsaX_reorder_raw.c.bak")):
         p = os.path.join(ref, "src", fname)
         st = extract_struct(p, "data")
@@ -219,12 +232,15 @@ def build(ref: str = DEFAULT_REF, cc: str | None = None, cxx: str | None = None)
         jobs = [
             ([cxx] + common + shape + ["-std=gnu++17", "-c", "ref_flagger.cpp"], "ref_flagger.o"),
             ([cc] + common + ["-std=gnu11", "-c", "ref_wrangle.c"], "ref_wrangle.o"),
+            ([cxx] + common + BFCORR_SHAPE + ["-DNANTS=96", "-std=gnu++17", "-c",
+                                              "ref_bfcorr.cpp"],
+             "ref_bfcorr.o"),
             ([cc] + common + reo + ["-std=gnu11", "-Dmassage=reference_massage_raw", "-c",
                                     "ref_massage_raw.c"], "ref_massage_raw.o"),
             ([cc] + common + reo + ["-std=gnu11", "-mavx512f", "-mavx512bw",
                                     "-Dmassage=reference_massage_bak", "-c", "ref_massage_bak.c"],
              "ref_massage_bak.o"),
-            ([cxx] + common + shape + reo + ["-std=gnu++17", "-c",
+            ([cxx] + common + shape + reo + BFCORR_SHAPE + ["-DNANTS_BF=96", "-std=gnu++17", "-c",
                                              os.path.join(HERE, "ref_harness.cpp")],
              "ref_harness.o"),
         ]

@@ -200,6 +200,43 @@ def geometric_weights(antpos, cal, flagged, ngrp: int, nbeam: int,
     return wre, wim
 
 
+def two_arm_weights(antpos_e, antpos_n, arm, cal, flagged, ngrp: int, nbeam: int,
+                    sfreq_mhz: float, sep_arcmin: float, dec_deg: float, pi: float = np.pi):
+    """populate_weights_matrix (src/dsaX_bfCorr.cu:815-863) with the gain
+    normalisation of its calc_weights (:869-928), in FP64: beams [0, nbeam/2)
+    from arm 0 (phase from antpos_e), [nbeam/2, nbeam) from arm 1 (antpos_n,
+    beam angle offset by -dec_deg degrees); gains cal / |cal|, zero for
+    flagged antennas and for antennas of the other arm.  Returns wre, wim
+    [ngrp][2 pol][nbeam][nant] (nant = len(antpos_e))."""
+    antpos_e = np.asarray(antpos_e, np.float64)
+    antpos_n = np.asarray(antpos_n, np.float64)
+    arm = np.asarray(arm)
+    nant = antpos_e.size
+    cal = np.asarray(cal, np.float64).reshape(nant, ngrp, 2, 2)
+    cr, ci = cal[..., 0], cal[..., 1]
+    n = np.sqrt(cr * cr + ci * ci)
+    n = np.where(n == 0, 1.0, n)
+    g_ = (cr + 1j * ci) / n                                   # [a][g][pol]
+    if flagged is not None:
+        g_ = np.where(np.asarray(flagged)[:, None, None] != 0, 0, g_)
+    nb_arm = nbeam // 2
+    w = np.zeros((ngrp, 2, nbeam, nant), np.complex128)
+    for A in (0, 1):
+        pos = antpos_e if A == 0 else antpos_n
+        bb = np.arange(nb_arm)
+        theta = sep_arcmin * ((nb_arm // 2 - 1) - bb) * pi / 10800.0
+        if A == 1:
+            theta = theta - dec_deg * pi / 180.0
+        for g in range(ngrp):
+            nu = (sfreq_mhz - g * 250.0 / 1024.0) * 1e6
+            afac = -2.0 * pi * nu * theta / 299792458.0        # [bb]
+            ph = np.exp(1j * afac[:, None] * pos[None, :])      # [bb][a]
+            ph = np.where((arm == A)[None, :], ph, 0)
+            for pol in range(2):
+                w[g, pol, A * nb_arm:(A + 1) * nb_arm] = ph * g_[None, :, g, pol]
+    return w.real.copy(), w.imag.copy()
+
+
 def beamform_power(blk: np.ndarray, wre: np.ndarray, wim: np.ndarray,
                    pkt_per_out: int = 16, g0: int = 0, ng: int | None = None) -> np.ndarray:
     """FP64 Stokes-I power [npkt/pkt_per_out][nbeam][ng]."""
@@ -652,6 +689,8 @@ def ref_lib(small: bool = False):
     L.ref_simple_extract.argtypes = [P, P]
     L.ref_gen_lookup.argtypes = [P]
     L.ref_reorder_gh.argtypes = [P, P, P]
+    L.ref_bfcorr_shape.argtypes = [P, P, P]
+    L.ref_populate_weights.argtypes = [P, P, P, P, P, P, f32]
     L.ref_massage_raw.argtypes = [P, P, i32]
     L.ref_massage_raw.restype = i32
     L.ref_massage_bak.argtypes = [P, P, i32]

@@ -7,10 +7,12 @@
  * code, and bench.py's reference arm times the reorders with it.  The
  * product library never loads it.
  *
- * The flagger's element kernels (scaley, flag, flagts) are CUDA kernels in
- * the reference; they read only blockIdx.x / threadIdx.x and global memory
- * (no shared memory, no barriers), so running every (block, thread) pair in
- * turn on the host computes exactly what their launches compute.
+ * The flagger's element kernels (scaley, flag, flagts) and the cuBLAS
+ * beamformer's populate_weights_matrix are CUDA kernels in the reference;
+ * they read only blockIdx.x / threadIdx.x and global memory (no shared
+ * memory, no barriers), so running every (block, thread) pair in turn on
+ * the host computes what their launches compute (up to the device's float
+ * cos/sin, which differ from the host's in the last bits).
  */
 #include "ref_stubs.h"
 
@@ -32,6 +34,9 @@ void gather_tsmask(int *h_idx, int *h_mask, int *n_mask);
 void calc_bpwr(float *h_spec, float *h_bpwr);
 void median_calc(float *arr);
 void scaley(unsigned char *data, float *spectrum, float *varspec);
+// src/dsaX_bfCorr.cu, compiled in ref_bfcorr.cpp (half stored as float)
+void populate_weights_matrix(float *antpos_e, float *antpos_n, float *calibs, float *wr, float *wi,
+                             float *fqs, float dec);
 void flag(unsigned char *data, int *midx, unsigned char *repval, float *bpwr);
 void flagts(unsigned char *data, int *midx, unsigned char *repval, float *bpwr);
 
@@ -90,6 +95,25 @@ void ref_flagts(unsigned char *data, int *midx, int n_mask, float *bpwr) {
       blockIdx.x = (int)b;
       threadIdx.x = t;
       flagts(data, midx, nullptr, bpwr);
+    }
+}
+
+// populate_weights_matrix<<<2*(NCHAN_PER_PACKET/8)*(NBEAMS/2)*128*(NANTS/2)/128, 128>>>
+// (src/dsaX_bfCorr.cu:921): wr / wi [2 arms][NCHAN_PER_PACKET/8][NBEAMS/2]
+// [4 t][NANTS/2][8 ch][2 t][2 pol]
+void ref_bfcorr_shape(int *nants, int *ngrp, int *nbeams) {
+  *nants = NANTS_BF;
+  *ngrp = NCHAN_PER_PACKET / 8;
+  *nbeams = NBEAMS;
+}
+void ref_populate_weights(float *antpos_e, float *antpos_n, float *calibs, float *wr, float *wi,
+                          float *fqs, float dec) {
+  const long long nblk = 2LL * (NCHAN_PER_PACKET / 8) * (NBEAMS / 2) * 128 * (NANTS_BF / 2) / 128;
+  for (long long b = 0; b < nblk; ++b)
+    for (int t = 0; t < 128; ++t) {
+      blockIdx.x = (int)b;
+      threadIdx.x = t;
+      populate_weights_matrix(antpos_e, antpos_n, calibs, wr, wi, fqs, dec);
     }
 }
 

@@ -96,6 +96,36 @@ def test_beamformer_geometric_weights(dsax, oracle):
     np.testing.assert_array_equal(u8b, u8)
 
 
+def test_beamformer_two_arm_declination_weights(dsax, oracle):
+    """The cuBLAS beamformer's two-arm weights (E-W arm beams from
+    eastings, N-S arm beams from northings with the declination offset) on
+    the tcgen05 beamformer: 256 beams, 32 antennas per arm, against the FP64
+    oracle with the same weights; the library's FP64 generation must match
+    the oracle's weights image exactly."""
+    rng = np.random.default_rng(31)
+    ae = rng.uniform(-400, 400, 64)
+    an = rng.uniform(-400, 400, 64)
+    arm = np.repeat([0, 1], 32)
+    arm[63] = -1                                   # the padded antenna
+    cal = rng.normal(size=(64, 2, 2, 2))
+    flagged = np.zeros(64, np.int32)
+    flagged[[5, 44]] = 1
+    sfreq, dec = 1498.75, 37.23 - 52.0
+    wre, wim = oracle.two_arm_weights(ae, an, arm, cal, flagged, 2, 256, sfreq, 1.0, dec)
+    blk = oracle.gen_block(78, 64, 63, 16, "gauss")
+    ref = oracle.beamform_power(blk, wre, wim, pkt_per_out=16)
+    scale = 128.0 / float(np.median(ref))
+    u8, f32 = _beamform(dsax, blk, wre, wim, 256, 16, scale)
+    _check(oracle, blk, wre, wim, u8, f32, 16, scale)
+    cfg = dsax.default_config(npkt=64, nant_in=63, nchan=16, nbeam=256, bf_pkt_per_out=16,
+                              bf_scale=scale)
+    with dsax.Context(cfg) as ctx:
+        ctx.set_two_arm_weights(ae, an, arm, cal, flagged, sfreq, 1.0, dec)
+        u8b, f32b = _beamform(dsax, blk, wre, wim, 256, 16, scale, ctx=ctx, set_w=False)
+    np.testing.assert_array_equal(f32b, f32)
+    np.testing.assert_array_equal(u8b, u8)
+
+
 def test_beamformer_single_antenna_tone(dsax, oracle):
     """Only antenna 7 carries a constant 3+2i and weights pick it with
     magnitude 1: every beam's power is |3+2i|^2 x samples."""
