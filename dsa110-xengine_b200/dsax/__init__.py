@@ -197,6 +197,8 @@ def _bind_optional(L):
         "dsax_run_batch": ([P, ctypes.POINTER(BlockDesc), I, I], I),
         "dsax_default_flag_clean_params": ([ctypes.POINTER(FlagCleanParams)], None),
         "dsax_probe_tensor_peak": ([P, I, I, ctypes.POINTER(ctypes.c_double)], I),
+        "dsax_ct_pack": ([P, P, I, I, I, I, P], I),
+        "dsax_ct_unpack": ([P, P, I, I, I, I, P, I, I, I, I], I),
         "dsax_flag_state_create": ([P, ctypes.POINTER(FlagParams), ctypes.POINTER(FlagCleanParams),
                                     I, ctypes.POINTER(P)], I),
         "dsax_flag_state_destroy": ([P], None),
@@ -441,6 +443,17 @@ class Context:
         rc = lib().dsax_flag_learned(self._h, _ptr(x), ctypes.byref(params), tds, _ptr(mask),
                                      _ptr(logits), mem)
         self._check(rc, "dsax_flag_learned")
+
+    def ct_pack(self, beams, nt: int, nb: int, nc: int, ndest: int, send):
+        """Beam corner turn, sending side: [nt][nb][nc] -> [ndest][nb/ndest][nt][nc]."""
+        self._check(lib().dsax_ct_pack(self._h, _ptr(beams), nt, nb, nc, ndest, _ptr(send)),
+                    "dsax_ct_pack")
+
+    def ct_unpack(self, recv, nsrc: int, nbl: int, nt: int, nc: int, fil, fil_nt: int,
+                  fil_nc: int, t0: int = 0, ch0: int = 0):
+        """Beam corner turn, receiving side: [nsrc][nbl][nt][nc] -> filterbank."""
+        self._check(lib().dsax_ct_unpack(self._h, _ptr(recv), nsrc, nbl, nt, nc, _ptr(fil), fil_nt,
+                                         fil_nc, t0, ch0), "dsax_ct_unpack")
 
     def probe_tensor_peak(self, kind: int = 0, reps: int = 3) -> float:
         """Measured dense tensor-core ops/s: kind 0 int8, 1 BF16, 2 FP8 E4M3."""

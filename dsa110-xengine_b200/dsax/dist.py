@@ -62,3 +62,29 @@ def corner_turn_beams(local, group=None):
     dist.all_to_all_single(recv.view(-1), send.view(-1), group=group)
     # recv[src][nb][T][C] -> [nb][T][src][C] -> [nb][T][W*C]
     return recv.permute(1, 2, 0, 3).reshape(nb, T, W * C)
+
+
+def beam_corner_turn(ctx, beams, fil, t0: int = 0, ch0: int = 0, group=None):
+    """The beam corner turn through the library: this rank's beamformer
+    output beams [T][NB][C] (uint8, device) is packed per destination on the
+    GPU (dsax_ct_pack), exchanged with one all-to-all (NCCL), and the
+    received subbands are placed into this rank's search filterbank
+    fil [NB/W][fil_T][fil_C] at sample t0 and channel ch0 + src * C
+    (dsax_ct_unpack).  Rank r receives beams NB/W * r .. NB/W * (r + 1) - 1 of
+    every rank's subband, ordered by source rank."""
+    import torch
+    import torch.distributed as dist
+    W = dist.get_world_size(group)
+    T, NB, C = beams.shape
+    nbl = NB // W
+    if NB % W:
+        raise ValueError("beam count must divide by the world size")
+    send = torch.empty(W * nbl * T * C, dtype=torch.uint8, device=beams.device)
+    recv = torch.empty_like(send)
+    ctx.ct_pack(beams, T, NB, C, W, send)
+    # the collective runs on torch's current stream: order it after the pack
+    torch.cuda.ExternalStream(ctx.stream).synchronize()
+    dist.all_to_all_single(recv, send, group=group)
+    torch.cuda.current_stream(beams.device).synchronize()
+    ctx.ct_unpack(recv, W, nbl, T, C, fil, fil.shape[1], fil.shape[2], t0, ch0)
+    return fil

@@ -401,6 +401,24 @@ int dsax_flag_state_noise(dsax_ctx *ctx, dsax_flag_state *st, void *noise);
 int dsax_flag_noalloc(const dsax_flag_params *p, const float *x, const float *oldspec,
                       uint8_t *chanmask, uint8_t *tsmask, int *counts, void *stream);
 
+/* ---- beam corner turn (beamformer -> search-side flagger) ----
+ * The socket corner turn of src/dsaX_dbnic.c:84-152 and
+ * src/dsaX_nicdb.c:180-196 as two device reorders around one all-to-all
+ * (NCCL over NVLink; the caller's collective, e.g. torch.distributed).
+ * dsax_ct_pack: this subband's beams [nt][nb][nc] (the beamformer's uint8
+ *   output layout) -> send [ndest][nb/ndest][nt][nc], one contiguous chunk
+ *   per destination (dbnic's per-search-node transpose).
+ * dsax_ct_unpack: the chunks received from nsrc subbands,
+ *   recv [nsrc][nbl][nt][nc] -> fil[nbl][t0 + t][ch0 + s nc + k] of a
+ *   [nbl][fil_nt][fil_nc] uint8 filterbank (nicdb's placement; the
+ *   reference uses fil_nc = 1024, ch0 = CHOFF/8 = 128, 16 subbands of 48
+ *   channels, so the unfilled channels are the flagger's guard bands).
+ * Device pointers; enqueued on the context stream. */
+int dsax_ct_pack(dsax_ctx *ctx, const uint8_t *beams, int nt, int nb, int nc, int ndest,
+                 uint8_t *send);
+int dsax_ct_unpack(dsax_ctx *ctx, const uint8_t *recv, int nsrc, int nbl, int nt, int nc,
+                   uint8_t *fil, int fil_nt, int fil_nc, int t0, int ch0);
+
 /* ---- batches of blocks ----
  * Many consecutive capture blocks in one submission, each with its own
  * subband width (nchan, a multiple of 8, at most the nchan the context

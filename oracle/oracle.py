@@ -705,3 +705,22 @@ def ref_available() -> bool:
     if os.path.exists(os.path.join(_HERE, "_ref", "libref.so")):
         return True
     return os.path.isdir(os.environ.get("DSAX_REFERENCE", "/root/reference"))
+
+
+# --------------------------------------------------------------------------
+# beam corner turn (src/dsaX_dbnic.c:84-152, src/dsaX_nicdb.c:180-196)
+# --------------------------------------------------------------------------
+def ct_pack(beams: np.ndarray, ndest: int) -> np.ndarray:
+    """dbnic's per-search-node transpose: beams [T][NB][C] ->
+    [ndest][NB/ndest][T][C] (op[j][i][k] = output[i][d*nbl + j][k])."""
+    T, NB, C = beams.shape
+    return np.ascontiguousarray(beams.reshape(T, ndest, NB // ndest, C).transpose(1, 2, 0, 3))
+
+
+def ct_unpack(recv: np.ndarray, fil: np.ndarray, t0: int, ch0: int) -> np.ndarray:
+    """nicdb's placement: recv [nsrc][nbl][T][C] into fil[nbl][t0 + t]
+    [ch0 + src C + k]."""
+    S, nbl, T, C = recv.shape
+    for s in range(S):
+        fil[:, t0:t0 + T, ch0 + s * C:ch0 + (s + 1) * C] = recv[s]
+    return fil

@@ -99,3 +99,57 @@ def test_beam_corner_turn_all_to_all_gloo():
             for t in range(T):
                 for ch in range(W * C):
                     assert got[bl, t, ch] == (t * 1000 + r * (NB // W) + bl) * 100 + ch
+
+
+def _ct_chain_worker(rank, world_size, port, out):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [os.path.join(root, "dsa110-xengine_b200"), os.path.join(root, "oracle")]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world_size), LOCAL_RANK=str(rank))
+    import numpy as np
+    import torch
+    import oracle
+    from dsax import dist as D
+    d = D.init("gloo", timeout_s=60)
+    W = world_size
+    T, NB, C, fil_nc, ch0 = 8, 16, 48, 256, 32
+    rng = np.random.default_rng(100 + rank)
+    beams = rng.integers(0, 256, (T, NB, C), dtype=np.uint8)   # this subband's beamformer output
+    # the exchange beam_corner_turn performs around its two device reorders:
+    # pack per destination, one all-to-all, place by source rank
+    send = torch.from_numpy(oracle.ct_pack(beams, W).reshape(-1).copy())
+    recv = torch.empty_like(send)
+    d.all_to_all_single(recv, send)
+    fil = np.zeros((NB // W, T, fil_nc), np.uint8)
+    oracle.ct_unpack(recv.numpy().reshape(W, NB // W, T, C), fil, 0, ch0)
+    d.barrier()
+    d.destroy_process_group()
+    out.put((rank, beams, fil))
+
+
+def test_beam_corner_turn_pack_exchange_place_gloo():
+    """World size 2, the beam corner turn's three steps (dbnic's pack, the
+    all-to-all, nicdb's placement at channel ch0 + subband x C): rank r's
+    filterbank holds beams r NB/W .. of every rank's subband, channels in
+    rank order, guard bands empty."""
+    import numpy as np
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ct_chain_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = {r: (b, f) for r, b, f in (q.get(timeout=120) for _ in procs)}
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    W, T, NB, C, ch0 = 2, 8, 16, 48, 32
+    for r in range(W):
+        fil = res[r][1]
+        for s in range(W):
+            np.testing.assert_array_equal(fil[:, :, ch0 + s * C:ch0 + (s + 1) * C],
+                                          res[s][0][:, r * NB // W:(r + 1) * NB // W, :]
+                                          .transpose(1, 0, 2))
+        assert not fil[:, :, :ch0].any() and not fil[:, :, ch0 + W * C:].any()
