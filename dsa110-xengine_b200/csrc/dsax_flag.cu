@@ -6,13 +6,11 @@
 //   calc_spectrum / calc_varspec / calc_maxspec /       statistics pass
 //   calc_ppspec (:175-376; the reference calls           (one HBM read)
 //   calc_spectrum in calc_maxspec's place at :1334 -- parity mode keeps that)
-//   total-power modulation check (:1313-1330)        -> flag_chan_kernel
-//   channflag x3, simple_channflag (:1340-1347),        (decisions on the
-//   calc_bpwr (:759-769), gather_mask                   GPU, per beam)
-//   flag (:459-474), then make_ts (:414-453)         -> flag_apply_kernel
-//                                                       (reads only the
-//                                                       flagged columns)
-//   simple_tsflag (:612-653), flagts (:479-494)      -> flag_ts_kernel
+//   total-power modulation check (:1313-1330)        -> flag_beam_kernel,
+//   channflag x3, simple_channflag (:1340-1347),        one CTA per beam:
+//   calc_bpwr (:759-769), gather_mask                   decisions on the
+//   flag (:459-474), then make_ts (:414-453)            GPU, reading only
+//   simple_tsflag (:612-653), flagts (:479-494)         the flagged chunks
 // and fix_zspec (:114-170) + median_calc (:771-798) for the scaley
 // baseline.  The shapes the reference hard-codes ([64][16384][1024] uint8,
 // ZeroChannels 128, nFiltSize 21, TBIN 128, FBIN 8, T/16) are parameters;
@@ -32,9 +30,7 @@ constexpr int kStatThreads = 256;
 constexpr int kStages = 3;
 constexpr int kStageTarget = 24576;   // bytes per pipeline stage (upper bound)
 constexpr int kMaxChan = 1024;
-constexpr int kChanThreads = 256;     // four decision groups of 64 threads
-constexpr int kApplyRows = 256;       // rows per apply CTA (one per thread)
-constexpr int kTsThreads = 256;
+constexpr int kBeamThreads = 512;     // per-beam decisions: four groups of 64 + all for rows
 constexpr int kMaxTsBase = 4096;
 constexpr int kLfMaxChan = 128;       // learned-flagger features: channels per beam
 constexpr int kDecThreads = 256;
@@ -115,7 +111,7 @@ __device__ __forceinline__ E repl_elem(float r) {
 // baseline the stage is normalised in shared memory first and written back
 // (the statistics then describe the normalised block, as in the reference).
 // Per row the slab's raw sum goes to rowsum (or to ts when there is one
-// slab); flag_apply_kernel turns it into the channel-mean series after the
+// slab); flag_beam_kernel turns it into the channel-mean series after the
 // flagged columns are replaced.
 template <typename E>
 __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagArgs a) {
@@ -209,6 +205,15 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
         sm_rs[r * G4 + g] = rr;
       }
     }
+    const bool bin_end = (st + 1) % spb == 0;
+    if (spb == 1 && active) {   // one stage per bin: its partials go out with the rows
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        sm_bp[p * cs + 4 * g + j] = bs[j];
+        s[j] += bs[j];
+        bs[j] = 0.0;
+      }
+    }
     if (a.pix_sum) {   // downsampled spectrogram: rs / tds whole pixel rows per stage
       __syncthreads();
       const float *sf = reinterpret_cast<const float *>(sp);
@@ -232,16 +237,18 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
       for (int k = 0; k < G4; ++k) r += sm_rs[tid * G4 + k];
       put_row(t0 + tid, r);
     }
-    if ((st + 1) % spb == 0) {   // the last stage of a TBIN bin: bin means per channel
-      if (active) {
+    if (bin_end) {   // the last stage of a TBIN bin: bin means per channel
+      if (spb > 1) {
+        if (active) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          sm_bp[p * cs + 4 * g + j] = bs[j];
-          s[j] += bs[j];
-          bs[j] = 0.0;
+          for (int j = 0; j < 4; ++j) {
+            sm_bp[p * cs + 4 * g + j] = bs[j];
+            s[j] += bs[j];
+            bs[j] = 0.0;
+          }
         }
+        __syncthreads();
       }
-      __syncthreads();
       if (tid < cs) {
         double bsum = 0.0;
         for (int k = 0; k < P; ++k) bsum += sm_bp[k * cs + tid];
@@ -391,29 +398,54 @@ __device__ void grp_channflag(const float *sb, float thr, const FlagArgs &a, uin
   }
 }
 
-// The channel decisions of one beam (one CTA), after the block-level steps:
-//  - total power of the block (sum of every beam's spectrum, FP64, the same
-//    order in every CTA) and, with modcheck, the modulation test against
-//    the previous flagged block (:1313-1330): at or above mod_thresh the
-//    block is replaced by noise and nothing else is flagged;
-//  - calc_bpwr (:759-769) when pwr is set: the beam's replacement level;
-//  - the four channel tests, concurrently in four groups of 64 threads:
-//    channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
-//    channflag(max, Thr), simple_channflag(pp, Thr / sqrt(FBIN)) (one-sided
-//    FBIN-channel mean; parity mode keeps the reference's spec[j] sum,
-//    :594), ORed into one mask, plus the permanent flag channels.
-__global__ void __launch_bounds__(flag::kChanThreads) flag_chan_kernel(FlagArgs a) {
-  const int b = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
-  const int C = a.nchan, G = a.guard, n = C - 2 * G, BC = a.nbeam * C;
-  extern __shared__ float dsh[];                          // [4 groups][3][C]
-  uint8_t *cmask = reinterpret_cast<uint8_t *>(dsh + 12 * C);   // [C]
+// Everything after the statistics pass, for one beam per CTA, in the order
+// of the reference's block loop (src/gpu_flagger.cu:1313-1398):
+//  1. total power of the block (every beam's spectrum summed in FP64, the
+//     same order in every CTA) and, with modcheck, the modulation test
+//     against the previous flagged block (:1313-1330): at or above
+//     mod_thresh the block is replaced by the noise block and nothing else
+//     is flagged;
+//  2. calc_bpwr (:759-769) when pwr is set: the beam's replacement level;
+//  3. the four channel tests, concurrently in four groups of 64 threads:
+//     channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
+//     channflag(max, Thr), simple_channflag(pp, Thr / sqrt(FBIN)) (one-sided
+//     FBIN-channel mean; parity mode keeps the reference's spec[j] sum,
+//     :594), ORed into one mask, plus the permanent flag channels;
+//  4. flag (:459-474) then make_ts (:414-453): the flagged columns are set to
+//     MN * bpwr (clean mode) and the channel-mean series is formed from the
+//     replaced data.  Only the 16-byte chunks of a row that hold flagged
+//     channels are read: ts = (row sum from the statistics pass + sum over
+//     flagged channels of (level - x)) / nchan.  L lanes share a row (L the
+//     power of two covering the active chunks, at most 32), so a few flagged
+//     channels cost a few sectors per row and a fully flagged row is read
+//     once, coalesced.  For uint8 every term is an exact integer, so ts
+//     equals the reference's float tree sum / NCHAN_P bit for bit;
+//  5. simple_tsflag (:612-653) and flagts (:479-494): median and MAD (lower
+//     medians, by radix select) of the first ts_base samples, rows with
+//     ts - med > TsThr * MAD flagged (one-sided); clean mode sets channels
+//     [guard, nchan - guard) of every flagged row to the level.
+// A replaced block gets the noise block written into every beam (clean
+// mode, :1323-1324); its masks are zero and ts keeps the raw row sums.
+template <typename E>
+__global__ void __launch_bounds__(flag::kBeamThreads) flag_beam_kernel(FlagArgs a) {
+  constexpr int ES = (int)sizeof(E), EPC = 16 / ES;   // elements per 16-byte chunk
+  const int b = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int C = a.nchan, G = a.guard, n = C - 2 * G, T = a.ntime, BC = a.nbeam * C;
+  const int NCH = C / EPC;
+  extern __shared__ __align__(16) float bsh[];
+  float *dsh = bsh;                                       // [4 groups][3][C]
+  float *tsb = dsh + 12 * C;                              // [ts_base]
+  float *tmp = tsb + a.ts_base;                           // [ts_base]
+  uint32_t *chk = reinterpret_cast<uint32_t *>(tmp + a.ts_base);   // [NCH]
+  uint8_t *cmask = reinterpret_cast<uint8_t *>(chk + NCH);          // [C]
   __shared__ uint32_t hist[4][256], sel[4][2];
-  __shared__ double red[flag::kChanThreads];
-  __shared__ int replaced_sh;
+  __shared__ double red[flag::kBeamThreads];
+  __shared__ int replaced_sh, nact_sh;
 
+  // 1-2: block-level steps
   if (a.modcheck || a.tpwr_out) {
     double acc = 0.0;
-    for (int i = tid; i < BC; i += flag::kChanThreads) acc += a.spec[i];
+    for (int i = tid; i < BC; i += flag::kBeamThreads) acc += a.spec[i];
     red[tid] = acc;
   }
   __syncthreads();
@@ -421,7 +453,7 @@ __global__ void __launch_bounds__(flag::kChanThreads) flag_chan_kernel(FlagArgs 
     int rep = 0;
     if (a.modcheck || a.tpwr_out) {
       double tp = 0.0;
-      for (int k = 0; k < flag::kChanThreads; ++k) tp += red[k];
+      for (int k = 0; k < flag::kBeamThreads; ++k) tp += red[k];
       if (a.modcheck) {
         const double prev = *a.prev_tpwr;
         if (prev > 0.0 && fabs(tp - prev) / prev >= (double)a.mod_thresh) rep = 1;
@@ -436,26 +468,43 @@ __global__ void __launch_bounds__(flag::kChanThreads) flag_chan_kernel(FlagArgs 
       a.bpwr[b] = (float)(((double)acc / (double)(C - 2 * G)) / (double)a.mn);
     }
   }
-  for (int c = tid; c < C; c += flag::kChanThreads) cmask[c] = 0;
+  for (int c = tid; c < C; c += flag::kBeamThreads) cmask[c] = 0;
   __syncthreads();
-  if (!replaced_sh) {
+  const bool replaced = replaced_sh != 0;
+  E *xw = a.clean ? elem_out<E>(a) : nullptr;
+  uint8_t *mb = a.tsmask + (int64_t)b * T;
+  if (replaced) {
+    for (int c = tid; c < C; c += flag::kBeamThreads) a.chanmask[b * C + c] = 0;
+    for (int t = tid; t < T; t += flag::kBeamThreads) mb[t] = 0;
+    const E *nz = static_cast<const E *>(a.noise);
+    if (xw && nz) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(nz);
+      uint4 *dst = reinterpret_cast<uint4 *>(xw + (int64_t)b * T * C);
+      const int64_t nv = (int64_t)T * C / EPC;
+      for (int64_t i = tid; i < nv; i += flag::kBeamThreads) dst[i] = src[i];
+    }
+    return;
+  }
+
+  // 3: channel decisions
+  if (warp < 8) {
     const int g = warp >> 1, gsize = 64, gtid = tid - 64 * g, bid = 1 + g;
-    float *sb = dsh + g * 3 * C, *corr = sb + C, *tmp = corr + C;
+    float *sb = dsh + g * 3 * C, *corr = sb + C, *tm = corr + C;
     const float *src = g == 0 ? a.spec : g == 1 ? a.var : g == 2 ? a.maxs : a.pp;
     for (int c = gtid; c < C; c += gsize)
       sb[c] = src[b * C + c] - ((g == 0 && a.oldspec) ? a.oldspec[b * C + c] : 0.0f);
     named_bar(bid, gsize);
     if (g < 3) {
       const float thr = g == 1 ? a.thresh + a.var_add : a.thresh;
-      grp_channflag(sb, thr, a, cmask, corr, tmp, hist[g], sel[g], gtid, gsize, bid);
+      grp_channflag(sb, thr, a, cmask, corr, tm, hist[g], sel[g], gtid, gsize, bid);
     } else {   // simple_channflag (:559-610)
       for (int i = gtid; i < n; i += gsize) corr[i] = sb[G + i];
       named_bar(bid, gsize);
       const int k = (n + 1) / 2 - 1;
       const float med = grp_radix_select(corr, n, k, hist[g], sel[g], gtid, gsize, bid);
-      for (int i = gtid; i < n; i += gsize) tmp[i] = fabsf(corr[i] - med);
+      for (int i = gtid; i < n; i += gsize) tm[i] = fabsf(corr[i] - med);
       named_bar(bid, gsize);
-      const float mad = grp_radix_select(tmp, n, k, hist[g], sel[g], gtid, gsize, bid);
+      const float mad = grp_radix_select(tm, n, k, hist[g], sel[g], gtid, gsize, bid);
       const float mythr = (float)((double)a.thresh / sqrt((double)a.fbin));
       for (int j = G + gtid; j < C - G - a.fbin; j += gsize) {
         float vv = 0.0f;
@@ -464,124 +513,106 @@ __global__ void __launch_bounds__(flag::kChanThreads) flag_chan_kernel(FlagArgs 
         if (vv > mythr * mad) cmask[j] = 1;
       }
     }
-    __syncthreads();
-    if (tid == 0)
-      for (int q = 0; q < a.nperm; ++q) {
-        const int j = a.perm[q];
-        if (j >= G && j < C - G) cmask[j] = 1;
-      }
   }
   __syncthreads();
-  int nflag = 0;
-  for (int c = tid; c < C; c += flag::kChanThreads) {
-    a.chanmask[b * C + c] = cmask[c];
-    nflag += cmask[c];
-  }
-  if (nflag && a.counts) atomicAdd(a.counts, nflag);
-}
-
-// flag (:459-474) followed by make_ts (:414-453): the flagged columns of a
-// beam are replaced by MN * bpwr[beam] (clean mode) and the channel-mean
-// time series is formed from the replaced data.  Only the flagged columns
-// are read: ts = (row sum from the statistics pass + sum over flagged
-// channels of (level - x)) / nchan.  For uint8 every term is an exact
-// integer, so ts equals the reference's float tree sum / NCHAN_P bit for
-// bit.  When the modulation check replaced the block, clean mode writes the
-// noise block into every beam (:1323-1324) and the series is that of the
-// noise.  One thread per row, grid (row chunks, beams).
-template <typename E>
-__global__ void __launch_bounds__(flag::kApplyRows) flag_apply_kernel(FlagArgs a) {
-  const int b = blockIdx.y, tid = threadIdx.x;
-  const int T = a.ntime, C = a.nchan;
-  const int t0 = blockIdx.x * flag::kApplyRows, t = t0 + tid;
-  __shared__ short fl[flag::kMaxChan];
-  __shared__ int nf_sh;
-  const bool replaced = a.status && a.status[0];
-  const E *xin = (a.spec0 && elem_out<E>(a)) ? elem_out<E>(a) : elem_in<E>(a);
-  E *xw = a.clean ? elem_out<E>(a) : nullptr;
-  if (replaced) {
-    const E *nz = static_cast<const E *>(a.noise);
-    const int rows = min(flag::kApplyRows, T - t0);
-    if (xw && nz)
-      for (int i = tid; i < rows * C; i += flag::kApplyRows)
-        xw[((int64_t)b * T + t0) * C + i] = nz[(int64_t)t0 * C + i];
-    if (t < T && nz) {
-      double r = 0.0;
-      for (int c = 0; c < C; ++c) r += (float)nz[(int64_t)t * C + c];
-      a.ts[(int64_t)b * T + t] = (float)(r / C);
+  if (tid == 0)
+    for (int q = 0; q < a.nperm; ++q) {
+      const int j = a.perm[q];
+      if (j >= G && j < C - G) cmask[j] = 1;
     }
-    return;
+  __syncthreads();
+  {
+    int nflag = 0;
+    for (int c = tid; c < C; c += flag::kBeamThreads) {
+      a.chanmask[b * C + c] = cmask[c];
+      nflag += cmask[c];
+    }
+    if (nflag && a.counts) atomicAdd(a.counts, nflag);
   }
-  if (tid == 0) {
-    int k = 0;
-    for (int c = 0; c < C; ++c)
-      if (a.chanmask[b * C + c]) fl[k++] = (short)c;
-    nf_sh = k;
+  // 4: the active chunks of a row, in channel order (warp 0, ballots):
+  // chunk index | element mask << 16
+  if (warp == 0) {
+    int base = 0;
+    for (int k0 = 0; k0 < NCH; k0 += 32) {
+      const int k = k0 + lane;
+      uint32_t m = 0u;
+      if (k < NCH)
+        for (int e = 0; e < EPC; ++e) m |= (uint32_t)cmask[k * EPC + e] << e;
+      const uint32_t bal = __ballot_sync(0xffffffffu, m != 0u);
+      if (m) chk[base + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)k | (m << 16);
+      base += __popc(bal);
+    }
+    if (lane == 0) nact_sh = base;
   }
   __syncthreads();
-  if (t >= T) return;
-  const int nf = nf_sh;
+  const int nact = nact_sh;
+  int L = 1;
+  while (L < nact && L < 32) L <<= 1;
+  const int rpw = 32 / L, sub = lane & (L - 1);   // rows per warp pass, lane within the row
   const E re = repl_elem<E>(a.mn * (a.bpwr ? a.bpwr[b] : 1.0f));
   const float rf = (float)re;
-  double corr = 0.0;
-  if (nf) {
-    const E *row = xin + ((int64_t)b * T + t) * C;
-    E *wrow = xw ? xw + ((int64_t)b * T + t) * C : nullptr;
-    for (int k = 0; k < nf; ++k) {
-      const int c = fl[k];
-      corr += (double)(rf - (float)row[c]);
-      if (wrow) wrow[c] = re;
+  const E *xin = (a.spec0 && elem_out<E>(a)) ? elem_out<E>(a) : elem_in<E>(a);
+  const int nw = flag::kBeamThreads / 32;
+  for (int t0 = warp * rpw; t0 < T; t0 += nw * rpw) {   // uniform per warp
+    const int t = t0 + lane / L;
+    double corr = 0.0;
+    if (t < T) {
+      const uint4 *row = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C);
+      uint4 *wrow = xw ? reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C) : nullptr;
+      for (int i = sub; i < nact; i += L) {
+        const uint32_t ce = chk[i];
+        const int k = (int)(ce & 0xFFFFu);
+        const uint32_t m = ce >> 16;
+        uint4 v = row[k];
+        E *ve = reinterpret_cast<E *>(&v);
+#pragma unroll
+        for (int e = 0; e < EPC; ++e)
+          if ((m >> e) & 1u) {
+            corr += (double)(rf - (float)ve[e]);
+            ve[e] = re;
+          }
+        if (wrow) wrow[k] = v;
+      }
+    }
+    for (int o = L >> 1; o > 0; o >>= 1) corr += __shfl_xor_sync(0xffffffffu, corr, o);
+    if (t < T && sub == 0) {
+      double rsum;
+      if (a.nslab == 1) {
+        rsum = a.ts[(int64_t)b * T + t];
+      } else {
+        rsum = 0.0;
+        for (int s = 0; s < a.nslab; ++s) rsum += a.rowsum[((int64_t)b * a.nslab + s) * T + t];
+      }
+      a.ts[(int64_t)b * T + t] = (float)((rsum + corr) / C);
     }
   }
-  double rsum;
-  if (a.nslab == 1) {
-    rsum = a.ts[(int64_t)b * T + t];
-  } else {
-    rsum = 0.0;
-    for (int s = 0; s < a.nslab; ++s) rsum += a.rowsum[((int64_t)b * a.nslab + s) * T + t];
-  }
-  a.ts[(int64_t)b * T + t] = (float)((rsum + corr) / C);
-}
+  __syncthreads();   // the series written above is read back by other threads
 
-// simple_tsflag (:612-653) and flagts (:479-494) for one beam: median and
-// MAD (lower medians, by radix select) of the first ts_base samples of the
-// series, rows with ts - med > TsThr * MAD flagged (one-sided); clean mode
-// then sets channels [guard, nchan - guard) of every flagged row to the
-// beam's level.
-template <typename E>
-__global__ void __launch_bounds__(flag::kTsThreads) flag_ts_kernel(FlagArgs a) {
-  const int b = blockIdx.x, tid = threadIdx.x;
-  const int T = a.ntime, C = a.nchan, G = a.guard;
-  uint8_t *mb = a.tsmask + (int64_t)b * T;
-  const bool replaced = a.status && a.status[0];
-  if (!a.tsflag || replaced) {
-    for (int t = tid; t < T; t += flag::kTsThreads) mb[t] = 0;
+  // 5: time-series flags
+  const float *tb = a.ts + (int64_t)b * T;
+  if (!a.tsflag) {
+    for (int t = tid; t < T; t += flag::kBeamThreads) mb[t] = 0;
     return;
   }
-  extern __shared__ float tsh[];   // [2][ts_base]
-  __shared__ uint32_t hist[256], sel[2];
-  const float *tb = a.ts + (int64_t)b * T;
-  float *tsb = tsh, *tmp = tsh + a.ts_base;
-  for (int i = tid; i < a.ts_base; i += flag::kTsThreads) tsb[i] = tb[i];
+  for (int i = tid; i < a.ts_base; i += flag::kBeamThreads) tsb[i] = tb[i];
   __syncthreads();
   const int kmed = (a.ts_base + 1) / 2 - 1;   // lower median
-  const float med = grp_radix_select(tsb, a.ts_base, kmed, hist, sel, tid, flag::kTsThreads, 1);
-  for (int i = tid; i < a.ts_base; i += flag::kTsThreads) tmp[i] = fabsf(tsb[i] - med);
+  const float med =
+      grp_radix_select(tsb, a.ts_base, kmed, hist[0], sel[0], tid, flag::kBeamThreads, 1);
+  for (int i = tid; i < a.ts_base; i += flag::kBeamThreads) tmp[i] = fabsf(tsb[i] - med);
   __syncthreads();
-  const float mad = grp_radix_select(tmp, a.ts_base, kmed, hist, sel, tid, flag::kTsThreads, 1);
+  const float mad =
+      grp_radix_select(tmp, a.ts_base, kmed, hist[0], sel[0], tid, flag::kBeamThreads, 1);
   const float lim = a.ts_thresh * mad;
   int nts = 0;
-  for (int t = tid; t < T; t += flag::kTsThreads) {
+  for (int t = tid; t < T; t += flag::kBeamThreads) {
     const uint8_t f = (tb[t] - med) > lim ? 1 : 0;
     mb[t] = f;
     nts += f;
   }
   if (nts && a.counts) atomicAdd(a.counts + 1, nts);
-  E *xw = a.clean ? elem_out<E>(a) : nullptr;
   if (!xw) return;
   __syncthreads();   // the row flags written above are read back by other threads
-  const E re = repl_elem<E>(a.mn * (a.bpwr ? a.bpwr[b] : 1.0f));
-  const int warp = tid >> 5, lane = tid & 31, nw = flag::kTsThreads / 32;
   for (int t = warp; t < T; t += nw) {
     if (!mb[t]) continue;
     E *row = xw + ((int64_t)b * T + t) * C;
@@ -695,8 +726,8 @@ int launch_flag_stats(FlagArgs a, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-// Statistics, channel decisions, column replacement + time series, time
-// series decisions (+ row replacement): four launches on one stream.
+// The statistics pass, then everything else per beam in one kernel: two
+// launches on one stream.
 int launch_flag(const FlagArgs &a0, cudaStream_t st) {
   FlagArgs a = a0;
   if (a.nchan > flag::kMaxChan || a.ts_base < 1 || a.ts_base > flag::kMaxTsBase ||
@@ -708,18 +739,17 @@ int launch_flag(const FlagArgs &a0, cudaStream_t st) {
   if (rc != 0) return rc;
   const bool u8 = a.xu8 != nullptr;
   a.rs = stage_rows(a, u8 ? 1 : 4);
-  const size_t sh_chan = sizeof(float) * 12 * (size_t)a.nchan + a.nchan;
-  static SmemAttrOnce attr_chan;
-  if (smem_attr_once(attr_chan, flag_chan_kernel, 64 * 1024) != cudaSuccess) return -2;
-  flag_chan_kernel<<<a.nbeam, flag::kChanThreads, sh_chan, st>>>(a);
-  const dim3 agrid((a.ntime + flag::kApplyRows - 1) / flag::kApplyRows, a.nbeam);
-  const size_t sh_ts = sizeof(float) * 2 * (size_t)a.ts_base;
+  const int nch = a.nchan * (u8 ? 1 : 4) / 16;
+  const size_t sh = sizeof(float) * (12 * (size_t)a.nchan + 2 * (size_t)a.ts_base) +
+                    sizeof(uint32_t) * nch + a.nchan;
   if (u8) {
-    flag_apply_kernel<uint8_t><<<agrid, flag::kApplyRows, 0, st>>>(a);
-    flag_ts_kernel<uint8_t><<<a.nbeam, flag::kTsThreads, sh_ts, st>>>(a);
+    static SmemAttrOnce attr;
+    if (smem_attr_once(attr, flag_beam_kernel<uint8_t>, 120 * 1024) != cudaSuccess) return -2;
+    flag_beam_kernel<uint8_t><<<a.nbeam, flag::kBeamThreads, sh, st>>>(a);
   } else {
-    flag_apply_kernel<float><<<agrid, flag::kApplyRows, 0, st>>>(a);
-    flag_ts_kernel<float><<<a.nbeam, flag::kTsThreads, sh_ts, st>>>(a);
+    static SmemAttrOnce attr;
+    if (smem_attr_once(attr, flag_beam_kernel<float>, 120 * 1024) != cudaSuccess) return -2;
+    flag_beam_kernel<float><<<a.nbeam, flag::kBeamThreads, sh, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

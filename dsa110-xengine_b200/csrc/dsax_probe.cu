@@ -76,6 +76,19 @@ __global__ void __launch_bounds__(probe::kThreads, 1) probe_mma_kernel(int nmma,
   if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
+// A wait on an mbarrier that nothing arrives on: the bounded wait must give
+// up after limit_ns, record DEV_ERR_WAIT_FULL in the error word and return.
+__global__ void wait_check_kernel(int *err, uint64_t limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ volatile int abort_sh;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    abort_sh = 0;
+    mbar_fence_init();
+    mbar_wait_bounded(&bar, 0u, &abort_sh, err, DEV_ERR_WAIT_FULL, limit_ns);
+  }
+}
+
 template <int KIND>
 static int probe_launch(int grid, int nmma, int *err, uint64_t limit, cudaStream_t st) {
   static SmemAttrOnce attr;
@@ -123,4 +136,13 @@ extern "C" int dsax_probe_tensor_peak(dsax_ctx *c, int kind, int reps, double *o
   cudaEventDestroy(e1);
   *ops_per_s = best;
   return rc;
+}
+
+extern "C" int dsax_check_wait_limit(dsax_ctx *c, unsigned long long limit_ns) {
+  if (!c || limit_ns == 0 || limit_ns > 10000000000ull) return DSAX_ERR_ARG;
+  DeviceGuard g(c->device);
+  wait_check_kernel<<<1, 32, 0, c->stream>>>(c->d_err, limit_ns);
+  const int rc = cuda_check(c, cudaGetLastError(), "wait check launch");
+  if (rc != DSAX_OK) return rc;
+  return dsax_sync(c);
 }

@@ -69,7 +69,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 63u) == 0) {
+    // the clock is read after the second failed try (so a short limit bites
+    // even where each try suspends the thread for a while) and then every
+    // 64 tries
+    if (it == 1u || (it & 63u) == 0) {
       if (*abort) return false;
       if (globaltimer() - t0 > limit_ns) {
         atomicOr(err, code);

@@ -198,6 +198,7 @@ def _bind_optional(L):
         "dsax_default_flag_clean_params": ([ctypes.POINTER(FlagCleanParams)], None),
         "dsax_probe_tensor_peak": ([P, I, I, ctypes.POINTER(ctypes.c_double)], I),
         "dsax_ct_pack": ([P, P, I, I, I, I, P], I),
+        "dsax_check_wait_limit": ([P, ctypes.c_ulonglong], I),
         "dsax_ct_unpack": ([P, P, I, I, I, I, P, I, I, I, I], I),
         "dsax_flag_state_create": ([P, ctypes.POINTER(FlagParams), ctypes.POINTER(FlagCleanParams),
                                     I, ctypes.POINTER(P)], I),

@@ -132,11 +132,12 @@ int dsax_host_free(dsax_ctx *ctx, void *ptr);
  * overwrite. */
 int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
 
-/* nblk CAPTURED blocks -> nblk xGPU triangular visibility buffers, with the
- * stages of consecutive blocks overlapped: block i+1's corner turn runs on a
- * side stream while block i is correlated, and with mem = DSAX_MEM_HOST the
- * copies in and out overlap both (pinned host buffers give asynchronous
- * DMA).  Replaces the per-block loop of src/dsaX_xgpu.cu:300-357 (H2D,
+/* nblk CAPTURED blocks -> nblk xGPU triangular visibility buffers.  With
+ * mem = DSAX_MEM_HOST the stages of consecutive blocks overlap: block i+1's
+ * copy in and corner turn run on side streams while block i is correlated
+ * and block i-1 copied out (pinned host buffers give asynchronous DMA).  In
+ * device mode each block is corner-turned and correlated in sequence on the
+ * context stream (overlapping the two on the GPU measured slower).  Replaces the per-block loop of src/dsaX_xgpu.cu:300-357 (H2D,
  * promoter, xgpuCudaXengine, matrix copy-out, one block at a time).  Device
  * mode enqueues (ordered on the context stream); host mode returns when all
  * visibilities are in the host buffers.  Output always overwrites.  Uses
@@ -197,6 +198,13 @@ int dsax_autotune(dsax_ctx *ctx, int reps, float *times_ms, int ntimes, int *bes
  * as the beamformer), 2: FP8 E4M3 (kind::f8f6f4).  No reference
  * counterpart: the denominator for the int8 and FP8 roofline fractions. */
 int dsax_probe_tensor_peak(dsax_ctx *ctx, int kind, int reps, double *ops_per_s);
+
+/* Failure detection check (no reference counterpart): one kernel waits on a
+ * barrier that nothing completes, with the same bounded wait the pipelines
+ * use, limited to limit_ns (<= 10 s).  Returns DSAX_ERR_TIMEOUT from the
+ * device error word, as any kernel whose wait expired does; the context
+ * stays usable. */
+int dsax_check_wait_limit(dsax_ctx *ctx, unsigned long long limit_ns);
 
 /* massage() on the GPU (src/dsaX_reorder_raw.c:153-169): captured block ->
  * REORDER-key layout [pkt][2*nchan][64][2 pol] (4+4-bit kept packed, padded
