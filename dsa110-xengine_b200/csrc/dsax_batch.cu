@@ -72,6 +72,7 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     f.counts = reinterpret_cast<int *>(fstats + 4 * nbc + (size_t)cf.nbeam * nout);
     f.chanmask = d.chanmask;
     f.tsmask = d.tsmask ? d.tsmask : reinterpret_cast<uint8_t *>(f.counts + 2);
+    f.ctr = reinterpret_cast<int *>(fstats + 4 * nbc + 2 * (size_t)cf.nbeam * nout + 64);
     // the flag counters accumulate with atomics: clear them per block (inside
     // the graph too, so every replay starts from zero)
     if (cudaMemsetAsync(f.counts, 0, 2 * sizeof(int), c->stream) != cudaSuccess) return -2;
@@ -107,7 +108,7 @@ int dsax_run_batch(dsax_ctx *c, const dsax_block_desc *blocks, int nblk, int use
   const size_t nscr = (size_t)maxch * cf.npkt * 256;
   const size_t nfb = (size_t)cf.nbeam * nout * (maxch / 8);
   const size_t nfs = 4 * (size_t)cf.nbeam * (maxch / 8) + (size_t)cf.nbeam * nout + 64 +
-                     (size_t)cf.nbeam * nout;
+                     (size_t)cf.nbeam * nout + flag_ctr_ints(cf.nbeam);
   int rc;
   if ((rc = ensure_buffer(c, c->aux[AUX_BATCH_SCRATCH], nscr + 4 * (nfb + nfs), "batch scratch")) !=
       DSAX_OK)

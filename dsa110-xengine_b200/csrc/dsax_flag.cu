@@ -6,11 +6,14 @@
 //   calc_spectrum / calc_varspec / calc_maxspec /       statistics pass
 //   calc_ppspec (:175-376; the reference calls           (one HBM read)
 //   calc_spectrum in calc_maxspec's place at :1334 -- parity mode keeps that)
-//   total-power modulation check (:1313-1330)        -> flag_beam_kernel,
-//   channflag x3, simple_channflag (:1340-1347),        one CTA per beam:
-//   calc_bpwr (:759-769), gather_mask                   decisions on the
-//   flag (:459-474), then make_ts (:414-453)            GPU, reading only
-//   simple_tsflag (:612-653), flagts (:479-494)         the flagged chunks
+//   total-power modulation check (:1313-1330)        -> the statistics CTAs
+//   channflag x3, simple_channflag (:1340-1347)         (the last one of a
+//                                                       beam / of the grid)
+//   calc_bpwr (:759-769), gather_mask,               -> flag_apply_kernel
+//   flag (:459-474), then make_ts (:414-453),           (reads only the
+//   simple_tsflag (:612-653), flagts (:479-494)         flagged chunks; the
+//                                                       beam's last CTA does
+//                                                       the series tests)
 // and fix_zspec (:114-170) + median_calc (:771-798) for the scaley
 // baseline.  The shapes the reference hard-codes ([64][16384][1024] uint8,
 // ZeroChannels 128, nFiltSize 21, TBIN 128, FBIN 8, T/16) are parameters;
@@ -30,7 +33,8 @@ constexpr int kStatThreads = 256;
 constexpr int kStages = 3;
 constexpr int kStageTarget = 24576;   // bytes per pipeline stage (upper bound)
 constexpr int kMaxChan = 1024;
-constexpr int kBeamThreads = 512;     // per-beam decisions: four groups of 64 + all for rows
+constexpr int kApplyThreads = 256;    // apply / time-series CTA
+constexpr int kApplyRows = 256;       // rows per apply CTA
 constexpr int kMaxTsBase = 4096;
 constexpr int kLfMaxChan = 128;       // learned-flagger features: channels per beam
 constexpr int kDecThreads = 256;
@@ -102,6 +106,11 @@ __device__ __forceinline__ E repl_elem(float r) {
   }
 }
 
+// The channel decisions of beam b (defined with the order statistics below)
+// and the block's total power; both run at the end of the statistics pass.
+__device__ void flag_decide_beam(const FlagArgs &a, int b, uint8_t *smem);
+__device__ void flag_total_power(const FlagArgs &a);
+
 // ---------------------------------------------------------------- statistics
 // One CTA per (channel slab of up to kFlagSlab channels, beam).  The slab's
 // rows stream through a three-stage cp.async ring of `rs` rows each (rs
@@ -111,7 +120,7 @@ __device__ __forceinline__ E repl_elem(float r) {
 // baseline the stage is normalised in shared memory first and written back
 // (the statistics then describe the normalised block, as in the reference).
 // Per row the slab's raw sum goes to rowsum (or to ts when there is one
-// slab); flag_beam_kernel turns it into the channel-mean series after the
+// slab); flag_apply_kernel turns it into the channel-mean series after the
 // flagged columns are replaced.
 template <typename E>
 __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagArgs a) {
@@ -136,8 +145,9 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
 
   extern __shared__ __align__(16) uint8_t fs_raw[];
   const uint32_t sbase = smem_u32(fs_raw);
-  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * stage_bytes);   // [RS][G4]
-  double *sm_bp = sm_rs + RS * G4;                                         // [P][cs]
+  const int GS = G4 | 1;   // odd row stride: the row sums read column-wise conflict-free
+  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * stage_bytes);   // [RS][GS]
+  double *sm_bp = sm_rs + RS * GS;                                         // [P][cs]
   double *sm_k = sm_bp + P * cs;                                           // [cs]
   float *sm_s0 = reinterpret_cast<float *>(sm_k + cs);                     // [cs]
 
@@ -165,26 +175,56 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     else
       a.rowsum[((int64_t)b * a.nslab + slab) * T + t] = (float)r;
   };
-  // normalise (if scaling) and accumulate the four channels of one row
-  double s[4], q[4], bs[4];
-  float m[4];
+  // normalise (if scaling) and accumulate the four channels of one row:
+  // FP64 for FP32 data, exact 64-bit integers for uint8 (no FP64 work)
+  constexpr bool kU8 = std::is_same<E, uint8_t>::value;
+  using Acc = typename std::conditional<kU8, long long, double>::type;
+  Acc s[4], q[4], bs[4], m[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) { s[j] = 0.0; q[j] = 0.0; bs[j] = 0.0; m[j] = -INFINITY; }
-  auto take = [&](float (&v)[4], int t, bool bin) -> double {
-    if (scale) {
+  for (int j = 0; j < 4; ++j) {
+    s[j] = 0; q[j] = 0; bs[j] = 0;
+    m[j] = kU8 ? (Acc)0 : (Acc)-INFINITY;
+  }
+  auto take = [&](uint8_t *src, int t, bool bin, bool keep) -> double {
+    float v[4];
+    if constexpr (kU8) {
+      uint32_t w = *reinterpret_cast<const uint32_t *>(src);
+      if (scale) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) v[j] = scaley1<E>(v[j], sm_s0[4 * g + j], sm_k[4 * g + j], a.mn);
-      if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
+        for (int j = 0; j < 4; ++j)
+          v[j] = scaley1<E>((float)((w >> (8 * j)) & 255u), sm_s0[4 * g + j], sm_k[4 * g + j], a.mn);
+        st4<E>(&w, v);
+        if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
+      }
+      int r = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int x = (int)((w >> (8 * j)) & 255u);
+        if (bin) bs[j] += x; else s[j] += x;
+        q[j] += x * x;
+        m[j] = m[j] > x ? m[j] : x;
+        r += x;
+      }
+      return (double)r;
+    } else {
+      ld4<E>(src, v);
+      if (scale) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          v[j] = scaley1<E>(v[j], sm_s0[4 * g + j], sm_k[4 * g + j], a.mn);
+        if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
+        if (keep) st4<E>(src, v);   // the pixel sums read the normalised stage
+      }
+      double r = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (bin) bs[j] += v[j]; else s[j] += v[j];
+        q[j] += (double)v[j] * v[j];
+        m[j] = fmax(m[j], (double)v[j]);
+        r += v[j];
+      }
+      return r;
     }
-    double r = 0.0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (bin) bs[j] += v[j]; else s[j] += v[j];
-      q[j] += (double)v[j] * v[j];
-      m[j] = fmaxf(m[j], v[j]);
-      r += v[j];
-    }
-    return r;
   };
   double bmax = -1e300, bmin = 1e300;   // owned by thread tid < cs (channel tid)
 
@@ -198,20 +238,16 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     const int t0 = st * RS;
     if (active) {
       for (int r = p; r < RS; r += P) {
-        float v[4];
-        ld4<E>(sp + r * rb + 4 * g * ES, v);
-        const double rr = take(v, t0 + r, true);
-        if (a.pix_sum && scale) st4<E>(sp + r * rb + 4 * g * ES, v);
-        sm_rs[r * G4 + g] = rr;
+        sm_rs[r * GS + g] = take(sp + r * rb + 4 * g * ES, t0 + r, true, a.pix_sum != nullptr);
       }
     }
     const bool bin_end = (st + 1) % spb == 0;
     if (spb == 1 && active) {   // one stage per bin: its partials go out with the rows
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        sm_bp[p * cs + 4 * g + j] = bs[j];
+        sm_bp[p * cs + 4 * g + j] = (double)bs[j];
         s[j] += bs[j];
-        bs[j] = 0.0;
+        bs[j] = 0;
       }
     }
     if (a.pix_sum) {   // downsampled spectrogram: rs / tds whole pixel rows per stage
@@ -234,7 +270,7 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     __syncthreads();
     if (tid < RS) {
       double r = 0.0;
-      for (int k = 0; k < G4; ++k) r += sm_rs[tid * G4 + k];
+      for (int k = 0; k < G4; ++k) r += sm_rs[tid * GS + k];
       put_row(t0 + tid, r);
     }
     if (bin_end) {   // the last stage of a TBIN bin: bin means per channel
@@ -242,9 +278,9 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
         if (active) {
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            sm_bp[p * cs + 4 * g + j] = bs[j];
+            sm_bp[p * cs + 4 * g + j] = (double)bs[j];
             s[j] += bs[j];
-            bs[j] = 0.0;
+            bs[j] = 0;
           }
         }
         __syncthreads();
@@ -265,16 +301,14 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     __syncthreads();
     const int rows = min(RS, T - t0);
     if (active) {
-      for (int r = p; r < rows; r += P) {
-        float v[4];
-        ld4<E>(xb + (int64_t)(t0 + r) * rstride + 4 * g * ES, v);
-        sm_rs[r * G4 + g] = take(v, t0 + r, false);
-      }
+      for (int r = p; r < rows; r += P)
+        sm_rs[r * GS + g] = take(const_cast<uint8_t *>(xb) + (int64_t)(t0 + r) * rstride + 4 * g * ES,
+                                 t0 + r, false, false);
     }
     __syncthreads();
     if (tid < rows) {
       double r = 0.0;
-      for (int k = 0; k < G4; ++k) r += sm_rs[tid * G4 + k];
+      for (int k = 0; k < G4; ++k) r += sm_rs[tid * GS + k];
       put_row(t0 + tid, r);
     }
   }
@@ -286,7 +320,7 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     if (active) {
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        sm_bp[p * cs + 4 * g + j] = pass == 0 ? s[j] : pass == 1 ? q[j] : (double)m[j];
+        sm_bp[p * cs + 4 * g + j] = (double)(pass == 0 ? s[j] : pass == 1 ? q[j] : m[j]);
     }
     __syncthreads();
     if (tid < cs) {
@@ -304,6 +338,27 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     a.var[o] = (float)var;
     a.maxs[o] = a.parity ? (float)mean : (float)tot[2];
     a.pp[o] = nbins > 0 ? (float)(bmax - bmin) : 0.0f;
+  }
+  if (!a.decide) return;
+  // The last slab CTA of the beam makes its channel decisions, and the last
+  // CTA of the grid the block-level total power: each CTA publishes its
+  // statistics (fence) before counting itself in; nothing waits.
+  __shared__ int last_sh;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last_sh = a.nslab == 1 ? 1 : (atomicAdd(a.ctr + b, 1) == a.nslab - 1);
+  __syncthreads();
+  if (last_sh) {
+    __threadfence();
+    flag_decide_beam(a, b, fs_raw);
+  }
+  if (!a.modcheck && !a.tpwr_out) return;
+  __syncthreads();
+  if (tid == 0) last_sh = atomicAdd(a.ctr + 2 * a.nbeam, 1) == (int)(gridDim.x * gridDim.y) - 1;
+  __syncthreads();
+  if (last_sh) {
+    __threadfence();
+    flag_total_power(a);
   }
 }
 
@@ -398,120 +453,44 @@ __device__ void grp_channflag(const float *sb, float thr, const FlagArgs &a, uin
   }
 }
 
-// Everything after the statistics pass, for one beam per CTA, in the order
-// of the reference's block loop (src/gpu_flagger.cu:1313-1398):
-//  1. total power of the block (every beam's spectrum summed in FP64, the
-//     same order in every CTA) and, with modcheck, the modulation test
-//     against the previous flagged block (:1313-1330): at or above
-//     mod_thresh the block is replaced by the noise block and nothing else
-//     is flagged;
-//  2. calc_bpwr (:759-769) when pwr is set: the beam's replacement level;
-//  3. the four channel tests, concurrently in four groups of 64 threads:
-//     channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
-//     channflag(max, Thr), simple_channflag(pp, Thr / sqrt(FBIN)) (one-sided
-//     FBIN-channel mean; parity mode keeps the reference's spec[j] sum,
-//     :594), ORed into one mask, plus the permanent flag channels;
-//  4. flag (:459-474) then make_ts (:414-453): the flagged columns are set to
-//     MN * bpwr (clean mode) and the channel-mean series is formed from the
-//     replaced data.  Only the 16-byte chunks of a row that hold flagged
-//     channels are read: ts = (row sum from the statistics pass + sum over
-//     flagged channels of (level - x)) / nchan.  L lanes share a row (L the
-//     power of two covering the active chunks, at most 32), so a few flagged
-//     channels cost a few sectors per row and a fully flagged row is read
-//     once, coalesced.  For uint8 every term is an exact integer, so ts
-//     equals the reference's float tree sum / NCHAN_P bit for bit;
-//  5. simple_tsflag (:612-653) and flagts (:479-494): median and MAD (lower
-//     medians, by radix select) of the first ts_base samples, rows with
-//     ts - med > TsThr * MAD flagged (one-sided); clean mode sets channels
-//     [guard, nchan - guard) of every flagged row to the level.
-// A replaced block gets the noise block written into every beam (clean
-// mode, :1323-1324); its masks are zero and ts keeps the raw row sums.
-template <typename E>
-__global__ void __launch_bounds__(flag::kBeamThreads) flag_beam_kernel(FlagArgs a) {
-  constexpr int ES = (int)sizeof(E), EPC = 16 / ES;   // elements per 16-byte chunk
-  const int b = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int C = a.nchan, G = a.guard, n = C - 2 * G, T = a.ntime, BC = a.nbeam * C;
-  const int NCH = C / EPC;
-  extern __shared__ __align__(16) float bsh[];
-  float *dsh = bsh;                                       // [4 groups][3][C]
-  float *tsb = dsh + 12 * C;                              // [ts_base]
-  float *tmp = tsb + a.ts_base;                           // [ts_base]
-  uint32_t *chk = reinterpret_cast<uint32_t *>(tmp + a.ts_base);   // [NCH]
-  uint8_t *cmask = reinterpret_cast<uint8_t *>(chk + NCH);          // [C]
+// The channel decisions of beam b, by the 256 threads of the statistics CTA
+// that completed the beam: the four tests concurrently in four groups of 64
+// threads -- channflag(spec - oldspec, Thr), channflag(var, Thr + 0.5),
+// channflag(max, Thr), simple_channflag(pp, Thr / sqrt(FBIN)) (one-sided
+// FBIN-channel mean; parity mode keeps the reference's spec[j] sum, :594) --
+// ORed into one mask, plus the permanent flag channels
+// (src/gpu_flagger.cu:1340-1347).  smem: 12 nchan floats + nchan bytes.
+__device__ void flag_decide_beam(const FlagArgs &a, int b, uint8_t *smem) {
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int C = a.nchan, G = a.guard, n = C - 2 * G;
+  float *dsh = reinterpret_cast<float *>(smem);                 // [4 groups][3][C]
+  uint8_t *cmask = reinterpret_cast<uint8_t *>(dsh + 12 * C);   // [C]
   __shared__ uint32_t hist[4][256], sel[4][2];
-  __shared__ double red[flag::kBeamThreads];
-  __shared__ int replaced_sh, nact_sh;
-
-  // 1-2: block-level steps
-  if (a.modcheck || a.tpwr_out) {
-    double acc = 0.0;
-    for (int i = tid; i < BC; i += flag::kBeamThreads) acc += a.spec[i];
-    red[tid] = acc;
-  }
+  for (int c = tid; c < C; c += flag::kStatThreads) cmask[c] = 0;
   __syncthreads();
-  if (tid == 0) {
-    int rep = 0;
-    if (a.modcheck || a.tpwr_out) {
-      double tp = 0.0;
-      for (int k = 0; k < flag::kBeamThreads; ++k) tp += red[k];
-      if (a.modcheck) {
-        const double prev = *a.prev_tpwr;
-        if (prev > 0.0 && fabs(tp - prev) / prev >= (double)a.mod_thresh) rep = 1;
-      }
-      if (b == 0 && a.tpwr_out) *a.tpwr_out = tp;
-    }
-    if (b == 0 && a.status) a.status[0] = rep;
-    replaced_sh = rep;
-    if (!rep && a.pwr && a.bpwr) {   // calc_bpwr: float sum over every channel, in order
-      float acc = 0.0f;
-      for (int c = 0; c < C; ++c) acc += a.spec[b * C + c];
-      a.bpwr[b] = (float)(((double)acc / (double)(C - 2 * G)) / (double)a.mn);
-    }
-  }
-  for (int c = tid; c < C; c += flag::kBeamThreads) cmask[c] = 0;
-  __syncthreads();
-  const bool replaced = replaced_sh != 0;
-  E *xw = a.clean ? elem_out<E>(a) : nullptr;
-  uint8_t *mb = a.tsmask + (int64_t)b * T;
-  if (replaced) {
-    for (int c = tid; c < C; c += flag::kBeamThreads) a.chanmask[b * C + c] = 0;
-    for (int t = tid; t < T; t += flag::kBeamThreads) mb[t] = 0;
-    const E *nz = static_cast<const E *>(a.noise);
-    if (xw && nz) {
-      const uint4 *src = reinterpret_cast<const uint4 *>(nz);
-      uint4 *dst = reinterpret_cast<uint4 *>(xw + (int64_t)b * T * C);
-      const int64_t nv = (int64_t)T * C / EPC;
-      for (int64_t i = tid; i < nv; i += flag::kBeamThreads) dst[i] = src[i];
-    }
-    return;
-  }
-
-  // 3: channel decisions
-  if (warp < 8) {
-    const int g = warp >> 1, gsize = 64, gtid = tid - 64 * g, bid = 1 + g;
-    float *sb = dsh + g * 3 * C, *corr = sb + C, *tm = corr + C;
-    const float *src = g == 0 ? a.spec : g == 1 ? a.var : g == 2 ? a.maxs : a.pp;
-    for (int c = gtid; c < C; c += gsize)
-      sb[c] = src[b * C + c] - ((g == 0 && a.oldspec) ? a.oldspec[b * C + c] : 0.0f);
+  const int g = warp >> 1, gsize = 64, gtid = tid - 64 * g, bid = 1 + g;
+  float *sb = dsh + g * 3 * C, *corr = sb + C, *tm = corr + C;
+  const float *src = g == 0 ? a.spec : g == 1 ? a.var : g == 2 ? a.maxs : a.pp;
+  for (int c = gtid; c < C; c += gsize)
+    sb[c] = src[b * C + c] - ((g == 0 && a.oldspec) ? a.oldspec[b * C + c] : 0.0f);
+  named_bar(bid, gsize);
+  if (g < 3) {
+    const float thr = g == 1 ? a.thresh + a.var_add : a.thresh;
+    grp_channflag(sb, thr, a, cmask, corr, tm, hist[g], sel[g], gtid, gsize, bid);
+  } else {   // simple_channflag (:559-610)
+    for (int i = gtid; i < n; i += gsize) corr[i] = sb[G + i];
     named_bar(bid, gsize);
-    if (g < 3) {
-      const float thr = g == 1 ? a.thresh + a.var_add : a.thresh;
-      grp_channflag(sb, thr, a, cmask, corr, tm, hist[g], sel[g], gtid, gsize, bid);
-    } else {   // simple_channflag (:559-610)
-      for (int i = gtid; i < n; i += gsize) corr[i] = sb[G + i];
-      named_bar(bid, gsize);
-      const int k = (n + 1) / 2 - 1;
-      const float med = grp_radix_select(corr, n, k, hist[g], sel[g], gtid, gsize, bid);
-      for (int i = gtid; i < n; i += gsize) tm[i] = fabsf(corr[i] - med);
-      named_bar(bid, gsize);
-      const float mad = grp_radix_select(tm, n, k, hist[g], sel[g], gtid, gsize, bid);
-      const float mythr = (float)((double)a.thresh / sqrt((double)a.fbin));
-      for (int j = G + gtid; j < C - G - a.fbin; j += gsize) {
-        float vv = 0.0f;
-        for (int q = 0; q < a.fbin; ++q) vv += a.parity ? sb[j] : sb[j + q];
-        vv = vv / (float)a.fbin - med;
-        if (vv > mythr * mad) cmask[j] = 1;
-      }
+    const int k = (n + 1) / 2 - 1;
+    const float med = grp_radix_select(corr, n, k, hist[g], sel[g], gtid, gsize, bid);
+    for (int i = gtid; i < n; i += gsize) tm[i] = fabsf(corr[i] - med);
+    named_bar(bid, gsize);
+    const float mad = grp_radix_select(tm, n, k, hist[g], sel[g], gtid, gsize, bid);
+    const float mythr = (float)((double)a.thresh / sqrt((double)a.fbin));
+    for (int j = G + gtid; j < C - G - a.fbin; j += gsize) {
+      float vv = 0.0f;
+      for (int q = 0; q < a.fbin; ++q) vv += a.parity ? sb[j] : sb[j + q];
+      vv = vv / (float)a.fbin - med;
+      if (vv > mythr * mad) cmask[j] = 1;
     }
   }
   __syncthreads();
@@ -521,23 +500,108 @@ __global__ void __launch_bounds__(flag::kBeamThreads) flag_beam_kernel(FlagArgs 
       if (j >= G && j < C - G) cmask[j] = 1;
     }
   __syncthreads();
-  {
-    int nflag = 0;
-    for (int c = tid; c < C; c += flag::kBeamThreads) {
-      a.chanmask[b * C + c] = cmask[c];
-      nflag += cmask[c];
-    }
-    if (nflag && a.counts) atomicAdd(a.counts, nflag);
+  int nflag = 0;
+  for (int c = tid; c < C; c += flag::kStatThreads) {
+    a.chanmask[b * C + c] = cmask[c];
+    nflag += cmask[c];
   }
-  // 4: the active chunks of a row, in channel order (warp 0, ballots):
-  // chunk index | element mask << 16
-  if (warp == 0) {
+  if (nflag && a.counts) atomicAdd(a.counts, nflag);
+}
+
+// Total power of the block (every beam's spectrum summed in FP64 in a fixed
+// order) and, with modcheck, the modulation test against the previous
+// flagged block (:1313-1330): at or above mod_thresh the block is replaced
+// by the noise block and nothing is flagged.  One CTA, the last one of the
+// statistics grid.
+__device__ void flag_total_power(const FlagArgs &a) {
+  __shared__ double red[flag::kStatThreads];
+  const int tid = threadIdx.x, BC = a.nbeam * a.nchan;
+  double acc = 0.0;
+  for (int i = tid; i < BC; i += flag::kStatThreads) acc += a.spec[i];
+  red[tid] = acc;
+  __syncthreads();
+  if (tid == 0) {
+    double tp = 0.0;
+    for (int k = 0; k < flag::kStatThreads; ++k) tp += red[k];
+    int rep = 0;
+    if (a.modcheck) {
+      const double prev = *a.prev_tpwr;
+      if (prev > 0.0 && fabs(tp - prev) / prev >= (double)a.mod_thresh) rep = 1;
+    }
+    if (a.tpwr_out) *a.tpwr_out = tp;
+    if (a.status) a.status[0] = rep;
+  }
+}
+
+// flag (:459-474) then make_ts (:414-453), and for the beam's last CTA
+// simple_tsflag (:612-653) and flagts (:479-494).  Grid (row chunks of
+// kApplyRows, beams).  The flagged channels' 16-byte chunks are listed once
+// per CTA (ballot scan, channel order); L lanes share a row, L the power of
+// two covering the listed chunks (at most 32), so a few flagged channels
+// cost a few sectors per row and a fully flagged row is read once,
+// coalesced.  Each listed chunk is read, its flagged channels set to the
+// level MN * bpwr (clean mode) and written back, and
+//   ts = (row sum from the statistics pass + sum over flagged channels of
+//         (level - x)) / nchan,
+// which for uint8 is a sum of exact integers, so it equals the reference's
+// float tree sum / NCHAN_P bit for bit.  Each CTA then counts itself in; the
+// beam's last one takes the median and MAD (lower medians, by radix select)
+// of the first ts_base samples, flags rows with ts - med > TsThr * MAD
+// (one-sided) and, in clean mode, sets channels [guard, nchan - guard) of
+// the flagged rows to the level.  A block the modulation check replaced
+// gets the noise block in every beam (clean mode, :1323-1324) and zero
+// masks; its ts keeps the raw row sums.
+template <typename E>
+__global__ void __launch_bounds__(flag::kApplyThreads) flag_apply_kernel(FlagArgs a) {
+  constexpr int ES = (int)sizeof(E), EPC = 16 / ES;   // elements per 16-byte chunk
+  const int b = blockIdx.y, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int C = a.nchan, G = a.guard, T = a.ntime, NCH = C / EPC;
+  const int t_begin = blockIdx.x * flag::kApplyRows;
+  const int t_end = min(T, t_begin + flag::kApplyRows);
+  constexpr int nw = flag::kApplyThreads / 32;
+  extern __shared__ __align__(16) uint32_t ash[];
+  uint32_t *chk = ash;                                            // [NCH]
+  float *tsb = reinterpret_cast<float *>(ash + NCH);              // [ts_base]
+  float *tmp = tsb + a.ts_base;                                   // [ts_base]
+  __shared__ uint32_t hist[256], sel[2];
+  __shared__ int nact_sh, last_sh;
+  __shared__ float lev_sh, lvl_sh;
+  E *xw = a.clean ? elem_out<E>(a) : nullptr;
+  uint8_t *mb = a.tsmask + (int64_t)b * T;
+  if (a.status && a.status[0]) {   // replaced by noise
+    const E *nz = static_cast<const E *>(a.noise);
+    if (xw && nz) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(nz + (int64_t)t_begin * C);
+      uint4 *dst = reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t_begin) * C);
+      const int64_t nv = (int64_t)(t_end - t_begin) * C / EPC;
+      for (int64_t i = tid; i < nv; i += flag::kApplyThreads) dst[i] = src[i];
+    }
+    for (int t = t_begin + tid; t < t_end; t += flag::kApplyThreads) mb[t] = 0;
+    if (blockIdx.x == 0)
+      for (int c = tid; c < C; c += flag::kApplyThreads) a.chanmask[b * C + c] = 0;
+    if (blockIdx.x == 0 && b == 0 && tid == 0 && a.counts) {
+      a.counts[0] = 0;
+      a.counts[1] = 0;
+    }
+    return;
+  }
+  if (tid == 0) {   // calc_bpwr (:759-769): float sum over every channel, in order
+    float lvl = a.bpwr ? a.bpwr[b] : 1.0f;
+    if (a.pwr && a.bpwr) {
+      float acc = 0.0f;
+      for (int c = 0; c < C; ++c) acc += a.spec[b * C + c];
+      lvl = (float)(((double)acc / (double)(C - 2 * G)) / (double)a.mn);
+    }
+    lvl_sh = lvl;
+    lev_sh = a.mn * lvl;
+  }
+  if (warp == 0) {   // the chunks holding flagged channels: index | element mask << 16
     int base = 0;
     for (int k0 = 0; k0 < NCH; k0 += 32) {
       const int k = k0 + lane;
       uint32_t m = 0u;
       if (k < NCH)
-        for (int e = 0; e < EPC; ++e) m |= (uint32_t)cmask[k * EPC + e] << e;
+        for (int e = 0; e < EPC; ++e) m |= (uint32_t)a.chanmask[b * C + k * EPC + e] << e;
       const uint32_t bal = __ballot_sync(0xffffffffu, m != 0u);
       if (m) chk[base + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)k | (m << 16);
       base += __popc(bal);
@@ -546,17 +610,16 @@ __global__ void __launch_bounds__(flag::kBeamThreads) flag_beam_kernel(FlagArgs 
   }
   __syncthreads();
   const int nact = nact_sh;
+  const E re = repl_elem<E>(lev_sh);
+  const float rf = (float)re;
   int L = 1;
   while (L < nact && L < 32) L <<= 1;
-  const int rpw = 32 / L, sub = lane & (L - 1);   // rows per warp pass, lane within the row
-  const E re = repl_elem<E>(a.mn * (a.bpwr ? a.bpwr[b] : 1.0f));
-  const float rf = (float)re;
+  const int rpw = 32 / L, sub = lane & (L - 1);
   const E *xin = (a.spec0 && elem_out<E>(a)) ? elem_out<E>(a) : elem_in<E>(a);
-  const int nw = flag::kBeamThreads / 32;
-  for (int t0 = warp * rpw; t0 < T; t0 += nw * rpw) {   // uniform per warp
-    const int t = t0 + lane / L;
+  for (int r0 = t_begin + warp * rpw; r0 < t_end; r0 += nw * rpw) {   // uniform per warp
+    const int t = r0 + lane / L;
     double corr = 0.0;
-    if (t < T) {
+    if (t < t_end) {
       const uint4 *row = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C);
       uint4 *wrow = xw ? reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C) : nullptr;
       for (int i = sub; i < nact; i += L) {
@@ -575,7 +638,7 @@ __global__ void __launch_bounds__(flag::kBeamThreads) flag_beam_kernel(FlagArgs 
       }
     }
     for (int o = L >> 1; o > 0; o >>= 1) corr += __shfl_xor_sync(0xffffffffu, corr, o);
-    if (t < T && sub == 0) {
+    if (t < t_end && sub == 0) {
       double rsum;
       if (a.nslab == 1) {
         rsum = a.ts[(int64_t)b * T + t];
@@ -586,26 +649,33 @@ __global__ void __launch_bounds__(flag::kBeamThreads) flag_beam_kernel(FlagArgs 
       a.ts[(int64_t)b * T + t] = (float)((rsum + corr) / C);
     }
   }
-  __syncthreads();   // the series written above is read back by other threads
-
-  // 5: time-series flags
-  const float *tb = a.ts + (int64_t)b * T;
+  // the beam's last CTA makes the time-series decisions
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    last_sh = atomicAdd(a.ctr + a.nbeam + b, 1) == (int)gridDim.x - 1;
+    if (blockIdx.x == 0 && a.pwr && a.bpwr) a.bpwr[b] = lvl_sh;
+  }
+  __syncthreads();
+  if (!last_sh) return;
+  __threadfence();
   if (!a.tsflag) {
-    for (int t = tid; t < T; t += flag::kBeamThreads) mb[t] = 0;
+    for (int t = tid; t < T; t += flag::kApplyThreads) mb[t] = 0;
     return;
   }
-  for (int i = tid; i < a.ts_base; i += flag::kBeamThreads) tsb[i] = tb[i];
+  const float *tb = a.ts + (int64_t)b * T;
+  for (int i = tid; i < a.ts_base; i += flag::kApplyThreads) tsb[i] = tb[i];
   __syncthreads();
   const int kmed = (a.ts_base + 1) / 2 - 1;   // lower median
   const float med =
-      grp_radix_select(tsb, a.ts_base, kmed, hist[0], sel[0], tid, flag::kBeamThreads, 1);
-  for (int i = tid; i < a.ts_base; i += flag::kBeamThreads) tmp[i] = fabsf(tsb[i] - med);
+      grp_radix_select(tsb, a.ts_base, kmed, hist, sel, tid, flag::kApplyThreads, 1);
+  for (int i = tid; i < a.ts_base; i += flag::kApplyThreads) tmp[i] = fabsf(tsb[i] - med);
   __syncthreads();
   const float mad =
-      grp_radix_select(tmp, a.ts_base, kmed, hist[0], sel[0], tid, flag::kBeamThreads, 1);
+      grp_radix_select(tmp, a.ts_base, kmed, hist, sel, tid, flag::kApplyThreads, 1);
   const float lim = a.ts_thresh * mad;
   int nts = 0;
-  for (int t = tid; t < T; t += flag::kBeamThreads) {
+  for (int t = tid; t < T; t += flag::kApplyThreads) {
     const uint8_t f = (tb[t] - med) > lim ? 1 : 0;
     mb[t] = f;
     nts += f;
@@ -701,8 +771,12 @@ static size_t stats_smem(const FlagArgs &a, int es) {
   size_t nbp = bp(cs);
   if (last && bp(last) > nbp) nbp = bp(last);
   const size_t stage = ((size_t)a.rs * cs * es + 127) & ~(size_t)127;
-  return flag::kStages * stage + sizeof(double) * ((size_t)a.rs * (cs / 4) + nbp + cs) +
-         sizeof(float) * cs;
+  const size_t stats = flag::kStages * stage +
+                       sizeof(double) * ((size_t)a.rs * ((cs / 4) | 1) + nbp + cs) +
+                       sizeof(float) * cs;
+  // the channel decisions reuse the buffer: 12 nchan floats + nchan bytes
+  const size_t dec = a.decide ? sizeof(float) * 12 * (size_t)a.nchan + a.nchan : 0;
+  return stats > dec ? stats : dec;
 }
 
 int launch_flag_stats(FlagArgs a, cudaStream_t st) {
@@ -726,31 +800,30 @@ int launch_flag_stats(FlagArgs a, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-// The statistics pass, then everything else per beam in one kernel: two
-// launches on one stream.
+// The statistics pass (which ends with the channel decisions and the total
+// power), then the row-chunked apply pass (whose last CTA per beam makes the
+// time-series decisions): two launches on one stream.
 int launch_flag(const FlagArgs &a0, cudaStream_t st) {
   FlagArgs a = a0;
   if (a.nchan > flag::kMaxChan || a.ts_base < 1 || a.ts_base > flag::kMaxTsBase ||
       a.ts_base > a.ntime)
     return -1;
+  if (!a.ctr) return -1;
   a.ts_mean = 0;
+  a.decide = 1;
   a.nslab = (a.nchan + kFlagSlab - 1) / kFlagSlab;
+  if (cudaMemsetAsync(a.ctr, 0, sizeof(int) * flag_ctr_ints(a.nbeam), st) != cudaSuccess) return -2;
   int rc = launch_flag_stats(a, st);
   if (rc != 0) return rc;
   const bool u8 = a.xu8 != nullptr;
   a.rs = stage_rows(a, u8 ? 1 : 4);
   const int nch = a.nchan * (u8 ? 1 : 4) / 16;
-  const size_t sh = sizeof(float) * (12 * (size_t)a.nchan + 2 * (size_t)a.ts_base) +
-                    sizeof(uint32_t) * nch + a.nchan;
-  if (u8) {
-    static SmemAttrOnce attr;
-    if (smem_attr_once(attr, flag_beam_kernel<uint8_t>, 120 * 1024) != cudaSuccess) return -2;
-    flag_beam_kernel<uint8_t><<<a.nbeam, flag::kBeamThreads, sh, st>>>(a);
-  } else {
-    static SmemAttrOnce attr;
-    if (smem_attr_once(attr, flag_beam_kernel<float>, 120 * 1024) != cudaSuccess) return -2;
-    flag_beam_kernel<float><<<a.nbeam, flag::kBeamThreads, sh, st>>>(a);
-  }
+  const size_t sh = sizeof(uint32_t) * nch + sizeof(float) * 2 * (size_t)a.ts_base;
+  const dim3 grid((a.ntime + flag::kApplyRows - 1) / flag::kApplyRows, a.nbeam);
+  if (u8)
+    flag_apply_kernel<uint8_t><<<grid, flag::kApplyThreads, sh, st>>>(a);
+  else
+    flag_apply_kernel<float><<<grid, flag::kApplyThreads, sh, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -1066,8 +1139,10 @@ extern "C" int dsax_flag_noalloc(const dsax_flag_params *p, const float *x, cons
       p->ts_base < 1 || p->ts_base > T || p->ts_base > 4096 || p->nperm < 0 || p->nperm > 8)
     return DSAX_ERR_ARG;
   const long long nbc = (long long)B * C, nbt = (long long)B * T;
-  const long long need = 4 * nbc + nbt + 2;   // spec, var, max, pp, ts, two counters
+  // spec, var, max, pp, ts, the two flag counts, the launches' completion counters
+  const long long need = 4 * nbc + nbt + 2 + (long long)flag_ctr_ints(B);
   if (need > kNoAllocScratchFloats) return DSAX_ERR_ARG;   // beyond the fixed 6 MiB
+  if (C % 4 || (reinterpret_cast<uintptr_t>(x) & 15u)) return DSAX_ERR_ARG;
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return DSAX_ERR_CUDA;
   float *s = noalloc_scratch(dev);
@@ -1083,6 +1158,7 @@ extern "C" int dsax_flag_noalloc(const dsax_flag_params *p, const float *x, cons
   for (int i = 0; i < p->nperm; ++i) a.perm[i] = p->perm[i];
   a.spec = s; a.var = s + nbc; a.maxs = s + 2 * nbc; a.pp = s + 3 * nbc; a.ts = s + 4 * nbc;
   a.counts = reinterpret_cast<int *>(s + 4 * nbc + nbt);
+  a.ctr = a.counts + 2;
   // the counters accumulate with atomics: clear them (the array keeps the
   // previous call's values)
   if (cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), st) != cudaSuccess) return DSAX_ERR_CUDA;

@@ -61,6 +61,7 @@ struct dsax_flag_state {
   int *counts = nullptr;    // [2], directly after status
   void *noise = nullptr;
   uint8_t *dmask = nullptr; // masks when the caller passes none (device mode)
+  int *ctr = nullptr;       // completion counters of the flagger launches
 };
 
 extern "C" {
@@ -111,8 +112,9 @@ int dsax_flag(dsax_ctx *c, const dsax_flag_params *p, const float *x, const floa
   const size_t nstat = 4 * nbc + nbt;
   const size_t nrow = nslabs(C) > 1 ? (size_t)B * nslabs(C) * T : 0;
   int rc;
-  if ((rc = ensure_buffer(c, c->aux[AUX_FLAG_STATS], (nstat + nrow) * 4 + 64, "flag statistics")) !=
-      DSAX_OK)
+  const size_t nctr = flag_ctr_ints(B);
+  if ((rc = ensure_buffer(c, c->aux[AUX_FLAG_STATS], (nstat + nrow + 2 + nctr) * 4 + 64,
+                          "flag statistics")) != DSAX_OK)
     return rc;
   FlagArgs a{};
   fill_args(a, p);
@@ -123,6 +125,7 @@ int dsax_flag(dsax_ctx *c, const dsax_flag_params *p, const float *x, const floa
   float *scratch = static_cast<float *>(c->aux[AUX_FLAG_STATS].ptr);
   a.rowsum = nrow ? scratch + nstat : nullptr;
   int *dcounts = reinterpret_cast<int *>(scratch + nstat + nrow);
+  a.ctr = dcounts + 2;
   a.counts = (mem == DSAX_MEM_DEVICE && counts) ? counts : dcounts;
   cudaError_t e = cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), c->stream);
   if (e != cudaSuccess) return cuda_check(c, e, "clear counts");
@@ -182,7 +185,8 @@ int dsax_flag_state_create(dsax_ctx *c, const dsax_flag_params *p,
   const size_t off_d = ((nf * 4 + 255) / 256) * 256;
   const size_t off_noise = off_d + 256;
   const size_t off_mask = ((off_noise + (size_t)T * C * es + 255) / 256) * 256;
-  const size_t total = off_mask + bc + bt;
+  const size_t off_ctr = ((off_mask + bc + bt + 255) / 256) * 256;
+  const size_t total = off_ctr + sizeof(int) * flag_ctr_ints(B);
   cudaError_t e = cudaMalloc(&st->buf.ptr, total);
   if (e != cudaSuccess) {
     delete st;
@@ -204,6 +208,7 @@ int dsax_flag_state_create(dsax_ctx *c, const dsax_flag_params *p,
   st->counts = reinterpret_cast<int *>(base + off_d + 48);
   st->noise = base + off_noise;
   st->dmask = base + off_mask;
+  st->ctr = reinterpret_cast<int *>(base + off_ctr);
   // zero everything (oldspec starts at 0, as h_oldspec does at :1214), then
   // the levels at 1 (:1234) and the noise block
   if ((e = cudaMemsetAsync(st->buf.ptr, 0, total, c->stream)) != cudaSuccess) {
@@ -290,6 +295,7 @@ int dsax_flag_clean(dsax_ctx *c, dsax_flag_state *st, void *data, uint8_t *chanm
   a.tsmask = dtm;
   a.counts = st->counts;
   a.status = st->status;
+  a.ctr = st->ctr;
   a.mn = st->cp.mn;
   a.sig = st->cp.sig;
   a.bpwr = st->bpwr;

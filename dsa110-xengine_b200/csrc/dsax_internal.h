@@ -131,7 +131,15 @@ struct FlagArgs {
   double *tpwr_out = nullptr;    // this block's total power
   int *status = nullptr;         // [0] = 1 when the block was replaced by noise
   const void *noise = nullptr;   // replacement block [ntime][nchan] (element type of x)
+  // completion counters, [2 nbeam + 2] ints zeroed by launch_flag: per-beam
+  // slab CTAs done, per-beam apply CTAs done, CTAs of the statistics grid
+  // done (the last arrival of each does the next step; nothing spins)
+  int *ctr = nullptr;
+  int decide = 0;                // statistics pass also makes the channel decisions
 };
+
+// ints of FlagArgs::ctr for nbeam beams
+inline size_t flag_ctr_ints(int nbeam) { return 2 * (size_t)nbeam + 2; }
 
 constexpr int kFlagSlab = 128;   // channels per statistics CTA
 

@@ -401,7 +401,8 @@ int dsax_flag_state_noise(dsax_ctx *ctx, dsax_flag_state *st, void *noise);
  * and every pointer (x, oldspec, chanmask, tsmask, counts) is device memory.
  * The statistics use a fixed 6 MiB device array compiled into the library
  * (held on every GPU that loads it until the process exits), so
- * 4*nbeam*nchan + nbeam*ntime + 2 must not exceed 1,572,864 floats; larger
+ * 4*nbeam*nchan + nbeam*ntime + 2*nbeam + 4 must not exceed 1,572,864 floats
+ * (nchan <= 128, a multiple of 4; x 16-byte aligned); larger
  * sizes return DSAX_ERR_ARG.  The first call on a device looks up that
  * array's address; make it before any stream capture.  All calls share the
  * array: calls that overlap on the GPU (other streams, other threads) race

@@ -54,7 +54,7 @@ def test_noalloc_matches_dsax_flag_twice(dsax):
 
 def test_noalloc_rejects_sizes_beyond_the_array(dsax):
     fn = _noalloc(dsax)
-    p = dsax.flag_params(512, 4096, 48)        # 512 * (4*48 + 4096) + 2 > 1,572,864
+    p = dsax.flag_params(512, 4096, 48)        # 512 * (4*48 + 4096 + 2) + 4 > 1,572,864
     rc = fn(ctypes.byref(p), ctypes.c_void_p(16), None, ctypes.c_void_p(16), ctypes.c_void_p(16),
             None, None)
     assert rc == dsax.DSAX_ERR_ARG
@@ -84,8 +84,8 @@ def _run_both(dsax, fn, ref_ctx, p, xd):
 
 
 def test_noalloc_at_the_size_limit_then_smaller(dsax):
-    """A shape that fills the array exactly (4*B*C + B*T + 2 = 1,572,864
-    floats, so the two counters are its last two floats) is accepted and
+    """A shape that fills the array exactly (4*B*C + B*T + 2*B + 4 =
+    1,572,864 floats, so the counters are its last floats) is accepted and
     matches dsax_flag; a smaller shape afterwards, whose statistics sit at
     other offsets of the same array, matches too."""
     import torch
@@ -93,8 +93,8 @@ def test_noalloc_at_the_size_limit_then_smaller(dsax):
     fn = _noalloc(dsax)
     limit = 1572864
     B, C = 2, 48
-    T = (limit - 2) // B - 4 * C
-    assert 4 * B * C + B * T + 2 == limit
+    T = (limit - 4) // B - 4 * C - 2
+    assert 4 * B * C + B * T + 2 * B + 4 == limit
     ref_ctx = dsax.Context(dsax.default_config(npkt=16, nchan=8))
     try:
         rng = np.random.default_rng(5)
@@ -119,7 +119,7 @@ def test_noalloc_at_the_size_limit_then_smaller(dsax):
 def test_noalloc_one_past_the_limit_is_rejected(dsax):
     fn = _noalloc(dsax)
     B, C = 2, 48
-    T = (1572864 - 2) // B - 4 * C + 1          # one float per beam too many
+    T = (1572864 - 4) // B - 4 * C - 2 + 1      # one float per beam too many
     p = dsax.flag_params(B, T, C, ts_base=4096)
     rc = fn(ctypes.byref(p), ctypes.c_void_p(16), None, ctypes.c_void_p(16), ctypes.c_void_p(16),
             None, None)
