@@ -433,14 +433,14 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
     };
     if (kBulk) {
       const uint32_t *rw_base = reinterpret_cast<const uint32_t *>(gbase + kOpStages * kStageBytes);
-      for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+      // the words of raw stage ks -> w, then the stage goes back to the loader
+      auto fetch = [&](int ks, uint32_t (&w)[2][8]) -> bool {
         const int r = ks % kRawStages;
         if (!mbar_wait_bounded(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
                                DEV_ERR_WAIT_FULL, a.wait_limit_ns))
-          break;
+          return false;
         const uint32_t *rw = rw_base + r * (kRawBytes / 4);
         const int pvalid = a.npkt - ks * kPktPerStage;
-        uint32_t w[2][8];
 #pragma unroll
         for (int e = 0; e < 2; ++e)
 #pragma unroll
@@ -453,7 +453,19 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
         // first (a write-after-read race across proxies).
         fence_proxy_async_smem();
         mbar_arrive(&rempty_bar[r]);
-        if (!unpack_store(ks, w)) break;
+        return true;
+      };
+      // one stage of words in registers ahead of the stage being unpacked,
+      // so the shared-memory loads overlap the previous stage's unpack
+      uint32_t wa[2][8], wb[2][8];
+      if (nks > 0 && fetch(0, wa)) {
+        for (int ks = 0; ks < nks && !abort_sh; ks += 2) {
+          if (ks + 1 < nks && !fetch(ks + 1, wb)) break;
+          if (!unpack_store(ks, wa)) break;
+          if (ks + 1 >= nks) break;
+          if (ks + 2 < nks && !fetch(ks + 2, wa)) break;
+          if (!unpack_store(ks + 1, wb)) break;
+        }
       }
     } else {
       // two stages of loads in flight ahead of the stage being unpacked
