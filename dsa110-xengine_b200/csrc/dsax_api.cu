@@ -167,6 +167,12 @@ void dsax_destroy(dsax_ctx *c) {
     }
   for (auto &ev : c->pev)
     if (ev) cudaEventDestroy(ev);
+  if (c->bstream) {
+    cudaStreamSynchronize(c->bstream);
+    cudaStreamDestroy(c->bstream);
+  }
+  for (auto &ev : c->bev)
+    if (ev) cudaEventDestroy(ev);
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -1,6 +1,11 @@
 // dsax_batch.cu -- many blocks in one submission: corner turn, correlate,
 // beamform and flag each block of a batch (subband widths may differ per
-// block), optionally captured once into a CUDA graph and replayed.
+// block), optionally captured once into a CUDA graph and replayed.  The
+// correlation chain (HBM-bound corner turn, then the correlator) runs on the
+// context stream and the beamform + flag chain (tensor-bound) on a second
+// stream, forked from and joined back to the context stream, so that the
+// two chains of the batch overlap on the GPU; each chain keeps its own
+// scratch, so blocks within a chain stay in order.
 #include <cstring>
 #include <vector>
 #include <cuda_runtime.h>
@@ -19,15 +24,15 @@ struct BatchPlan {
   cudaGraphExec_t exec = nullptr;
 };
 
-// Enqueues one block's stages on the context stream.
+// Enqueues one block's stages: correlation on sc, beamform + flag on sb.
 int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float *fb,
-                  float *fstats) {
+                  float *fstats, cudaStream_t sc, cudaStream_t sb) {
   const dsax_config &cf = c->cfg;
   const int npkt = cf.npkt, nchan = d.nchan, ngrp = nchan / 8, ppo = cf.bf_pkt_per_out;
   const int nout = npkt / ppo;
   if (d.vis) {
     if (launch_reorder_chanmajor(static_cast<const uint8_t *>(d.blk), scratch, npkt, cf.nant_in,
-                                 nchan, c->stream) != 0)
+                                 nchan, sc) != 0)
       return -2;
     CorrArgs a{};
     a.in = scratch;
@@ -37,7 +42,7 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     a.nant_in = 64;
     a.nchan = nchan;
     a.wait_limit_ns = cf.wait_limit_ns;
-    if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path != 3) != 0) return -2;
+    if (launch_correlate_chanmajor(a, sc, c->cfg.corr_path != 3) != 0) return -2;
   }
   if (d.beams || d.chanmask) {
     BfArgs b{};
@@ -53,7 +58,7 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     b.ppo = ppo;
     b.scale = cf.bf_scale;
     b.wait_limit_ns = cf.wait_limit_ns;
-    if (launch_beamform(b, c->num_sms, c->stream) != 0) return -2;
+    if (launch_beamform(b, c->num_sms, sb) != 0) return -2;
   }
   if (d.chanmask) {
     dsax_flag_params p;
@@ -75,8 +80,8 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     f.ctr = reinterpret_cast<int *>(fstats + 4 * nbc + 2 * (size_t)cf.nbeam * nout + 64);
     // the flag counters accumulate with atomics: clear them per block (inside
     // the graph too, so every replay starts from zero)
-    if (cudaMemsetAsync(f.counts, 0, 2 * sizeof(int), c->stream) != cudaSuccess) return -2;
-    if (launch_flag(f, c->stream) != 0) return -2;
+    if (cudaMemsetAsync(f.counts, 0, 2 * sizeof(int), sb) != cudaSuccess) return -2;
+    if (launch_flag(f, sb) != 0) return -2;
   }
   return 0;
 }
@@ -124,10 +129,26 @@ int dsax_run_batch(dsax_ctx *c, const dsax_block_desc *blocks, int nblk, int use
     cudaError_t e = cudaGraphLaunch(plan->exec, c->stream);
     return e == cudaSuccess ? DSAX_OK : cuda_check(c, e, "graph launch");
   }
-  if (!use_graph) {
+  if (!c->bstream) {
+    cudaError_t e0 = cudaStreamCreateWithFlags(&c->bstream, cudaStreamNonBlocking);
+    for (auto &ev : c->bev)
+      if (e0 == cudaSuccess && !ev) e0 = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e0 != cudaSuccess) return cuda_check(c, e0, "batch stream");
+  }
+  // fork the beamform chain off the context stream, run both chains, join
+  auto enqueue_all = [&]() -> int {
+    if (cudaEventRecord(c->bev[0], c->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(c->bstream, c->bev[0], 0) != cudaSuccess)
+      return -2;
     for (int i = 0; i < nblk; ++i)
-      if (enqueue_block(c, blocks[i], scratch, fb, fs) != 0)
-        return cuda_check(c, cudaGetLastError(), "batch launch");
+      if (enqueue_block(c, blocks[i], scratch, fb, fs, c->stream, c->bstream) != 0) return -2;
+    if (cudaEventRecord(c->bev[1], c->bstream) != cudaSuccess ||
+        cudaStreamWaitEvent(c->stream, c->bev[1], 0) != cudaSuccess)
+      return -2;
+    return 0;
+  };
+  if (!use_graph) {
+    if (enqueue_all() != 0) return cuda_check(c, cudaGetLastError(), "batch launch");
     return DSAX_OK;
   }
   // (re)capture
@@ -141,8 +162,7 @@ int dsax_run_batch(dsax_ctx *c, const dsax_block_desc *blocks, int nblk, int use
   plan->blocks.assign(blocks, blocks + nblk);
   cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_check(c, e, "begin capture");
-  int lrc = 0;
-  for (int i = 0; i < nblk && !lrc; ++i) lrc = enqueue_block(c, blocks[i], scratch, fb, fs);
+  const int lrc = enqueue_all();
   e = cudaStreamEndCapture(c->stream, &plan->graph);
   if (lrc || e != cudaSuccess) return cuda_check(c, e != cudaSuccess ? e : cudaErrorUnknown, "capture");
   e = cudaGraphInstantiate(&plan->exec, plan->graph, 0);

@@ -81,6 +81,10 @@ struct dsax_ctx {
   // and per-buffer events, created on first use
   cudaStream_t side[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t pev[9] = {};
+  // dsax_run_batch: the beamform + flag chain's stream and its fork/join
+  // events, created on first use
+  cudaStream_t bstream = nullptr;
+  cudaEvent_t bev[2] = {};
   dsax::LfNet lf_storage;
   unsigned lf_wimg_version = ~0u;   // parameter version the inference weight images hold
   int lf_pad_geom[3] = {0, 0, 0};   // (B, H, W) whose grid borders are zero
