@@ -560,8 +560,10 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the beamformer / flagger / batch side measurements")
     ap.add_argument("--corr-path", type=int, default=0,
-                    help="0 default (=3), 1 fused kernel, 2 REORDER-layout corner turn, "
-                         "3 channel-major corner turn + bulk-copy-fed correlator")
+                    help="0 default (=4), 1 fused kernel, 2 REORDER-layout corner turn, "
+                         "3 channel-major corner turn + directly fed correlator, "
+                         "4 the same, bulk-copy fed, 5 as 4 with 16 unpack warps, "
+                         "6 captured block read directly by 4-CTA clusters, 7 as 6 with 16 unpack warps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -634,7 +636,7 @@ def main():
     # One dsax_correlate call per block (corner turn + correlate on the
     # library stream); the end-to-end leg below uses dsax_correlate_many,
     # whose host-buffer form overlaps the PCIe copies with the device work.
-    pipelined = cfg.corr_path in (0, 3, 4) and not args.serial
+    pipelined = cfg.corr_path in (0, 3, 4, 5, 6, 7) and not args.serial
     with ClockSampler(dev) as clk:
         ev0.record(stream)
         for s in range(args.steps):
@@ -747,7 +749,11 @@ def main():
                        "corr_path": ["channel-major corner turn + bulk-fed correlate", "fused",
                                      "REORDER-layout corner turn + correlate",
                                      "channel-major corner turn + directly fed correlate",
-                                     "channel-major corner turn + bulk-fed correlate"][cfg.corr_path],
+                                     "channel-major corner turn + bulk-fed correlate",
+                                     "channel-major corner turn + bulk-fed correlate, 16 unpack warps",
+                                     "captured block read directly (4-CTA clusters, no corner turn)",
+                                     "captured block read directly (4-CTA clusters), 16 unpack warps"
+                                     ][cfg.corr_path],
                        "l2": "inputs larger than L2: 3 resident 198 MB blocks rotated",
                        "parallelism": f"blocks independent per GPU x{ws}"},
             "realtime_factor": value / ws * REALTIME_S,

@@ -232,7 +232,13 @@ static int correlate_device(dsax_ctx *c, int fmt, const void *in, float *vis, in
   a.in = static_cast<const uint8_t *>(in);
   if (fmt == DSAX_FMT_CHANMAJOR) {
     a.nant_in = 64;
-    if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path != 3) != 0)
+    if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path) != 0)
+      return cuda_check(c, cudaGetLastError(), "correlator launch");
+    return DSAX_OK;
+  }
+  if (fmt == DSAX_FMT_CAPTURED && corr_path_fused(c->cfg.corr_path) && captured_cluster_ok(a)) {
+    // the correlator reads the captured block directly (no corner turn)
+    if (launch_correlate_captured_cluster(a, c->stream, corr_path_unpack_warps(c->cfg.corr_path)) != 0)
       return cuda_check(c, cudaGetLastError(), "correlator launch");
     return DSAX_OK;
   }
@@ -254,7 +260,7 @@ static int correlate_device(dsax_ctx *c, int fmt, const void *in, float *vis, in
         return cuda_check(c, cudaGetLastError(), "corner-turn launch");
       a.in = tmp;
       a.nant_in = 64;
-      if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path != 3) != 0)
+      if (launch_correlate_chanmajor(a, c->stream, c->cfg.corr_path) != 0)
         return cuda_check(c, cudaGetLastError(), "correlator launch");
       return DSAX_OK;
     }

@@ -31,18 +31,26 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
   const int npkt = cf.npkt, nchan = d.nchan, ngrp = nchan / 8, ppo = cf.bf_pkt_per_out;
   const int nout = npkt / ppo;
   if (d.vis) {
-    if (launch_reorder_chanmajor(static_cast<const uint8_t *>(d.blk), scratch, npkt, cf.nant_in,
-                                 nchan, sc) != 0)
-      return -2;
     CorrArgs a{};
-    a.in = scratch;
+    a.in = static_cast<const uint8_t *>(d.blk);
     a.vis = d.vis;
     a.err = c->d_err;
     a.npkt = npkt;
-    a.nant_in = 64;
+    a.nant_in = cf.nant_in;
     a.nchan = nchan;
     a.wait_limit_ns = cf.wait_limit_ns;
-    if (launch_correlate_chanmajor(a, sc, c->cfg.corr_path != 3) != 0) return -2;
+    if (corr_path_fused(cf.corr_path) && captured_cluster_ok(a)) {
+      // the correlator reads the captured block directly (no corner turn)
+      if (launch_correlate_captured_cluster(a, sc, corr_path_unpack_warps(cf.corr_path)) != 0)
+        return -2;
+    } else {
+      if (launch_reorder_chanmajor(static_cast<const uint8_t *>(d.blk), scratch, npkt, cf.nant_in,
+                                   nchan, sc) != 0)
+        return -2;
+      a.in = scratch;
+      a.nant_in = 64;
+      if (launch_correlate_chanmajor(a, sc, cf.corr_path) != 0) return -2;
+    }
   }
   if (d.beams || d.chanmask) {
     BfArgs b{};

@@ -26,10 +26,12 @@
 //   warp  8   : TMEM allocator and single-thread UMMA issuer.
 // Every pipeline wait is bounded (dsax_ptx.cuh).
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "dsax_internal.h"
 #include "dsax_ptx.cuh"
+#include "dsax_tmap.h"
 
 namespace dsax {
 
@@ -293,6 +295,26 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
 // prmt and sign-extends nibbles with carry-free bytewise adds.  Lanes 4..7 of each group of 8
 // store the two pols in the opposite order, so every 16-byte store
 // instruction covers all eight bank groups of the 128-byte swizzle.
+// NW = 16 (bulk-fed only) doubles the unpack warps: warps 8..15 repeat the
+// mapping of warps 0..7 for time slot 1 while warps 0..7 take slot 0 (each
+// raw word is read twice, each thread does half the byte work), and the
+// epilogue splits every warp's column blocks between the two halves.
+//
+// Feeds (FEED): 0 direct loads and 1 one bulk copy per stage, both from the
+// channel-major corner turn; 2 the captured block itself, with no corner
+// turn.  FEED 2 runs in clusters of four CTAs, the four channels of one
+// 16-byte row of the captured layout.  Per 64-packet stage, CTA r of the
+// cluster loads one TMA box [16 packets][nant_in antennas][16 bytes]
+// (packets 16r..16r+15 of the stage, all four channels; rows past the
+// block read zero), and two transposer warps split it by channel: 16 bytes
+// (four antennas of one channel) at a time go into the raw stage of the
+// channel's CTA with st.async, counted on that CTA's raw-full mbarrier.
+// Each CTA's raw stage thus receives 4 KB from each of the four CTAs in the
+// same [64 packets][64 antennas][4 bytes] layout as the bulk feed, and the
+// unpack, UMMA and epilogue are those of FEED 1.  A raw slot is re-armed,
+// and the four sources told that it is free (remote mbarrier arrivals), once
+// the unpack warps have read it.  Every HBM byte of the block is read once
+// and crosses the SM-to-SM network at most once; no multicast is used.
 namespace corrcm {
 constexpr int kPktPerStage = 64;
 constexpr int kTile = 128 * 128;                   // 128 rows x 128 B of K
@@ -300,10 +322,17 @@ constexpr int kStageBytes = 2 * kTile;             // two time slots
 constexpr int kOpStages = 4;
 constexpr int kRawBytes = kPktPerStage * 256;      // bulk-fed variant: one 16 KB stage
 constexpr int kRawStages = 4;
-// 8 unpack/epilogue warps + UMMA warp (+ loader warp for the bulk-fed variant)
-template <bool kBulk> constexpr int threads() { return kBulk ? 320 : 288; }
-template <bool kBulk> constexpr int smem_bytes() {
-  return 1024 + kOpStages * kStageBytes + (kBulk ? kRawStages * kRawBytes : 0);
+constexpr int kClusterCh = 4;                      // FEED 2: channels (CTAs) per cluster
+constexpr int kLandPkts = kPktPerStage / kClusterCh;   // packets of a TMA box
+constexpr int kLandBytes = kLandPkts * 64 * 16;    // its largest size (64 antennas)
+// NW unpack/epilogue warps + UMMA warp (+ bulk loader warp for FEED 1; TMA
+// warp, raw-slot manager warp and two transposer warps for FEED 2)
+template <int FEED, int NW> constexpr int threads() {
+  return 32 * NW + 32 + (FEED == 1 ? 32 : FEED == 2 ? 128 : 0);
+}
+template <int FEED> constexpr int smem_bytes() {
+  return 1024 + kOpStages * kStageBytes + (FEED >= 1 ? kRawStages * kRawBytes : 0) +
+         (FEED == 2 ? 2 * kLandBytes : 0);
 }
 constexpr uint32_t kIdescN128 = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 128);
 static_assert(kOpStages * kStageBytes >= 2 * 128 * 128 * 4, "C^T scratch reuses the stages");
@@ -318,56 +347,79 @@ __device__ __forceinline__ uint32_t sext_hi4(uint32_t w) {
   return ((((w >> 4) & 0x0F0F0F0Fu) ^ 0x08080808u) + 0x78787878u) ^ 0x80808080u;
 }
 
-template <bool kBulk>
-__global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(CorrArgs a) {
+template <int FEED, int NW>
+__global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
+    corr_cm_kernel(const __grid_constant__ CUtensorMap tmap, CorrArgs a) {
   using namespace corrcm;
+  constexpr bool kBulk = FEED >= 1;   // unpack from raw stages in shared memory
+  constexpr bool kCl = FEED == 2;
+  static_assert(NW == 8 || (NW == 16 && kBulk), "8 unpack warps, or 16 when stage-fed");
+  constexpr int kUnpackThreads = 32 * NW;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kOpStages];
   __shared__ __align__(8) uint64_t empty_bar[kOpStages];
   __shared__ __align__(8) uint64_t rfull_bar[kRawStages];
   __shared__ __align__(8) uint64_t rempty_bar[kRawStages];
   __shared__ __align__(8) uint64_t accum_bar;
+  __shared__ __align__(8) uint64_t land_full[2];          // FEED 2: TMA box landed
+  __shared__ __align__(8) uint64_t land_empty[2];         // FEED 2: box read by the transposers
+  __shared__ __align__(8) uint64_t dest_free[kRawStages]; // FEED 2: slot free in all 4 CTAs
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ch = blockIdx.x;
+  const uint32_t crank = kCl ? cluster_ctarank() : 0u;     // channel within the cluster's four
+  const int nks = (a.npkt + kPktPerStage - 1) / kPktPerStage;
   const uint32_t sbase = (smem_u32(smem_raw) + 1023u) & ~1023u;
   uint8_t *const gbase = smem_raw + (sbase - smem_u32(smem_raw));   // generic view of sbase
 
   if (tid == 0) {
     for (int s = 0; s < kOpStages; ++s) {
-      mbar_init(&full_bar[s], 256);
+      mbar_init(&full_bar[s], kUnpackThreads);
       mbar_init(&empty_bar[s], 1);
     }
     for (int r = 0; r < kRawStages; ++r) {
       mbar_init(&rfull_bar[r], 1);
-      mbar_init(&rempty_bar[r], 256);
+      mbar_init(&rempty_bar[r], kUnpackThreads);
     }
     mbar_init(&accum_bar, 1);
+    if (kCl) {
+      for (int b2 = 0; b2 < 2; ++b2) {
+        mbar_init(&land_full[b2], 1);
+        mbar_init(&land_empty[b2], 64);
+      }
+      for (int r = 0; r < kRawStages; ++r) {
+        mbar_init(&dest_free[r], kClusterCh);
+        // the first round of raw stages is armed here; the slot manager
+        // re-arms each slot after the unpack has read it
+        if (r < nks) mbar_arrive_expect_tx(&rfull_bar[r], kRawBytes);
+      }
+    }
     abort_sh = 0;
     mbar_fence_init();
   }
-  if (warp == 8) {
+  if (warp == NW) {
     tmem_alloc(&tmem_base_sh, 512);
     tmem_relinquish();
   }
   const uint32_t raw_base = sbase + kOpStages * kStageBytes;   // kBulk only
   tc_fence_before();
   __syncthreads();
+  if (kCl) cluster_barrier();   // every CTA's barriers exist before any remote access
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
   if ((tmem & 0xFFFFu) != 0u) {
     if (tid == 0) atomicOr(a.err, DEV_ERR_TMEM);
     abort_sh = 1;
   }
-  const int nks = (a.npkt + kPktPerStage - 1) / kPktPerStage;
   const uint32_t *chan_src = reinterpret_cast<const uint32_t *>(a.in + (int64_t)ch * a.npkt * 256);
 
-  if (warp < 8) {
+  if (warp < NW) {
     // ------------------------------------------------------------ unpack
     const int ant = lane + 32 * (warp & 1);
-    const uint32_t c = (uint32_t)(warp >> 1);          // 16-byte chunk of each half (0..3)
+    const uint32_t c = (uint32_t)((warp >> 1) & 3);    // 16-byte chunk of each half (0..3)
+    const int tsel = warp >> 3;                        // NW = 16: the one time slot
     const uint32_t flip = (uint32_t)(lane >> 2) & 1u;  // store pol 1 first
     // tile offsets of this thread's chunks, store order sp = 0, 1 (pol = sp ^ flip)
     uint32_t o_re[2], o_im[2];
@@ -393,31 +445,42 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
                              a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
         return false;
       // X[sl][e][h]: sample slot sl = 2t + pol of packets q = 4h .. 4h+3
+      // (NW = 16: only the slots of time slot tsel, at sl = 0, 1)
       uint32_t X[4][2][2];
+      const uint32_t sel_t = tsel ? 0x7362u : 0x5140u;
 #pragma unroll
       for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const uint32_t *v = &w[e][4 * h];
-          const uint32_t t0 = __byte_perm(v[0], v[1], 0x5140u);
-          const uint32_t t1 = __byte_perm(v[0], v[1], 0x7362u);
-          const uint32_t t2 = __byte_perm(v[2], v[3], 0x5140u);
-          const uint32_t t3 = __byte_perm(v[2], v[3], 0x7362u);
-          X[0][e][h] = __byte_perm(t0, t2, 0x5410u);
-          X[1][e][h] = __byte_perm(t0, t2, 0x7632u);
-          X[2][e][h] = __byte_perm(t1, t3, 0x5410u);
-          X[3][e][h] = __byte_perm(t1, t3, 0x7632u);
+          if (NW == 16) {
+            const uint32_t ta = __byte_perm(v[0], v[1], sel_t);
+            const uint32_t tb = __byte_perm(v[2], v[3], sel_t);
+            X[0][e][h] = __byte_perm(ta, tb, 0x5410u);
+            X[1][e][h] = __byte_perm(ta, tb, 0x7632u);
+          } else {
+            const uint32_t t0 = __byte_perm(v[0], v[1], 0x5140u);
+            const uint32_t t1 = __byte_perm(v[0], v[1], 0x7362u);
+            const uint32_t t2 = __byte_perm(v[2], v[3], 0x5140u);
+            const uint32_t t3 = __byte_perm(v[2], v[3], 0x7362u);
+            X[0][e][h] = __byte_perm(t0, t2, 0x5410u);
+            X[1][e][h] = __byte_perm(t0, t2, 0x7632u);
+            X[2][e][h] = __byte_perm(t1, t3, 0x5410u);
+            X[3][e][h] = __byte_perm(t1, t3, 0x7632u);
+          }
         }
       const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
 #pragma unroll
-      for (int t = 0; t < 2; ++t) {
+      for (int tt = 0; tt < (NW == 16 ? 1 : 2); ++tt) {
+        const int t = NW == 16 ? tsel : tt;   // time slot (tile)
+        const int xs = 2 * tt;                // its slots in X
 #pragma unroll
         for (int sp = 0; sp < 2; ++sp) {
           const uint32_t pol = (uint32_t)sp ^ flip;
           uint32_t re[4], im[4];
 #pragma unroll
           for (int k = 0; k < 4; ++k) {   // chunk word k = (e, h) = (k >> 1, k & 1)
-            const uint32_t x0 = X[2 * t][k >> 1][k & 1], x1 = X[2 * t + 1][k >> 1][k & 1];
+            const uint32_t x0 = X[xs][k >> 1][k & 1], x1 = X[xs + 1][k >> 1][k & 1];
             const uint32_t x = pol ? x1 : x0;
             re[k] = sext_lo4(x);
             im[k] = sext_hi4(x);
@@ -436,8 +499,8 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
       // the words of raw stage ks -> w, then the stage goes back to the loader
       auto fetch = [&](int ks, uint32_t (&w)[2][8]) -> bool {
         const int r = ks % kRawStages;
-        if (!mbar_wait_bounded(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
-                               DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+        if (!mbar_wait_bounded<kCl>(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh,
+                                    a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns))
           return false;
         const uint32_t *rw = rw_base + r * (kRawBytes / 4);
         const int pvalid = a.npkt - ks * kPktPerStage;
@@ -483,7 +546,101 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
         if (!unpack_store(ks + 2, wc)) break;
       }
     }
-  } else if (kBulk && warp == 9) {
+  } else if (kCl && warp == NW + 1) {
+    // ------------------------------------------------------------ TMA loader (FEED 2)
+    if (lane == 0) {
+      const uint32_t land_bytes = (uint32_t)(kLandPkts * a.nant_in * 16);
+      const uint32_t land_base = raw_base + kRawStages * kRawBytes;
+      const int x0 = 4 * (ch - (int)crank);   // byte offset of the cluster's four channels
+      int ks = 0;
+      for (; ks < nks && !abort_sh; ++ks) {
+        const int bsel = ks & 1;
+        if (!mbar_wait_bounded(&land_empty[bsel], ((uint32_t)(ks >> 1) & 1u) ^ 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+          break;
+        mbar_arrive_expect_tx(&land_full[bsel], land_bytes);
+        tma_load_3d(land_base + (uint32_t)bsel * kLandBytes, &tmap, x0, 0,
+                    ks * kPktPerStage + kLandPkts * (int)crank, &land_full[bsel]);
+      }
+      // boxes still landing after an abort: wait for them before exit
+      volatile int no_abort = 0;
+      for (int k2 = ks - 2; k2 < ks; ++k2)
+        if (k2 >= 0)
+          mbar_wait_bounded(&land_full[k2 & 1], (uint32_t)(k2 >> 1) & 1u, &no_abort, a.err,
+                            DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
+    }
+    __syncwarp();
+  } else if (kCl && warp == NW + 2) {
+    // ------------------------------------------------------------ raw-slot manager (FEED 2)
+    if (lane == 0) {
+      int ks = 0;
+      for (; ks < nks && !abort_sh; ++ks) {
+        const int r = ks % kRawStages;
+        if (!mbar_wait_bounded(&rempty_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+          break;
+        if (ks + kRawStages < nks) {   // arm the slot for stage ks + R, then free it everywhere
+          mbar_arrive_expect_tx(&rfull_bar[r], kRawBytes);
+          for (uint32_t q = 0; q < (uint32_t)kClusterCh; ++q)
+            mbar_arrive_remote(cluster_map(&dest_free[r], q));
+        }
+      }
+      // stages armed but not seen consumed (only after an abort): wait until
+      // the stores the other CTAs may still have in flight to this CTA land
+      volatile int no_abort = 0;
+      for (int k2 = ks; k2 < nks && k2 < ks + kRawStages; ++k2)
+        mbar_wait_bounded<true>(&rfull_bar[k2 % kRawStages], (uint32_t)(k2 / kRawStages) & 1u,
+                                &no_abort, a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
+    }
+    __syncwarp();
+  } else if (kCl && warp > NW + 2) {
+    // ------------------------------------------------------------ transposers (FEED 2)
+    // Thread tt: packet pl of the box and antenna quads aq0 + 4i; lanes of a
+    // warp span 8 packets, so with an odd antenna count (a row pitch of an
+    // odd number of 16-byte units) their 16-byte reads hit distinct banks.
+    const int tt = tid - 32 * (NW + 3);                    // 0..63
+    const int pl = (tt & 7) | ((tt >> 5) << 3);           // 0..15
+    const int aq0 = (tt >> 3) & 3;
+    const int NA = a.nant_in;
+    const uint8_t *gland = gbase + kOpStages * kStageBytes + kRawStages * kRawBytes;
+    for (int ks = 0; ks < nks && !abort_sh; ++ks) {
+      const int bsel = ks & 1, r = ks % kRawStages;
+      if (!mbar_wait_bounded(&land_full[bsel], (uint32_t)(ks >> 1) & 1u, &abort_sh, a.err,
+                             DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+        break;
+      if (ks >= kRawStages &&
+          !mbar_wait_bounded<true>(&dest_free[r], (uint32_t)(ks / kRawStages - 1) & 1u, &abort_sh,
+                                   a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+        break;
+      const uint8_t *land = gland + bsel * kLandBytes + pl * NA * 16;
+      const uint32_t roff = (uint32_t)r * kRawBytes +
+                            (uint32_t)((kLandPkts * (int)crank + pl) * 64) * 4u;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int aq = aq0 + 4 * i;
+        uint4 v[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int ant = 4 * aq + e;
+          v[e] = ant < NA ? *reinterpret_cast<const uint4 *>(land + ant * 16) : make_uint4(0, 0, 0, 0);
+        }
+        const uint32_t off = roff + (uint32_t)aq * 16u;
+#pragma unroll
+        for (uint32_t q = 0; q < (uint32_t)kClusterCh; ++q) {
+          // channel q of the four antennas -> CTA q
+          const uint32_t w0 = q == 0 ? v[0].x : q == 1 ? v[0].y : q == 2 ? v[0].z : v[0].w;
+          const uint32_t w1 = q == 0 ? v[1].x : q == 1 ? v[1].y : q == 2 ? v[1].z : v[1].w;
+          const uint32_t w2 = q == 0 ? v[2].x : q == 1 ? v[2].y : q == 2 ? v[2].z : v[2].w;
+          const uint32_t w3 = q == 0 ? v[3].x : q == 1 ? v[3].y : q == 2 ? v[3].z : v[3].w;
+          st_async_v4(cluster_map_u32(raw_base + off, q), w0, w1, w2, w3,
+                      cluster_map(&rfull_bar[r], q));
+        }
+      }
+      // the next box (async proxy) overwrites this one: order the reads first
+      fence_proxy_async_smem();
+      mbar_arrive(&land_empty[bsel]);
+    }
+  } else if (FEED == 1 && warp == NW + 1) {
     // ------------------------------------------------------------ bulk loader
     if (lane == 0) {
       int ks = 0;
@@ -509,7 +666,7 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
                             &no_abort, a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
-  } else {
+  } else if (warp == NW) {
     // ------------------------------------------------------------ UMMA issuer
     if (lane == 0) {
       for (int ks = 0; ks < nks && !abort_sh; ++ks) {
@@ -543,12 +700,15 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
   }
 
   // ---------------------------------------------------------------- epilogue
-  if (warp < 8) {
+  if (warp < NW) {
     bool ok = mbar_wait_bounded(&accum_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
                                 a.wait_limit_ns);
     tc_fence_after();
     ok = __all_sync(0xffffffffu, ok && !abort_sh);
-    const int q = warp & 3, t = warp >> 2;
+    // TMEM lane quadrant q (warp % 4), time slot t; with NW = 16 the two
+    // warps of each (q, t) take alternate column blocks (hh)
+    constexpr int kCbStep = NW / 8;
+    const int q = warp & 3, t = (warp >> 2) & 1, hh = warp >> 3;
     const int m = 32 * q + lane;                   // row = 2 * antenna + pol
     const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
     // C^T through shared memory (every MMA has completed, so the operand
@@ -556,7 +716,7 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
     uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase + t * (128 * 128 * 4));
     if (ok) {
 #pragma unroll
-      for (int cb = 0; cb < 8; ++cb) {
+      for (int cb = hh; cb < 8; cb += kCbStep) {
         uint32_t cv[16];
         tmem_ld16(trow + 128u + 16u * cb, cv);
         tmem_wait_ld();
@@ -564,13 +724,13 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
         for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
       }
     }
-    named_bar(1, 256);
+    named_bar(1, kUnpackThreads);
     if (ok) {
       const int i = m >> 1, pi = m & 1;
       float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
       const int64_t tri = (int64_t)i * (i + 1) / 2;
       const int ncb = 2 * q + 2;
-      for (int cb = 0; cb < ncb; ++cb) {
+      for (int cb = hh; cb < ncb; cb += kCbStep) {
         uint32_t re[16], cr[16];
         tmem_ld16(trow + 16u * cb, re);
         tmem_ld16(trow + 128u + 16u * cb, cr);
@@ -598,7 +758,9 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 8) {
+  // no CTA leaves while another may still address its shared memory
+  if (kCl) cluster_barrier();
+  if (warp == NW) {
     if (lane == 0) {
       volatile int no_abort = 0;
       mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, drain_limit(a.wait_limit_ns));
@@ -609,21 +771,63 @@ __global__ void __launch_bounds__(corrcm::threads<kBulk>(), 1) corr_cm_kernel(Co
   }
 }
 
-template <bool kBulk>
-static int launch_cm(const CorrArgs &a, cudaStream_t st) {
-  static SmemAttrOnce attr;
-  if (smem_attr_once(attr, corr_cm_kernel<kBulk>, corrcm::smem_bytes<kBulk>()) != cudaSuccess)
-    return -2;
-  void *args[] = {(void *)&a};
-  return cudaLaunchKernel((const void *)corr_cm_kernel<kBulk>, dim3(a.nchan),
-                          dim3(corrcm::threads<kBulk>()), args, corrcm::smem_bytes<kBulk>(),
-                          st) == cudaSuccess
-             ? 0
-             : -2;
+// FEED 2: the captured block [npkt][nant_in][nchan][4 B] as a 3-D uint8
+// tensor (bytes of a packet-antenna row, antennas, packets); boxes of 16
+// bytes x nant_in x 16 packets, zero fill past the last packet.
+static int encode_captured_map(CUtensorMap *map, const CorrArgs &a) {
+  EncodeTiledFn fn = tensor_map_encoder();
+  if (!fn) return -1;
+  const cuuint64_t dims[3] = {(cuuint64_t)a.nchan * 4, (cuuint64_t)a.nant_in, (cuuint64_t)a.npkt};
+  const cuuint64_t strides[2] = {(cuuint64_t)a.nchan * 4, (cuuint64_t)a.nchan * 4 * a.nant_in};
+  const cuuint32_t box[3] = {16u, (cuuint32_t)a.nant_in, (cuuint32_t)corrcm::kLandPkts};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t *>(a.in), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -1;
 }
 
-int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, bool bulk_fed) {
-  return bulk_fed ? launch_cm<true>(a, st) : launch_cm<false>(a, st);
+template <int FEED, int NW>
+static int launch_cm(const CorrArgs &a, cudaStream_t st) {
+  static SmemAttrOnce attr;
+  constexpr int smem = corrcm::smem_bytes<FEED>();
+  if (smem_attr_once(attr, corr_cm_kernel<FEED, NW>, smem) != cudaSuccess) return -2;
+  CUtensorMap tmap;
+  memset(&tmap, 0, sizeof(tmap));
+  if (FEED == 2 && encode_captured_map(&tmap, a) != 0) return -2;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)a.nchan, 1, 1);
+  cfg.blockDim = dim3(corrcm::threads<FEED, NW>(), 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = FEED == 2 ? (unsigned)corrcm::kClusterCh : 1u;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, corr_cm_kernel<FEED, NW>, tmap, a) == cudaSuccess ? 0 : -2;
+}
+
+int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, int corr_path) {
+  switch (corr_path) {
+    case 3: return launch_cm<0, 8>(a, st);
+    case 5:
+    case 7: return launch_cm<1, 16>(a, st);
+    default: return launch_cm<1, 8>(a, st);
+  }
+}
+
+bool captured_cluster_ok(const CorrArgs &a) {
+  return a.nchan % corrcm::kClusterCh == 0 && a.nant_in >= 1 && a.nant_in <= 64 &&
+         (reinterpret_cast<uintptr_t>(a.in) & 15u) == 0 && tensor_map_encoder() != nullptr;
+}
+
+int launch_correlate_captured_cluster(const CorrArgs &a, cudaStream_t st, int unpack_warps) {
+  if (!captured_cluster_ok(a)) return -1;
+  return unpack_warps == 16 ? launch_cm<2, 16>(a, st) : launch_cm<2, 8>(a, st);
 }
 
 int launch_correlate(const CorrArgs &a, int fmt, cudaStream_t st) {

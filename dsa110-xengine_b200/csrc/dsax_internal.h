@@ -115,8 +115,10 @@ struct FlagArgs {
   float *pix_sum = nullptr, *pix_max = nullptr;
   int tds = 0;
   // statistics-pass geometry, set by the launcher
-  int nslab = 1;                 // channel slabs of kFlagSlab channels (CTAs per beam)
-  int rs = 0;                    // rows per pipeline stage (divides tbin)
+  int nslab = 1;                 // channel slabs of kFlagSlab channels
+  int rs = 0;                    // rows per pipeline stage (a multiple of sp)
+  int sp = 1;                    // lanes per channel group (power of two dividing tbin and 32)
+  int kc = 1;                    // time chunks per slab (the cluster size)
   int ts_mean = 0;               // 1: the statistics pass writes ts = row mean (no apply pass)
   // data path (src/gpu_flagger.cu:1290-1410)
   int clean = 0;                 // 1: replace flagged columns / rows in xw / xw8
@@ -169,7 +171,17 @@ namespace dsax {
 // Channel-major corner turn: [nchan][npkt][64][4 B] (internal layout).
 int launch_reorder_chanmajor(const uint8_t *in, uint8_t *out, int npkt, int nant_in, int nchan,
                              cudaStream_t st);
-// bulk_fed: the operand feed is one cp.async.bulk per 64-packet stage (true)
-// or direct coalesced loads into registers (false).
-int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, bool bulk_fed);
+// corr_path selects the operand feed: 3 direct coalesced loads into
+// registers, 5 and 7 one cp.async.bulk per 64-packet stage unpacked by 16
+// warps, anything else (4, 6) the same bulk feed unpacked by 8 warps.
+int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, int corr_path);
+// The captured block [npkt][nant_in][nchan][4 B] correlated directly (no
+// corner turn): clusters of four channel CTAs, TMA boxes split across the
+// cluster through distributed shared memory.  Needs nchan % 4 == 0 and a
+// 16-byte aligned block; returns -1 otherwise.
+bool captured_cluster_ok(const CorrArgs &a);
+int launch_correlate_captured_cluster(const CorrArgs &a, cudaStream_t st, int unpack_warps);
+// corr_path 6 (8 unpack warps) and 7 (16) select the captured-block feed.
+inline bool corr_path_fused(int corr_path) { return corr_path == 6 || corr_path == 7; }
+inline int corr_path_unpack_warps(int corr_path) { return corr_path == 7 ? 16 : 8; }
 }  // namespace dsax

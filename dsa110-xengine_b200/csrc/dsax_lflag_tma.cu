@@ -32,6 +32,7 @@
 #include "dsax_internal.h"
 #include "dsax_lflag.h"
 #include "dsax_ptx.cuh"
+#include "dsax_tmap.h"
 
 namespace dsax {
 
@@ -583,28 +584,11 @@ __global__ void __launch_bounds__(lf1::kThreads, 1)
 
 namespace {
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
-  return fn;
-}
-
 // Tensor map over a padded grid [npp][ch] BF16 with 130-pixel boxes: ch =
 // 64 (128-byte rows, 128-byte swizzle) or 8 (16-byte rows, no swizzle);
 // zero fill out of bounds.
 int encode_grid_map(CUtensorMap *map, const uint16_t *grid, int64_t npp, int ch) {
-  EncodeTiledFn fn = encode_fn();
+  EncodeTiledFn fn = tensor_map_encoder();
   if (!fn || npp < 1 || npp > (int64_t)0x7fffffff || (ch != 64 && ch != 8)) return -1;
   const cuuint64_t dims[2] = {(cuuint64_t)ch, (cuuint64_t)npp};
   const cuuint64_t strides[1] = {(cuuint64_t)ch * 2};

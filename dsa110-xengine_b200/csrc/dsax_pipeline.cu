@@ -7,7 +7,8 @@
 // corner turn (HBM-bound) runs on a side stream while block i is correlated
 // (bound by the unpack warps, with HBM bandwidth to spare), and in host mode
 // the PCIe copies in and out overlap both (in device mode the corner turn
-// stays on the context stream, see below).  Buffers are double-buffered and
+// stays on the context stream, see below).  The fused paths (corr_path 6,
+// 7) have no corner turn: only the copies overlap the correlations.  Buffers are double-buffered and
 // every reuse waits on the event of the stage that last read the buffer.
 #include <cuda_runtime.h>
 
@@ -49,11 +50,22 @@ extern "C" int dsax_correlate_many(dsax_ctx *c, const void *const *blocks, void 
   const size_t nvis = dsax_vis_bytes(&c->cfg);
   auto up = [](size_t n) { return (n + 255) & ~(size_t)255; };
   const bool host = mem == DSAX_MEM_HOST;
-  const size_t need = 2 * up(nreo) + (host ? 2 * up(nin) + 2 * up(nvis) : 0);
+  // corr_path 6 / 7: the correlator reads the captured block itself (no
+  // corner turn, no channel-major buffer); device blocks were checked for
+  // 16-byte alignment above and the host-mode staging buffers are aligned
+  CorrArgs probe{};
+  probe.npkt = c->cfg.npkt;
+  probe.nant_in = c->cfg.nant_in;
+  probe.nchan = c->cfg.nchan;
+  probe.in = host ? nullptr : static_cast<const uint8_t *>(blocks[0]);
+  const bool fused = corr_path_fused(c->cfg.corr_path) && captured_cluster_ok(probe);
+  const bool need_reo = !fused;
+  const size_t need = (need_reo ? 2 * up(nreo) : 0) + (host ? 2 * up(nin) + 2 * up(nvis) : 0);
   if ((rc = ensure_buffer(c, c->aux[AUX_PIPE], need, "correlate_many buffers")) != DSAX_OK) return rc;
   uint8_t *base = static_cast<uint8_t *>(c->aux[AUX_PIPE].ptr);
-  uint8_t *reo[2] = {base, base + up(nreo)};
-  uint8_t *din[2] = {base + 2 * up(nreo), base + 2 * up(nreo) + up(nin)};
+  const size_t oreo = need_reo ? 2 * up(nreo) : 0;
+  uint8_t *reo[2] = {base, base + up(nreo)};   // unused by the fused paths
+  uint8_t *din[2] = {base + oreo, base + oreo + up(nin)};
   uint8_t *dvis[2] = {din[1] + up(nin), din[1] + up(nin) + up(nvis)};
 
   // In device mode each block's corner turn runs on the context stream right
@@ -78,34 +90,44 @@ extern "C" int dsax_correlate_many(dsax_ctx *c, const void *const *blocks, void 
   a.err = c->d_err;
   a.wait_limit_ns = c->cfg.wait_limit_ns;
   a.accumulate = 0;
-  const bool bulk = c->cfg.corr_path != 3;
   for (int i = 0; i < nblk && e == cudaSuccess; ++i) {
     const int b = i & 1;
     const uint8_t *src = static_cast<const uint8_t *>(blocks[i]);
     if (host) {
-      // copy in: the corner turn of block i-2 has finished reading din[b]
-      if (i >= 2) e = cudaStreamWaitEvent(h2d, ev[E_REO + b], 0);
+      // copy in: the stage that read din[b] for block i-2 has finished
+      if (i >= 2) e = cudaStreamWaitEvent(h2d, ev[(fused ? E_CORR : E_REO) + b], 0);
       if (e == cudaSuccess) e = cudaMemcpyAsync(din[b], src, nin, cudaMemcpyHostToDevice, h2d);
       if (e == cudaSuccess) e = cudaEventRecord(ev[E_H2D + b], h2d);
-      if (e == cudaSuccess) e = cudaStreamWaitEvent(rs, ev[E_H2D + b], 0);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(fused ? cs : rs, ev[E_H2D + b], 0);
       src = din[b];
     }
-    // corner turn: the correlation of block i-2 has finished reading reo[b]
-    if (e == cudaSuccess && i >= 2) e = cudaStreamWaitEvent(rs, ev[E_CORR + b], 0);
-    if (e != cudaSuccess) break;
-    if (launch_reorder_chanmajor(src, reo[b], c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan, rs) != 0) {
-      e = cudaGetLastError();
-      if (e == cudaSuccess) e = cudaErrorInvalidValue;
-      break;
+    if (!fused) {
+      // corner turn: the correlation of block i-2 has finished reading reo[b]
+      if (e == cudaSuccess && i >= 2) e = cudaStreamWaitEvent(rs, ev[E_CORR + b], 0);
+      if (e != cudaSuccess) break;
+      if (launch_reorder_chanmajor(src, reo[b], c->cfg.npkt, c->cfg.nant_in, c->cfg.nchan, rs) != 0) {
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaErrorInvalidValue;
+        break;
+      }
+      e = cudaEventRecord(ev[E_REO + b], rs);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev[E_REO + b], 0);
     }
-    e = cudaEventRecord(ev[E_REO + b], rs);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev[E_REO + b], 0);
     // correlate: in host mode the copy-out of block i-2 has finished reading dvis[b]
     if (e == cudaSuccess && host && i >= 2) e = cudaStreamWaitEvent(cs, ev[E_D2H + b], 0);
     if (e != cudaSuccess) break;
-    a.in = reo[b];
     a.vis = host ? reinterpret_cast<float *>(dvis[b]) : static_cast<float *>(vis[i]);
-    if (launch_correlate_chanmajor(a, cs, bulk) != 0) {
+    int lrc;
+    if (fused) {
+      a.in = src;
+      a.nant_in = c->cfg.nant_in;
+      lrc = launch_correlate_captured_cluster(a, cs, corr_path_unpack_warps(c->cfg.corr_path));
+    } else {
+      a.in = reo[b];
+      a.nant_in = 64;
+      lrc = launch_correlate_chanmajor(a, cs, c->cfg.corr_path);
+    }
+    if (lrc != 0) {
       e = cudaGetLastError();
       if (e == cudaSuccess) e = cudaErrorInvalidValue;
       break;

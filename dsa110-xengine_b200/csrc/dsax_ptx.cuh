@@ -47,28 +47,41 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
       : "memory");
 }
 
+// kCluster: acquire at cluster scope (the phase was completed by another
+// CTA of the cluster: a remote arrive or remote stores with complete_tx).
+template <bool kCluster = false>
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
+  if (kCluster)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
   return ok != 0;
 }
 
 // Bounded wait on `bar` reaching phase parity `parity`.  Returns false (and
 // records `code` in *err, raises *abort) when the limit expires or another
 // thread already aborted.
+template <bool kCluster = false>
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
                                                   volatile int *abort, int *err,
                                                   int code, uint64_t limit_ns) {
-  if (mbar_try_wait(bar, parity)) return true;
+  if (mbar_try_wait<kCluster>(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t it = 1;; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait<kCluster>(bar, parity)) return true;
     // the clock is read after the second failed try (so a short limit bites
     // even where each try suspends the thread for a while) and then every
     // 64 tries
@@ -250,6 +263,57 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
         "=r"(r[31])
       : "r"(taddr)
+      : "memory");
+}
+
+// ------------------------------------------------------------ clusters
+// Rank of this CTA in its cluster.
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// Every thread of every CTA of the cluster (release / acquire).
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+               "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// The shared::cluster address of this CTA's shared variable at `p` in CTA
+// `rank` of the cluster.
+__device__ __forceinline__ uint32_t cluster_map(const void *p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_map_u32(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+// One arrival on an mbarrier of another CTA of the cluster (release).
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar)
+               : "memory");
+}
+// 16 bytes into another CTA's shared memory, counted as transaction bytes
+// on that CTA's mbarrier.
+__device__ __forceinline__ void st_async_v4(uint32_t cluster_dst, uint32_t a, uint32_t b, uint32_t c,
+                                            uint32_t d, uint32_t cluster_bar) {
+  asm volatile(
+      "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+          cluster_dst),
+      "r"(a), "r"(b), "r"(c), "r"(d), "r"(cluster_bar)
+      : "memory");
+}
+
+// 3-D tiled TMA load (no multicast) into this CTA's shared memory,
+// completing on `bar` with the box's byte count.
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *map, int x, int y, int z,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
 

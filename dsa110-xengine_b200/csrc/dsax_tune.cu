@@ -4,7 +4,10 @@
 // correlator (corr_path): (1) one fused kernel on the captured layout,
 // (2) corner turn to the REORDER layout + row-load correlator, (3) corner
 // turn to channel-major streams + correlator fed by direct coalesced loads,
-// (4) the same correlator fed by one bulk copy per 64-packet stage.
+// (4) the same correlator fed by one bulk copy per 64-packet stage and
+// unpacked by 8 warps, (5) as 4 with 16 unpack warps, (6) no corner turn:
+// the captured block read directly by clusters of four channel CTAs, (7) as
+// 6 with 16 unpack warps.
 #include <cstring>
 #include <cuda_runtime.h>
 
@@ -41,13 +44,14 @@ extern "C" int dsax_autotune(dsax_ctx *c, int reps, float *times_ms, int ntimes,
   float *vis = reinterpret_cast<float *>(blk + ((nin + 255) & ~(size_t)255));
   fill_pattern<<<1024, 256, 0, c->stream>>>(blk, nin, 12345u);
   const int saved = c->cfg.corr_path;
-  const int paths[4] = {1, 2, 3, 4};
+  constexpr int kNumPaths = 7;
+  const int paths[kNumPaths] = {1, 2, 3, 4, 5, 6, 7};
   float best = 1e30f;
   int bestp = 4;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < kNumPaths; ++k) {
     c->cfg.corr_path = paths[k];
     for (int w = 0; w < 2; ++w)
       if ((rc = dsax_correlate_fmt(c, DSAX_FMT_CAPTURED, blk, vis, DSAX_MEM_DEVICE, 0)) != DSAX_OK)

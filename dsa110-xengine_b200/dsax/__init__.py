@@ -467,12 +467,12 @@ class Context:
     def autotune(self, reps: int = 10):
         """Returns ({corr_path: ms}, chosen corr_path); the context keeps the choice."""
         import numpy as np
-        t = np.zeros(4, np.float32)
+        t = np.zeros(7, np.float32)
         best = ctypes.c_int(0)
-        self._check(lib().dsax_autotune(self._h, reps, _ptr(t), 4, ctypes.byref(best)),
+        self._check(lib().dsax_autotune(self._h, reps, _ptr(t), 7, ctypes.byref(best)),
                     "dsax_autotune")
         self.cfg.corr_path = best.value
-        return {k + 1: float(t[k]) for k in range(4)}, best.value
+        return {k + 1: float(t[k]) for k in range(7)}, best.value
 
     # -- batches -----------------------------------------------------------
     def run_batch(self, descs, use_graph: bool = True):

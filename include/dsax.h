@@ -74,8 +74,15 @@ typedef struct dsax_config {
                             2 = corner turn to the REORDER layout + correlate,
                             3 = corner turn to channel-major streams + correlate
                                 fed by direct coalesced loads,
-                            4 = as 3, fed by one bulk copy per 64-packet stage.
-                            3 and 4 also select the feed for DSAX_FMT_CHANMAJOR */
+                            4 = as 3, fed by one bulk copy per 64-packet stage,
+                            5 = as 4, unpacked by 16 warps instead of 8,
+                            6 = no corner turn: the correlator reads the
+                                captured block in clusters of four channel
+                                CTAs (TMA boxes split through distributed
+                                shared memory; needs nchan % 4 == 0, else 4),
+                            7 = as 6, unpacked by 16 warps.
+                            3 to 7 also select the feed for
+                            DSAX_FMT_CHANMAJOR (6 as 4, 7 as 5) */
     int bf_fp8;          /* beamformer operands: 0 BF16 (tcgen05 kind::f16), 1 FP8
                             E4M3 with a per-antenna power-of-two scale
                             (kind::f8f6f4; the 4-bit data, shifted by the
@@ -186,10 +193,10 @@ int dsax_extract_ex(dsax_ctx *ctx, const void *vis, void *out, int order, float 
 int dsax_correlate_extract_ex(dsax_ctx *ctx, const void *in, void *out, int order, float *autos,
                               int mem);
 
-/* Autotuner: times the captured-block correlator variants (corr_path 1, 2,
- * 3, 4) on a synthetic block of the context's geometry (reps launches each),
+/* Autotuner: times the captured-block correlator variants (corr_path 1 to
+ * 7) on a synthetic block of the context's geometry (reps launches each),
  * sets the context's corr_path to the fastest, and returns the per-variant
- * milliseconds (times_ms[0..3] for paths 1..4, if given) and the choice. */
+ * milliseconds (times_ms[0..6] for paths 1..7, up to ntimes) and the choice. */
 int dsax_autotune(dsax_ctx *ctx, int reps, float *times_ms, int ntimes, int *best_path);
 
 /* Measured dense tensor-core throughput of the context's GPU (ops/s, best

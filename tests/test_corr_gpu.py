@@ -29,7 +29,7 @@ def _run(dsax, blk, fmt=0, nant_in=None, ctx=None, accumulate=False, vis=None, c
             ctx.close()
 
 
-@pytest.mark.parametrize("corr_path", [1, 2, 3, 4])
+@pytest.mark.parametrize("corr_path", [1, 2, 3, 4, 5, 6, 7])
 def test_config1_small_uniform_bit_exact(dsax, oracle, corr_path):
     """64 dual-pol antennas, 48 channels, 2048 packets (xGPU NTIME), samples
     uniform on [-8, 7]: whole output bit-exact (fused and corner-turn paths)."""
@@ -66,7 +66,7 @@ def _full_block(oracle):
     return _FULL["blk"], _FULL["vis"]
 
 
-@pytest.mark.parametrize("corr_path", [1, 2, 3, 4])
+@pytest.mark.parametrize("corr_path", [1, 2, 3, 4, 5, 6, 7])
 def test_config2_full_block(dsax, oracle, corr_path):
     """Full block [2048][63->64][384][2][2], Gaussian sigma 2.5 clipped to
     [-8, 7]: all 768 frequencies x 2080 baselines x 4 products bit-exact
@@ -123,11 +123,22 @@ def test_corner_turn_chanmajor(dsax, oracle):
         np.testing.assert_array_equal(got, want)
 
 
-@pytest.mark.parametrize("corr_path", [1, 2, 3, 4])
+@pytest.mark.parametrize("corr_path", [1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("npkt,nant,nchan", [(4, 63, 8), (100, 63, 5), (64, 1, 1), (1, 64, 3),
                                              (130, 64, 2), (64, 63, 33)])
 def test_ragged_shapes(dsax, oracle, npkt, nant, nchan, corr_path):
     blk = oracle.gen_block(npkt + 13 * nant + nchan, npkt, nant, nchan, "uniform")
+    np.testing.assert_array_equal(_run(dsax, blk, corr_path=corr_path), oracle.correlate(blk))
+
+
+@pytest.mark.parametrize("corr_path", [6, 7])
+@pytest.mark.parametrize("npkt,nant,nchan", [(4, 63, 8), (100, 63, 4), (64, 1, 4), (1, 64, 4),
+                                             (130, 64, 8), (64, 63, 36), (200, 40, 12)])
+def test_captured_cluster_ragged_shapes(dsax, oracle, npkt, nant, nchan, corr_path):
+    """The fused captured-block feed (clusters of four channel CTAs) on
+    shapes that leave TMA boxes partly or wholly past the last packet, and
+    odd, even and tiny antenna counts."""
+    blk = oracle.gen_block(3 * npkt + 7 * nant + nchan, npkt, nant, nchan, "uniform")
     np.testing.assert_array_equal(_run(dsax, blk, corr_path=corr_path), oracle.correlate(blk))
 
 
@@ -150,7 +161,7 @@ def test_ramp_block(dsax, oracle):
     np.testing.assert_array_equal(_run(dsax, blk), oracle.correlate(blk))
 
 
-@pytest.mark.parametrize("corr_path,nchan", [(0, 16), (3, 16), (0, 160)])
+@pytest.mark.parametrize("corr_path,nchan", [(0, 16), (3, 16), (0, 160), (5, 160), (6, 160), (7, 16)])
 def test_accumulate_integrates_blocks(dsax, oracle, corr_path, nchan):
     """accumulate=1 adds into vis like xGPU's device integration buffer (160
     channels: more CTAs than SMs)."""
@@ -194,7 +205,7 @@ def test_autotune_picks_fastest_and_stays_exact(dsax, oracle):
     cfg = dsax.default_config(npkt=256, nant_in=63, nchan=64)
     with dsax.Context(cfg) as ctx:
         times, best = ctx.autotune(reps=3)
-        assert best in (1, 2, 3, 4) and all(t > 0 for t in times.values())
+        assert best in (1, 2, 3, 4, 5, 6, 7) and all(t > 0 for t in times.values())
         assert times[best] == min(times.values())
         d_in = torch.from_numpy(blk.reshape(-1)).cuda()
         vis = torch.zeros(128 * 2080 * 8, dtype=torch.float32, device="cuda")
@@ -205,7 +216,7 @@ def test_autotune_picks_fastest_and_stays_exact(dsax, oracle):
                                       oracle.correlate(blk))
 
 
-@pytest.mark.parametrize("corr_path", [3, 4])
+@pytest.mark.parametrize("corr_path", [3, 4, 5, 6])
 def test_correlate_many_device_pipelined(dsax, oracle, corr_path):
     """Five blocks through dsax_correlate_many (corner turns overlapped with
     correlations on a side stream): each output bit-exact."""

@@ -38,7 +38,7 @@ def _sync_status(dsax, ctx):
         return e.status
 
 
-@pytest.mark.parametrize("corr_path", [3, 4])
+@pytest.mark.parametrize("corr_path", [3, 4, 5, 6])
 def test_correlator_with_a_1ns_wait_limit_returns(dsax, oracle, corr_path):
     """A full block with every pipeline wait limited to 1 ns: the kernel
     returns (no hang) with either a recorded timeout (a wait that needed a
