@@ -306,33 +306,42 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
 // 16-byte row of the captured layout.  Per 64-packet stage, CTA r of the
 // cluster loads one TMA box [16 packets][nant_in antennas][16 bytes]
 // (packets 16r..16r+15 of the stage, all four channels; rows past the
-// block read zero), and two transposer warps split it by channel: 16 bytes
-// (four antennas of one channel) at a time go into the raw stage of the
-// channel's CTA with st.async, counted on that CTA's raw-full mbarrier.
-// Each CTA's raw stage thus receives 4 KB from each of the four CTAs in the
-// same [64 packets][64 antennas][4 bytes] layout as the bulk feed, and the
+// block read zero) into a landing slot.  Two transposer warps read the box
+// into registers and write it back in place split by channel, [channel q]
+// [16 packets][64 antennas][4 bytes] (antenna 63 zero), and one thread
+// sends each 4 KB piece to channel q's CTA with one shared-to-shared bulk
+// copy, counted as transaction bytes on that CTA's raw-full mbarrier.  Each
+// CTA's raw stage thus receives 4 KB from each of the four CTAs in the same
+// [64 packets][64 antennas][4 bytes] layout as the bulk feed, and the
 // unpack, UMMA and epilogue are those of FEED 1.  A raw slot is re-armed,
 // and the four sources told that it is free (remote mbarrier arrivals), once
-// the unpack warps have read it.  Every HBM byte of the block is read once
-// and crosses the SM-to-SM network at most once; no multicast is used.
+// the unpack warps have read it; a source loads the next box into its
+// landing slot only when every destination has consumed the slot's previous
+// round, which also means its bulk copies out of that landing slot are done.
+// Every HBM byte of the block is read once and crosses the SM-to-SM network
+// at most once, in 4 KB copies; no multicast is used.  (Sixteen-byte remote
+// stores with per-store transaction counts ran at about 4 GB/s per SM.)
 namespace corrcm {
 constexpr int kPktPerStage = 64;
 constexpr int kTile = 128 * 128;                   // 128 rows x 128 B of K
 constexpr int kStageBytes = 2 * kTile;             // two time slots
 constexpr int kOpStages = 4;
 constexpr int kRawBytes = kPktPerStage * 256;      // bulk-fed variant: one 16 KB stage
-constexpr int kRawStages = 4;
 constexpr int kClusterCh = 4;                      // FEED 2: channels (CTAs) per cluster
 constexpr int kLandPkts = kPktPerStage / kClusterCh;   // packets of a TMA box
-constexpr int kLandBytes = kLandPkts * 64 * 16;    // its largest size (64 antennas)
+constexpr int kLandBytes = kLandPkts * 64 * 16;    // a landing slot (box <= 64 antennas)
+static_assert(kLandBytes == kClusterCh * kLandPkts * 64 * 4, "landing slot holds the split box");
+// raw stages: 4 for the bulk feed; 3 for FEED 2, which also keeps one
+// landing slot per raw stage
+template <int FEED> constexpr int raw_stages() { return FEED == 2 ? 3 : 4; }
 // NW unpack/epilogue warps + UMMA warp (+ bulk loader warp for FEED 1; TMA
 // warp, raw-slot manager warp and two transposer warps for FEED 2)
 template <int FEED, int NW> constexpr int threads() {
   return 32 * NW + 32 + (FEED == 1 ? 32 : FEED == 2 ? 128 : 0);
 }
 template <int FEED> constexpr int smem_bytes() {
-  return 1024 + kOpStages * kStageBytes + (FEED >= 1 ? kRawStages * kRawBytes : 0) +
-         (FEED == 2 ? 2 * kLandBytes : 0);
+  return 1024 + kOpStages * kStageBytes + (FEED >= 1 ? raw_stages<FEED>() * kRawBytes : 0) +
+         (FEED == 2 ? raw_stages<FEED>() * kLandBytes : 0);
 }
 constexpr uint32_t kIdescN128 = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 128);
 static_assert(kOpStages * kStageBytes >= 2 * 128 * 128 * 4, "C^T scratch reuses the stages");
@@ -353,6 +362,7 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   using namespace corrcm;
   constexpr bool kBulk = FEED >= 1;   // unpack from raw stages in shared memory
   constexpr bool kCl = FEED == 2;
+  constexpr int kRawStages = raw_stages<FEED>();
   static_assert(NW == 8 || (NW == 16 && kBulk), "8 unpack warps, or 16 when stage-fed");
   constexpr int kUnpackThreads = 32 * NW;
   extern __shared__ uint8_t smem_raw[];
@@ -361,9 +371,8 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   __shared__ __align__(8) uint64_t rfull_bar[kRawStages];
   __shared__ __align__(8) uint64_t rempty_bar[kRawStages];
   __shared__ __align__(8) uint64_t accum_bar;
-  __shared__ __align__(8) uint64_t land_full[2];          // FEED 2: TMA box landed
-  __shared__ __align__(8) uint64_t land_empty[2];         // FEED 2: box read by the transposers
-  __shared__ __align__(8) uint64_t dest_free[kRawStages]; // FEED 2: slot free in all 4 CTAs
+  __shared__ __align__(8) uint64_t land_full[kRawStages]; // FEED 2: TMA box landed
+  __shared__ __align__(8) uint64_t dest_free[kRawStages]; // FEED 2: slot consumed in all 4 CTAs
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
 
@@ -385,11 +394,8 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
     }
     mbar_init(&accum_bar, 1);
     if (kCl) {
-      for (int b2 = 0; b2 < 2; ++b2) {
-        mbar_init(&land_full[b2], 1);
-        mbar_init(&land_empty[b2], 64);
-      }
       for (int r = 0; r < kRawStages; ++r) {
+        mbar_init(&land_full[r], 1);
         mbar_init(&dest_free[r], kClusterCh);
         // the first round of raw stages is armed here; the slot manager
         // re-arms each slot after the unpack has read it
@@ -548,26 +554,29 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
     }
   } else if (kCl && warp == NW + 1) {
     // ------------------------------------------------------------ TMA loader (FEED 2)
+    // Landing slot r is reloaded for stage ks only after all four CTAs have
+    // consumed stage ks - R, i.e. after the bulk copies out of it landed.
     if (lane == 0) {
       const uint32_t land_bytes = (uint32_t)(kLandPkts * a.nant_in * 16);
       const uint32_t land_base = raw_base + kRawStages * kRawBytes;
       const int x0 = 4 * (ch - (int)crank);   // byte offset of the cluster's four channels
       int ks = 0;
       for (; ks < nks && !abort_sh; ++ks) {
-        const int bsel = ks & 1;
-        if (!mbar_wait_bounded(&land_empty[bsel], ((uint32_t)(ks >> 1) & 1u) ^ 1u, &abort_sh, a.err,
-                               DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+        const int r = ks % kRawStages;
+        if (ks >= kRawStages &&
+            !mbar_wait_bounded<true>(&dest_free[r], (uint32_t)(ks / kRawStages - 1) & 1u, &abort_sh,
+                                     a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
           break;
-        mbar_arrive_expect_tx(&land_full[bsel], land_bytes);
-        tma_load_3d(land_base + (uint32_t)bsel * kLandBytes, &tmap, x0, 0,
-                    ks * kPktPerStage + kLandPkts * (int)crank, &land_full[bsel]);
+        mbar_arrive_expect_tx(&land_full[r], land_bytes);
+        tma_load_3d(land_base + (uint32_t)r * kLandBytes, &tmap, x0, 0,
+                    ks * kPktPerStage + kLandPkts * (int)crank, &land_full[r]);
       }
       // boxes still landing after an abort: wait for them before exit
       volatile int no_abort = 0;
-      for (int k2 = ks - 2; k2 < ks; ++k2)
+      for (int k2 = ks - kRawStages; k2 < ks; ++k2)
         if (k2 >= 0)
-          mbar_wait_bounded(&land_full[k2 & 1], (uint32_t)(k2 >> 1) & 1u, &no_abort, a.err,
-                            DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
+          mbar_wait_bounded(&land_full[k2 % kRawStages], (uint32_t)(k2 / kRawStages) & 1u,
+                            &no_abort, a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
   } else if (kCl && warp == NW + 2) {
@@ -595,50 +604,63 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
     __syncwarp();
   } else if (kCl && warp > NW + 2) {
     // ------------------------------------------------------------ transposers (FEED 2)
-    // Thread tt: packet pl of the box and antenna quads aq0 + 4i; lanes of a
-    // warp span 8 packets, so with an odd antenna count (a row pitch of an
-    // odd number of 16-byte units) their 16-byte reads hit distinct banks.
+    // Thread tt holds antenna quad aq of packets pl0 + 4i.  It reads the
+    // quad's four 16-byte rows (all four channels of one antenna each) in an
+    // order rotated by aq, so that a warp's reads, and its 16-byte writes of
+    // consecutive quads, hit distinct banks; the rotation is undone in
+    // registers.  All 64 threads read before any writes (the split box
+    // reuses the landing slot).
     const int tt = tid - 32 * (NW + 3);                    // 0..63
-    const int pl = (tt & 7) | ((tt >> 5) << 3);           // 0..15
-    const int aq0 = (tt >> 3) & 3;
+    const int aq = tt & 15, pl0 = tt >> 4;
     const int NA = a.nant_in;
+    const uint32_t land_base = raw_base + kRawStages * kRawBytes;
     const uint8_t *gland = gbase + kOpStages * kStageBytes + kRawStages * kRawBytes;
     for (int ks = 0; ks < nks && !abort_sh; ++ks) {
-      const int bsel = ks & 1, r = ks % kRawStages;
-      if (!mbar_wait_bounded(&land_full[bsel], (uint32_t)(ks >> 1) & 1u, &abort_sh, a.err,
+      const int r = ks % kRawStages;
+      if (!mbar_wait_bounded(&land_full[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh, a.err,
                              DEV_ERR_WAIT_FULL, a.wait_limit_ns))
         break;
-      if (ks >= kRawStages &&
-          !mbar_wait_bounded<true>(&dest_free[r], (uint32_t)(ks / kRawStages - 1) & 1u, &abort_sh,
-                                   a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
-        break;
-      const uint8_t *land = gland + bsel * kLandBytes + pl * NA * 16;
-      const uint32_t roff = (uint32_t)r * kRawBytes +
-                            (uint32_t)((kLandPkts * (int)crank + pl) * 64) * 4u;
+      const uint8_t *land = gland + r * kLandBytes;
+      uint4 v[4][4];   // [item i][slot e]: antenna 4 aq + ((e + aq) & 3) of packet pl0 + 4i
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const int aq = aq0 + 4 * i;
-        uint4 v[4];
+        const int pl = pl0 + 4 * i;
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-          const int ant = 4 * aq + e;
-          v[e] = ant < NA ? *reinterpret_cast<const uint4 *>(land + ant * 16) : make_uint4(0, 0, 0, 0);
-        }
-        const uint32_t off = roff + (uint32_t)aq * 16u;
-#pragma unroll
-        for (uint32_t q = 0; q < (uint32_t)kClusterCh; ++q) {
-          // channel q of the four antennas -> CTA q
-          const uint32_t w0 = q == 0 ? v[0].x : q == 1 ? v[0].y : q == 2 ? v[0].z : v[0].w;
-          const uint32_t w1 = q == 0 ? v[1].x : q == 1 ? v[1].y : q == 2 ? v[1].z : v[1].w;
-          const uint32_t w2 = q == 0 ? v[2].x : q == 1 ? v[2].y : q == 2 ? v[2].z : v[2].w;
-          const uint32_t w3 = q == 0 ? v[3].x : q == 1 ? v[3].y : q == 2 ? v[3].z : v[3].w;
-          st_async_v4(cluster_map_u32(raw_base + off, q), w0, w1, w2, w3,
-                      cluster_map(&rfull_bar[r], q));
+          const int ant = 4 * aq + ((e + aq) & 3);
+          v[i][e] = ant < NA ? *reinterpret_cast<const uint4 *>(land + (pl * NA + ant) * 16)
+                             : make_uint4(0u, 0u, 0u, 0u);
         }
       }
-      // the next box (async proxy) overwrites this one: order the reads first
-      fence_proxy_async_smem();
-      mbar_arrive(&land_empty[bsel]);
+      named_bar(2, 64);   // the whole box is in registers
+      const uint32_t slot = land_base + (uint32_t)r * kLandBytes;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        // undo the rotation: t[s] = antenna 4 aq + s
+        uint4 t0 = v[i][0], t1 = v[i][1], t2 = v[i][2], t3 = v[i][3];
+        if (aq & 1) {
+          const uint4 x = t3; t3 = t2; t2 = t1; t1 = t0; t0 = x;
+        }
+        if (aq & 2) {
+          uint4 x = t0; t0 = t2; t2 = x;
+          x = t1; t1 = t3; t3 = x;
+        }
+        const uint32_t off = (uint32_t)(((pl0 + 4 * i) * 64 + 4 * aq) * 4);
+        st_shared_v4(slot + 0u * 4096u + off, t0.x, t1.x, t2.x, t3.x);
+        st_shared_v4(slot + 1u * 4096u + off, t0.y, t1.y, t2.y, t3.y);
+        st_shared_v4(slot + 2u * 4096u + off, t0.z, t1.z, t2.z, t3.z);
+        st_shared_v4(slot + 3u * 4096u + off, t0.w, t1.w, t2.w, t3.w);
+      }
+      fence_proxy_async_smem();   // the bulk copies (async proxy) read these writes
+      named_bar(2, 64);
+      if (tt == 0) {
+        // channel q's 4 KB -> packets 16 crank .. +15 of CTA q's raw slot r
+        const uint32_t dst = raw_base + (uint32_t)r * kRawBytes + crank * 4096u;
+#pragma unroll
+        for (uint32_t q = 0; q < (uint32_t)kClusterCh; ++q)
+          bulk_s2s_cluster(cluster_map_u32(dst, q), slot + q * 4096u, 4096u,
+                           cluster_map(&rfull_bar[r], q));
+      }
     }
   } else if (FEED == 1 && warp == NW + 1) {
     // ------------------------------------------------------------ bulk loader

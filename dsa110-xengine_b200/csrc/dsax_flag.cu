@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   float mf[4];
   int mi[4];
   double bmax[4], bmin[4];
+  int bin_rows = 0;   // rows of the current bin seen so far (uniform per warp)
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     s[j] = 0; q[j] = 0; smark[j] = 0;
@@ -277,9 +278,11 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
         // the row's partial over this warp's channel groups
         for (int o = SP; o < 32; o <<= 1) rpart += __shfl_xor_sync(0xffffffffu, rpart, o);
         if (lane < SP && rr < rows) sm_rs[rr * NWS + warp] = rpart;
-        // the last row group of a TBIN bin: bin means per channel
-        const int tg = t0 + j0;
-        if ((tg + SP) % TB == 0 && tg < bend) {
+        // the last row group of a TBIN bin: bin means per channel (the
+        // chunk starts on a bin boundary; rows from bend on are in no bin)
+        bin_rows += SP;
+        if (bin_rows == TB && t0 + j0 < bend) {
+          bin_rows = 0;
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             double bs = (double)(s[j] - smark[j]);
@@ -644,27 +647,20 @@ __global__ void __launch_bounds__(flag::kApplyThreads) flag_apply_kernel(FlagArg
   while (L < nact && L < 32) L <<= 1;
   const int rpw = 32 / L, sub = lane & (L - 1);
   const E *xin = (a.spec0 && elem_out<E>(a)) ? elem_out<E>(a) : elem_in<E>(a);
-  for (int r0 = t_begin + warp * rpw; r0 < t_end; r0 += nw * rpw) {   // uniform per warp
-    const int t = r0 + lane / L;
+  // one listed chunk of one row: replace the flagged elements, return the
+  // correction to the row sum
+  auto fix_chunk = [&](uint4 &v, uint32_t m) -> double {
     double corr = 0.0;
-    if (t < t_end) {
-      const uint4 *row = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C);
-      uint4 *wrow = xw ? reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C) : nullptr;
-      for (int i = sub; i < nact; i += L) {
-        const uint32_t ce = chk[i];
-        const int k = (int)(ce & 0xFFFFu);
-        const uint32_t m = ce >> 16;
-        uint4 v = row[k];
-        E *ve = reinterpret_cast<E *>(&v);
+    E *ve = reinterpret_cast<E *>(&v);
 #pragma unroll
-        for (int e = 0; e < EPC; ++e)
-          if ((m >> e) & 1u) {
-            corr += (double)(rf - (float)ve[e]);
-            ve[e] = re;
-          }
-        if (wrow) wrow[k] = v;
+    for (int e = 0; e < EPC; ++e)
+      if ((m >> e) & 1u) {
+        corr += (double)(rf - (float)ve[e]);
+        ve[e] = re;
       }
-    }
+    return corr;
+  };
+  auto finish_row = [&](int t, double corr) {
     for (int o = L >> 1; o > 0; o >>= 1) corr += __shfl_xor_sync(0xffffffffu, corr, o);
     if (t < t_end && sub == 0) {
       double rsum;
@@ -675,6 +671,50 @@ __global__ void __launch_bounds__(flag::kApplyThreads) flag_apply_kernel(FlagArg
         for (int s = 0; s < a.nslab; ++s) rsum += a.rowsum[((int64_t)b * a.nslab + s) * T + t];
       }
       a.ts[(int64_t)b * T + t] = (float)((rsum + corr) / C);
+    }
+  };
+  if (nact <= 32) {
+    // at most one chunk per lane and row: four row groups' loads in flight
+    // per lane before any is used
+    constexpr int kB = 4;
+    const uint32_t ce = sub < nact ? chk[sub] : 0u;
+    const int k = (int)(ce & 0xFFFFu);
+    const uint32_t m = ce >> 16;
+    for (int r0 = t_begin + warp * rpw; r0 < t_end; r0 += kB * nw * rpw) {   // uniform per warp
+      uint4 v[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int t = r0 + u * nw * rpw + lane / L;
+        v[u] = make_uint4(0u, 0u, 0u, 0u);
+        if (t < t_end && sub < nact)
+          v[u] = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C)[k];
+      }
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const int t = r0 + u * nw * rpw + lane / L;
+        double corr = 0.0;
+        if (t < t_end && sub < nact) {
+          corr = fix_chunk(v[u], m);
+          if (xw) reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C)[k] = v[u];
+        }
+        finish_row(t, corr);
+      }
+    }
+  } else {
+    for (int r0 = t_begin + warp * rpw; r0 < t_end; r0 += nw * rpw) {   // uniform per warp
+      const int t = r0 + lane / L;
+      double corr = 0.0;
+      if (t < t_end) {
+        const uint4 *row = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C);
+        uint4 *wrow = xw ? reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C) : nullptr;
+        for (int i = sub; i < nact; i += L) {
+          const uint32_t ce = chk[i];
+          uint4 v = row[ce & 0xFFFFu];
+          corr += fix_chunk(v, ce >> 16);
+          if (wrow) wrow[ce & 0xFFFFu] = v;
+        }
+      }
+      finish_row(t, corr);
     }
   }
   // the beam's last CTA makes the time-series decisions

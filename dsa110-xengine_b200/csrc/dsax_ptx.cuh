@@ -295,14 +295,14 @@ __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_bar) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar)
                : "memory");
 }
-// 16 bytes into another CTA's shared memory, counted as transaction bytes
-// on that CTA's mbarrier.
-__device__ __forceinline__ void st_async_v4(uint32_t cluster_dst, uint32_t a, uint32_t b, uint32_t c,
-                                            uint32_t d, uint32_t cluster_bar) {
+// Bulk copy from this CTA's shared memory into another CTA's of the cluster
+// (no multicast), counted as transaction bytes on that CTA's mbarrier.
+__device__ __forceinline__ void bulk_s2s_cluster(uint32_t cluster_dst, uint32_t src, uint32_t bytes,
+                                                 uint32_t cluster_bar) {
   asm volatile(
-      "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+      "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
           cluster_dst),
-      "r"(a), "r"(b), "r"(c), "r"(d), "r"(cluster_bar)
+      "r"(src), "r"(bytes), "r"(cluster_bar)
       : "memory");
 }
 

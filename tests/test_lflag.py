@@ -215,7 +215,7 @@ def test_training_reaches_plain_flagger_masks(dsax, oracle):
     with dsax.Context(dsax.default_config(npkt=16, nchan=8)) as ctx:
         ctx.lf_init(7)
         untrained = [LO.prf1(*lflag.evaluate(ctx, xb, tds)) for xb in test_blocks]
-        losses = lflag.train(ctx, train_blocks, steps=1000, beams_per_step=16, tds=tds)
+        losses = lflag.train(ctx, train_blocks, steps=2000, beams_per_step=16, tds=tds)
         print("loss first/last", losses[0], losses[-1])
         trained = [LO.prf1(*lflag.evaluate(ctx, xb, tds)) for xb in test_blocks]
         # threshold rule on one feature (no learning): best over features and cuts
