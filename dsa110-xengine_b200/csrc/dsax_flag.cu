@@ -24,6 +24,7 @@
 
 #include "dsax_internal.h"
 #include "dsax_ptx.cuh"
+#include "dsax_scaley.h"
 #include "../../include/dsax.h"
 
 namespace dsax {
@@ -178,11 +179,13 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   double *sm_fin = sm_rs + RS * NWS;                                   // [5][cs]
   double *sm_k = sm_fin + 5 * cs;                                      // [cs]
   float *sm_s0 = reinterpret_cast<float *>(sm_k + cs);                 // [cs]
+  float *sm_k2 = sm_s0 + cs;                                           // [cs] float(2k)
 
   if (scale)
     for (int c = tid; c < cs; c += flag::kStatThreads) {
       sm_s0[c] = a.spec0[b * C + c0 + c];
       sm_k[c] = (double)a.sig / (double)sqrtf(a.var0[b * C + c0 + c]);
+      sm_k2[c] = (float)(2.0 * sm_k[c]);
     }
   __syncthreads();
 
@@ -241,8 +244,8 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
               float v[4];
 #pragma unroll
               for (int j = 0; j < 4; ++j)
-                v[j] = scaley1<E>((float)((w >> (8 * j)) & 255u), sm_s0[4 * g + j], sm_k[4 * g + j],
-                                  a.mn);
+                v[j] = scaley_u8((float)((w >> (8 * j)) & 255u), sm_s0[4 * g + j], sm_k2[4 * g + j],
+                                 sm_k[4 * g + j], a.mn);
               st4<E>(&w, v);
               if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
             }
@@ -864,7 +867,7 @@ static bool stat_geom(const FlagArgs &a, int es, StatGeom &gm) {
   if (kc < 1) return false;
   const int nws = ((G4 * sp + 31) / 32) | 1;
   const size_t stats = (size_t)flag::kStages * rs * rp +
-                       sizeof(double) * ((size_t)rs * nws + 6 * (size_t)cs) + sizeof(float) * cs;
+                       sizeof(double) * ((size_t)rs * nws + 6 * (size_t)cs) + sizeof(float) * 2 * cs;
   // the channel decisions reuse the buffer: 12 nchan floats + nchan bytes
   const size_t dec = a.decide ? sizeof(float) * 12 * (size_t)a.nchan + a.nchan : 0;
   gm.sp = sp;
