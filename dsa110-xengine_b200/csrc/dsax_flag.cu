@@ -189,14 +189,24 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     }
   __syncthreads();
 
+  const int ir0 = tid / ck, ik0 = tid - ir0 * ck;
+  const int idr = flag::kStatThreads / ck, idk = flag::kStatThreads - idr * ck;
   auto issue = [&](int st) {
     if (st < nst) {
       const int t0 = r0 + st * RS, rows = min(RS, r1 - t0);
       const uint8_t *src = xb + (int64_t)t0 * rstride;
       const uint32_t dst = sbase + (uint32_t)(st % S) * (uint32_t)(RS * RP);
-      for (int i = tid; i < rows * ck; i += flag::kStatThreads) {
-        const int r = i / ck, k = i - r * ck;
+      // chunk i = tid + 256 n of the stage: (row, 16-byte chunk) stepped
+      // without divisions
+      int r = ir0, k = ik0;
+      while (r < rows) {
         cp_async16(dst + r * RP + 16 * k, src + r * rstride + 16 * k);
+        r += idr;
+        k += idk;
+        if (k >= ck) {
+          k -= ck;
+          ++r;
+        }
       }
     }
     cp_async_commit();
@@ -208,18 +218,22 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
       a.rowsum[((int64_t)b * a.nslab + slab) * T + t] = (float)r;
   };
 
-  // per-thread column partials over its rows: FP64 for FP32 data; for
-  // uint8 32-bit integers (at most 32768 rows per thread, checked by the
-  // launcher: 32768 * 255^2 < 2^31) and a bin mark
+  // Per-thread column partials over its rows.  uint8: exact 32-bit
+  // integers (at most 32768 rows per thread, which the launcher enforces:
+  // 32768 * 255^2 < 2^31).  FP32: the rows of one stage (at most rs / sp)
+  // in FP32, folded into FP64 totals at the end of every stage.  Bin sums
+  // are differences of the running totals at bin ends (mark).
   using Acc = typename std::conditional<kU8, int, double>::type;
   Acc s[4], q[4], smark[4];
-  float mf[4];
+  float sf[4], qf[4], mf[4];
   int mi[4];
   double bmax[4], bmin[4];
   int bin_rows = 0;   // rows of the current bin seen so far (uniform per warp)
+  const double inv_tb = 1.0 / TB;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     s[j] = 0; q[j] = 0; smark[j] = 0;
+    sf[j] = 0.f; qf[j] = 0.f;
     mf[j] = -INFINITY; mi[j] = -1;
     bmax[j] = -1e300; bmin[j] = 1e300;
   }
@@ -258,7 +272,7 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
               mi[j] = max(mi[j], x);
               r += x;
             }
-            rpart = (double)r;
+            rpart = (double)r;   // exact
           } else {
             float v[4];
             ld4<E>(src, v);
@@ -271,11 +285,11 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-              s[j] += (double)v[j];
-              q[j] += (double)v[j] * v[j];
+              sf[j] += v[j];
+              qf[j] = fmaf(v[j], v[j], qf[j]);
               mf[j] = fmaxf(mf[j], v[j]);
-              rpart += (double)v[j];
             }
+            rpart = (double)((v[0] + v[1]) + (v[2] + v[3]));
           }
         }
         // the row's partial over this warp's channel groups
@@ -288,13 +302,29 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
           bin_rows = 0;
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            double bs = (double)(s[j] - smark[j]);
-            smark[j] = s[j];
+            double bs;
+            if constexpr (kU8) {
+              bs = (double)(s[j] - smark[j]);
+              smark[j] = s[j];
+            } else {
+              const double cur = s[j] + (double)sf[j];
+              bs = cur - smark[j];
+              smark[j] = cur;
+            }
             for (int o = 1; o < SP; o <<= 1) bs += __shfl_xor_sync(0xffffffffu, bs, o);
-            const double mb = bs / TB;
+            const double mb = bs * inv_tb;
             bmax[j] = fmax(bmax[j], mb);
             bmin[j] = fmin(bmin[j], mb);
           }
+        }
+      }
+      if constexpr (!kU8) {   // fold the stage's FP32 partials into the totals
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          s[j] += (double)sf[j];
+          q[j] += (double)qf[j];
+          sf[j] = 0.f;
+          qf[j] = 0.f;
         }
       }
     }
@@ -825,9 +855,11 @@ static int gcd_int(int x, int y) {
 }
 
 // Chunks per slab: the cluster size (1, 2, 4 or 8) whose grid fills the
-// device's CTA slots (two per SM) best, the smallest within 2 % of the best;
-// uint8 needs at most 32768 rows per thread (32-bit integer partials).
-static int stat_chunks(const FlagArgs &a, int sp, bool u8) {
+// device's CTA slots (two per SM) best, the smallest within 2 % of the best,
+// among those that leave every chunk at least 16 stages (the ring's fill
+// and the cross-chunk combine are per-CTA costs); uint8 needs at most 32768
+// rows per thread (32-bit integer partials).
+static int stat_chunks(const FlagArgs &a, int sp, int rs, bool u8) {
   int dev = 0, nsm = 148;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -842,6 +874,7 @@ static int stat_chunks(const FlagArgs &a, int sp, bool u8) {
     if (k > 1 && k > nbins) break;
     const int64_t rows = (int64_t)((nbins + k - 1) / k) * a.tbin + a.tbin;   // + tail rows
     if (u8 && rows / sp > 32768) continue;
+    if (k > 1 && rows < (int64_t)16 * rs) continue;   // keep the ring busy: >= 16 stages
     const double w = base * k / slots;
     eff[i] = w / ceil(w);
     if (eff[i] > best) best = eff[i];
@@ -863,7 +896,7 @@ static bool stat_geom(const FlagArgs &a, int es, StatGeom &gm) {
   if (rs < unit) rs = unit;
   FlagArgs t = a;
   t.nslab = (a.nchan + kFlagSlab - 1) / kFlagSlab;
-  const int kc = stat_chunks(t, sp, es == 1);
+  const int kc = stat_chunks(t, sp, rs, es == 1);
   if (kc < 1) return false;
   const int nws = ((G4 * sp + 31) / 32) | 1;
   const size_t stats = (size_t)flag::kStages * rs * rp +
