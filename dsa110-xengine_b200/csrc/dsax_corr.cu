@@ -339,16 +339,9 @@ template <int FEED> constexpr int raw_stages() { return FEED == 2 ? 3 : 4; }
 template <int FEED, int NW> constexpr int threads() {
   return 32 * NW + 32 + (FEED == 1 ? 32 : FEED == 2 ? 128 : 0);
 }
-// epilogue: C^T of one time slot (64 KB) and that slot's triangle (2080
-// baselines x 4 products x re/im FP32 = 66,560 bytes, the output layout)
-constexpr int kTriBytes = 2080 * 32;
-constexpr int kEpiBytes = 128 * 128 * 4 + kTriBytes;
-template <int FEED> constexpr int pipe_bytes() {
-  return kOpStages * kStageBytes + (FEED >= 1 ? raw_stages<FEED>() * kRawBytes : 0) +
-         (FEED == 2 ? raw_stages<FEED>() * kLandBytes : 0);
-}
 template <int FEED> constexpr int smem_bytes() {
-  return 1024 + (pipe_bytes<FEED>() > kEpiBytes ? pipe_bytes<FEED>() : kEpiBytes);
+  return 1024 + kOpStages * kStageBytes + (FEED >= 1 ? raw_stages<FEED>() * kRawBytes : 0) +
+         (FEED == 2 ? raw_stages<FEED>() * kLandBytes : 0);
 }
 constexpr uint32_t kIdescN128 = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 128);
 static_assert(kOpStages * kStageBytes >= 2 * 128 * 128 * 4, "C^T scratch reuses the stages");
@@ -382,7 +375,6 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   __shared__ __align__(8) uint64_t dest_free[kRawStages]; // FEED 2: slot consumed in all 4 CTAs
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
-  __shared__ volatile int epi_bad_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ch = blockIdx.x;
@@ -411,7 +403,6 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
       }
     }
     abort_sh = 0;
-    epi_bad_sh = 0;
     mbar_fence_init();
   }
   if (warp == NW) {
@@ -731,79 +722,61 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   }
 
   // ---------------------------------------------------------------- epilogue
-  // One time slot at a time (every MMA has completed, so the pipeline's
-  // shared memory is free): C^T into shared memory (row m of C at word
-  // (col ^ (m & 31)) of a 512-byte row), then the slot's lower triangle in
-  // the output layout into a staging buffer, then one bulk store (a bulk
-  // FP32 add in accumulate mode; every value is an integer below 2^24, so
-  // the sum is exact) of its 66,560 contiguous bytes.  Warp (q, h): TMEM
-  // lane quadrant q = warp % 4, column blocks h, h + NH, ...
   if (warp < NW) {
     bool ok = mbar_wait_bounded(&accum_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
                                 a.wait_limit_ns);
     tc_fence_after();
     ok = __all_sync(0xffffffffu, ok && !abort_sh);
-    // one verdict for all epilogue warps (tid 0 issues the bulk stores)
-    if (!ok && lane == 0) epi_bad_sh = 1;
-    named_bar(1, kUnpackThreads);
-    ok = epi_bad_sh == 0;
-    constexpr int NH = NW / 4;
-    const int q = warp & 3, h = warp >> 2;
+    // TMEM lane quadrant q (warp % 4), time slot t; with NW = 16 the two
+    // warps of each (q, t) take alternate column blocks (hh)
+    constexpr int kCbStep = NW / 8;
+    const int q = warp & 3, t = (warp >> 2) & 1, hh = warp >> 3;
     const int m = 32 * q + lane;                   // row = 2 * antenna + pol
-    const int i = m >> 1, pi = m & 1;
-    const int tri = i * (i + 1) / 2;
-    const int ncb = 2 * q + 2;
-    uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase);
-    const uint32_t stg = sbase + 128u * 128u * 4u;
-    for (int t = 0; t < 2; ++t) {
-      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
-      if (ok) {
+    const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
+    // C^T through shared memory (every MMA has completed, so the operand
+    // stages are free): row m of C at word (col ^ (m & 31)) of a 512-byte row.
+    uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase + t * (128 * 128 * 4));
+    if (ok) {
 #pragma unroll
-        for (int cb = h; cb < 8; cb += NH) {
-          uint32_t cv[16];
-          tmem_ld16(trow + 128u + 16u * cb, cv);
-          tmem_wait_ld();
+      for (int cb = hh; cb < 8; cb += kCbStep) {
+        uint32_t cv[16];
+        tmem_ld16(trow + 128u + 16u * cb, cv);
+        tmem_wait_ld();
 #pragma unroll
-          for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
-        }
+        for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
       }
-      // the previous slot's bulk store has read the staging buffer
-      if (t == 1 && tid == 0 && ok) bulk_wait_read_all();
-      named_bar(1, kUnpackThreads);
-      if (ok) {
-        for (int cb = h; cb < ncb; cb += NH) {
-          uint32_t re[16], cr[16];
-          tmem_ld16(trow + 16u * cb, re);
-          tmem_ld16(trow + 128u + 16u * cb, cr);
-          tmem_wait_ld();
+    }
+    named_bar(1, kUnpackThreads);
+    if (ok) {
+      const int i = m >> 1, pi = m & 1;
+      float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
+      const int64_t tri = (int64_t)i * (i + 1) / 2;
+      const int ncb = 2 * q + 2;
+      for (int cb = hh; cb < ncb; cb += kCbStep) {
+        uint32_t re[16], cr[16];
+        tmem_ld16(trow + 16u * cb, re);
+        tmem_ld16(trow + 128u + 16u * cb, cr);
+        tmem_wait_ld();
 #pragma unroll
-          for (int jj = 0; jj < 8; ++jj) {
-            const int j = 8 * cb + jj;
-            if (j <= i) {
-              const int b0 = 2 * j, b1 = 2 * j + 1;
-              const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
-              const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
-              st_shared_v4(stg + (uint32_t)(((tri + j) * 4 + 2 * pi) * 8),
-                           __float_as_uint((float)(int32_t)re[2 * jj]),
-                           __float_as_uint((float)((int32_t)cr[2 * jj] - ct0)),
-                           __float_as_uint((float)(int32_t)re[2 * jj + 1]),
-                           __float_as_uint((float)((int32_t)cr[2 * jj + 1] - ct1)));
+        for (int jj = 0; jj < 8; ++jj) {
+          const int j = 8 * cb + jj;
+          if (j <= i) {
+            const int b0 = 2 * j, b1 = 2 * j + 1;
+            const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
+            const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
+            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)((int32_t)cr[2 * jj] - ct0),
+                                   (float)(int32_t)re[2 * jj + 1],
+                                   (float)((int32_t)cr[2 * jj + 1] - ct1));
+            float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
+            if (a.accumulate) {
+              const float4 old = *dst;
+              o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
             }
+            *dst = o;
           }
         }
       }
-      fence_proxy_async_smem();   // the bulk store (async proxy) reads the staging buffer
-      named_bar(1, kUnpackThreads);
-      if (tid == 0 && ok) {
-        float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
-        if (a.accumulate)
-          bulk_s2g_add_f32(vis, stg, (uint32_t)kTriBytes);
-        else
-          bulk_s2g(vis, stg, (uint32_t)kTriBytes);
-        bulk_commit_group();
-      }
     }
-    if (tid == 0 && ok) bulk_wait_all();   // the stores are complete before the CTA exits
   }
   tc_fence_before();
   __syncthreads();

@@ -113,73 +113,51 @@ __device__ void flag_decide_beam(const FlagArgs &a, int b, uint8_t *smem);
 __device__ void flag_total_power(const FlagArgs &a);
 
 // ---------------------------------------------------------------- statistics
-// The same shared-memory variable in CTA `rank` of this CTA's cluster.
-__device__ __forceinline__ double ld_cluster_f64(const double *p, uint32_t rank) {
-  const uint32_t r = cluster_map(p, rank);
-  double v;
-  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(r) : "memory");
-  return v;
-}
-
-// Grid (slab x chunk, beam) in clusters of kc CTAs along x: the CTA of
-// chunk k (its rank in the cluster) streams the rows of the k-th run of
-// whole TBIN bins of its beam's channel slab (<= kFlagSlab channels; the
-// last chunk also takes the rows after the last whole bin) through a
-// three-stage cp.async ring of rs rows each.  Rows sit rp bytes apart in
-// shared memory, an odd number of 16-byte units, so that consecutive rows
-// fall in different bank groups.  Thread tid = g * sp + p (sp, a power of
-// two dividing TBIN and 32) owns channels 4g..4g+3 and rows p, p + sp, ...
-// of every stage: the sp threads of a channel group are lanes of one warp,
-// so the bin sums and the column totals reduce with shuffles, and so do a
-// row's partial sums over the channel groups of a warp (one shared-memory
-// entry per warp and row, summed by one thread per row).  FP32 data
-// accumulate in FP64, uint8 data in exact integers.  With a scaley baseline
-// every value is normalised as it is read (and written to xw; the
-// statistics then describe the normalised block, as in the reference).
+// One CTA per (channel slab of up to kFlagSlab channels, beam).  The slab's
+// rows stream through a three-stage cp.async ring of `rs` rows each (rs
+// divides TBIN).  Thread (p, g) owns channels 4g..4g+3 of the slab and rows
+// p, p + P, ... of every stage (the lanes of a warp cover consecutive
+// 16-byte pieces of a row: conflict-free shared reads, coalesced global
+// writes); sums are FP64 for FP32 data and 32-bit integers for uint8 (at
+// most 32768 rows per thread, so 255^2 products stay below 2^31; the
+// launcher checks it), finished in shared memory in a fixed order (four
+// interleaved partial sums per reduction), so results do not depend on
+// scheduling.  With a scaley
+// baseline the stage is normalised in shared memory first and written back
+// (the statistics then describe the normalised block, as in the reference).
 // Per row the slab's raw sum goes to rowsum (or to ts when there is one
 // slab); flag_apply_kernel turns it into the channel-mean series after the
-// flagged columns are replaced.  At the end the cluster's CTAs combine
-// their column partials in chunk order through distributed shared memory,
-// and rank 0 writes the statistics and goes on to the decisions.
+// flagged columns are replaced.
 template <typename E>
 __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagArgs a) {
   constexpr int S = flag::kStages;
   constexpr int ES = (int)sizeof(E);
-  constexpr bool kU8 = std::is_same<E, uint8_t>::value;
-  const int KC = a.kc;
-  const int slab = blockIdx.x / KC, b = blockIdx.y;
-  const int kc = KC > 1 ? (int)cluster_ctarank() : 0;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int T = a.ntime, C = a.nchan, TB = a.tbin, RS = a.rs, SP = a.sp;
+  const int slab = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
+  const int T = a.ntime, C = a.nchan, TB = a.tbin, RS = a.rs;
   const int c0 = slab * kFlagSlab;
   const int cs = min(kFlagSlab, C - c0);
-  const int G4 = cs >> 2;
-  const int g = tid / SP, p = tid - g * SP;
-  const bool active = g < G4;
-  const int nwa = (G4 * SP + 31) >> 5;         // warps holding active threads
-  const int NWS = nwa | 1;                      // odd stride of the row partials
-  const int rb = cs * ES, ck = rb >> 4;         // bytes and 16-byte chunks of a slab row
-  const int RP = (ck | 1) << 4;                 // row pitch in shared memory
+  const int G4 = cs >> 2, P = flag::kStatThreads / G4;
+  const int p = tid / G4, g = tid - p * G4;
+  const bool active = p < P;
+  const int nbins = T / TB, spb = TB / RS, nst = nbins * spb;
+  const int rb = cs * ES;                        // bytes of one slab row (multiple of 16)
+  const int ck = rb >> 4;                        // 16-byte chunks per row
+  const int stage_bytes = (RS * rb + 127) & ~127;
   const int64_t rstride = (int64_t)C * ES;
   const uint8_t *xb =
       reinterpret_cast<const uint8_t *>(elem_in<E>(a) + (int64_t)b * T * C + c0);
   E *xw = elem_out<E>(a);
   const bool scale = a.spec0 != nullptr;
-  // this chunk's rows
-  const int nbins = T / TB;
-  const int per = (nbins + KC - 1) / KC;
-  const int bin0 = min(nbins, kc * per), bin1 = min(nbins, bin0 + per);
-  const int r0 = bin0 * TB, r1 = (kc == KC - 1) ? T : bin1 * TB;
-  const int bend = nbins * TB;                  // rows from here on are in no bin
-  const int nst = (r1 - r0 + RS - 1) / RS;
 
   extern __shared__ __align__(16) uint8_t fs_raw[];
   const uint32_t sbase = smem_u32(fs_raw);
-  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * RS * RP);   // [RS][NWS]
-  double *sm_fin = sm_rs + RS * NWS;                                   // [5][cs]
-  double *sm_k = sm_fin + 5 * cs;                                      // [cs]
-  float *sm_s0 = reinterpret_cast<float *>(sm_k + cs);                 // [cs]
-  float *sm_k2 = sm_s0 + cs;                                           // [cs] float(2k)
+  const int GS = G4 | 1;   // odd row stride: the row sums read column-wise conflict-free
+  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * stage_bytes);   // [RS][GS]
+  double *sm_bp = sm_rs + RS * GS;                                         // [P][cs]
+  double *sm_k = sm_bp + P * cs;                                           // [cs]
+  float *sm_s0 = reinterpret_cast<float *>(sm_k + cs);                     // [cs]
+  float *sm_k2 = sm_s0 + cs;                                               // [cs] float(2k)
+  const double inv_tb = 1.0 / TB;
 
   if (scale)
     for (int c = tid; c < cs; c += flag::kStatThreads) {
@@ -188,25 +166,27 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
       sm_k2[c] = (float)(2.0 * sm_k[c]);
     }
   __syncthreads();
+  // sum of n doubles at v[0], v[stride], ... in four interleaved chains
+  auto sum4 = [](const double *v, int n, int stride) -> double {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int k = 0;
+    for (; k + 4 <= n; k += 4) {
+      a0 += v[k * stride];
+      a1 += v[(k + 1) * stride];
+      a2 += v[(k + 2) * stride];
+      a3 += v[(k + 3) * stride];
+    }
+    for (; k < n; ++k) a0 += v[k * stride];
+    return (a0 + a1) + (a2 + a3);
+  };
 
-  const int ir0 = tid / ck, ik0 = tid - ir0 * ck;
-  const int idr = flag::kStatThreads / ck, idk = flag::kStatThreads - idr * ck;
   auto issue = [&](int st) {
     if (st < nst) {
-      const int t0 = r0 + st * RS, rows = min(RS, r1 - t0);
-      const uint8_t *src = xb + (int64_t)t0 * rstride;
-      const uint32_t dst = sbase + (uint32_t)(st % S) * (uint32_t)(RS * RP);
-      // chunk i = tid + 256 n of the stage: (row, 16-byte chunk) stepped
-      // without divisions
-      int r = ir0, k = ik0;
-      while (r < rows) {
-        cp_async16(dst + r * RP + 16 * k, src + r * rstride + 16 * k);
-        r += idr;
-        k += idk;
-        if (k >= ck) {
-          k -= ck;
-          ++r;
-        }
+      const uint8_t *src = xb + (int64_t)st * RS * rstride;
+      const uint32_t dst = sbase + (uint32_t)(st % S) * stage_bytes;
+      for (int i = tid; i < RS * ck; i += flag::kStatThreads) {
+        const int r = i / ck, k = i - r * ck;
+        cp_async16(dst + r * rb + 16 * k, src + r * rstride + 16 * k);
       }
     }
     cp_async_commit();
@@ -217,26 +197,60 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     else
       a.rowsum[((int64_t)b * a.nslab + slab) * T + t] = (float)r;
   };
-
-  // Per-thread column partials over its rows.  uint8: exact 32-bit
-  // integers (at most 32768 rows per thread, which the launcher enforces:
-  // 32768 * 255^2 < 2^31).  FP32: the rows of one stage (at most rs / sp)
-  // in FP32, folded into FP64 totals at the end of every stage.  Bin sums
-  // are differences of the running totals at bin ends (mark).
+  // normalise (if scaling) and accumulate the four channels of one row:
+  // FP64 for FP32 data, exact 32-bit integers for uint8 (no FP64 work)
+  constexpr bool kU8 = std::is_same<E, uint8_t>::value;
   using Acc = typename std::conditional<kU8, int, double>::type;
-  Acc s[4], q[4], smark[4];
-  float sf[4], qf[4], mf[4];
-  int mi[4];
-  double bmax[4], bmin[4];
-  int bin_rows = 0;   // rows of the current bin seen so far (uniform per warp)
-  const double inv_tb = 1.0 / TB;
+  Acc s[4], q[4], bs[4];
+  float m[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    s[j] = 0; q[j] = 0; smark[j] = 0;
-    sf[j] = 0.f; qf[j] = 0.f;
-    mf[j] = -INFINITY; mi[j] = -1;
-    bmax[j] = -1e300; bmin[j] = 1e300;
+    s[j] = 0; q[j] = 0; bs[j] = 0;
+    m[j] = kU8 ? 0.0f : -INFINITY;
   }
+  auto take = [&](uint8_t *src, int t, bool bin, bool keep) -> double {
+    float v[4];
+    if constexpr (kU8) {
+      uint32_t w = *reinterpret_cast<const uint32_t *>(src);
+      if (scale) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          v[j] = scaley_u8((float)((w >> (8 * j)) & 255u), sm_s0[4 * g + j], sm_k2[4 * g + j],
+                           sm_k[4 * g + j], a.mn);
+        st4<E>(&w, v);
+        if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
+      }
+      int r = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int x = (int)((w >> (8 * j)) & 255u);
+        if (bin) bs[j] += x; else s[j] += x;
+        q[j] += x * x;
+        m[j] = fmaxf(m[j], (float)x);
+        r += x;
+      }
+      return (double)r;
+    } else {
+      ld4<E>(src, v);
+      if (scale) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          v[j] = scaley1<E>(v[j], sm_s0[4 * g + j], sm_k[4 * g + j], a.mn);
+        if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
+        if (keep) st4<E>(src, v);   // the pixel sums read the normalised stage
+      }
+      double r = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (bin) bs[j] += v[j]; else s[j] += v[j];
+        q[j] += (double)v[j] * v[j];
+        m[j] = fmaxf(m[j], v[j]);
+        r += v[j];
+      }
+      return r;
+    }
+  };
+  double bmax = -1e300, bmin = 1e300;   // owned by thread tid < cs (channel tid)
 
 #pragma unroll
   for (int i = 0; i < S - 1; ++i) issue(i);
@@ -244,99 +258,31 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     issue(st + S - 1);
     cp_async_wait<S - 1>();
     __syncthreads();
-    uint8_t *sp = fs_raw + (st % S) * RS * RP;
-    const int t0 = r0 + st * RS, rows = min(RS, r1 - t0);
-    if (warp < nwa) {
-      for (int j0 = 0; j0 < rows; j0 += SP) {   // row group j0 .. j0 + SP - 1 (uniform)
-        const int rr = j0 + p, t = t0 + rr;
-        double rpart = 0.0;
-        if (active && rr < rows) {
-          uint8_t *src = sp + rr * RP + 4 * g * ES;
-          if constexpr (kU8) {
-            uint32_t w = *reinterpret_cast<const uint32_t *>(src);
-            if (scale) {
-              float v[4];
-#pragma unroll
-              for (int j = 0; j < 4; ++j)
-                v[j] = scaley_u8((float)((w >> (8 * j)) & 255u), sm_s0[4 * g + j], sm_k2[4 * g + j],
-                                 sm_k[4 * g + j], a.mn);
-              st4<E>(&w, v);
-              if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
-            }
-            int r = 0;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const int x = (int)((w >> (8 * j)) & 255u);
-              s[j] += x;
-              q[j] += x * x;
-              mi[j] = max(mi[j], x);
-              r += x;
-            }
-            rpart = (double)r;   // exact
-          } else {
-            float v[4];
-            ld4<E>(src, v);
-            if (scale) {
-#pragma unroll
-              for (int j = 0; j < 4; ++j)
-                v[j] = scaley1<E>(v[j], sm_s0[4 * g + j], sm_k[4 * g + j], a.mn);
-              if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
-              if (a.pix_sum) st4<E>(src, v);   // the pixel sums read the normalised stage
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              sf[j] += v[j];
-              qf[j] = fmaf(v[j], v[j], qf[j]);
-              mf[j] = fmaxf(mf[j], v[j]);
-            }
-            rpart = (double)((v[0] + v[1]) + (v[2] + v[3]));
-          }
-        }
-        // the row's partial over this warp's channel groups
-        for (int o = SP; o < 32; o <<= 1) rpart += __shfl_xor_sync(0xffffffffu, rpart, o);
-        if (lane < SP && rr < rows) sm_rs[rr * NWS + warp] = rpart;
-        // the last row group of a TBIN bin: bin means per channel (the
-        // chunk starts on a bin boundary; rows from bend on are in no bin)
-        bin_rows += SP;
-        if (bin_rows == TB && t0 + j0 < bend) {
-          bin_rows = 0;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            double bs;
-            if constexpr (kU8) {
-              bs = (double)(s[j] - smark[j]);
-              smark[j] = s[j];
-            } else {
-              const double cur = s[j] + (double)sf[j];
-              bs = cur - smark[j];
-              smark[j] = cur;
-            }
-            for (int o = 1; o < SP; o <<= 1) bs += __shfl_xor_sync(0xffffffffu, bs, o);
-            const double mb = bs * inv_tb;
-            bmax[j] = fmax(bmax[j], mb);
-            bmin[j] = fmin(bmin[j], mb);
-          }
-        }
-      }
-      if constexpr (!kU8) {   // fold the stage's FP32 partials into the totals
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          s[j] += (double)sf[j];
-          q[j] += (double)qf[j];
-          sf[j] = 0.f;
-          qf[j] = 0.f;
-        }
+    uint8_t *sp = fs_raw + (st % S) * stage_bytes;
+    const int t0 = st * RS;
+    if (active) {
+      for (int r = p; r < RS; r += P) {
+        sm_rs[r * GS + g] = take(sp + r * rb + 4 * g * ES, t0 + r, true, a.pix_sum != nullptr);
       }
     }
-    __syncthreads();
+    const bool bin_end = (st + 1) % spb == 0;
+    if (spb == 1 && active) {   // one stage per bin: its partials go out with the rows
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        sm_bp[p * cs + 4 * g + j] = (double)bs[j];
+        s[j] += bs[j];
+        bs[j] = 0;
+      }
+    }
     if (a.pix_sum) {   // downsampled spectrogram: rs / tds whole pixel rows per stage
+      __syncthreads();
       const float *sf = reinterpret_cast<const float *>(sp);
-      const int npr = rows / a.tds, H = T / a.tds;
+      const int npr = RS / a.tds, H = T / a.tds;
       for (int i = tid; i < npr * cs; i += flag::kStatThreads) {
         const int pr = i / cs, c = i - pr * cs;
         float sum = 0.f, mx = -INFINITY;
         for (int r = 0; r < a.tds; ++r) {
-          const float v = sf[(pr * a.tds + r) * (RP / 4) + c];
+          const float v = sf[(pr * a.tds + r) * cs + c];
           sum += v;
           mx = fmaxf(mx, v);
         }
@@ -345,65 +291,73 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
         a.pix_max[o] = mx;
       }
     }
-    for (int r = tid; r < rows; r += flag::kStatThreads) {
-      double v = 0.0;
-      for (int k = 0; k < nwa; ++k) v += sm_rs[r * NWS + k];
-      put_row(t0 + r, v);
+    __syncthreads();
+    if (tid < RS) put_row(t0 + tid, sum4(sm_rs + tid * GS, G4, 1));
+    if (bin_end) {   // the last stage of a TBIN bin: bin means per channel
+      if (spb > 1) {
+        if (active) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            sm_bp[p * cs + 4 * g + j] = (double)bs[j];
+            s[j] += bs[j];
+            bs[j] = 0;
+          }
+        }
+        __syncthreads();
+      }
+      if (tid < cs) {
+        const double mb = sum4(sm_bp + tid, P, cs) * inv_tb;
+        bmax = fmax(bmax, mb);
+        bmin = fmin(bmin, mb);
+      }
     }
   }
   cp_async_wait<0>();
-
-  // column totals of the chunk: reduce over the sp lanes of each group
-  if (warp < nwa) {
+  // rows beyond the last whole bin (T % TB): sums, squares, max and row
+  // sums, read directly
+  for (int t0 = nbins * TB; t0 < T; t0 += RS) {
+    __syncthreads();
+    const int rows = min(RS, T - t0);
+    if (active) {
+      for (int r = p; r < rows; r += P)
+        sm_rs[r * GS + g] = take(const_cast<uint8_t *>(xb) + (int64_t)(t0 + r) * rstride + 4 * g * ES,
+                                 t0 + r, false, false);
+    }
+    __syncthreads();
+    if (tid < rows) put_row(t0 + tid, sum4(sm_rs + tid * GS, G4, 1));
+  }
+  // per-channel totals over the P row phases, in phase order
+  double tot[3] = {0.0, 0.0, -INFINITY};
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      double sv = (double)s[j], qv = (double)q[j];
-      double mv = kU8 ? (double)mi[j] : (double)mf[j];
-      double hi = bmax[j], lo = bmin[j];
-      for (int o = 1; o < SP; o <<= 1) {
-        sv += __shfl_xor_sync(0xffffffffu, sv, o);
-        qv += __shfl_xor_sync(0xffffffffu, qv, o);
-        mv = fmax(mv, __shfl_xor_sync(0xffffffffu, mv, o));
-        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      }
-      if (active && p == 0) {
-        const int c = 4 * g + j;
-        sm_fin[c] = sv;
-        sm_fin[cs + c] = qv;
-        sm_fin[2 * cs + c] = mv;
-        sm_fin[3 * cs + c] = hi;
-        sm_fin[4 * cs + c] = lo;
+  for (int pass = 0; pass < 3; ++pass) {
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        sm_bp[p * cs + 4 * g + j] =
+            pass == 0 ? (double)s[j] : pass == 1 ? (double)q[j] : (double)m[j];
+    }
+    __syncthreads();
+    if (tid < cs) {
+      if (pass < 2) {
+        tot[pass] = sum4(sm_bp + tid, P, cs);
+      } else {
+        for (int k = 0; k < P; ++k) tot[2] = fmax(tot[2], sm_bp[k * cs + tid]);
       }
     }
   }
-  __syncthreads();
-  if (KC > 1) cluster_barrier();   // every chunk's partials are in place
-  if (kc == 0 && tid < cs) {       // combine in chunk order
-    double tot[5] = {0.0, 0.0, -INFINITY, -1e300, 1e300};
-    for (int r = 0; r < KC; ++r) {
-      double v[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k)
-        v[k] = r == 0 ? sm_fin[k * cs + tid] : ld_cluster_f64(sm_fin + k * cs + tid, (uint32_t)r);
-      tot[0] += v[0];
-      tot[1] += v[1];
-      tot[2] = fmax(tot[2], v[2]);
-      tot[3] = fmax(tot[3], v[3]);
-      tot[4] = fmin(tot[4], v[4]);
-    }
+  if (tid < cs) {
     const double mean = tot[0] / T;
     const double var = fmax(tot[1] / T - mean * mean, 0.0);
     const int o = b * C + c0 + tid;
     a.spec[o] = (float)mean;
     a.var[o] = (float)var;
     a.maxs[o] = a.parity ? (float)mean : (float)tot[2];
-    a.pp[o] = nbins > 0 ? (float)(tot[3] - tot[4]) : 0.0f;
+    a.pp[o] = nbins > 0 ? (float)(bmax - bmin) : 0.0f;
   }
-  if (KC > 1) cluster_barrier();   // the partials stay until rank 0 has read them
-  if (kc != 0 || !a.decide) return;
+  if (!a.decide) return;
   // The last slab CTA of the beam makes its channel decisions, and the last
-  // slab CTA of the grid the block-level total power: each publishes its
+  // CTA of the grid the block-level total power: each CTA publishes its
   // statistics (fence) before counting itself in; nothing waits.
   __shared__ int last_sh;
   __threadfence();
@@ -416,7 +370,7 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   }
   if (!a.modcheck && !a.tpwr_out) return;
   __syncthreads();
-  if (tid == 0) last_sh = atomicAdd(a.ctr + 2 * a.nbeam, 1) == a.nslab * a.nbeam - 1;
+  if (tid == 0) last_sh = atomicAdd(a.ctr + 2 * a.nbeam, 1) == (int)(gridDim.x * gridDim.y) - 1;
   __syncthreads();
   if (last_sh) {
     __threadfence();
@@ -838,76 +792,14 @@ __global__ void flag_medcalc_kernel(float *arr0, float *arr1, int nbeam, int nch
 }
 
 // ---------------------------------------------------------------- launchers
-// Statistics-pass geometry (flag_stats_kernel): lanes per channel group sp,
-// rows per stage rs, time chunks per slab kc and the dynamic shared memory.
-struct StatGeom {
-  int sp = 0, rs = 0, kc = 1;
-  size_t smem = 0;
-};
-
-static int gcd_int(int x, int y) {
-  while (y) {
-    const int r = x % y;
-    x = y;
-    y = r;
-  }
-  return x;
-}
-
-// Chunks per slab: the cluster size (1, 2, 4 or 8) whose grid fills the
-// device's CTA slots (two per SM) best, the smallest within 2 % of the best,
-// among those that leave every chunk at least 16 stages (the ring's fill
-// and the cross-chunk combine are per-CTA costs); uint8 needs at most 32768
-// rows per thread (32-bit integer partials).
-static int stat_chunks(const FlagArgs &a, int sp, int rs, bool u8) {
-  int dev = 0, nsm = 148;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-    nsm = 148;
-  const double slots = 2.0 * nsm;
-  const double base = (double)a.nslab * a.nbeam;
-  const int nbins = a.ntime / a.tbin;
-  double eff[4] = {0, 0, 0, 0};
-  double best = 0.0;
-  for (int i = 0; i < 4; ++i) {
-    const int k = 1 << i;
-    if (k > 1 && k > nbins) break;
-    const int64_t rows = (int64_t)((nbins + k - 1) / k) * a.tbin + a.tbin;   // + tail rows
-    if (u8 && rows / sp > 32768) continue;
-    if (k > 1 && rows < (int64_t)16 * rs) continue;   // keep the ring busy: >= 16 stages
-    const double w = base * k / slots;
-    eff[i] = w / ceil(w);
-    if (eff[i] > best) best = eff[i];
-  }
-  if (best <= 0.0) return 0;
-  for (int i = 0; i < 4; ++i)
-    if (eff[i] > 0.0 && eff[i] >= best - 0.02) return 1 << i;
-  return 0;
-}
-
-static bool stat_geom(const FlagArgs &a, int es, StatGeom &gm) {
+static int stage_rows(const FlagArgs &a, int es) {
   const int cs = a.nchan < kFlagSlab ? a.nchan : kFlagSlab;
-  const int G4 = cs / 4;
-  int sp = 32;
-  while (sp > 1 && (sp * G4 > flag::kStatThreads || a.tbin % sp)) sp >>= 1;
-  const int rp = (((cs * es) >> 4) | 1) << 4;
-  const int unit = a.pix_sum ? sp / gcd_int(sp, a.tds) * a.tds : sp;
-  int rs = unit * (flag::kStageTarget / (rp * unit));
-  if (rs < unit) rs = unit;
-  FlagArgs t = a;
-  t.nslab = (a.nchan + kFlagSlab - 1) / kFlagSlab;
-  const int kc = stat_chunks(t, sp, rs, es == 1);
-  if (kc < 1) return false;
-  const int nws = ((G4 * sp + 31) / 32) | 1;
-  const size_t stats = (size_t)flag::kStages * rs * rp +
-                       sizeof(double) * ((size_t)rs * nws + 6 * (size_t)cs) + sizeof(float) * 2 * cs;
-  // the channel decisions reuse the buffer: 12 nchan floats + nchan bytes
-  const size_t dec = a.decide ? sizeof(float) * 12 * (size_t)a.nchan + a.nchan : 0;
-  gm.sp = sp;
-  gm.rs = rs;
-  gm.kc = kc;
-  gm.smem = stats > dec ? stats : dec;
-  return gm.smem <= 160 * 1024;
+  int lim = flag::kStageTarget / (cs * es);
+  if (lim > flag::kStatThreads) lim = flag::kStatThreads;
+  if (lim > a.tbin) lim = a.tbin;
+  for (int d = lim; d >= 1; --d)
+    if (a.tbin % d == 0 && (!a.pix_sum || d % a.tds == 0)) return d;
+  return 0;
 }
 
 bool flag_shape_ok(const FlagArgs &a) {
@@ -919,40 +811,52 @@ bool flag_shape_ok(const FlagArgs &a) {
   if (a.pix_sum && (u8 || a.nchan > kFlagSlab || a.tds < 1 || a.tbin % a.tds ||
                     a.ntime % a.tbin))
     return false;
-  StatGeom gm;
-  return stat_geom(a, es, gm);
+  // uint8 sums are 32-bit: at most 32768 rows per thread (P of the full slab)
+  const int cs = a.nchan < kFlagSlab ? a.nchan : kFlagSlab;
+  const int P = flag::kStatThreads / (cs / 4);
+  if (u8 && (a.ntime + P - 1) / P > 32768) return false;
+  FlagArgs t = a;
+  return stage_rows(t, es) > 0;
 }
 
-template <typename E>
-static int launch_stats_kernel(const FlagArgs &a, const StatGeom &gm, cudaStream_t st) {
-  static SmemAttrOnce attr;
-  if (smem_attr_once(attr, flag_stats_kernel<E>, 160 * 1024) != cudaSuccess) return -2;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(a.nslab * gm.kc), (unsigned)a.nbeam, 1);
-  cfg.blockDim = dim3(flag::kStatThreads, 1, 1);
-  cfg.dynamicSmemBytes = gm.smem;
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = (unsigned)gm.kc;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, flag_stats_kernel<E>, a) == cudaSuccess ? 0 : -2;
+// The largest layout over the launch's slabs: the full slab width cs and,
+// when nchan is not a multiple of it, the narrower last slab (whose P x cs
+// bin partials can exceed the full slab's).  Kept tight: at 48 channels two
+// CTAs must share an SM.
+static size_t stats_smem(const FlagArgs &a, int es) {
+  const int cs = a.nchan < kFlagSlab ? a.nchan : kFlagSlab;
+  const int last = a.nchan > kFlagSlab ? a.nchan % kFlagSlab : 0;
+  auto bp = [](int w) { return (size_t)(flag::kStatThreads / (w / 4)) * w; };
+  size_t nbp = bp(cs);
+  if (last && bp(last) > nbp) nbp = bp(last);
+  const size_t stage = ((size_t)a.rs * cs * es + 127) & ~(size_t)127;
+  const size_t stats = flag::kStages * stage +
+                       sizeof(double) * ((size_t)a.rs * ((cs / 4) | 1) + nbp + cs) +
+                       sizeof(float) * 2 * cs;
+  // the channel decisions reuse the buffer: 12 nchan floats + nchan bytes
+  const size_t dec = a.decide ? sizeof(float) * 12 * (size_t)a.nchan + a.nchan : 0;
+  return stats > dec ? stats : dec;
 }
 
 int launch_flag_stats(FlagArgs a, cudaStream_t st) {
   if (!flag_shape_ok(a)) return -1;
   const bool u8 = a.xu8 != nullptr;
-  StatGeom gm;
-  if (!stat_geom(a, u8 ? 1 : 4, gm)) return -1;
-  a.rs = gm.rs;
-  a.sp = gm.sp;
-  a.kc = gm.kc;
+  const int es = u8 ? 1 : 4;
+  a.rs = stage_rows(a, es);
   a.nslab = (a.nchan + kFlagSlab - 1) / kFlagSlab;
   if (a.nslab > 1 && !a.rowsum) return -1;
-  return u8 ? launch_stats_kernel<uint8_t>(a, gm, st) : launch_stats_kernel<float>(a, gm, st);
+  const size_t sh = stats_smem(a, es);
+  const dim3 grid(a.nslab, a.nbeam);
+  if (u8) {
+    static SmemAttrOnce attr;
+    if (smem_attr_once(attr, flag_stats_kernel<uint8_t>, 160 * 1024) != cudaSuccess) return -2;
+    flag_stats_kernel<uint8_t><<<grid, flag::kStatThreads, sh, st>>>(a);
+  } else {
+    static SmemAttrOnce attr;
+    if (smem_attr_once(attr, flag_stats_kernel<float>, 160 * 1024) != cudaSuccess) return -2;
+    flag_stats_kernel<float><<<grid, flag::kStatThreads, sh, st>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 // The statistics pass (which ends with the channel decisions and the total

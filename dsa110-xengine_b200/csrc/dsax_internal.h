@@ -115,10 +115,8 @@ struct FlagArgs {
   float *pix_sum = nullptr, *pix_max = nullptr;
   int tds = 0;
   // statistics-pass geometry, set by the launcher
-  int nslab = 1;                 // channel slabs of kFlagSlab channels
-  int rs = 0;                    // rows per pipeline stage (a multiple of sp)
-  int sp = 1;                    // lanes per channel group (power of two dividing tbin and 32)
-  int kc = 1;                    // time chunks per slab (the cluster size)
+  int nslab = 1;                 // channel slabs of kFlagSlab channels (CTAs per beam)
+  int rs = 0;                    // rows per pipeline stage (divides tbin)
   int ts_mean = 0;               // 1: the statistics pass writes ts = row mean (no apply pass)
   // data path (src/gpu_flagger.cu:1290-1410)
   int clean = 0;                 // 1: replace flagged columns / rows in xw / xw8

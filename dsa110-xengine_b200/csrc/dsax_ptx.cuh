@@ -306,31 +306,6 @@ __device__ __forceinline__ void bulk_s2s_cluster(uint32_t cluster_dst, uint32_t 
       : "memory");
 }
 
-// Bulk store of `bytes` from this CTA's shared memory to global memory, and
-// the same as an FP32 add into global memory; bulk async-group completion.
-__device__ __forceinline__ void bulk_s2g(void *dst, uint32_t src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_s2g_add_f32(void *dst, uint32_t src, uint32_t bytes) {
-  asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f32 [%0], [%1], %2;" ::"l"(
-                   dst),
-               "r"(src), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit_group() {
-  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-}
-// every committed bulk group has finished reading its shared-memory source
-__device__ __forceinline__ void bulk_wait_read_all() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-// every committed bulk group has completed (its writes are done)
-__device__ __forceinline__ void bulk_wait_all() {
-  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-}
-
 // 3-D tiled TMA load (no multicast) into this CTA's shared memory,
 // completing on `bar` with the box's byte count.
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *map, int x, int y, int z,

@@ -297,7 +297,8 @@ int dsax_agc_state(dsax_ctx *ctx, float *scale, int *started, int *blocks);
  * are parameters here. */
 typedef struct dsax_flag_params {
     int nbeam, ntime, nchan; /* filterbank [nbeam][ntime][nchan], 4 <= nchan <= 1024;
-                                nchan a multiple of 4 (FP32) or 16 (uint8)        */
+                                nchan a multiple of 4 (FP32) or 16 (uint8); uint8
+                                ntime <= 262,144 (exact 32-bit partial sums)      */
     int guard;     /* ZeroChannels guard band at each edge (128 of 1024)           */
     int filt;      /* nFiltSize forward median window (21)                          */
     int tbin;      /* TBIN samples per peak-to-peak bin (128)                       */
