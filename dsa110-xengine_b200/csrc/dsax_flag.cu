@@ -149,26 +149,43 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   E *xw = elem_out<E>(a);
   const bool scale = a.spec0 != nullptr;
 
+  constexpr bool kU8 = std::is_same<E, uint8_t>::value;
+  // row partials: exact ints for uint8, doubles for FP32
+  using RsT = typename std::conditional<kU8, int, double>::type;
   extern __shared__ __align__(16) uint8_t fs_raw[];
   const uint32_t sbase = smem_u32(fs_raw);
   const int GS = G4 | 1;   // odd row stride: the row sums read column-wise conflict-free
-  double *sm_rs = reinterpret_cast<double *>(fs_raw + S * stage_bytes);   // [RS][GS]
-  double *sm_bp = sm_rs + RS * GS;                                         // [P][cs]
+  RsT *sm_rs = reinterpret_cast<RsT *>(fs_raw + S * stage_bytes);         // [RS][GS]
+  double *sm_bp = reinterpret_cast<double *>(
+      fs_raw + S * stage_bytes + ((sizeof(RsT) * RS * GS + 15) & ~(size_t)15));   // [P][cs]
   double *sm_k = sm_bp + P * cs;                                           // [cs]
   float *sm_s0 = reinterpret_cast<float *>(sm_k + cs);                     // [cs]
   float *sm_k2 = sm_s0 + cs;                                               // [cs] float(2k)
+  uint8_t *sm_lut = reinterpret_cast<uint8_t *>(sm_k2 + cs);               // uint8: [256][cs]
   const double inv_tb = 1.0 / TB;
 
-  if (scale)
+  if (scale) {
     for (int c = tid; c < cs; c += flag::kStatThreads) {
       sm_s0[c] = a.spec0[b * C + c0 + c];
       sm_k[c] = (double)a.sig / (double)sqrtf(a.var0[b * C + c0 + c]);
       sm_k2[c] = (float)(2.0 * sm_k[c]);
     }
+    if constexpr (kU8) {
+      // uint8 has 256 inputs per channel: scaley as a table [x][channel],
+      // read by the lanes of a warp (consecutive channel groups) from
+      // distinct banks
+      __syncthreads();
+      for (int i = tid; i < 256 * cs; i += flag::kStatThreads) {
+        const int x = i / cs, c = i - x * cs;
+        sm_lut[i] = (uint8_t)scaley_u8((float)x, sm_s0[c], sm_k2[c], sm_k[c], a.mn);
+      }
+    }
+  }
   __syncthreads();
-  // sum of n doubles at v[0], v[stride], ... in four interleaved chains
-  auto sum4 = [](const double *v, int n, int stride) -> double {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  // sum of n values at v[0], v[stride], ... in four interleaved chains
+  auto sum4 = [](const auto *v, int n, int stride) -> double {
+    using V = typename std::remove_cv<typename std::remove_pointer<decltype(v)>::type>::type;
+    V a0 = 0, a1 = 0, a2 = 0, a3 = 0;
     int k = 0;
     for (; k + 4 <= n; k += 4) {
       a0 += v[k * stride];
@@ -177,7 +194,7 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
       a3 += v[(k + 3) * stride];
     }
     for (; k < n; ++k) a0 += v[k * stride];
-    return (a0 + a1) + (a2 + a3);
+    return (double)((a0 + a1) + (a2 + a3));
   };
 
   auto issue = [&](int st) {
@@ -199,26 +216,26 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   };
   // normalise (if scaling) and accumulate the four channels of one row:
   // FP64 for FP32 data, exact 32-bit integers for uint8 (no FP64 work)
-  constexpr bool kU8 = std::is_same<E, uint8_t>::value;
   using Acc = typename std::conditional<kU8, int, double>::type;
+  using MaxT = typename std::conditional<kU8, int, float>::type;
   Acc s[4], q[4], bs[4];
-  float m[4];
+  MaxT m[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     s[j] = 0; q[j] = 0; bs[j] = 0;
-    m[j] = kU8 ? 0.0f : -INFINITY;
+    m[j] = kU8 ? (MaxT)0 : (MaxT)-INFINITY;
   }
-  auto take = [&](uint8_t *src, int t, bool bin, bool keep) -> double {
+  auto take = [&](uint8_t *src, int t, bool bin, bool keep) -> RsT {
     float v[4];
     if constexpr (kU8) {
       uint32_t w = *reinterpret_cast<const uint32_t *>(src);
       if (scale) {
+        uint32_t o = 0u;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-          v[j] = scaley_u8((float)((w >> (8 * j)) & 255u), sm_s0[4 * g + j], sm_k2[4 * g + j],
-                           sm_k[4 * g + j], a.mn);
-        st4<E>(&w, v);
-        if (xw) st4<E>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g, v);
+          o |= (uint32_t)sm_lut[((w >> (8 * j)) & 255u) * cs + 4 * g + j] << (8 * j);
+        w = o;
+        if (xw) *reinterpret_cast<uint32_t *>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g) = w;
       }
       int r = 0;
 #pragma unroll
@@ -226,10 +243,10 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
         const int x = (int)((w >> (8 * j)) & 255u);
         if (bin) bs[j] += x; else s[j] += x;
         q[j] += x * x;
-        m[j] = fmaxf(m[j], (float)x);
+        m[j] = max(m[j], x);
         r += x;
       }
-      return (double)r;
+      return r;
     } else {
       ld4<E>(src, v);
       if (scale) {
@@ -570,9 +587,7 @@ __device__ void flag_total_power(const FlagArgs &a) {
 template <typename E>
 __global__ void __launch_bounds__(flag::kApplyThreads) flag_apply_kernel(FlagArgs a) {
   constexpr int ES = (int)sizeof(E), EPC = 16 / ES;   // elements per 16-byte chunk
-  // beams in reverse order: the statistics pass finished the last beams
-  // last, so their rows are the likeliest to be still in L2
-  const int b = gridDim.y - 1 - blockIdx.y, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int b = blockIdx.y, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int C = a.nchan, G = a.guard, T = a.ntime, NCH = C / EPC;
   const int t_begin = blockIdx.x * flag::kApplyRows;
   const int t_end = min(T, t_begin + flag::kApplyRows);
@@ -634,20 +649,27 @@ __global__ void __launch_bounds__(flag::kApplyThreads) flag_apply_kernel(FlagArg
   while (L < nact && L < 32) L <<= 1;
   const int rpw = 32 / L, sub = lane & (L - 1);
   const E *xin = (a.spec0 && elem_out<E>(a)) ? elem_out<E>(a) : elem_in<E>(a);
-  // one listed chunk of one row: replace the flagged elements, return the
-  // correction to the row sum
-  auto fix_chunk = [&](uint4 &v, uint32_t m) -> double {
+  for (int r0 = t_begin + warp * rpw; r0 < t_end; r0 += nw * rpw) {   // uniform per warp
+    const int t = r0 + lane / L;
     double corr = 0.0;
-    E *ve = reinterpret_cast<E *>(&v);
+    if (t < t_end) {
+      const uint4 *row = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C);
+      uint4 *wrow = xw ? reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C) : nullptr;
+      for (int i = sub; i < nact; i += L) {
+        const uint32_t ce = chk[i];
+        const int k = (int)(ce & 0xFFFFu);
+        const uint32_t m = ce >> 16;
+        uint4 v = row[k];
+        E *ve = reinterpret_cast<E *>(&v);
 #pragma unroll
-    for (int e = 0; e < EPC; ++e)
-      if ((m >> e) & 1u) {
-        corr += (double)(rf - (float)ve[e]);
-        ve[e] = re;
+        for (int e = 0; e < EPC; ++e)
+          if ((m >> e) & 1u) {
+            corr += (double)(rf - (float)ve[e]);
+            ve[e] = re;
+          }
+        if (wrow) wrow[k] = v;
       }
-    return corr;
-  };
-  auto finish_row = [&](int t, double corr) {
+    }
     for (int o = L >> 1; o > 0; o >>= 1) corr += __shfl_xor_sync(0xffffffffu, corr, o);
     if (t < t_end && sub == 0) {
       double rsum;
@@ -658,50 +680,6 @@ __global__ void __launch_bounds__(flag::kApplyThreads) flag_apply_kernel(FlagArg
         for (int s = 0; s < a.nslab; ++s) rsum += a.rowsum[((int64_t)b * a.nslab + s) * T + t];
       }
       a.ts[(int64_t)b * T + t] = (float)((rsum + corr) / C);
-    }
-  };
-  if (nact <= 32) {
-    // at most one chunk per lane and row: four row groups' loads in flight
-    // per lane before any is used
-    constexpr int kB = 4;
-    const uint32_t ce = sub < nact ? chk[sub] : 0u;
-    const int k = (int)(ce & 0xFFFFu);
-    const uint32_t m = ce >> 16;
-    for (int r0 = t_begin + warp * rpw; r0 < t_end; r0 += kB * nw * rpw) {   // uniform per warp
-      uint4 v[kB];
-#pragma unroll
-      for (int u = 0; u < kB; ++u) {
-        const int t = r0 + u * nw * rpw + lane / L;
-        v[u] = make_uint4(0u, 0u, 0u, 0u);
-        if (t < t_end && sub < nact)
-          v[u] = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C)[k];
-      }
-#pragma unroll
-      for (int u = 0; u < kB; ++u) {
-        const int t = r0 + u * nw * rpw + lane / L;
-        double corr = 0.0;
-        if (t < t_end && sub < nact) {
-          corr = fix_chunk(v[u], m);
-          if (xw) reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C)[k] = v[u];
-        }
-        finish_row(t, corr);
-      }
-    }
-  } else {
-    for (int r0 = t_begin + warp * rpw; r0 < t_end; r0 += nw * rpw) {   // uniform per warp
-      const int t = r0 + lane / L;
-      double corr = 0.0;
-      if (t < t_end) {
-        const uint4 *row = reinterpret_cast<const uint4 *>(xin + ((int64_t)b * T + t) * C);
-        uint4 *wrow = xw ? reinterpret_cast<uint4 *>(xw + ((int64_t)b * T + t) * C) : nullptr;
-        for (int i = sub; i < nact; i += L) {
-          const uint32_t ce = chk[i];
-          uint4 v = row[ce & 0xFFFFu];
-          corr += fix_chunk(v, ce >> 16);
-          if (wrow) wrow[ce & 0xFFFFu] = v;
-        }
-      }
-      finish_row(t, corr);
     }
   }
   // the beam's last CTA makes the time-series decisions
@@ -830,9 +808,11 @@ static size_t stats_smem(const FlagArgs &a, int es) {
   size_t nbp = bp(cs);
   if (last && bp(last) > nbp) nbp = bp(last);
   const size_t stage = ((size_t)a.rs * cs * es + 127) & ~(size_t)127;
-  const size_t stats = flag::kStages * stage +
-                       sizeof(double) * ((size_t)a.rs * ((cs / 4) | 1) + nbp + cs) +
-                       sizeof(float) * 2 * cs;
+  // row partials (int for uint8, double for FP32), bin partials, scaley
+  // constants, and for scaled uint8 the [256][cs] table
+  const size_t rsb = ((size_t)(es == 1 ? 4 : 8) * a.rs * ((cs / 4) | 1) + 15) & ~(size_t)15;
+  const size_t stats = flag::kStages * stage + rsb + sizeof(double) * (nbp + cs) +
+                       sizeof(float) * 2 * cs + (es == 1 && a.spec0 ? (size_t)256 * cs : 0);
   // the channel decisions reuse the buffer: 12 nchan floats + nchan bytes
   const size_t dec = a.decide ? sizeof(float) * 12 * (size_t)a.nchan + a.nchan : 0;
   return stats > dec ? stats : dec;
