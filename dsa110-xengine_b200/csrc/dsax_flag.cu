@@ -197,13 +197,23 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     return (double)((a0 + a1) + (a2 + a3));
   };
 
+  // 16-byte piece i = tid + 256 n of a stage is (row, chunk) = divmod(i,
+  // ck), stepped without divisions
+  const int ir0 = tid / ck, ik0 = tid - ir0 * ck;
+  const int idr = flag::kStatThreads / ck, idk = flag::kStatThreads - idr * ck;
   auto issue = [&](int st) {
     if (st < nst) {
       const uint8_t *src = xb + (int64_t)st * RS * rstride;
       const uint32_t dst = sbase + (uint32_t)(st % S) * stage_bytes;
-      for (int i = tid; i < RS * ck; i += flag::kStatThreads) {
-        const int r = i / ck, k = i - r * ck;
+      int r = ir0, k = ik0;
+      while (r < RS) {
         cp_async16(dst + r * rb + 16 * k, src + r * rstride + 16 * k);
+        r += idr;
+        k += idk;
+        if (k >= ck) {
+          k -= ck;
+          ++r;
+        }
       }
     }
     cp_async_commit();
@@ -237,16 +247,14 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
         w = o;
         if (xw) *reinterpret_cast<uint32_t *>(xw + ((int64_t)b * T + t) * C + c0 + 4 * g) = w;
       }
-      int r = 0;
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int x = (int)((w >> (8 * j)) & 255u);
         if (bin) bs[j] += x; else s[j] += x;
         q[j] += x * x;
         m[j] = max(m[j], x);
-        r += x;
       }
-      return r;
+      return (int)__dp4a(w, 0x01010101u, 0u);   // the row's four bytes summed
     } else {
       ld4<E>(src, v);
       if (scale) {
