@@ -74,6 +74,8 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     p.tbin = nout >= 64 ? 16 : (nout >= 16 ? nout / 4 : 1);
     p.filt = p.filt > ngrp - 2 * p.guard ? ngrp - 2 * p.guard : p.filt;
     FlagArgs f{};
+    f.err = c->d_err;
+    f.wait_limit_ns = cf.wait_limit_ns;
     f.x = fb;
     f.nbeam = cf.nbeam; f.ntime = nout; f.nchan = ngrp;
     f.guard = p.guard; f.filt = p.filt; f.tbin = p.tbin; f.fbin = p.fbin;

@@ -18,13 +18,17 @@
 // baseline.  The shapes the reference hard-codes ([64][16384][1024] uint8,
 // ZeroChannels 128, nFiltSize 21, TBIN 128, FBIN 8, T/16) are parameters;
 // the filterbank may be uint8 (the reference's type) or FP32.
+#include <atomic>
 #include <cstdint>
+#include <cstring>
 #include <type_traits>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "dsax_internal.h"
 #include "dsax_ptx.cuh"
 #include "dsax_scaley.h"
+#include "dsax_tmap.h"
 #include "../../include/dsax.h"
 
 namespace dsax {
@@ -40,15 +44,6 @@ constexpr int kMaxTsBase = 4096;
 constexpr int kLfMaxChan = 128;       // learned-flagger features: channels per beam
 constexpr int kDecThreads = 256;
 }  // namespace flag
-
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // ---------------------------------------------------------------- elements
 // Four consecutive channels of one row: FP32 (16 bytes) or uint8 (4 bytes).
@@ -114,8 +109,12 @@ __device__ void flag_total_power(const FlagArgs &a);
 
 // ---------------------------------------------------------------- statistics
 // One CTA per (channel slab of up to kFlagSlab channels, beam).  The slab's
-// rows stream through a three-stage cp.async ring of `rs` rows each (rs
-// divides TBIN).  Thread (p, g) owns channels 4g..4g+3 of the slab and rows
+// rows stream through a three-stage ring of `rs` rows each (rs divides
+// TBIN), one 2-D TMA box [rs rows][min(nchan, 128) channels] per stage
+// (channels past nchan read zero), completing on the stage's mbarrier; the
+// waits are bounded (a.wait_limit_ns, recorded in a.err).  Every thread
+// fences its generic reads of a stage before the barrier after which the
+// stage is loaded again.  Thread (p, g) owns channels 4g..4g+3 of the slab and rows
 // p, p + P, ... of every stage (the lanes of a warp cover consecutive
 // 16-byte pieces of a row: conflict-free shared reads, coalesced global
 // writes); sums are FP64 for FP32 data and 32-bit integers for uint8 (at
@@ -129,7 +128,8 @@ __device__ void flag_total_power(const FlagArgs &a);
 // slab); flag_apply_kernel turns it into the channel-mean series after the
 // flagged columns are replaced.
 template <typename E>
-__global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagArgs a) {
+__global__ void __launch_bounds__(flag::kStatThreads, 2)
+    flag_stats_kernel(const __grid_constant__ CUtensorMap tmap, FlagArgs a) {
   constexpr int S = flag::kStages;
   constexpr int ES = (int)sizeof(E);
   const int slab = blockIdx.x, b = blockIdx.y, tid = threadIdx.x;
@@ -140,8 +140,8 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   const int p = tid / G4, g = tid - p * G4;
   const bool active = p < P;
   const int nbins = T / TB, spb = TB / RS, nst = nbins * spb;
-  const int rb = cs * ES;                        // bytes of one slab row (multiple of 16)
-  const int ck = rb >> 4;                        // 16-byte chunks per row
+  const int bx = C < kFlagSlab ? C : kFlagSlab;   // channels of a TMA box row
+  const int rb = bx * ES;                        // bytes of one staged row (multiple of 16)
   const int stage_bytes = (RS * rb + 127) & ~127;
   const int64_t rstride = (int64_t)C * ES;
   const uint8_t *xb =
@@ -152,7 +152,14 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   constexpr bool kU8 = std::is_same<E, uint8_t>::value;
   // row partials: exact ints for uint8, doubles for FP32
   using RsT = typename std::conditional<kU8, int, double>::type;
-  extern __shared__ __align__(16) uint8_t fs_raw[];
+  extern __shared__ __align__(128) uint8_t fs_raw[];
+  __shared__ __align__(8) uint64_t sfull[S];
+  __shared__ volatile int sabort;
+  if (tid == 0) {
+    for (int s2 = 0; s2 < S; ++s2) mbar_init(&sfull[s2], 1);
+    sabort = 0;
+    mbar_fence_init();
+  }
   const uint32_t sbase = smem_u32(fs_raw);
   const int GS = G4 | 1;   // odd row stride: the row sums read column-wise conflict-free
   RsT *sm_rs = reinterpret_cast<RsT *>(fs_raw + S * stage_bytes);         // [RS][GS]
@@ -197,26 +204,16 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
     return (double)((a0 + a1) + (a2 + a3));
   };
 
-  // 16-byte piece i = tid + 256 n of a stage is (row, chunk) = divmod(i,
-  // ck), stepped without divisions
-  const int ir0 = tid / ck, ik0 = tid - ir0 * ck;
-  const int idr = flag::kStatThreads / ck, idk = flag::kStatThreads - idr * ck;
+  // stage st: one TMA box, issued by thread 0
+  const uint32_t box_bytes = (uint32_t)(RS * rb);
+  int issued = 0;
   auto issue = [&](int st) {
     if (st < nst) {
-      const uint8_t *src = xb + (int64_t)st * RS * rstride;
-      const uint32_t dst = sbase + (uint32_t)(st % S) * stage_bytes;
-      int r = ir0, k = ik0;
-      while (r < RS) {
-        cp_async16(dst + r * rb + 16 * k, src + r * rstride + 16 * k);
-        r += idr;
-        k += idk;
-        if (k >= ck) {
-          k -= ck;
-          ++r;
-        }
-      }
+      mbar_arrive_expect_tx(&sfull[st % S], box_bytes);
+      tma_load_2d(sbase + (uint32_t)(st % S) * stage_bytes, &tmap, c0, b * T + st * RS,
+                  &sfull[st % S]);
+      issued = st + 1;
     }
-    cp_async_commit();
   };
   auto put_row = [&](int t, double r) {
     if (a.nslab == 1)
@@ -277,12 +274,15 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
   };
   double bmax = -1e300, bmin = 1e300;   // owned by thread tid < cs (channel tid)
 
-#pragma unroll
-  for (int i = 0; i < S - 1; ++i) issue(i);
+  if (tid == 0)
+    for (int i = 0; i < S - 1; ++i) issue(i);
+  int consumed = 0;
   for (int st = 0; st < nst; ++st) {
-    issue(st + S - 1);
-    cp_async_wait<S - 1>();
-    __syncthreads();
+    if (tid == 0) issue(st + S - 1);   // its slot was released at the end of stage st - 1
+    const bool ok = mbar_wait_bounded(&sfull[st % S], (uint32_t)(st / S) & 1u, &sabort, a.err,
+                                      DEV_ERR_WAIT_FULL, a.wait_limit_ns);
+    if (__syncthreads_or(!ok)) break;
+    consumed = st + 1;
     uint8_t *sp = fs_raw + (st % S) * stage_bytes;
     const int t0 = st * RS;
     if (active) {
@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
         a.pix_max[o] = mx;
       }
     }
+    fence_proxy_async_smem();   // this stage's generic reads before its next TMA write
     __syncthreads();
     if (tid < RS) put_row(t0 + tid, sum4(sm_rs + tid * GS, G4, 1));
     if (bin_end) {   // the last stage of a TBIN bin: bin means per channel
@@ -337,7 +338,15 @@ __global__ void __launch_bounds__(flag::kStatThreads, 2) flag_stats_kernel(FlagA
       }
     }
   }
-  cp_async_wait<0>();
+  // boxes still landing after an abort: wait for them before exit
+  if (tid == 0) {
+    volatile int no_abort = 0;
+    for (int k = consumed; k < issued; ++k)
+      mbar_wait_bounded(&sfull[k % S], (uint32_t)(k / S) & 1u, &no_abort, a.err, DEV_ERR_WAIT_FULL,
+                        drain_limit(a.wait_limit_ns));
+  }
+  __syncthreads();
+  if (sabort) return;   // recorded in a.err; no statistics from this CTA
   // rows beyond the last whole bin (T % TB): sums, squares, max and row
   // sums, read directly
   for (int t0 = nbins * TB; t0 < T; t0 += RS) {
@@ -826,6 +835,43 @@ static size_t stats_smem(const FlagArgs &a, int es) {
   return stats > dec ? stats : dec;
 }
 
+// The library-wide error word of flagger launches made without a context
+// (dsax_flag_noalloc, the learned-flagger features), one per device.
+static __device__ int g_flag_err;
+static int *flag_err_word() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  static std::atomic<int *> addr[64] = {};
+  int *p = addr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    void *q = nullptr;
+    if (cudaGetSymbolAddress(&q, g_flag_err) != cudaSuccess) return nullptr;
+    p = static_cast<int *>(q);
+    addr[dev].store(p, std::memory_order_release);
+  }
+  return p;
+}
+
+// The filterbank as a 2-D tensor [nbeam * ntime rows][nchan] of its element
+// type, boxes [rs rows][min(nchan, 128) channels], zero fill past nchan.
+static int encode_filterbank_map(CUtensorMap *map, const FlagArgs &a) {
+  EncodeTiledFn fn = tensor_map_encoder();
+  if (!fn) return -1;
+  const bool u8 = a.xu8 != nullptr;
+  const int es = u8 ? 1 : 4;
+  const int bx = a.nchan < kFlagSlab ? a.nchan : kFlagSlab;
+  const cuuint64_t dims[2] = {(cuuint64_t)a.nchan, (cuuint64_t)a.nbeam * (cuuint64_t)a.ntime};
+  const cuuint64_t strides[1] = {(cuuint64_t)a.nchan * es};
+  const cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)a.rs};
+  const cuuint32_t estr[2] = {1u, 1u};
+  void *base = u8 ? (void *)a.xu8 : (void *)a.x;
+  const CUresult r = fn(map, u8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                        base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : -1;
+}
+
 int launch_flag_stats(FlagArgs a, cudaStream_t st) {
   if (!flag_shape_ok(a)) return -1;
   const bool u8 = a.xu8 != nullptr;
@@ -833,16 +879,22 @@ int launch_flag_stats(FlagArgs a, cudaStream_t st) {
   a.rs = stage_rows(a, es);
   a.nslab = (a.nchan + kFlagSlab - 1) / kFlagSlab;
   if (a.nslab > 1 && !a.rowsum) return -1;
+  if (!a.err) a.err = flag_err_word();
+  if (!a.err) return -2;
+  if (!a.wait_limit_ns) a.wait_limit_ns = 1000000000ull;
+  CUtensorMap map;
+  memset(&map, 0, sizeof(map));
+  if (encode_filterbank_map(&map, a) != 0) return -2;
   const size_t sh = stats_smem(a, es);
   const dim3 grid(a.nslab, a.nbeam);
   if (u8) {
     static SmemAttrOnce attr;
     if (smem_attr_once(attr, flag_stats_kernel<uint8_t>, 160 * 1024) != cudaSuccess) return -2;
-    flag_stats_kernel<uint8_t><<<grid, flag::kStatThreads, sh, st>>>(a);
+    flag_stats_kernel<uint8_t><<<grid, flag::kStatThreads, sh, st>>>(map, a);
   } else {
     static SmemAttrOnce attr;
     if (smem_attr_once(attr, flag_stats_kernel<float>, 160 * 1024) != cudaSuccess) return -2;
-    flag_stats_kernel<float><<<grid, flag::kStatThreads, sh, st>>>(a);
+    flag_stats_kernel<float><<<grid, flag::kStatThreads, sh, st>>>(map, a);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

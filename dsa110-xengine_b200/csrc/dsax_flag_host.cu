@@ -118,6 +118,8 @@ int dsax_flag(dsax_ctx *c, const dsax_flag_params *p, const float *x, const floa
     return rc;
   FlagArgs a{};
   fill_args(a, p);
+  a.err = c->d_err;
+  a.wait_limit_ns = c->cfg.wait_limit_ns;
   float *sbuf = (mem == DSAX_MEM_DEVICE && stats) ? stats
                                                   : static_cast<float *>(c->aux[AUX_FLAG_STATS].ptr);
   a.spec = sbuf; a.var = sbuf + nbc; a.maxs = sbuf + 2 * nbc; a.pp = sbuf + 3 * nbc;
@@ -281,6 +283,8 @@ int dsax_flag_clean(dsax_ctx *c, dsax_flag_state *st, void *data, uint8_t *chanm
   if (!aligned16(dx)) return set_error(c, DSAX_ERR_ARG, "filterbank must be 16-byte aligned");
   FlagArgs a{};
   fill_args(a, p);
+  a.err = c->d_err;
+  a.wait_limit_ns = c->cfg.wait_limit_ns;
   if (es == 1) {
     a.xu8 = static_cast<const uint8_t *>(dx);
     a.xw8 = static_cast<uint8_t *>(dx);

@@ -136,6 +136,11 @@ struct FlagArgs {
   // done (the last arrival of each does the next step; nothing spins)
   int *ctr = nullptr;
   int decide = 0;                // statistics pass also makes the channel decisions
+  // bounded waits of the statistics pass (TMA stages): where a wait that
+  // ran out is recorded (a context's error word; null: a library-wide word)
+  // and the bound (0: 1 s)
+  int *err = nullptr;
+  unsigned long long wait_limit_ns = 0;
 };
 
 // ints of FlagArgs::ctr for nbeam beams

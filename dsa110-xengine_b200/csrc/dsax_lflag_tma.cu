@@ -75,17 +75,6 @@ __device__ __forceinline__ uint32_t tma_pack_bf16x2(float lo, float hi) {
   return r;
 }
 
-// 2-D tiled TMA load (no multicast) into this CTA's shared memory,
-// completing on `bar` with the box's byte count.
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
-                                            uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
 template <int COUT, bool PROJ>
 __global__ void __launch_bounds__(lftma::kThreads, 1)
     lf_conv_tma_kernel(const __grid_constant__ CUtensorMap tin, LfTmaArgs a) {

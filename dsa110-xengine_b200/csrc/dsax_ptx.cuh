@@ -306,6 +306,17 @@ __device__ __forceinline__ void bulk_s2s_cluster(uint32_t cluster_dst, uint32_t 
       : "memory");
 }
 
+// 2-D tiled TMA load (no multicast) into this CTA's shared memory,
+// completing on `bar` with the box's byte count (`map`: a CUtensorMap).
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *map, int x, int y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // 3-D tiled TMA load (no multicast) into this CTA's shared memory,
 // completing on `bar` with the box's byte count.
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const void *map, int x, int y, int z,
