@@ -403,7 +403,7 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
     return res
 
 
-def bench_flaggers(dsax, synth, dev, steps, train_steps=1000):
+def bench_flaggers(dsax, synth, dev, steps, train_steps=2000):
     """Flagger workload: plain vs learned flagger on [256][4096][48] FP32
     (chi2(2) + RFI), plus the plain flagger's data path (dsax_flag_clean) on
     that block and on a reference-shaped uint8 block [64][16384][1024].
@@ -555,7 +555,7 @@ def main():
                     help="run one side workload alone (profiling); prints its JSON")
     ap.add_argument("--serial", action="store_true",
                     help="one dsax_correlate call per block (no cross-block overlap)")
-    ap.add_argument("--lf-train-steps", type=int, default=1000,
+    ap.add_argument("--lf-train-steps", type=int, default=2000,
                     help="training steps of the learned flagger before it is timed")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the beamformer / flagger / batch side measurements")
