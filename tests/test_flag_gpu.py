@@ -69,8 +69,12 @@ def test_flagger_oldspec_and_perm(dsax, oracle):
 
 
 @pytest.mark.parametrize("B,T,C,guard", [(3, 1000, 48, 6), (5, 512, 64, 8), (2, 300, 32, 0),
-                                         (1, 4096, 24, 1)])
+                                         (1, 4096, 24, 1), (2, 700, 320, 20), (3, 512, 200, 12),
+                                         (2, 256, 4, 0)])
 def test_flagger_shapes(dsax, oracle, B, T, C, guard):
+    """Ragged shapes: rows past the last whole bin, several 128-channel
+    slabs (320), a last slab narrower than the 128-channel TMA box (200: its
+    box reads zeros past nchan), and the smallest width (4)."""
     x, _ = oracle.gen_filterbank(B * T + C, nbeam=B, ntime=T, nchan=C, n_tones=B, n_bursts=B,
                                  n_drift=1)
     _compare(dsax, oracle, x, guard=guard, filt=min(21, C - 2 * guard), tbin=100)
