@@ -278,23 +278,29 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
 // Channel-major correlator.  Input [nchan][npkt][64 ant][4 B] (one contiguous
 // stream per channel, written by reorder_cm_kernel).
 //
-// Per 64-packet stage and time slot t, one K-major operand tile
-//     A row (2 ant + pol) = [ R (64 B) | I (64 B) ]
-// with packet P at K byte 8 (P mod 8) + P / 8 of each half (a permutation
-// shared by every operand).  Two MMA groups per tile:
-//     Re = A A^T           (K = 128: R R^T + I I^T)     TMEM cols t*256 + [0, 128)
-//     C  = I R^T           (K = 64, I and R halves)     TMEM cols t*256 + [128, 256)
-// and the epilogue forms Im = C - C^T (C^T through shared memory), so the
-// tile needs neither a negated copy nor a second rotated tile.
+// Per 64-packet stage and time slot t, two K-major SWIZZLE_64B operand
+// tiles of 128 rows (2 ant + pol) x 64 bytes, R then I (8 KB each, so that
+// [R; I] is one 256-row operand), with packet P at K byte 8 (P mod 8) + P / 8
+// (a permutation shared by every operand).  Two MMA groups per slot:
+//     R [R; I]^T   (N = 256, K = 64)  -> R R^T | R I^T   TMEM cols t*256 + [0, 256)
+//     I I^T        (N = 128, K = 64)  += into cols t*256 + [0, 128)
+// so cols [0, 128) hold Re = R R^T + I I^T and cols [128, 256) hold
+// E = R I^T = C^T for C = I R^T; the epilogue forms Im = C - C^T from E and
+// its transpose (through shared memory).  The tensor time equals one N = 128
+// group per 32 bytes of K; the operand reads are 80 KB per stage (a single
+// [R | I] tile with Re = A A^T and C = I R^T as four and two N = 128 MMAs
+// read 96 KB).
 // Thread (antenna, c) owns the 16 packets P = 2c + e + 8q (e = 0, 1;
-// q = 0..7), i.e. 16-byte chunk c of each half.  Its 16 words come either
+// q = 0..7), i.e. 16-byte chunk c of the R and of the I tile.  Its 16 words come either
 // straight from global memory (kBulk = false: lanes = consecutive
 // antennas, coalesced, two stages ahead in registers) or from 16 KB stages
 // that a loader warp brings in with one cp.async.bulk each, four ahead
 // (kBulk = true; conflict-free shared reads).  It transposes bytes with
 // prmt and sign-extends nibbles with carry-free bytewise adds.  Lanes 4..7 of each group of 8
 // store the two pols in the opposite order, so every 16-byte store
-// instruction covers all eight bank groups of the 128-byte swizzle.
+// instruction covers all eight bank groups (the 64-byte swizzle spreads
+// four consecutive antennas' chunks over four groups, the pol the other
+// four).
 // NW = 16 (bulk-fed only) doubles the unpack warps: warps 8..15 repeat the
 // mapping of warps 0..7 for time slot 1 while warps 0..7 take slot 0 (each
 // raw word is read twice, each thread does half the byte work), and the
@@ -344,6 +350,8 @@ template <int FEED> constexpr int smem_bytes() {
          (FEED == 2 ? raw_stages<FEED>() * kLandBytes : 0);
 }
 constexpr uint32_t kIdescN128 = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 128);
+constexpr uint32_t kIdescN256 = umma_idesc(/*S32*/ 2, /*s8*/ 1, /*s8*/ 1, 128, 256);
+constexpr uint32_t kHalfTile = 128 * 64;           // one 64-byte-row tile (R or I)
 static_assert(kOpStages * kStageBytes >= 2 * 128 * 128 * 4, "C^T scratch reuses the stages");
 }  // namespace corrcm
 
@@ -432,8 +440,8 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
 #pragma unroll
     for (int sp = 0; sp < 2; ++sp) {
       const uint32_t row = (uint32_t)(2 * ant) + ((uint32_t)sp ^ flip);
-      o_re[sp] = sw128_offset(row, c);
-      o_im[sp] = sw128_offset(row, c + 4u);
+      o_re[sp] = sw64_offset(row, c);
+      o_im[sp] = kHalfTile + sw64_offset(row, c);
     }
     // w[e][q]: packet 2c + e + 8q of the stage, word = bytes [t0p0, t0p1, t1p0, t1p1]
     auto load = [&](int ks, uint32_t (&w)[2][8]) {
@@ -700,18 +708,17 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
         const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
 #pragma unroll
         for (int t = 0; t < 2; ++t) {
-          const uint32_t tile = stage + (uint32_t)t * kTile;
-          const uint32_t dre = tmem + (uint32_t)t * 256u, dc = dre + 128u;
+          const uint32_t tr = stage + (uint32_t)t * kTile, ti = tr + kHalfTile;
+          const uint32_t dre = tmem + (uint32_t)t * 256u;
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {   // Re: K = 128 bytes = 4 x 32
-            const uint64_t d = umma_desc_sw128(tile + 32u * kk, 1024u);
-            umma_i8(dre, d, d, kIdescN128, (ks | kk) != 0);
+          for (int kk = 0; kk < 2; ++kk) {   // R [R; I]^T: K = 64 bytes = 2 x 32
+            const uint64_t d = umma_desc_sw64(tr + 32u * kk, 512u);
+            umma_i8(dre, d, d, kIdescN256, (ks | kk) != 0);
           }
 #pragma unroll
-          for (int kk = 0; kk < 2; ++kk) {   // C = I R^T: K = 64 bytes = 2 x 32
-            const uint64_t di = umma_desc_sw128(tile + 64u + 32u * kk, 1024u);
-            const uint64_t dr = umma_desc_sw128(tile + 32u * kk, 1024u);
-            umma_i8(dc, di, dr, kIdescN128, (ks | kk) != 0);
+          for (int kk = 0; kk < 2; ++kk) {   // += I I^T into the first 128 columns
+            const uint64_t d = umma_desc_sw64(ti + 32u * kk, 512u);
+            umma_i8(dre, d, d, kIdescN128, 1u);
           }
         }
         umma_commit(&empty_bar[s]);
@@ -764,9 +771,10 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
             const int b0 = 2 * j, b1 = 2 * j + 1;
             const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
             const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
-            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)((int32_t)cr[2 * jj] - ct0),
+            // cr = E[m][.] = C[.][m], ct = C[m][.]: Im = C[m][.] - C[.][m]
+            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(ct0 - (int32_t)cr[2 * jj]),
                                    (float)(int32_t)re[2 * jj + 1],
-                                   (float)((int32_t)cr[2 * jj + 1] - ct1));
+                                   (float)(ct1 - (int32_t)cr[2 * jj + 1]));
             float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
             if (a.accumulate) {
               const float4 old = *dst;

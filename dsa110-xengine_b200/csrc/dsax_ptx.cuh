@@ -204,6 +204,18 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr, uint32_t sbo
   return d;
 }
 
+// The same for a K-major SWIZZLE_64B tile (64-byte rows, 8-row atoms of
+// 512 bytes, atom stride sbo); layout type 4.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)4u << 61;
+  return d;
+}
+
 // Instruction descriptor: c_format [4,6) (1=F32, 2=S32), a_format [7,10),
 // b_format [10,13), a/b major [15],[16] (0 = K-major), N>>3 [17,23),
 // M>>4 [24,29).
@@ -216,6 +228,13 @@ __host__ __device__ constexpr uint32_t umma_idesc(uint32_t cfmt, uint32_t afmt, 
 // SWIZZLE_128B tile whose base is 1024-byte aligned (rows of 128 bytes).
 __device__ __forceinline__ uint32_t sw128_offset(uint32_t row, uint32_t chunk) {
   return (row >> 3) * 1024u + (row & 7u) * 128u + (((chunk ^ (row & 7u)) & 7u) << 4);
+}
+
+// Byte offset of 16-byte chunk `chunk` (0..3) of row `row` inside a K-major
+// SWIZZLE_64B tile whose base is 512-byte aligned (rows of 64 bytes): the
+// chunk index is XORed with bits 7-8 of the row's byte offset.
+__device__ __forceinline__ uint32_t sw64_offset(uint32_t row, uint32_t chunk) {
+  return (row >> 3) * 512u + (row & 7u) * 64u + (((chunk ^ (row >> 1)) & 3u) << 4);
 }
 
 __device__ __forceinline__ void st_shared_v4(uint32_t saddr, uint32_t a, uint32_t b, uint32_t c,
