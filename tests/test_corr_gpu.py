@@ -142,6 +142,14 @@ def test_captured_cluster_ragged_shapes(dsax, oracle, npkt, nant, nchan, corr_pa
     np.testing.assert_array_equal(_run(dsax, blk, corr_path=corr_path), oracle.correlate(blk))
 
 
+@pytest.mark.parametrize("corr_path", [3, 4])
+def test_more_channels_than_sms_bit_exact(dsax, oracle, corr_path):
+    """300 channels: more CTAs than SMs, a partial last wave."""
+    npkt, nant, nchan = 64, 63, 300
+    blk = oracle.gen_block(31, npkt, nant, nchan, "gauss")
+    np.testing.assert_array_equal(_run(dsax, blk, corr_path=corr_path), oracle.correlate(blk))
+
+
 def test_extreme_values(dsax, oracle):
     """Every sample -8-8i (largest magnitude; -(-8) = 8 in the rotated
     operand) and a block of all +7+7i."""
