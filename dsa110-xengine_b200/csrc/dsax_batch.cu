@@ -4,7 +4,8 @@
 // correlation chain (HBM-bound corner turn, then the correlator) runs on the
 // context stream and the beamform + flag chain (tensor-bound) on a second
 // stream, forked from and joined back to the context stream, so that the
-// two chains of the batch overlap on the GPU; each chain keeps its own
+// two chains may overlap where one leaves SMs idle (both mostly fill the
+// GPU, so the measured gain is within noise); each chain keeps its own
 // scratch, so blocks within a chain stay in order.
 #include <cstring>
 #include <vector>
