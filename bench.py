@@ -346,6 +346,14 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
         e2e_ms = (time.perf_counter() - t0) * 1e3 / e_steps
         lib.dsax_host_free(ctx.handle, p_in)
         lib.dsax_host_free(ctx.handle, p_out)
+    # the one-CTA-per-beam-tile form (bf_path 1), for comparison with the
+    # default CTA pairs
+    cfg1 = dsax.default_config(bf_scale=scale, bf_path=1)
+    with dsax.Context(cfg1, device=dev) as ctx:
+        ctx.set_weights(wre, wim)
+        st = torch.cuda.ExternalStream(ctx.stream)
+        ms1 = _time_loop(st, lambda i: ctx.beamform(blk_dev[i % len(blk_dev)], out), steps)
+        ctx.sync()
     # the FP8 E4M3 operands (per-antenna power-of-two weight scale)
     cfg8 = dsax.default_config(bf_scale=scale, bf_fp8=1)
     with dsax.Context(cfg8, device=dev) as ctx:
@@ -383,7 +391,11 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
     res = {"workload": "64 ant x 2 pol x 384 ch x 4096 t -> 128 x 256 x 48 uint8, 256 beams, BF16",
            "blocks_per_s": 1e3 / ms, "ms_per_block": ms, "realtime_factor": 1e3 / ms * REALTIME_S,
            "gpu_launches_per_block": 1,
-           "roofline": {"bound": "tensor", "kernel": "bf_kernel", "achieved": tf,
+           "kernel_form": "CTA pairs: two 64-beam tiles share each data stage through one "
+                          "tcgen05.mma.cta_group::2 (M = 256)",
+           "one_cta_form": {"ms_per_block": ms1, "achieved_tflops": BF_FLOPS / (ms1 * 1e-3) / 1e12,
+                            "kernel": "bf_kernel (bf_path 1)"},
+           "roofline": {"bound": "tensor", "kernel": "bf_pair_kernel", "achieved": tf,
                         "peak": burst, "unit": "TFLOP/s", "frac": tf / burst,
                         "frac_of_sustained": tf / sust, "peak_kind": f"{kind} BF16 dense (cuBLAS)"},
            "error_vs_fp64": err,

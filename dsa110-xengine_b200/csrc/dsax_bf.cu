@@ -31,6 +31,10 @@
 //   warps 8-11: epilogue (TMEM -> |.|^2 row sums -> outputs)
 //   warp  12  : TMEM allocation, weight loader (bulk copy), single-thread
 //               UMMA issuer
+// This one-CTA form (bf_kernel) runs FP8 and odd beam-tile counts; BF16
+// with an even count runs as CTA pairs (bf_pair_kernel, below), which
+// halves the conversion and operand traffic per SM.
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -48,7 +52,8 @@ constexpr int kDTileBytes = kN * kKBlockBytes;        // 256 rows x 128 B = 32 K
 constexpr int kProducers = 256;                       // 8 producer warps
 constexpr int kRawRowBytes = kProducers * 16;         // one 16 B load per producer thread
 constexpr int kRawBytes = 8 * kRawRowBytes;           // 32 KB: one packet group, both pols
-constexpr int kThreads = kProducers + 128 + 32;       // + 4 epilogue warps + UMMA warp
+// + 4 or 8 epilogue warps + the UMMA warp
+constexpr int threads(int epi_warps) { return kProducers + 32 * epi_warps + 32; }
 // Operand type: BF16 (K = 64 antennas x {re, im} = 128 elements in two
 // 128-byte K blocks) or FP8 E4M3 (the same K in one 128-byte K block).
 template <bool kFp8> struct T {
@@ -115,8 +120,18 @@ __device__ __forceinline__ float hsum_f32x2(uint64_t v) {
   return lo + hi;
 }
 
-// Unit u of a CTA's range: r = u / 2 enumerates (channel group g, packet
-// group pg) as g * npg + pg; pol = u % 2.  The beam tile is fixed per CTA.
+// The units of a CTA's slot: they enumerate (channel group g, packet group
+// pg, pol) g-major, and slot s of nslots takes a contiguous range of whole
+// output times (align units).
+struct BfRange {
+  int u_lo, u_hi;
+};
+__device__ __forceinline__ BfRange bf_range(int slot, int nslots, int ngrp, int npg, int align) {
+  const int nchunks = ngrp * npg * 2 / align;
+  return {(int)((long long)slot * nchunks / nslots) * align,
+          (int)((long long)(slot + 1) * nchunks / nslots) * align};
+}
+// Unit u: channel group g, packet group pg, pol = u % 2.
 __device__ __forceinline__ void bf_decode(int u, int npg, int &g, int &pg, int &pol) {
   pol = u & 1;
   const int r = u >> 1;
@@ -124,10 +139,12 @@ __device__ __forceinline__ void bf_decode(int u, int npg, int &g, int &pg, int &
   g = r / npg;
 }
 
-template <bool kFp8>
-__global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
+template <bool kFp8, int kEpiW>
+__global__ void __launch_bounds__(bf::threads(kEpiW), 1) bf_kernel(BfArgs a) {
   using namespace bf;
   using TT = T<kFp8>;
+  constexpr int kMmaWarp = 8 + kEpiW;                 // TMEM owner, weight loader, UMMA issuer
+  constexpr int kEpiThreads = 32 * kEpiW;
   constexpr int kWBytes = TT::kWBytes, kStageBytes = TT::kStageBytes, kStages = TT::kStages;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kStages];
@@ -139,7 +156,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   __shared__ __align__(8) uint64_t final_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
-  __shared__ float red[4][64];
+  __shared__ float red[kEpiW / 4][128];   // one output's row partials per column share
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
@@ -153,10 +170,9 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   // Ranges are whole output times (pgs_per_out packet groups).
   const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / kPktPerStage;
   const int align = 2 * (a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1);
-  const int nchunks = ngrp * npg * 2 / align;
   const int nslots = gridDim.x / nbt, slot = blockIdx.x / nbt, bt = blockIdx.x % nbt;
-  const int u_lo = (int)((long long)slot * nchunks / nslots) * align;
-  const int u_hi = (int)((long long)(slot + 1) * nchunks / nslots) * align;
+  const BfRange rg = bf_range(slot, nslots, ngrp, npg, align);
+  const int u_lo = rg.u_lo, u_hi = rg.u_hi;
 
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -165,7 +181,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull_bar[b], 1);
-      mbar_init(&tempty_bar[b], 128);
+      mbar_init(&tempty_bar[b], kEpiThreads);
     }
     mbar_init(&wload_bar, 1);
     mbar_init(&wdrain_bar, 1);
@@ -173,7 +189,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
     abort_sh = 0;
     mbar_fence_init();
   }
-  if (warp == 12) {
+  if (warp == kMmaWarp) {
     tmem_alloc(&tmem_base_sh, 512);
     tmem_relinquish();
   }
@@ -317,9 +333,13 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       mbar_arrive(&full_bar[s]);
     }
     asm volatile("cp.async.wait_all;" ::: "memory");   // no copy outlives an aborted loop
-  } else if (warp < 12) {
+  } else if (warp < kMmaWarp) {
     // ------------------------------------------------------------ epilogue
+    // kEpiW / 4 warps per TMEM lane quarter (warp % 4), each taking an equal
+    // share of the 256 accumulator columns.
     const int q = warp & 3;                          // TMEM lane quarter (warp % 4)
+    const int half = (warp - 8) >> 2;                // column share
+    constexpr int kCW = (kN / 32) / (kEpiW / 4);     // 32-column loads per warp
     const int m = 32 * q + lane;                     // accumulator row
     const int nsub = a.ppo < kPktPerStage ? kPktPerStage / a.ppo : 1;  // outputs per stage
     const int span = kN / nsub;                      // columns per output (>= 64)
@@ -341,7 +361,8 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       // BF16 (measured 4.5 % faster), scalar FMAs for FP8 (there the packed
       // form measured 3 % slower)
 #pragma unroll
-      for (int c = 0; c < (ok ? kN / 32 : 0); ++c) {
+      for (int cc = 0; cc < (ok ? kCW : 0); ++cc) {
+        const int c = half * kCW + cc;
         uint32_t r0[32];
         tmem_ld32(taddr + 32u * c, r0);
         tmem_wait_ld();
@@ -379,19 +400,20 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
       int g, pg, pol;
       bf_decode(u, npg, g, pg, pol);
       if (pol == 1 && ((pg + 1) % pgs_per_out) == 0) {
-        // rows m and m + 64 hold Re and Im of the same beam
-        if (m >= 64) {
+        // rows m and m + 64 hold Re and Im of the same beam; the column
+        // shares of a row are summed through shared memory, one output at
+        // a time (static shared memory is at its limit beside the stages)
+        const int beam = 64 * bt + m;
 #pragma unroll
-          for (int sI = 0; sI < 4; ++sI)
-            if (sI < nsub) red[sI][m - 64] = acc[sI];
-        }
-        named_bar(1, 128);
-        if (m < 64 && !abort_sh) {
-          const int beam = 64 * bt + m;
+        for (int sI = 0; sI < 4; ++sI) {
+          if (sI >= nsub) break;
+          red[half][m] = acc[sI];
+          named_bar(1, kEpiThreads);
+          if (half == 0 && m < 64 && !abort_sh) {
+            float Ps = red[0][m] + red[0][m + 64];
 #pragma unroll
-          for (int sI = 0; sI < 4; ++sI) {
-            if (sI >= nsub) break;
-            const float P = (acc[sI] + red[sI][m]) * a.pscale;
+            for (int h2 = 1; h2 < kEpiW / 4; ++h2) Ps += red[h2][m] + red[h2][m + 64];
+            const float P = Ps * a.pscale;
             const int to = a.ppo <= kPktPerStage ? pg * nsub + sI : pg / pgs_per_out;
             const int64_t o = ((int64_t)to * a.nbeam + beam) * ngrp + g;
             if (a.out_f32) a.out_f32[o] = P;
@@ -405,12 +427,12 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
             }
             bpow += P;
           }
+          named_bar(1, kEpiThreads);
         }
-        named_bar(1, 128);
         acc[0] = acc[1] = acc[2] = acc[3] = 0.f;
       }
     }
-    if (a.beam_power && m < 64 && bpow != 0.f) atomicAdd(a.beam_power + 64 * bt + m, bpow);
+    if (a.beam_power && half == 0 && m < 64 && bpow != 0.f) atomicAdd(a.beam_power + 64 * bt + m, bpow);
   } else {
     // ------------------------------------------------------------ weights + UMMA
     if (lane == 0) {
@@ -475,7 +497,7 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
 
   tc_fence_before();
   __syncthreads();
-  if (warp == 12) {
+  if (warp == kMmaWarp) {
     if (lane == 0) {
       volatile int no_abort = 0;
       mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM,
@@ -487,26 +509,417 @@ __global__ void __launch_bounds__(bf::kThreads, 1) bf_kernel(BfArgs a) {
   }
 }
 
-template <bool kFp8>
-static int launch_bf(const BfArgs &a, int num_sms, cudaStream_t st) {
-  static SmemAttrOnce attr;
-  if (smem_attr_once(attr, bf_kernel<kFp8>, bf::T<kFp8>::kSmemBytes) != cudaSuccess) return -2;
-  const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / bf::kPktPerStage;
+// ---------------------------------------------------------------- CTA pairs
+// bf_pair_kernel: the BF16 beamformer with the two beam tiles of a 2-CTA
+// cluster sharing each data stage through one cta_group::2 MMA (M = 256:
+// 2 x 64 beams x re/im, N = 256 samples, K = 128).  Each CTA converts
+// only its half of a stage's packets (8 of 16) into its own shared memory,
+// and the pair's MMA reads both halves, so the 4-bit -> BF16 conversion,
+// the staging copies and the shared-memory operand reads per SM drop from
+// (A + B + B) to (A + B/2 + B/2) of a stage while the tensor work per SM
+// stays the same.  The even CTA issues the MMAs; D lanes 0-127 (its beam
+// tile) land in its TMEM, lanes 128-255 (the odd CTA's tile) in the odd
+// CTA's TMEM, and each CTA's epilogue reduces its own tile as bf_kernel
+// does, with two warps per TMEM lane quarter (eight in all: with the
+// producers' work halved, the epilogue sets the pace; 4 and 16 measured
+// slower).
+//   warps 0-7 : producers; each warp's lane 0 arrives on the even CTA's
+//               stage barrier (8 + 8 warp arrivals complete a stage)
+//   warps 8-15: epilogue; each warp's lane 0 frees the accumulator on the
+//               even CTA's barrier (8 + 8 arrivals)
+//   warp  16  : TMEM allocation (both CTAs), own weight tile (both CTAs),
+//               MMA issue (even CTA); stage / accumulator / weight-drain
+//               releases are multicast commits to both CTAs
+// Cross-CTA arrivals use the default release-at-CTA-scope form (the form
+// of the CUDA templates' CTA-pair pipelines); release at cluster scope
+// cost a memory barrier per arrival and measured about 25 % slower.
+namespace bfp {
+constexpr int kPktPerCta = 8;                        // packets of a 16-packet stage per CTA
+constexpr int kDHalfBytes = 128 * bf::kKBlockBytes;  // 128 B rows x 128 B = 16 KB per K block
+constexpr int kStageBytes = 2 * kDHalfBytes;         // BF16: two K blocks
+constexpr int kStages = 4;
+constexpr int kWBytes = 2 /*pol*/ * 2 /*kb*/ * bf::kWTileBytes;   // own beam tile, 64 KB
+constexpr int kRawRowBytes = bf::kProducers * 16;    // one 16 B load per producer thread
+constexpr int kRawBytes = 4 * kRawRowBytes;          // 16 KB: 8 packets x 64 ant x 32 B
+constexpr int threads(int epi_warps) { return bf::kProducers + 32 * epi_warps + 32; }
+constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
+constexpr uint32_t kIdesc = umma_idesc(1, 1, 1, 256, bf::kN);
+constexpr uint16_t kBoth = 0x3;                      // CTA mask of the pair
+}  // namespace bfp
+
+template <int kEpiW>
+__global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs a) {
+  constexpr int kMmaWarp = 8 + kEpiW;                 // TMEM, weights, MMA issue
+  constexpr int kEpiThreads = 32 * kEpiW;
+  using bf::kKBlockBytes;
+  using bf::kN;
+  using bf::kPktPerStage;
+  using bf::kWTileBytes;
+  constexpr int kStages = bfp::kStages, kStageBytes = bfp::kStageBytes;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kStages];   // even CTA: 16 producer-warp arrivals
+  __shared__ __align__(8) uint64_t empty_bar[kStages];  // both: one commit
+  __shared__ __align__(8) uint64_t tfull_bar[2];        // both: one commit
+  __shared__ __align__(8) uint64_t tempty_bar[2];       // even CTA: 2 x kEpiW epilogue-warp arrivals
+  __shared__ __align__(8) uint64_t wload_bar;           // own weight copy landed
+  __shared__ __align__(8) uint64_t wpeer_bar;           // even CTA: the odd CTA's weights landed
+  __shared__ __align__(8) uint64_t wdrain_bar;          // both: MMAs on the old weights done
+  __shared__ __align__(8) uint64_t final_bar;           // both: every MMA done
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ volatile int abort_sh;
+  __shared__ float red[kEpiW / 4][128];   // one output's row partials per column share
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  // identical offsets in both CTAs (same kernel, same static shared memory)
+  const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+  const uint32_t wsm = base;                          // own A tile [pol][kb][128 x 128 B]
+  const uint32_t dsm = base + bfp::kWBytes;           // B halves [s][kb][128 x 128 B]
+  const uint32_t raw = dsm + kStages * kStageBytes;   // producer staging [4][256][16 B]
+
+  // Work split as bf_kernel: the nbt CTAs of a slot share a (g, pg) range;
+  // nbt is even and a cluster is two consecutive blockIdx, so the beam
+  // tile's parity is the CTA's rank in the pair.
+  const int ngrp = a.nchan / 8, nbt = a.nbeam / 64, npg = a.npkt / kPktPerStage;
+  const int align = 2 * (a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1);
+  const int nslots = gridDim.x / nbt, slot = blockIdx.x / nbt, bt = blockIdx.x % nbt;
+  const BfRange rg = bf_range(slot, nslots, ngrp, npg, align);
+  const int u_lo = rg.u_lo, u_hi = rg.u_hi;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full_bar[s], 16);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull_bar[b], 1);
+      mbar_init(&tempty_bar[b], 2 * kEpiW);
+    }
+    mbar_init(&wload_bar, 1);
+    mbar_init(&wpeer_bar, 1);
+    mbar_init(&wdrain_bar, 1);
+    mbar_init(&final_bar, 1);
+    abort_sh = 0;
+    mbar_fence_init();
+  }
+  if (warp == kMmaWarp) {
+    tmem_alloc_pair(&tmem_base_sh, 512);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  cluster_barrier();      // both CTAs' barriers exist before any remote arrival
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  if ((tmem & 0xFFFFu) != 0u) {
+    if (tid == 0) atomicOr(a.err, DEV_ERR_TMEM);
+    abort_sh = 1;
+  }
+  // the even CTA's barriers, in the cluster window (also for the even CTA)
+  const uint32_t full0 = cluster_map(&full_bar[0], 0);
+  const uint32_t tempty0 = cluster_map(&tempty_bar[0], 0);
+  const uint32_t wpeer0 = cluster_map(&wpeer_bar, 0);
+
+  if (warp < 8) {
+    // ------------------------------------------------------------ producers
+    // Thread (kb, q8, j, h): K block kb, packet 8 rank + q8 of the stage,
+    // antennas 32 kb + 4j .. +3, channels 4h .. 4h+3 of the group: four
+    // 16 B loads per packet group (both pols), eight 16 B stores per stage.
+    const int h = tid & 1, j = (tid >> 1) & 7, q8 = (tid >> 4) & 7, kb = tid >> 7;
+    const int q = bfp::kPktPerCta * (int)rank + q8;
+    const int64_t ant_stride = (int64_t)a.nchan * 4;
+    const int64_t pkt_stride = (int64_t)a.nant_in * ant_stride;
+    const uint32_t myraw = raw + 16u * (uint32_t)tid;
+    uint4 Ucur[4];
+    auto stage_group = [&](int r) {
+      const int g = r / npg, pg = r % npg;
+      const int p = pg * kPktPerStage + q;
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii) {
+        const int ant = 32 * kb + 4 * j + ii;
+        const bool ok = ant < a.nant_in && p < a.npkt;
+        const uint8_t *src =
+            a.in + (ok ? p * pkt_stride + ant * ant_stride + (int64_t)(8 * g + 4 * h) * 4 : 0);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                         myraw + (uint32_t)ii * bfp::kRawRowBytes),
+                     "l"(src), "r"(ok ? 16 : 0)
+                     : "memory");
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (u_lo < u_hi) stage_group(u_lo >> 1);
+    // every exit from this loop is warp-uniform (the warp meets in
+    // __syncwarp / __all_sync below)
+    for (int u = u_lo, i = 0; u < u_hi; ++u, ++i) {
+      if (__any_sync(0xffffffffu, abort_sh != 0)) break;
+      const int s = i % kStages;
+      const uint32_t ph = (uint32_t)(i / kStages) & 1u;
+      const int pol = u & 1;
+      if (pol == 0) {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+                       : "=r"(Ucur[k].x), "=r"(Ucur[k].y), "=r"(Ucur[k].z), "=r"(Ucur[k].w)
+                       : "r"(myraw + (uint32_t)k * bfp::kRawRowBytes)
+                       : "memory");
+        }
+        if (u + 2 < u_hi) stage_group((u >> 1) + 1);
+      }
+      const bool ok = mbar_wait_bounded(&empty_bar[s], ph ^ 1u, &abort_sh, a.err,
+                                              DEV_ERR_WAIT_EMPTY, a.wait_limit_ns);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      const uint32_t sel = (uint32_t)pol | ((4u + pol) << 4) | ((2u + pol) << 8) | ((6u + pol) << 12);
+      const uint32_t tile = dsm + (uint32_t)s * kStageBytes + (uint32_t)kb * bfp::kDHalfBytes;
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        const uint32_t u0 = w == 0 ? Ucur[0].x : w == 1 ? Ucur[0].y : w == 2 ? Ucur[0].z : Ucur[0].w;
+        const uint32_t u1 = w == 0 ? Ucur[1].x : w == 1 ? Ucur[1].y : w == 2 ? Ucur[1].z : Ucur[1].w;
+        const uint32_t u2 = w == 0 ? Ucur[2].x : w == 1 ? Ucur[2].y : w == 2 ? Ucur[2].z : Ucur[2].w;
+        const uint32_t u3 = w == 0 ? Ucur[3].x : w == 1 ? Ucur[3].y : w == 2 ? Ucur[3].z : Ucur[3].w;
+        const uint32_t t01 = __byte_perm(u0, u1, sel);
+        const uint32_t t23 = __byte_perm(u2, u3, sel);
+#pragma unroll
+        for (int odd = 0; odd < 2; ++odd) {
+          const uint32_t x = __byte_perm(t01, t23, odd ? 0x7632u : 0x5410u);
+          uint32_t o[4];
+          nib8_to_bf16x8(x, o);
+          const int k = 8 * h + 2 * w + odd;      // chunnel = 2*chan + time
+          const uint32_t row = (uint32_t)(16 * q8 + k);   // row of this CTA's B half
+          st_shared_v4(tile + sw128_offset(row, (uint32_t)j), o[0], o[1], o[2], o[3]);
+        }
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(full0 + 8u * (uint32_t)s);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");   // no copy outlives an aborted loop
+  } else if (warp < kMmaWarp) {
+    // ------------------------------------------------------------ epilogue
+    // kEpiW / 4 warps per TMEM lane quarter (warp % 4), each taking an equal
+    // share of the 256 accumulator columns.
+    const int qq = warp & 3;                         // TMEM lane quarter (warp % 4)
+    const int half = (warp - 8) >> 2;                // column share
+    constexpr int kCW = (kN / 32) / (kEpiW / 4);     // 32-column loads per warp
+    const int m = 32 * qq + lane;                    // accumulator row of this CTA's tile
+    const int nsub = a.ppo < kPktPerStage ? kPktPerStage / a.ppo : 1;
+    const int span = kN / nsub;
+    const int pgs_per_out = a.ppo > kPktPerStage ? a.ppo / kPktPerStage : 1;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    float bpow = 0.f;
+    for (int u = u_lo, i = 0; u < u_hi; ++u, ++i) {
+      const int b = i & 1;
+      const uint32_t ph = (uint32_t)(i >> 1) & 1u;
+      bool ok = mbar_wait_bounded(&tfull_bar[b], ph, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
+                                  a.wait_limit_ns);
+      tc_fence_after();
+      ok = __all_sync(0xffffffffu, ok && !abort_sh);
+      const uint32_t taddr = tmem + ((uint32_t)(32 * qq) << 16) + (uint32_t)b * 256u;
+#pragma unroll
+      for (int cc = 0; cc < (ok ? kCW : 0); ++cc) {
+        const int c = half * kCW + cc;
+        uint32_t r0[32];
+        tmem_ld32(taddr + 32u * c, r0);
+        tmem_wait_ld();
+        uint64_t s2[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+        for (int e = 0; e < 32; e += 8)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) s2[k] = sqacc_f32x2(r0[e + 2 * k], r0[e + 2 * k + 1], s2[k]);
+        const float sq =
+            (hsum_f32x2(s2[0]) + hsum_f32x2(s2[1])) + (hsum_f32x2(s2[2]) + hsum_f32x2(s2[3]));
+        const int sub = (32 * c) / span;
+        if (nsub == 1) acc[0] += sq;
+        else if (sub == 0) acc[0] += sq;
+        else if (sub == 1) acc[1] += sq;
+        else if (sub == 2) acc[2] += sq;
+        else acc[3] += sq;
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(tempty0 + 8u * (uint32_t)b);
+
+      int g, pg, pol;
+      bf_decode(u, npg, g, pg, pol);
+      if (pol == 1 && ((pg + 1) % pgs_per_out) == 0) {
+        // rows m and m + 64 hold Re and Im of the same beam; the column
+        // shares of a row are summed through shared memory, one output at
+        // a time
+        const int beam = 64 * bt + m;
+#pragma unroll
+        for (int sI = 0; sI < 4; ++sI) {
+          if (sI >= nsub) break;
+          red[half][m] = acc[sI];
+          named_bar(1, kEpiThreads);
+          if (half == 0 && m < 64 && !abort_sh) {
+            float Ps = red[0][m] + red[0][m + 64];
+#pragma unroll
+            for (int h2 = 1; h2 < kEpiW / 4; ++h2) Ps += red[h2][m] + red[h2][m + 64];
+            const float P = Ps * a.pscale;
+            const int to = a.ppo <= kPktPerStage ? pg * nsub + sI : pg / pgs_per_out;
+            const int64_t o = ((int64_t)to * a.nbeam + beam) * ngrp + g;
+            if (a.out_f32) a.out_f32[o] = P;
+            if (a.out_fb) a.out_fb[((int64_t)beam * (a.npkt / a.ppo) + to) * ngrp + g] = P;
+            if (a.out_u8) {
+              int v = a.agc_scale ? __float2int_rn(P * __ldg(a.agc_scale + beam)) / 2
+                                  : __float2int_rn(P * a.scale);
+              a.out_u8[o] = (uint8_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+            }
+            bpow += P;
+          }
+          named_bar(1, kEpiThreads);
+        }
+        acc[0] = acc[1] = acc[2] = acc[3] = 0.f;
+      }
+    }
+    if (a.beam_power && half == 0 && m < 64 && bpow != 0.f)
+      atomicAdd(a.beam_power + 64 * bt + m, bpow);
+  } else {
+    // ------------------------------------------------------------ weights + MMA
+    if (lane == 0) {
+      int cur_g = -1;
+      uint32_t nload = 0, ndrain = 0;
+      for (int u = u_lo, i = 0; u < u_hi && !abort_sh; ++u, ++i) {
+        int g, pg, pol;
+        bf_decode(u, npg, g, pg, pol);
+        if (g != cur_g) {
+          if (i > 0) {  // no MMA may still read either CTA's old weights
+            if (leader) umma_commit_pair(&wdrain_bar, bfp::kBoth);
+            if (!mbar_wait_bounded<true>(&wdrain_bar, ndrain & 1u, &abort_sh, a.err,
+                                         DEV_ERR_WAIT_ACCUM, a.wait_limit_ns))
+              break;
+            ++ndrain;
+          }
+          mbar_arrive_expect_tx(&wload_bar, (uint32_t)bfp::kWBytes);
+          const uint8_t *src = a.wimg + (int64_t)(g * nbt + bt) * bfp::kWBytes;
+#pragma unroll
+          for (int c = 0; c < bfp::kWBytes / 16384; ++c)
+            bulk_g2s(wsm + 16384u * c, src + 16384 * c, 16384u, &wload_bar);
+          if (!mbar_wait_bounded(&wload_bar, nload & 1u, &abort_sh, a.err, DEV_ERR_WAIT_FULL,
+                                 a.wait_limit_ns)) {
+            volatile int no_abort = 0;
+            mbar_wait_bounded(&wload_bar, nload & 1u, &no_abort, a.err, DEV_ERR_WAIT_FULL,
+                              drain_limit(a.wait_limit_ns));
+            break;
+          }
+          if (!leader) {
+            mbar_arrive_cluster(wpeer0);
+          } else if (!mbar_wait_bounded<true>(&wpeer_bar, nload & 1u, &abort_sh, a.err,
+                                              DEV_ERR_WAIT_FULL, a.wait_limit_ns)) {
+            break;
+          }
+          ++nload;
+          cur_g = g;
+        }
+        if (!leader) continue;
+        const int s = i % kStages;
+        const int b = i & 1;
+        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)(i / kStages) & 1u, &abort_sh, a.err,
+                                     DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+          break;
+        if (!mbar_wait_bounded(&tempty_bar[b], ((uint32_t)(i >> 1) & 1u) ^ 1u, &abort_sh,
+                                     a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
+          break;
+        tc_fence_after();
+        const uint32_t wpol = wsm + (uint32_t)pol * (2u * kWTileBytes);
+        const uint32_t stage = dsm + (uint32_t)s * kStageBytes;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {   // 32-byte K steps (16 bf16)
+          const uint32_t kb = kk >> 2, koff = 32u * (kk & 3);
+          const uint64_t ad = umma_desc_sw128(wpol + kb * kWTileBytes + koff, 1024u);
+          const uint64_t bd = umma_desc_sw128(stage + kb * bfp::kDHalfBytes + koff, 1024u);
+          umma_f16_pair(tmem + (uint32_t)b * 256u, ad, bd, bfp::kIdesc, kk > 0);
+        }
+        umma_commit_pair(&empty_bar[s], bfp::kBoth);
+        umma_commit_pair(&tfull_bar[b], bfp::kBoth);
+      }
+      if (leader) umma_commit_pair(&final_bar, bfp::kBoth);
+    }
+    __syncwarp();
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    if (lane == 0) {
+      volatile int no_abort = 0;
+      mbar_wait_bounded<true>(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM,
+                              drain_limit(a.wait_limit_ns));
+    }
+    __syncwarp();
+  }
+  tc_fence_before();
+  cluster_barrier();      // both CTAs past their last TMEM read and remote arrival
+  tc_fence_after();
+  if (warp == kMmaWarp) tmem_dealloc_pair(tmem, 512);
+}
+
+// Slots of a launch: at most one per pair of units of whole output times.
+static int bf_slots(const BfArgs &a, int nslots) {
+  const int ngrp = a.nchan / 8, npg = a.npkt / bf::kPktPerStage;
   const int align = 2 * (a.ppo > bf::kPktPerStage ? a.ppo / bf::kPktPerStage : 1);
   const int nchunks = ngrp * npg * 2 / align;
-  int nslots = num_sms / nbt;
   if (nslots < 1) nslots = 1;
-  if (nslots > nchunks) nslots = nchunks;
+  return nslots > nchunks ? nchunks : nslots;
+}
+
+template <int kEpiW>
+static int launch_bf_pair(const BfArgs &a, int num_sms, cudaStream_t st) {
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, bf_pair_kernel<kEpiW>, bfp::kSmemBytes) != cudaSuccess) return -2;
+  const int nbt = a.nbeam / 64;
+  cudaLaunchConfig_t cfg = {};
+  cfg.blockDim = dim3(bfp::threads(kEpiW), 1, 1);
+  cfg.dynamicSmemBytes = bfp::kSmemBytes;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  // One wave: as many slots as pairs of SMs can hold clusters at once (an
+  // SM left without a partner in its GPC takes none), per device.
+  static std::atomic<int> max_clusters[64];   // per kernel instantiation and device
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -2;
+  int maxc = dev >= 0 && dev < 64 ? max_clusters[dev].load(std::memory_order_relaxed) : 0;
+  if (maxc <= 0) {
+    cfg.gridDim = dim3((unsigned)(2 * num_sms), 1, 1);
+    if (cudaOccupancyMaxActiveClusters(&maxc, bf_pair_kernel<kEpiW>, &cfg) != cudaSuccess ||
+        maxc < 1)
+      maxc = num_sms / 2;
+    if (dev >= 0 && dev < 64) max_clusters[dev].store(maxc, std::memory_order_relaxed);
+  }
+  const int nslots = bf_slots(a, maxc / (nbt / 2));
+  cfg.gridDim = dim3((unsigned)(nslots * nbt), 1, 1);
+  return cudaLaunchKernelEx(&cfg, bf_pair_kernel<kEpiW>, a) == cudaSuccess ? 0 : -2;
+}
+
+bool beamform_pair_ok(const BfArgs &a) { return !a.fp8 && a.nbeam % 128 == 0; }
+
+template <bool kFp8, int kEpiW>
+static int launch_bf(const BfArgs &a, int num_sms, cudaStream_t st) {
+  static SmemAttrOnce attr;
+  if (smem_attr_once(attr, bf_kernel<kFp8, kEpiW>, bf::T<kFp8>::kSmemBytes) != cudaSuccess)
+    return -2;
+  const int nbt = a.nbeam / 64;
+  const int nslots = bf_slots(a, num_sms / nbt);
   const int grid = nslots * nbt;
   void *args[] = {(void *)&a};
-  return cudaLaunchKernel((const void *)bf_kernel<kFp8>, dim3(grid), dim3(bf::kThreads), args,
-                          bf::T<kFp8>::kSmemBytes, st) == cudaSuccess
+  return cudaLaunchKernel((const void *)bf_kernel<kFp8, kEpiW>, dim3(grid),
+                          dim3(bf::threads(kEpiW)), args, bf::T<kFp8>::kSmemBytes,
+                          st) == cudaSuccess
              ? 0
              : -2;
 }
 
 int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
-  return a.fp8 ? launch_bf<true>(a, num_sms, st) : launch_bf<false>(a, num_sms, st);
+  // default and 2: CTA pairs where they apply (BF16, an even number of
+  // 64-beam tiles); 1, FP8 and the rest: one CTA per beam tile
+  if (a.path != 1 && beamform_pair_ok(a)) return launch_bf_pair<8>(a, num_sms, st);
+  return a.fp8 ? launch_bf<true, 4>(a, num_sms, st) : launch_bf<false, 4>(a, num_sms, st);
 }
 
 }  // namespace dsax

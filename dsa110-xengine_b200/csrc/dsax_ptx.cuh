@@ -285,6 +285,45 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
       : "memory");
 }
 
+// ---------------------------------------------------------------- tcgen05, CTA pairs
+// cta_group::2: the two CTAs of a 2-CTA cluster share one MMA of M = 256
+// (A rows 0-127 and D lanes in the even CTA, 128-255 in the odd one; B
+// columns 0..N/2-1 from the even CTA's shared memory, N/2..N-1 from the
+// odd one's, both at the same shared-memory offsets).  Every tcgen05
+// instruction of such a kernel uses cta_group::2.
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t *dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish_pair() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+// D[tmem] (+)= A * B^T over the pair, kind::f16; issued by the even CTA.
+__device__ __forceinline__ void umma_f16_pair(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                              uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// One arrival on the mbarrier at `bar`'s offset in each CTA of `cta_mask`
+// once all previously issued pair MMAs of this thread have completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t *bar, uint16_t cta_mask) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 "
+      "[%0], %1;" ::"r"(smem_u32(bar)),
+      "h"(cta_mask)
+      : "memory");
+}
+
 // ------------------------------------------------------------ clusters
 // Rank of this CTA in its cluster.
 __device__ __forceinline__ uint32_t cluster_ctarank() {
@@ -313,6 +352,13 @@ __device__ __forceinline__ uint32_t cluster_map_u32(uint32_t saddr, uint32_t ran
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_bar) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar)
                : "memory");
+}
+// One arrival on an mbarrier of a CTA of the cluster with the default
+// semantics (release at CTA scope, as the CTA-pair pipelines of the CUDA
+// templates use): the producer's shared-memory writes are made visible to
+// the tensor-core (async) proxy by fence.proxy.async before it.
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_bar) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
 }
 // Bulk copy from this CTA's shared memory into another CTA's of the cluster
 // (no multicast), counted as transaction bytes on that CTA's mbarrier.

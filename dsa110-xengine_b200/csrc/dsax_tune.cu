@@ -7,7 +7,8 @@
 // (4) the same correlator fed by one bulk copy per 64-packet stage and
 // unpacked by 8 warps, (5) as 4 with 16 unpack warps, (6) no corner turn:
 // the captured block read directly by clusters of four channel CTAs, (7) as
-// 6 with 16 unpack warps.
+// 6 with 16 unpack warps.  Candidates for the beamformer (bf_path): (1)
+// one CTA per 64-beam tile, (2) CTA pairs sharing a cta_group::2 MMA.
 #include <cstring>
 #include <cuda_runtime.h>
 
@@ -77,6 +78,55 @@ extern "C" int dsax_autotune(dsax_ctx *c, int reps, float *times_ms, int ntimes,
     return rc;
   }
   c->cfg.corr_path = bestp;
+  if (best_path) *best_path = bestp;
+  return DSAX_OK;
+}
+
+extern "C" int dsax_autotune_beamformer(dsax_ctx *c, int reps, float *times_ms, int ntimes,
+                                        int *best_path) {
+  if (!c || reps < 1) return DSAX_ERR_ARG;
+  if (!c->weights_ready) return set_error(c, DSAX_ERR_ARG, "dsax_set_weights not called");
+  DeviceGuard g(c->device);
+  const size_t nin = dsax_block_bytes(&c->cfg, DSAX_FMT_CAPTURED);
+  const size_t nout = dsax_beam_bytes(&c->cfg);
+  int rc;
+  if ((rc = ensure_buffer(c, c->aux[AUX_TUNE], nin + nout + 256, "autotune block")) != DSAX_OK)
+    return rc;
+  uint8_t *blk = static_cast<uint8_t *>(c->aux[AUX_TUNE].ptr);
+  uint8_t *beams = blk + ((nin + 255) & ~(size_t)255);
+  fill_pattern<<<1024, 256, 0, c->stream>>>(blk, nin, 54321u);
+  const int saved = c->cfg.bf_path;
+  constexpr int kNumPaths = 2;
+  const int paths[kNumPaths] = {1, 2};
+  float best = 1e30f;
+  int bestp = 2;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int k = 0; k < kNumPaths; ++k) {
+    c->cfg.bf_path = paths[k];
+    for (int w = 0; w < 2; ++w)
+      if ((rc = dsax_beamform(c, blk, beams, nullptr, DSAX_MEM_DEVICE)) != DSAX_OK) break;
+    if (rc != DSAX_OK) break;
+    cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps; ++r)
+      if ((rc = dsax_beamform(c, blk, beams, nullptr, DSAX_MEM_DEVICE)) != DSAX_OK) break;
+    cudaEventRecord(e1, c->stream);
+    if (rc != DSAX_OK) break;
+    if ((rc = dsax_sync(c)) != DSAX_OK) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= reps;
+    if (times_ms && k < ntimes) times_ms[k] = ms;
+    if (ms < best) { best = ms; bestp = paths[k]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != DSAX_OK) {
+    c->cfg.bf_path = saved;
+    return rc;
+  }
+  c->cfg.bf_path = bestp;
   if (best_path) *best_path = bestp;
   return DSAX_OK;
 }

@@ -53,6 +53,7 @@ class Config(ctypes.Structure):
         ("wait_limit_ns", ctypes.c_ulonglong),
         ("corr_path", ctypes.c_int),
         ("bf_fp8", ctypes.c_int),
+        ("bf_path", ctypes.c_int),
     ]
 
 
@@ -209,6 +210,7 @@ def _bind_optional(L):
         "dsax_flag_state_set_baseline": ([P, P, P, P], I),
         "dsax_flag_state_noise": ([P, P, P], I),
         "dsax_autotune": ([P, I, P, I, P], I),
+        "dsax_autotune_beamformer": ([P, I, P, I, P], I),
     }
     for name, (args, res) in table.items():
         if hasattr(L, name):
@@ -473,6 +475,17 @@ class Context:
                     "dsax_autotune")
         self.cfg.corr_path = best.value
         return {k + 1: float(t[k]) for k in range(7)}, best.value
+
+    def autotune_beamformer(self, reps: int = 10):
+        """Returns ({bf_path: ms}, chosen bf_path); the context keeps the
+        choice (dsax_set_weights first)."""
+        import numpy as np
+        t = np.zeros(2, np.float32)
+        best = ctypes.c_int(0)
+        self._check(lib().dsax_autotune_beamformer(self._h, reps, _ptr(t), 2, ctypes.byref(best)),
+                    "dsax_autotune_beamformer")
+        self.cfg.bf_path = best.value
+        return {k + 1: float(t[k]) for k in range(2)}, best.value
 
     # -- batches -----------------------------------------------------------
     def run_batch(self, descs, use_graph: bool = True):

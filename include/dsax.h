@@ -87,6 +87,12 @@ typedef struct dsax_config {
                             E4M3 with a per-antenna power-of-two scale
                             (kind::f8f6f4; the 4-bit data, shifted by the
                             antenna's exponent, are exact in E4M3) */
+    int bf_path;         /* beamformer kernel form: 0 = default (2 where it
+                            applies, else 1), 1 = one CTA per 64-beam tile,
+                            2 = CTA pairs: the two beam tiles of a 2-CTA
+                                cluster share each data stage through one
+                                cta_group::2 MMA of M = 256 (BF16 with
+                                nbeam % 128 == 0; else as 1) */
 } dsax_config;
 
 typedef struct dsax_ctx dsax_ctx;
@@ -198,6 +204,14 @@ int dsax_correlate_extract_ex(dsax_ctx *ctx, const void *in, void *out, int orde
  * sets the context's corr_path to the fastest, and returns the per-variant
  * milliseconds (times_ms[0..6] for paths 1..7, up to ntimes) and the choice. */
 int dsax_autotune(dsax_ctx *ctx, int reps, float *times_ms, int ntimes, int *best_path);
+
+/* Beamformer autotuner: times the kernel forms (bf_path 1 and 2) with the
+ * context's weights (dsax_set_weights first) on a synthetic block of its
+ * geometry, sets bf_path to the faster, and returns the milliseconds
+ * (times_ms[0..1] for paths 1..2, up to ntimes) and the choice.  Both forms
+ * compute the same beams (FP32 power within 1e-5 relative). */
+int dsax_autotune_beamformer(dsax_ctx *ctx, int reps, float *times_ms, int ntimes,
+                             int *best_path);
 
 /* Measured dense tensor-core throughput of the context's GPU (ops/s, best
  * of reps): every SM issues back-to-back tcgen05.mma M=128 N=256 from shared

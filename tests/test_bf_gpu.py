@@ -13,11 +13,11 @@ REL_TOL = 5e-3
 MEAN_TOL = 1e-3
 
 
-def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None, set_w=True):
+def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None, set_w=True, bf_path=0):
     import torch
     npkt, nant, nchan = blk.shape[:3]
     cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
-                              bf_pkt_per_out=ppo, bf_scale=scale)
+                              bf_pkt_per_out=ppo, bf_scale=scale, bf_path=bf_path)
     own = ctx is None
     ctx = ctx or dsax.Context(cfg)
     try:
@@ -63,14 +63,31 @@ def test_beamformer_config3_full_block(dsax, oracle):
     assert np.median(u8) > 60 and np.median(u8) < 200   # fixed scaling lands mid-range
 
 
+@pytest.mark.parametrize("bf_path", [1, 2])
 @pytest.mark.parametrize("nbeam,ppo,npkt,nant,nchan", [(64, 16, 32, 63, 8), (128, 4, 64, 64, 16),
                                                        (256, 8, 48, 63, 8), (192, 32, 64, 40, 24)])
-def test_beamformer_shapes(dsax, oracle, nbeam, ppo, npkt, nant, nchan):
+def test_beamformer_shapes(dsax, oracle, nbeam, ppo, npkt, nant, nchan, bf_path):
     blk = oracle.gen_block(nbeam + ppo + npkt, npkt, nant, nchan, "gauss")
     wre, wim = oracle.random_phase_weights(nbeam, nchan // 8, nbeam)
     scale = 128.0 / (2 * ppo * 16 * nant * 2 * 6.25 * 0.93)
-    u8, f32 = _beamform(dsax, blk, wre, wim, nbeam, ppo, scale)
+    u8, f32 = _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, bf_path=bf_path)
     _check(oracle, blk, wre, wim, u8, f32, ppo, scale)
+
+
+@pytest.mark.parametrize("bf_path", [2])
+def test_beamformer_paths_agree_full_block(dsax, oracle, bf_path):
+    """The CTA-pair kernel (cta_group::2) against the one-CTA kernel on a
+    full block: the same products, the epilogue's partial sums added in
+    another order, so FP32 power within 1e-5 relative and uint8 within
+    1 LSB."""
+    blk = oracle.gen_block(304, 2048, 63, 384, "gauss")
+    wre, wim = oracle.random_phase_weights(10, 48, 256)
+    scale = 128.0 / (512 * 64 * 2 * 6.25)
+    u8a, fa = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=1)
+    u8b, fb = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=bf_path)
+    rel = np.abs(fb.astype(np.float64) - fa) / np.maximum(fa, 1e-30)
+    assert rel.max() < 1e-5, rel.max()
+    assert np.abs(u8b.astype(int) - u8a.astype(int)).max() <= 1
 
 
 def test_beamformer_geometric_weights(dsax, oracle):
@@ -222,3 +239,20 @@ def test_beamformer_fp8(dsax, oracle, weights):
     rel = np.abs(got - ref) / np.maximum(ref, 1e-30)
     print(f"FP8 vs FP64 weights: mean rel {rel.mean():.2e}, max rel {rel.max():.2e}")
     assert rel.mean() < 2e-2
+
+
+def test_autotune_beamformer_picks_fastest_and_stays_correct(dsax, oracle):
+    """dsax_autotune_beamformer times both kernel forms on the context's
+    geometry, keeps the faster, and the beams stay within the oracle
+    tolerances afterwards."""
+    blk = oracle.gen_block(707, 256, 63, 64, "gauss")
+    wre, wim = oracle.random_phase_weights(12, 8, 256)
+    scale = 128.0 / (2 * 16 * 16 * 63 * 2 * 6.25 * 0.93)
+    cfg = dsax.default_config(npkt=256, nant_in=63, nchan=64, bf_scale=scale)
+    with dsax.Context(cfg) as ctx:
+        ctx.set_weights(wre, wim)
+        times, best = ctx.autotune_beamformer(reps=3)
+        assert best in (1, 2) and all(t > 0 for t in times.values())
+        assert times[best] == min(times.values())
+        u8, f32 = _beamform(dsax, blk, wre, wim, 256, 16, scale, ctx=ctx, set_w=False)
+    _check(oracle, blk, wre, wim, u8, f32, 16, scale)

@@ -67,7 +67,11 @@ def test_correlator_with_a_1ns_wait_limit_returns(dsax, oracle, corr_path):
         np.testing.assert_array_equal(got[2 * c:2 * c + 2], oracle.correlate(blk, ch0=c, nch=1))
 
 
-def test_beamformer_with_a_1ns_wait_limit_returns(dsax, oracle):
+@pytest.mark.parametrize("bf_path", [1, 2])
+def test_beamformer_with_a_1ns_wait_limit_returns(dsax, oracle, bf_path):
+    """Both kernel forms (one CTA per beam tile; CTA pairs sharing a
+    cta_group::2 MMA, whose waits span both CTAs) return after their waits
+    run out, and a fresh context is correct afterwards."""
     import torch
     blk = oracle.gen_block(809, 256, 63, 48, "gauss")
     wre, wim = oracle.random_phase_weights(10, 6, 256)
@@ -75,12 +79,13 @@ def test_beamformer_with_a_1ns_wait_limit_returns(dsax, oracle):
     nout = (256 // 16) * 256 * 6
     f32 = torch.zeros(nout, dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
-    with dsax.Context(dsax.default_config(npkt=256, nchan=48, wait_limit_ns=1)) as ctx:
+    with dsax.Context(dsax.default_config(npkt=256, nchan=48, wait_limit_ns=1,
+                                          bf_path=bf_path)) as ctx:
         ctx.set_weights(wre, wim)
         ctx.beamform(d_in, None, f32)
         assert _sync_status(dsax, ctx) in (dsax.DSAX_OK, dsax.DSAX_ERR_TIMEOUT)
         ctx.sync()
-    with dsax.Context(dsax.default_config(npkt=256, nchan=48)) as ctx:
+    with dsax.Context(dsax.default_config(npkt=256, nchan=48, bf_path=bf_path)) as ctx:
         ctx.set_weights(wre, wim)
         f32.zero_()
         torch.cuda.synchronize()
