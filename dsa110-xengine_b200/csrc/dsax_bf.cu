@@ -536,26 +536,36 @@ __global__ void __launch_bounds__(bf::threads(kEpiW), 1) bf_kernel(BfArgs a) {
 namespace bfp {
 constexpr int kPktPerCta = 8;                        // packets of a 16-packet stage per CTA
 constexpr int kDHalfBytes = 128 * bf::kKBlockBytes;  // 128 B rows x 128 B = 16 KB per K block
-constexpr int kStageBytes = 2 * kDHalfBytes;         // BF16: two K blocks
-constexpr int kStages = 4;
-constexpr int kWBytes = 2 /*pol*/ * 2 /*kb*/ * bf::kWTileBytes;   // own beam tile, 64 KB
-constexpr int kRawRowBytes = bf::kProducers * 16;    // one 16 B load per producer thread
-constexpr int kRawBytes = 4 * kRawRowBytes;          // 16 KB: 8 packets x 64 ant x 32 B
+constexpr int kRawBytes = 16384;                     // 8 packets x 64 ant x 32 B
 constexpr int threads(int epi_warps) { return bf::kProducers + 32 * epi_warps + 32; }
-constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
-constexpr uint32_t kIdesc = umma_idesc(1, 1, 1, 256, bf::kN);
 constexpr uint16_t kBoth = 0x3;                      // CTA mask of the pair
+// BF16: two 128-byte K blocks per operand row; FP8 E4M3: one.
+template <bool kFp8> struct T {
+  static constexpr int kKB = kFp8 ? 1 : 2;
+  static constexpr int kStageBytes = kKB * kDHalfBytes;
+  static constexpr int kStages = kFp8 ? 6 : 4;
+  static constexpr int kWBytes = 2 /*pol*/ * kKB * bf::kWTileBytes;   // own beam tile
+  // raw staging per thread: BF16 four 16 B loads (4 antennas x 4 channels),
+  // FP8 eight 8 B loads (8 antennas x 2 channels)
+  static constexpr int kRawLoads = kFp8 ? 8 : 4;
+  static constexpr int kRawLoadBytes = kFp8 ? 8 : 16;
+  static constexpr int kRawRowBytes = bf::kProducers * kRawLoadBytes;
+  static constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
+  static constexpr uint32_t kIdesc =
+      kFp8 ? umma_idesc(1, 0, 0, 256, bf::kN) : umma_idesc(1, 1, 1, 256, bf::kN);
+};
 }  // namespace bfp
 
-template <int kEpiW>
+template <bool kFp8, int kEpiW>
 __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs a) {
+  using TT = bfp::T<kFp8>;
   constexpr int kMmaWarp = 8 + kEpiW;                 // TMEM, weights, MMA issue
   constexpr int kEpiThreads = 32 * kEpiW;
   using bf::kKBlockBytes;
   using bf::kN;
   using bf::kPktPerStage;
   using bf::kWTileBytes;
-  constexpr int kStages = bfp::kStages, kStageBytes = bfp::kStageBytes;
+  constexpr int kStages = TT::kStages, kStageBytes = TT::kStageBytes;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kStages];   // even CTA: 16 producer-warp arrivals
   __shared__ __align__(8) uint64_t empty_bar[kStages];  // both: one commit
@@ -575,7 +585,7 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
   // identical offsets in both CTAs (same kernel, same static shared memory)
   const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
   const uint32_t wsm = base;                          // own A tile [pol][kb][128 x 128 B]
-  const uint32_t dsm = base + bfp::kWBytes;           // B halves [s][kb][128 x 128 B]
+  const uint32_t dsm = base + TT::kWBytes;            // B halves [s][kb][128 x 128 B]
   const uint32_t raw = dsm + kStages * kStageBytes;   // producer staging [4][256][16 B]
 
   // Work split as bf_kernel: the nbt CTAs of a slot share a (g, pg) range;
@@ -622,28 +632,51 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
 
   if (warp < 8) {
     // ------------------------------------------------------------ producers
-    // Thread (kb, q8, j, h): K block kb, packet 8 rank + q8 of the stage,
-    // antennas 32 kb + 4j .. +3, channels 4h .. 4h+3 of the group: four
-    // 16 B loads per packet group (both pols), eight 16 B stores per stage.
-    const int h = tid & 1, j = (tid >> 1) & 7, q8 = (tid >> 4) & 7, kb = tid >> 7;
+    // BF16: thread (kb, q8, j, h): K block kb, packet 8 rank + q8 of the
+    // stage, antennas 32 kb + 4j .. +3, channels 4h .. 4h+3 of the group:
+    // four 16 B loads per packet group (both pols), eight 16 B stores per
+    // stage.  FP8: thread (q8, j, kh, w2): packet 8 rank + q8, antennas
+    // 8j .. 8j+7 (one 16-byte K chunk of the single K block), channels
+    // 4kh + 2w2 + {0, 1}: eight 8 B loads, four 16 B stores per stage.
+    const int q8 = kFp8 ? tid >> 5 : (tid >> 4) & 7;
+    const int j = kFp8 ? (tid >> 2) & 7 : (tid >> 1) & 7;
+    const int h = kFp8 ? (tid >> 1) & 1 : tid & 1;     // channel half
+    const int w2 = tid & 1;                            // FP8: channel pair of the half
+    const int kb = kFp8 ? 0 : tid >> 7;
     const int q = bfp::kPktPerCta * (int)rank + q8;
     const int64_t ant_stride = (int64_t)a.nchan * 4;
     const int64_t pkt_stride = (int64_t)a.nant_in * ant_stride;
-    const uint32_t myraw = raw + 16u * (uint32_t)tid;
-    uint4 Ucur[4];
+    const uint32_t myraw = raw + (uint32_t)TT::kRawLoadBytes * (uint32_t)tid;
+    uint32_t U[TT::kRawLoads][TT::kRawLoadBytes / 4];
+    // FP8: exponent offsets 8d of this thread's 8 antennas, one byte per
+    // E4M3 output byte ([re, im] per antenna, two antennas per word)
+    uint32_t shift_add[4] = {0u, 0u, 0u, 0u};
+    if (kFp8 && a.e4m3_add) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t a0 = (uint32_t)a.e4m3_add[8 * j + 2 * e] & 0x7Fu;
+        const uint32_t a1 = (uint32_t)a.e4m3_add[8 * j + 2 * e + 1] & 0x7Fu;
+        shift_add[e] = a0 | (a0 << 8) | (a1 << 16) | (a1 << 24);
+      }
+    }
     auto stage_group = [&](int r) {
       const int g = r / npg, pg = r % npg;
       const int p = pg * kPktPerStage + q;
 #pragma unroll
-      for (int ii = 0; ii < 4; ++ii) {
-        const int ant = 32 * kb + 4 * j + ii;
+      for (int ii = 0; ii < TT::kRawLoads; ++ii) {
+        const int ant = kFp8 ? 8 * j + ii : 32 * kb + 4 * j + ii;
         const bool ok = ant < a.nant_in && p < a.npkt;
-        const uint8_t *src =
-            a.in + (ok ? p * pkt_stride + ant * ant_stride + (int64_t)(8 * g + 4 * h) * 4 : 0);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
-                         myraw + (uint32_t)ii * bfp::kRawRowBytes),
-                     "l"(src), "r"(ok ? 16 : 0)
-                     : "memory");
+        const int chan = 8 * g + 4 * h + (kFp8 ? 2 * w2 : 0);
+        const uint8_t *src = a.in + (ok ? p * pkt_stride + ant * ant_stride + (int64_t)chan * 4 : 0);
+        const uint32_t dst = myraw + (uint32_t)ii * TT::kRawRowBytes;
+        if constexpr (kFp8)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src),
+                       "r"(ok ? 8 : 0)
+                       : "memory");
+        else
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                       "r"(ok ? 16 : 0)
+                       : "memory");
       }
       asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -658,35 +691,64 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
       if (pol == 0) {
         asm volatile("cp.async.wait_all;" ::: "memory");
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
-                       : "=r"(Ucur[k].x), "=r"(Ucur[k].y), "=r"(Ucur[k].z), "=r"(Ucur[k].w)
-                       : "r"(myraw + (uint32_t)k * bfp::kRawRowBytes)
-                       : "memory");
+        for (int k = 0; k < TT::kRawLoads; ++k) {
+          const uint32_t src = myraw + (uint32_t)k * TT::kRawRowBytes;
+          if constexpr (kFp8)
+            asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];"
+                         : "=r"(U[k][0]), "=r"(U[k][1])
+                         : "r"(src)
+                         : "memory");
+          else
+            asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(U[k][0]), "=r"(U[k][1]), "=r"(U[k][2]), "=r"(U[k][3])
+                         : "r"(src)
+                         : "memory");
         }
         if (u + 2 < u_hi) stage_group((u >> 1) + 1);
       }
       const bool ok = mbar_wait_bounded(&empty_bar[s], ph ^ 1u, &abort_sh, a.err,
-                                              DEV_ERR_WAIT_EMPTY, a.wait_limit_ns);
+                                        DEV_ERR_WAIT_EMPTY, a.wait_limit_ns);
       if (!__all_sync(0xffffffffu, ok)) break;
       const uint32_t sel = (uint32_t)pol | ((4u + pol) << 4) | ((2u + pol) << 8) | ((6u + pol) << 12);
       const uint32_t tile = dsm + (uint32_t)s * kStageBytes + (uint32_t)kb * bfp::kDHalfBytes;
+      if constexpr (kFp8) {
 #pragma unroll
-      for (int w = 0; w < 4; ++w) {
-        const uint32_t u0 = w == 0 ? Ucur[0].x : w == 1 ? Ucur[0].y : w == 2 ? Ucur[0].z : Ucur[0].w;
-        const uint32_t u1 = w == 0 ? Ucur[1].x : w == 1 ? Ucur[1].y : w == 2 ? Ucur[1].z : Ucur[1].w;
-        const uint32_t u2 = w == 0 ? Ucur[2].x : w == 1 ? Ucur[2].y : w == 2 ? Ucur[2].z : Ucur[2].w;
-        const uint32_t u3 = w == 0 ? Ucur[3].x : w == 1 ? Ucur[3].y : w == 2 ? Ucur[3].z : Ucur[3].w;
-        const uint32_t t01 = __byte_perm(u0, u1, sel);
-        const uint32_t t23 = __byte_perm(u2, u3, sel);
+        for (int wl = 0; wl < 2; ++wl) {                // channel 4h + 2 w2 + wl of the group
+          // t[ag][pair]: antennas 8j + 4ag + 2pair, +1 at time 0 (bits 0-15)
+          // and time 1 (bits 16-31)
+          uint32_t t[2][2];
 #pragma unroll
-        for (int odd = 0; odd < 2; ++odd) {
-          const uint32_t x = __byte_perm(t01, t23, odd ? 0x7632u : 0x5410u);
-          uint32_t o[4];
-          nib8_to_bf16x8(x, o);
-          const int k = 8 * h + 2 * w + odd;      // chunnel = 2*chan + time
-          const uint32_t row = (uint32_t)(16 * q8 + k);   // row of this CTA's B half
-          st_shared_v4(tile + sw128_offset(row, (uint32_t)j), o[0], o[1], o[2], o[3]);
+          for (int ag = 0; ag < 2; ++ag) {
+            t[ag][0] = __byte_perm(U[4 * ag][wl], U[4 * ag + 1][wl], sel);
+            t[ag][1] = __byte_perm(U[4 * ag + 2][wl], U[4 * ag + 3][wl], sel);
+          }
+#pragma unroll
+          for (int odd = 0; odd < 2; ++odd) {
+            uint32_t o[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const uint32_t sel2 = t[e >> 1][e & 1] >> (16 * odd);
+              o[e] = a.e4m3_add ? nib2_to_e4m3x4_shift(sel2, shift_add[e]) : nib2_to_e4m3x4(sel2);
+            }
+            const int k = 8 * h + 2 * (2 * w2 + wl) + odd;   // chunnel = 2*chan + time
+            const uint32_t row = (uint32_t)(16 * q8 + k);     // row of this CTA's B half
+            st_shared_v4(tile + sw128_offset(row, (uint32_t)j), o[0], o[1], o[2], o[3]);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const uint32_t t01 = __byte_perm(U[0][w], U[1][w], sel);
+          const uint32_t t23 = __byte_perm(U[2][w], U[3][w], sel);
+#pragma unroll
+          for (int odd = 0; odd < 2; ++odd) {
+            const uint32_t x = __byte_perm(t01, t23, odd ? 0x7632u : 0x5410u);
+            uint32_t o[4];
+            nib8_to_bf16x8(x, o);
+            const int k = 8 * h + 2 * w + odd;      // chunnel = 2*chan + time
+            const uint32_t row = (uint32_t)(16 * q8 + k);   // row of this CTA's B half
+            st_shared_v4(tile + sw128_offset(row, (uint32_t)j), o[0], o[1], o[2], o[3]);
+          }
         }
       }
       fence_proxy_async_smem();
@@ -721,13 +783,28 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
         uint32_t r0[32];
         tmem_ld32(taddr + 32u * c, r0);
         tmem_wait_ld();
-        uint64_t s2[4] = {0ull, 0ull, 0ull, 0ull};
+        float sq;
+        if constexpr (kFp8) {   // scalar chains (the packed form measured slower for FP8)
+          float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
-        for (int e = 0; e < 32; e += 8)
+          for (int e = 0; e < 32; e += 4) {
+            const float v0 = __uint_as_float(r0[e]), v1 = __uint_as_float(r0[e + 1]);
+            const float v2 = __uint_as_float(r0[e + 2]), v3 = __uint_as_float(r0[e + 3]);
+            s0 = fmaf(v0, v0, s0);
+            s1 = fmaf(v1, v1, s1);
+            s2 = fmaf(v2, v2, s2);
+            s3 = fmaf(v3, v3, s3);
+          }
+          sq = (s0 + s1) + (s2 + s3);
+        } else {
+          uint64_t s2[4] = {0ull, 0ull, 0ull, 0ull};
 #pragma unroll
-          for (int k = 0; k < 4; ++k) s2[k] = sqacc_f32x2(r0[e + 2 * k], r0[e + 2 * k + 1], s2[k]);
-        const float sq =
-            (hsum_f32x2(s2[0]) + hsum_f32x2(s2[1])) + (hsum_f32x2(s2[2]) + hsum_f32x2(s2[3]));
+          for (int e = 0; e < 32; e += 8)
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+              s2[k] = sqacc_f32x2(r0[e + 2 * k], r0[e + 2 * k + 1], s2[k]);
+          sq = (hsum_f32x2(s2[0]) + hsum_f32x2(s2[1])) + (hsum_f32x2(s2[2]) + hsum_f32x2(s2[3]));
+        }
         const int sub = (32 * c) / span;
         if (nsub == 1) acc[0] += sq;
         else if (sub == 0) acc[0] += sq;
@@ -790,10 +867,10 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
               break;
             ++ndrain;
           }
-          mbar_arrive_expect_tx(&wload_bar, (uint32_t)bfp::kWBytes);
-          const uint8_t *src = a.wimg + (int64_t)(g * nbt + bt) * bfp::kWBytes;
+          mbar_arrive_expect_tx(&wload_bar, (uint32_t)TT::kWBytes);
+          const uint8_t *src = a.wimg + (int64_t)(g * nbt + bt) * TT::kWBytes;
 #pragma unroll
-          for (int c = 0; c < bfp::kWBytes / 16384; ++c)
+          for (int c = 0; c < TT::kWBytes / 16384; ++c)
             bulk_g2s(wsm + 16384u * c, src + 16384 * c, 16384u, &wload_bar);
           if (!mbar_wait_bounded(&wload_bar, nload & 1u, &abort_sh, a.err, DEV_ERR_WAIT_FULL,
                                  a.wait_limit_ns)) {
@@ -821,14 +898,17 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
                                      a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
           break;
         tc_fence_after();
-        const uint32_t wpol = wsm + (uint32_t)pol * (2u * kWTileBytes);
+        const uint32_t wpol = wsm + (uint32_t)pol * (uint32_t)(TT::kKB * kWTileBytes);
         const uint32_t stage = dsm + (uint32_t)s * kStageBytes;
 #pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {   // 32-byte K steps (16 bf16)
+        for (int kk = 0; kk < 4 * TT::kKB; ++kk) {   // 32-byte K steps (16 bf16 / 32 e4m3)
           const uint32_t kb = kk >> 2, koff = 32u * (kk & 3);
           const uint64_t ad = umma_desc_sw128(wpol + kb * kWTileBytes + koff, 1024u);
           const uint64_t bd = umma_desc_sw128(stage + kb * bfp::kDHalfBytes + koff, 1024u);
-          umma_f16_pair(tmem + (uint32_t)b * 256u, ad, bd, bfp::kIdesc, kk > 0);
+          if constexpr (kFp8)
+            umma_f8_pair(tmem + (uint32_t)b * 256u, ad, bd, TT::kIdesc, kk > 0);
+          else
+            umma_f16_pair(tmem + (uint32_t)b * 256u, ad, bd, TT::kIdesc, kk > 0);
         }
         umma_commit_pair(&empty_bar[s], bfp::kBoth);
         umma_commit_pair(&tfull_bar[b], bfp::kBoth);
@@ -863,14 +943,14 @@ static int bf_slots(const BfArgs &a, int nslots) {
   return nslots > nchunks ? nchunks : nslots;
 }
 
-template <int kEpiW>
+template <bool kFp8, int kEpiW>
 static int launch_bf_pair(const BfArgs &a, int num_sms, cudaStream_t st) {
   static SmemAttrOnce attr;
-  if (smem_attr_once(attr, bf_pair_kernel<kEpiW>, bfp::kSmemBytes) != cudaSuccess) return -2;
+  if (smem_attr_once(attr, bf_pair_kernel<kFp8, kEpiW>, bfp::T<kFp8>::kSmemBytes) != cudaSuccess) return -2;
   const int nbt = a.nbeam / 64;
   cudaLaunchConfig_t cfg = {};
   cfg.blockDim = dim3(bfp::threads(kEpiW), 1, 1);
-  cfg.dynamicSmemBytes = bfp::kSmemBytes;
+  cfg.dynamicSmemBytes = bfp::T<kFp8>::kSmemBytes;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -887,17 +967,17 @@ static int launch_bf_pair(const BfArgs &a, int num_sms, cudaStream_t st) {
   int maxc = dev >= 0 && dev < 64 ? max_clusters[dev].load(std::memory_order_relaxed) : 0;
   if (maxc <= 0) {
     cfg.gridDim = dim3((unsigned)(2 * num_sms), 1, 1);
-    if (cudaOccupancyMaxActiveClusters(&maxc, bf_pair_kernel<kEpiW>, &cfg) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveClusters(&maxc, bf_pair_kernel<kFp8, kEpiW>, &cfg) != cudaSuccess ||
         maxc < 1)
       maxc = num_sms / 2;
     if (dev >= 0 && dev < 64) max_clusters[dev].store(maxc, std::memory_order_relaxed);
   }
   const int nslots = bf_slots(a, maxc / (nbt / 2));
   cfg.gridDim = dim3((unsigned)(nslots * nbt), 1, 1);
-  return cudaLaunchKernelEx(&cfg, bf_pair_kernel<kEpiW>, a) == cudaSuccess ? 0 : -2;
+  return cudaLaunchKernelEx(&cfg, bf_pair_kernel<kFp8, kEpiW>, a) == cudaSuccess ? 0 : -2;
 }
 
-bool beamform_pair_ok(const BfArgs &a) { return !a.fp8 && a.nbeam % 128 == 0; }
+bool beamform_pair_ok(const BfArgs &a) { return a.nbeam % 128 == 0; }
 
 template <bool kFp8, int kEpiW>
 static int launch_bf(const BfArgs &a, int num_sms, cudaStream_t st) {
@@ -918,7 +998,8 @@ static int launch_bf(const BfArgs &a, int num_sms, cudaStream_t st) {
 int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
   // default and 2: CTA pairs where they apply (BF16, an even number of
   // 64-beam tiles); 1, FP8 and the rest: one CTA per beam tile
-  if (a.path != 1 && beamform_pair_ok(a)) return launch_bf_pair<8>(a, num_sms, st);
+  if (a.path != 1 && beamform_pair_ok(a))
+    return a.fp8 ? launch_bf_pair<true, 8>(a, num_sms, st) : launch_bf_pair<false, 8>(a, num_sms, st);
   return a.fp8 ? launch_bf<true, 4>(a, num_sms, st) : launch_bf<false, 4>(a, num_sms, st);
 }
 

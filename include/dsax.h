@@ -91,8 +91,8 @@ typedef struct dsax_config {
                             applies, else 1), 1 = one CTA per 64-beam tile,
                             2 = CTA pairs: the two beam tiles of a 2-CTA
                                 cluster share each data stage through one
-                                cta_group::2 MMA of M = 256 (BF16 with
-                                nbeam % 128 == 0; else as 1) */
+                                cta_group::2 MMA of M = 256 (BF16 or
+                                FP8, nbeam % 128 == 0; else as 1) */
 } dsax_config;
 
 typedef struct dsax_ctx dsax_ctx;

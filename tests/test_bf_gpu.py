@@ -13,11 +13,11 @@ REL_TOL = 5e-3
 MEAN_TOL = 1e-3
 
 
-def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None, set_w=True, bf_path=0):
+def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None, set_w=True, bf_path=0, fp8=0):
     import torch
     npkt, nant, nchan = blk.shape[:3]
     cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
-                              bf_pkt_per_out=ppo, bf_scale=scale, bf_path=bf_path)
+                              bf_pkt_per_out=ppo, bf_scale=scale, bf_path=bf_path, bf_fp8=fp8)
     own = ctx is None
     ctx = ctx or dsax.Context(cfg)
     try:
@@ -74,17 +74,17 @@ def test_beamformer_shapes(dsax, oracle, nbeam, ppo, npkt, nant, nchan, bf_path)
     _check(oracle, blk, wre, wim, u8, f32, ppo, scale)
 
 
-@pytest.mark.parametrize("bf_path", [2])
-def test_beamformer_paths_agree_full_block(dsax, oracle, bf_path):
+@pytest.mark.parametrize("fp8", [0, 1])
+def test_beamformer_paths_agree_full_block(dsax, oracle, fp8):
     """The CTA-pair kernel (cta_group::2) against the one-CTA kernel on a
-    full block: the same products, the epilogue's partial sums added in
-    another order, so FP32 power within 1e-5 relative and uint8 within
-    1 LSB."""
+    full block, BF16 and FP8: the same products, the epilogue's partial
+    sums added in another order, so FP32 power within 1e-5 relative and
+    uint8 within 1 LSB."""
     blk = oracle.gen_block(304, 2048, 63, 384, "gauss")
     wre, wim = oracle.random_phase_weights(10, 48, 256)
     scale = 128.0 / (512 * 64 * 2 * 6.25)
-    u8a, fa = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=1)
-    u8b, fb = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=bf_path)
+    u8a, fa = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=1, fp8=fp8)
+    u8b, fb = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=2, fp8=fp8)
     rel = np.abs(fb.astype(np.float64) - fa) / np.maximum(fa, 1e-30)
     assert rel.max() < 1e-5, rel.max()
     assert np.abs(u8b.astype(int) - u8a.astype(int)).max() <= 1
@@ -196,10 +196,12 @@ def test_agc_bandpass_sequence(dsax, oracle):
     assert clamped > 0
 
 
+@pytest.mark.parametrize("bf_path", [1, 2])
 @pytest.mark.parametrize("weights", ["unit", "calibrated"])
-def test_beamformer_fp8(dsax, oracle, weights):
+def test_beamformer_fp8(dsax, oracle, weights, bf_path):
     """FP8 E4M3 operands (kind::f8f6f4) with the per-antenna power-of-two
-    scale (calibrated: gains spread over e^6 between antennas): against the FP64
+    scale, one CTA per beam tile (bf_path 1) and CTA pairs (2; calibrated:
+    gains spread over e^6 between antennas): against the FP64
     oracle run with the same E4M3-rounded
     weights the FP32 power agrees to 1e-4 (the data are exact in E4M3 and
     the products exact in FP32); against the unrounded FP64 weights the
@@ -223,7 +225,7 @@ def test_beamformer_fp8(dsax, oracle, weights):
     ref = oracle.beamform_power(blk, wre, wim, pkt_per_out=ppo)
     scale = 128.0 / float(np.median(ref))
     cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
-                              bf_pkt_per_out=ppo, bf_scale=scale, bf_fp8=1)
+                              bf_pkt_per_out=ppo, bf_scale=scale, bf_fp8=1, bf_path=bf_path)
     with dsax.Context(cfg) as ctx:
         ctx.set_weights(wre, wim)
         d_in = torch.from_numpy(blk.reshape(-1)).cuda()
