@@ -546,12 +546,34 @@ def bench_batch(dsax, synth, dev, steps):
         graph_ms = _time_loop(st, lambda i: ctx.run_batch(descs, use_graph=True), steps)
         eager_ms = _time_loop(st, lambda i: ctx.run_batch(descs, use_graph=False), steps)
         ctx.sync()
+    # the same batch with the one-CTA-per-beam-tile beamformer (bf_path 1)
+    cfg1 = dsax.default_config(nchan=768, bf_scale=128.0 / (512 * 64 * 2 * 6.25), bf_path=1)
+    with dsax.Context(cfg1, device=dev) as ctx:
+        ctx.set_weights(wre, wim)
+        st = torch.cuda.ExternalStream(ctx.stream)
+        graph1_ms = _time_loop(st, lambda i: ctx.run_batch(descs, use_graph=True), steps)
+        ctx.sync()
     nb = len(widths)
+    # work of the batch, and its rate over the whole batch time (the stages
+    # share that time on two streams, so these are lower bounds per stage)
+    bf_flop = BF_FLOPS * sum(widths) / 384.0
+    corr_bytes = sum(2048 * 63 * w * 4 + 2 * w * 2080 * 8 for w in widths)
+    burst, _, kind = _bf16_peak()
+    hbm = _peaks()[0]
     return {"workload": "16 blocks x 2048 pkt x 63 ant, widths " + ",".join(map(str, widths)),
             "widths": widths,
             "graph": {"blocks_per_s": nb * 1e3 / graph_ms, "ms_per_batch": graph_ms},
             "per_block_launches": {"blocks_per_s": nb * 1e3 / eager_ms, "ms_per_batch": eager_ms},
+            "graph_one_cta_beamformer": {"blocks_per_s": nb * 1e3 / graph1_ms,
+                                         "ms_per_batch": graph1_ms},
             "realtime_factor_graph": nb * 1e3 / graph_ms * REALTIME_S * 384.0 / np.mean(widths),
+            "over_batch_time": {
+                "beamformer_tflops": bf_flop / (graph_ms * 1e-3) / 1e12,
+                "beamformer_frac_of_bf16_burst": bf_flop / (graph_ms * 1e-3) / 1e12 / burst,
+                "correlation_alg_gbs": corr_bytes / (graph_ms * 1e-3) / 1e9,
+                "correlation_frac_of_hbm": corr_bytes / (graph_ms * 1e-3) / 1e9 / hbm,
+                "note": "each stage's work over the whole batch time (lower bounds): the "
+                        "beamformer takes about 60 % of it, the correlation chain 30 %"},
             "gpu_launches_per_batch": 5 * nb}
 
 

@@ -65,7 +65,8 @@ def test_beamformer_config3_full_block(dsax, oracle):
 
 @pytest.mark.parametrize("bf_path", [1, 2])
 @pytest.mark.parametrize("nbeam,ppo,npkt,nant,nchan", [(64, 16, 32, 63, 8), (128, 4, 64, 64, 16),
-                                                       (256, 8, 48, 63, 8), (192, 32, 64, 40, 24)])
+                                                       (256, 8, 48, 63, 8), (192, 32, 64, 40, 24),
+                                                       (256, 32, 96, 40, 24), (512, 16, 32, 63, 16)])
 def test_beamformer_shapes(dsax, oracle, nbeam, ppo, npkt, nant, nchan, bf_path):
     blk = oracle.gen_block(nbeam + ppo + npkt, npkt, nant, nchan, "gauss")
     wre, wim = oracle.random_phase_weights(nbeam, nchan // 8, nbeam)
