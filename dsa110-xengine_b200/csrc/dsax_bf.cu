@@ -539,26 +539,28 @@ constexpr int kDHalfBytes = 128 * bf::kKBlockBytes;  // 128 B rows x 128 B = 16 
 constexpr int kRawBytes = 16384;                     // 8 packets x 64 ant x 32 B
 constexpr int threads(int epi_warps) { return bf::kProducers + 32 * epi_warps + 32; }
 constexpr uint16_t kBoth = 0x3;                      // CTA mask of the pair
-// BF16: two 128-byte K blocks per operand row; FP8 E4M3: one.
-template <bool kFp8> struct T {
+// BF16: two 128-byte K blocks per operand row; FP8 E4M3: one.  kRD raw
+// staging slots (packet groups of loads in flight ahead of the one being
+// converted).
+template <bool kFp8, int kRD> struct T {
   static constexpr int kKB = kFp8 ? 1 : 2;
   static constexpr int kStageBytes = kKB * kDHalfBytes;
-  static constexpr int kStages = kFp8 ? 6 : 4;
+  static constexpr int kStages = kFp8 ? 6 : (kRD > 1 ? 3 : 4);
   static constexpr int kWBytes = 2 /*pol*/ * kKB * bf::kWTileBytes;   // own beam tile
   // raw staging per thread: BF16 four 16 B loads (4 antennas x 4 channels),
   // FP8 eight 8 B loads (8 antennas x 2 channels)
   static constexpr int kRawLoads = kFp8 ? 8 : 4;
   static constexpr int kRawLoadBytes = kFp8 ? 8 : 16;
   static constexpr int kRawRowBytes = bf::kProducers * kRawLoadBytes;
-  static constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRawBytes;
+  static constexpr int kSmemBytes = 1024 + kWBytes + kStages * kStageBytes + kRD * kRawBytes;
   static constexpr uint32_t kIdesc =
       kFp8 ? umma_idesc(1, 0, 0, 256, bf::kN) : umma_idesc(1, 1, 1, 256, bf::kN);
 };
 }  // namespace bfp
 
-template <bool kFp8, int kEpiW, int kLdG>
+template <bool kFp8, int kEpiW, int kLdG, int kRD>
 __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs a) {
-  using TT = bfp::T<kFp8>;
+  using TT = bfp::T<kFp8, kRD>;
   constexpr int kMmaWarp = 8 + kEpiW;                 // TMEM, weights, MMA issue
   constexpr int kEpiThreads = 32 * kEpiW;
   using bf::kKBlockBytes;
@@ -662,13 +664,14 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
     auto stage_group = [&](int r) {
       const int g = r / npg, pg = r % npg;
       const int p = pg * kPktPerStage + q;
+      const uint32_t slot = (uint32_t)(r % kRD) * bfp::kRawBytes;
 #pragma unroll
       for (int ii = 0; ii < TT::kRawLoads; ++ii) {
         const int ant = kFp8 ? 8 * j + ii : 32 * kb + 4 * j + ii;
         const bool ok = ant < a.nant_in && p < a.npkt;
         const int chan = 8 * g + 4 * h + (kFp8 ? 2 * w2 : 0);
         const uint8_t *src = a.in + (ok ? p * pkt_stride + ant * ant_stride + (int64_t)chan * 4 : 0);
-        const uint32_t dst = myraw + (uint32_t)ii * TT::kRawRowBytes;
+        const uint32_t dst = myraw + slot + (uint32_t)ii * TT::kRawRowBytes;
         if constexpr (kFp8)
           asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src),
                        "r"(ok ? 8 : 0)
@@ -680,7 +683,11 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
       }
       asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    if (u_lo < u_hi) stage_group(u_lo >> 1);
+    // packet groups r = u / 2 of the range: the first kRD are staged now,
+    // group r + kRD when group r is read (into the slot it frees)
+#pragma unroll
+    for (int d = 0; d < kRD; ++d)
+      if (2 * ((u_lo >> 1) + d) < u_hi) stage_group((u_lo >> 1) + d);
     // every exit from this loop is warp-uniform (the warp meets in
     // __syncwarp / __all_sync below)
     for (int u = u_lo, i = 0; u < u_hi; ++u, ++i) {
@@ -689,10 +696,16 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
       const uint32_t ph = (uint32_t)(i / kStages) & 1u;
       const int pol = u & 1;
       if (pol == 0) {
-        asm volatile("cp.async.wait_all;" ::: "memory");
+        const int r = u >> 1;
+        // group r's copies landed (with two slots the next group may still be in flight)
+        if (kRD > 1 && 2 * (r + 1) < u_hi)
+          asm volatile("cp.async.wait_group 1;" ::: "memory");
+        else
+          asm volatile("cp.async.wait_all;" ::: "memory");
+        const uint32_t slot = (uint32_t)(r % kRD) * bfp::kRawBytes;
 #pragma unroll
         for (int k = 0; k < TT::kRawLoads; ++k) {
-          const uint32_t src = myraw + (uint32_t)k * TT::kRawRowBytes;
+          const uint32_t src = myraw + slot + (uint32_t)k * TT::kRawRowBytes;
           if constexpr (kFp8)
             asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];"
                          : "=r"(U[k][0]), "=r"(U[k][1])
@@ -704,7 +717,7 @@ __global__ void __launch_bounds__(bfp::threads(kEpiW), 1) bf_pair_kernel(BfArgs 
                          : "r"(src)
                          : "memory");
         }
-        if (u + 2 < u_hi) stage_group((u >> 1) + 1);
+        if (2 * (r + kRD) < u_hi) stage_group(r + kRD);
       }
       const bool ok = mbar_wait_bounded(&empty_bar[s], ph ^ 1u, &abort_sh, a.err,
                                         DEV_ERR_WAIT_EMPTY, a.wait_limit_ns);
@@ -948,14 +961,14 @@ static int bf_slots(const BfArgs &a, int nslots) {
   return nslots > nchunks ? nchunks : nslots;
 }
 
-template <bool kFp8, int kEpiW, int kLdG>
+template <bool kFp8, int kEpiW, int kLdG, int kRD>
 static int launch_bf_pair(const BfArgs &a, int num_sms, cudaStream_t st) {
   static SmemAttrOnce attr;
-  if (smem_attr_once(attr, bf_pair_kernel<kFp8, kEpiW, kLdG>, bfp::T<kFp8>::kSmemBytes) != cudaSuccess) return -2;
+  if (smem_attr_once(attr, bf_pair_kernel<kFp8, kEpiW, kLdG, kRD>, bfp::T<kFp8, kRD>::kSmemBytes) != cudaSuccess) return -2;
   const int nbt = a.nbeam / 64;
   cudaLaunchConfig_t cfg = {};
   cfg.blockDim = dim3(bfp::threads(kEpiW), 1, 1);
-  cfg.dynamicSmemBytes = bfp::T<kFp8>::kSmemBytes;
+  cfg.dynamicSmemBytes = bfp::T<kFp8, kRD>::kSmemBytes;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -972,14 +985,14 @@ static int launch_bf_pair(const BfArgs &a, int num_sms, cudaStream_t st) {
   int maxc = dev >= 0 && dev < 64 ? max_clusters[dev].load(std::memory_order_relaxed) : 0;
   if (maxc <= 0) {
     cfg.gridDim = dim3((unsigned)(2 * num_sms), 1, 1);
-    if (cudaOccupancyMaxActiveClusters(&maxc, bf_pair_kernel<kFp8, kEpiW, kLdG>, &cfg) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveClusters(&maxc, bf_pair_kernel<kFp8, kEpiW, kLdG, kRD>, &cfg) != cudaSuccess ||
         maxc < 1)
       maxc = num_sms / 2;
     if (dev >= 0 && dev < 64) max_clusters[dev].store(maxc, std::memory_order_relaxed);
   }
   const int nslots = bf_slots(a, maxc / (nbt / 2));
   cfg.gridDim = dim3((unsigned)(nslots * nbt), 1, 1);
-  return cudaLaunchKernelEx(&cfg, bf_pair_kernel<kFp8, kEpiW, kLdG>, a) == cudaSuccess ? 0 : -2;
+  return cudaLaunchKernelEx(&cfg, bf_pair_kernel<kFp8, kEpiW, kLdG, kRD>, a) == cudaSuccess ? 0 : -2;
 }
 
 bool beamform_pair_ok(const BfArgs &a) { return a.nbeam % 128 == 0; }
@@ -1004,8 +1017,12 @@ int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
   // default and 2: CTA pairs where they apply (BF16, an even number of
   // 64-beam tiles); 1, FP8 and the rest: one CTA per beam tile
   // FP8 epilogues keep two TMEM loads in flight (2.4 % faster; BF16 1 % slower)
+  // FP8: two raw staging slots beside its six 16 KB stages (1 % faster);
+  // BF16 keeps one slot and four 32 KB stages (three stages and two slots
+  // measured 4 % slower)
   if (a.path != 1 && beamform_pair_ok(a))
-    return a.fp8 ? launch_bf_pair<true, 8, 2>(a, num_sms, st) : launch_bf_pair<false, 8, 1>(a, num_sms, st);
+    return a.fp8 ? launch_bf_pair<true, 8, 2, 2>(a, num_sms, st)
+                 : launch_bf_pair<false, 8, 1, 1>(a, num_sms, st);
   return a.fp8 ? launch_bf<true, 4>(a, num_sms, st) : launch_bf<false, 4>(a, num_sms, st);
 }
 
