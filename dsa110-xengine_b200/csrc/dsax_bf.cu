@@ -510,9 +510,10 @@ __global__ void __launch_bounds__(bf::threads(kEpiW), 1) bf_kernel(BfArgs a) {
 }
 
 // ---------------------------------------------------------------- CTA pairs
-// bf_pair_kernel: the BF16 beamformer with the two beam tiles of a 2-CTA
-// cluster sharing each data stage through one cta_group::2 MMA (M = 256:
-// 2 x 64 beams x re/im, N = 256 samples, K = 128).  Each CTA converts
+// bf_pair_kernel: the beamformer (BF16 or FP8 E4M3 operands) with the two
+// beam tiles of a 2-CTA cluster sharing each data stage through one
+// cta_group::2 MMA (M = 256: 2 x 64 beams x re/im, N = 256 samples,
+// K = 128).  Each CTA converts
 // only its half of a stage's packets (8 of 16) into its own shared memory,
 // and the pair's MMA reads both halves, so the 4-bit -> BF16 conversion,
 // the staging copies and the shared-memory operand reads per SM drop from
@@ -522,7 +523,7 @@ __global__ void __launch_bounds__(bf::threads(kEpiW), 1) bf_kernel(BfArgs a) {
 // CTA's TMEM, and each CTA's epilogue reduces its own tile as bf_kernel
 // does, with two warps per TMEM lane quarter (eight in all: with the
 // producers' work halved, the epilogue sets the pace; 4 and 16 measured
-// slower).
+// slower) and kLdG 32-column TMEM loads in flight per wait.
 //   warps 0-7 : producers; each warp's lane 0 arrives on the even CTA's
 //               stage barrier (8 + 8 warp arrivals complete a stage)
 //   warps 8-15: epilogue; each warp's lane 0 frees the accumulator on the
