@@ -301,6 +301,18 @@ __global__ void __launch_bounds__(corr::kThreads, 1) corr_kernel(CorrArgs a) {
 // instruction covers all eight bank groups (the 64-byte swizzle spreads
 // four consecutive antennas' chunks over four groups, the pol the other
 // four).
+// Persistent (FEED 0 / 1): one CTA per SM, each correlating channels
+// blockIdx.x, + gridDim.x, ...; the raw and operand rings and their
+// barrier phases run on across a CTA's channels, so the loader brings the
+// next channel's first stages in while the unpack warps run this channel's
+// epilogue, and TMEM, barriers and the pipeline are set up once per SM
+// instead of once per channel.  The next channel's MMAs overwrite the
+// accumulators only after every unpack warp has left the epilogue (named
+// barrier, then its first stage's full barrier).
+// Epilogue balance: the lower triangle in 16 x 16 antenna blocks (I, J) is
+// written by TMEM lane quadrant I, except block (3, 0), which quadrant 0
+// writes as the conjugates of its own rows, so that no warp writes more
+// than three blocks (four before).
 // NW = 16 (bulk-fed only) doubles the unpack warps: warps 8..15 repeat the
 // mapping of warps 0..7 for time slot 1 while warps 0..7 take slot 0 (each
 // raw word is read twice, each thread does half the byte work), and the
@@ -378,14 +390,19 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   __shared__ __align__(8) uint64_t empty_bar[kOpStages];
   __shared__ __align__(8) uint64_t rfull_bar[kRawStages];
   __shared__ __align__(8) uint64_t rempty_bar[kRawStages];
-  __shared__ __align__(8) uint64_t accum_bar;
+  __shared__ __align__(8) uint64_t accum_bar;            // a channel's accumulators complete
+  __shared__ __align__(8) uint64_t final_bar;            // every MMA of the CTA complete
   __shared__ __align__(8) uint64_t land_full[kRawStages]; // FEED 2: TMA box landed
   __shared__ __align__(8) uint64_t dest_free[kRawStages]; // FEED 2: slot consumed in all 4 CTAs
   __shared__ uint32_t tmem_base_sh;
   __shared__ volatile int abort_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ch = blockIdx.x;
+  const int ch = blockIdx.x;   // FEED 2: the CTA's channel
+  // FEED 0 / 1: channels blockIdx.x, + gridDim.x, ... (a grid of fewer CTAs
+  // than channels loops; the rings and barrier phases run on across the
+  // channels, stage G = ci * nks + ks of channel ci); FEED 2: one channel
+  const int nchc = kCl ? 1 : (a.nchan - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   const uint32_t crank = kCl ? cluster_ctarank() : 0u;     // channel within the cluster's four
   const int nks = (a.npkt + kPktPerStage - 1) / kPktPerStage;
   const uint32_t sbase = (smem_u32(smem_raw) + 1023u) & ~1023u;
@@ -401,6 +418,7 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
       mbar_init(&rempty_bar[r], kUnpackThreads);
     }
     mbar_init(&accum_bar, 1);
+    mbar_init(&final_bar, 1);
     if (kCl) {
       for (int r = 0; r < kRawStages; ++r) {
         mbar_init(&land_full[r], 1);
@@ -427,7 +445,6 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
     if (tid == 0) atomicOr(a.err, DEV_ERR_TMEM);
     abort_sh = 1;
   }
-  const uint32_t *chan_src = reinterpret_cast<const uint32_t *>(a.in + (int64_t)ch * a.npkt * 256);
 
   if (warp < NW) {
     // ------------------------------------------------------------ unpack
@@ -443,6 +460,8 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
       o_re[sp] = sw64_offset(row, c);
       o_im[sp] = kHalfTile + sw64_offset(row, c);
     }
+    int gs0 = 0;                                       // stages of the earlier channels
+    const uint32_t *chan_src = nullptr;                // FEED 0: the channel's stream
     // w[e][q]: packet 2c + e + 8q of the stage, word = bytes [t0p0, t0p1, t1p0, t1p1]
     auto load = [&](int ks, uint32_t (&w)[2][8]) {
 #pragma unroll
@@ -454,8 +473,9 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
         }
     };
     auto unpack_store = [&](int ks, const uint32_t (&w)[2][8]) -> bool {
-      const int s = ks % kOpStages;
-      if (!mbar_wait_bounded(&empty_bar[s], ((uint32_t)(ks / kOpStages) & 1u) ^ 1u, &abort_sh,
+      const int G = gs0 + ks;
+      const int s = G % kOpStages;
+      if (!mbar_wait_bounded(&empty_bar[s], ((uint32_t)(G / kOpStages) & 1u) ^ 1u, &abort_sh,
                              a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
         return false;
       // X[sl][e][h]: sample slot sl = 2t + pol of packets q = 4h .. 4h+3
@@ -508,56 +528,165 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
       mbar_arrive(&full_bar[s]);
       return true;
     };
-    if (kBulk) {
-      const uint32_t *rw_base = reinterpret_cast<const uint32_t *>(gbase + kOpStages * kStageBytes);
-      // the words of raw stage ks -> w, then the stage goes back to the loader
-      auto fetch = [&](int ks, uint32_t (&w)[2][8]) -> bool {
-        const int r = ks % kRawStages;
-        if (!mbar_wait_bounded<kCl>(&rfull_bar[r], (uint32_t)(ks / kRawStages) & 1u, &abort_sh,
-                                    a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns))
-          return false;
-        const uint32_t *rw = rw_base + r * (kRawBytes / 4);
-        const int pvalid = a.npkt - ks * kPktPerStage;
+    const uint32_t *rw_base = reinterpret_cast<const uint32_t *>(gbase + kOpStages * kStageBytes);
+    // the words of raw stage ks -> w, then the stage goes back to the loader
+    auto fetch = [&](int ks, uint32_t (&w)[2][8]) -> bool {
+      const int G = gs0 + ks;
+      const int r = G % kRawStages;
+      if (!mbar_wait_bounded<kCl>(&rfull_bar[r], (uint32_t)(G / kRawStages) & 1u, &abort_sh,
+                                  a.err, DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+        return false;
+      const uint32_t *rw = rw_base + r * (kRawBytes / 4);
+      const int pvalid = a.npkt - ks * kPktPerStage;
 #pragma unroll
-        for (int e = 0; e < 2; ++e)
+      for (int e = 0; e < 2; ++e)
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int P = 2 * (int)c + e + 8 * q;
-            w[e][q] = P < pvalid ? rw[P * 64 + ant] : 0u;
+        for (int q = 0; q < 8; ++q) {
+          const int P = 2 * (int)c + e + 8 * q;
+          w[e][q] = P < pvalid ? rw[P * 64 + ant] : 0u;
+        }
+      // The next bulk copy (async proxy) overwrites this stage: order these
+      // generic-proxy reads before it, or under load the copy can land
+      // first (a write-after-read race across proxies).
+      fence_proxy_async_smem();
+      mbar_arrive(&rempty_bar[r]);
+      return true;
+    };
+#pragma unroll 1
+    for (int ci = 0; ci < nchc; ++ci) {
+      const int ch = (int)blockIdx.x + ci * (kCl ? 0 : (int)gridDim.x);
+      gs0 = ci * nks;
+      chan_src = reinterpret_cast<const uint32_t *>(a.in + (int64_t)ch * a.npkt * 256);
+      if (kBulk) {
+        // one stage of words in registers ahead of the stage being unpacked,
+        // so the shared-memory loads overlap the previous stage's unpack
+        uint32_t wa[2][8], wb[2][8];
+        if (nks > 0 && fetch(0, wa)) {
+          for (int ks = 0; ks < nks && !abort_sh; ks += 2) {
+            if (ks + 1 < nks && !fetch(ks + 1, wb)) break;
+            if (!unpack_store(ks, wa)) break;
+            if (ks + 1 >= nks) break;
+            if (ks + 2 < nks && !fetch(ks + 2, wa)) break;
+            if (!unpack_store(ks + 1, wb)) break;
           }
-        // The next bulk copy (async proxy) overwrites this stage: order these
-        // generic-proxy reads before it, or under load the copy can land
-        // first (a write-after-read race across proxies).
-        fence_proxy_async_smem();
-        mbar_arrive(&rempty_bar[r]);
-        return true;
-      };
-      // one stage of words in registers ahead of the stage being unpacked,
-      // so the shared-memory loads overlap the previous stage's unpack
-      uint32_t wa[2][8], wb[2][8];
-      if (nks > 0 && fetch(0, wa)) {
-        for (int ks = 0; ks < nks && !abort_sh; ks += 2) {
-          if (ks + 1 < nks && !fetch(ks + 1, wb)) break;
+        }
+      } else {
+        // two stages of loads in flight ahead of the stage being unpacked
+        uint32_t wa[2][8], wb[2][8], wc[2][8];
+        load(0, wa);
+        load(1, wb);
+        for (int ks = 0; ks < nks && !abort_sh; ks += 3) {
+          load(ks + 2, wc);
           if (!unpack_store(ks, wa)) break;
           if (ks + 1 >= nks) break;
-          if (ks + 2 < nks && !fetch(ks + 2, wa)) break;
+          load(ks + 3, wa);
           if (!unpack_store(ks + 1, wb)) break;
+          if (ks + 2 >= nks) break;
+          load(ks + 4, wb);
+          if (!unpack_store(ks + 2, wc)) break;
         }
       }
-    } else {
-      // two stages of loads in flight ahead of the stage being unpacked
-      uint32_t wa[2][8], wb[2][8], wc[2][8];
-      load(0, wa);
-      load(1, wb);
-      for (int ks = 0; ks < nks && !abort_sh; ks += 3) {
-        load(ks + 2, wc);
-        if (!unpack_store(ks, wa)) break;
-        if (ks + 1 >= nks) break;
-        load(ks + 3, wa);
-        if (!unpack_store(ks + 1, wb)) break;
-        if (ks + 2 >= nks) break;
-        load(ks + 4, wb);
-        if (!unpack_store(ks + 2, wc)) break;
+      // ------------------------------------------------------------ epilogue
+      bool ok = mbar_wait_bounded(&accum_bar, (uint32_t)ci & 1u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
+                                  a.wait_limit_ns);
+      tc_fence_after();
+      ok = __all_sync(0xffffffffu, ok && !abort_sh);
+      // TMEM lane quadrant q (warp % 4), time slot t; with NW = 16 the two
+      // warps of each (q, t) take alternate column blocks (hh)
+      constexpr int kCbStep = NW / 8;
+      const int q = warp & 3, t = (warp >> 2) & 1, hh = warp >> 3;
+      const int m = 32 * q + lane;                   // row = 2 * antenna + pol
+      const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
+      // C^T through shared memory (every MMA has completed, so the operand
+      // stages are free): row m of C at word (col ^ (m & 31)) of a 512-byte row.
+      uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase + t * (128 * 128 * 4));
+      if (ok) {
+#pragma unroll
+        for (int cb = hh; cb < 8; cb += kCbStep) {
+          uint32_t cv[16];
+          tmem_ld16(trow + 128u + 16u * cb, cv);
+          tmem_wait_ld();
+#pragma unroll
+          for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
+        }
+      }
+      named_bar(1, kUnpackThreads);
+      if (ok) {
+        const int i = m >> 1, pi = m & 1;
+        float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
+        const int64_t tri = (int64_t)i * (i + 1) / 2;
+        const int ncb = 2 * q + 2;
+        // The triangle in 16 x 16 antenna blocks (I, J), I >= J: quadrant q
+        // writes row block q, except that block (3, 0) goes to quadrant 0
+        // as the conjugates of its own rows (V_ij = conj V_ji), so that no
+        // warp does more than three blocks (48 column steps instead of 64
+        // for quadrant 3).
+        for (int cb = (q == 3 ? 2 : 0) + hh; cb < ncb; cb += kCbStep) {
+          uint32_t re[16], cr[16];
+          tmem_ld16(trow + 16u * cb, re);
+          tmem_ld16(trow + 128u + 16u * cb, cr);
+          tmem_wait_ld();
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int j = 8 * cb + jj;
+            if (j <= i) {
+              const int b0 = 2 * j, b1 = 2 * j + 1;
+              const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
+              const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
+              // cr = E[m][.] = C[.][m], ct = C[m][.]: Im = C[m][.] - C[.][m]
+              float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(ct0 - (int32_t)cr[2 * jj]),
+                                     (float)(int32_t)re[2 * jj + 1],
+                                     (float)(ct1 - (int32_t)cr[2 * jj + 1]));
+              float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
+              if (a.accumulate) {
+                const float4 old = *dst;
+                o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
+              }
+              *dst = o;
+            }
+          }
+        }
+        if (q == 0) {
+          // block (3, 0) from rows m' = 2j + pj, j < 16: output (i, j) for
+          // i = 48..63 is V_ij = conj V_ji, Re from Re[m'][2i + pi], Im =
+          // E[m'][n] - E[n][m'] (n = 2i + pi); the two pols of j (lanes
+          // 2j, 2j + 1) swap one value so that each writes one 16-byte pair
+          const int j = m >> 1, pj = m & 1;
+          for (int ib = hh; ib < 2; ib += kCbStep) {
+            uint32_t re[16], er[16];
+            tmem_ld16(trow + 96u + 16u * ib, re);
+            tmem_ld16(trow + 128u + 96u + 16u * ib, er);
+            tmem_wait_ld();
+#pragma unroll
+            for (int ii = 0; ii < 8; ++ii) {
+              const int ic = 48 + 8 * ib + ii;   // output row antenna i
+              const int n0 = 2 * ic, n1 = 2 * ic + 1;
+              const int32_t en0 = (int32_t)Cs[n0 * 128 + (m ^ (n0 & 31))];   // E[n0][m']
+              const int32_t en1 = (int32_t)Cs[n1 * 128 + (m ^ (n1 & 31))];
+              const float r0 = (float)(int32_t)re[2 * ii], i0 = (float)((int32_t)er[2 * ii] - en0);
+              const float r1 = (float)(int32_t)re[2 * ii + 1],
+                          i1 = (float)((int32_t)er[2 * ii + 1] - en1);
+              // pj = 0 keeps pi = 0 and sends pi = 1; pj = 1 the reverse
+              const float sr = __shfl_xor_sync(0xffffffffu, pj ? r0 : r1, 1);
+              const float si = __shfl_xor_sync(0xffffffffu, pj ? i0 : i1, 1);
+              float4 o = pj ? make_float4(sr, si, r1, i1) : make_float4(r0, i0, sr, si);
+              const int64_t trc = (int64_t)ic * (ic + 1) / 2;
+              float4 *dst = reinterpret_cast<float4 *>(vis + ((trc + j) * 4 + 2 * pj) * 2);
+              if (a.accumulate) {
+                const float4 old = *dst;
+                o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
+              }
+              *dst = o;
+            }
+          }
+        }
+      }
+      // every warp is done with this channel's accumulators and with the
+      // C^T scratch (the operand stages) before the next channel's stages
+      // are written and its MMAs issued
+      if (ci + 1 < nchc) {
+        tc_fence_before();
+        named_bar(1, kUnpackThreads);
       }
     }
   } else if (kCl && warp == NW + 1) {
@@ -673,24 +802,28 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   } else if (FEED == 1 && warp == NW + 1) {
     // ------------------------------------------------------------ bulk loader
     if (lane == 0) {
-      int ks = 0;
-      for (; ks < nks && !abort_sh; ++ks) {
-        const int r = ks % kRawStages;
-        if (!mbar_wait_bounded(&rempty_bar[r], ((uint32_t)(ks / kRawStages) & 1u) ^ 1u, &abort_sh,
+      // the stages of all the CTA's channels in order: the next channel's
+      // first stages load while this one's epilogue runs
+      int G = 0;
+      for (; G < nchc * nks && !abort_sh; ++G) {
+        const int ci = G / nks, ks = G - ci * nks;
+        const int chg = (int)blockIdx.x + ci * (int)gridDim.x;
+        const int r = G % kRawStages;
+        if (!mbar_wait_bounded(&rempty_bar[r], ((uint32_t)(G / kRawStages) & 1u) ^ 1u, &abort_sh,
                                a.err, DEV_ERR_WAIT_EMPTY, a.wait_limit_ns))
           break;
         const int npk = min(kPktPerStage, a.npkt - ks * kPktPerStage);
         const uint32_t bytes = (uint32_t)npk * 256u;
         mbar_arrive_expect_tx(&rfull_bar[r], bytes);
         bulk_g2s(raw_base + (uint32_t)r * kRawBytes,
-                 a.in + (int64_t)ch * a.npkt * 256 + (int64_t)ks * kPktPerStage * 256, bytes,
+                 a.in + (int64_t)chg * a.npkt * 256 + (int64_t)ks * kPktPerStage * 256, bytes,
                  &rfull_bar[r]);
       }
       // copies still landing after an abort (their stages are never
       // consumed): wait for the last one issued on each raw stage before the
       // CTA exits; each stage has at most one copy outstanding
       volatile int no_abort = 0;
-      for (int k2 = ks - kRawStages; k2 < ks; ++k2)
+      for (int k2 = G - kRawStages; k2 < G; ++k2)
         if (k2 >= 0)
           mbar_wait_bounded(&rfull_bar[k2 % kRawStages], (uint32_t)(k2 / kRawStages) & 1u,
                             &no_abort, a.err, DEV_ERR_WAIT_FULL, drain_limit(a.wait_limit_ns));
@@ -699,11 +832,19 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   } else if (warp == NW) {
     // ------------------------------------------------------------ UMMA issuer
     if (lane == 0) {
-      for (int ks = 0; ks < nks && !abort_sh; ++ks) {
-        const int s = ks % kOpStages;
-        if (!mbar_wait_bounded(&full_bar[s], (uint32_t)(ks / kOpStages) & 1u, &abort_sh, a.err,
-                               DEV_ERR_WAIT_FULL, a.wait_limit_ns))
+      bool go = true;
+      for (int ci = 0; ci < nchc && go; ++ci) {
+      for (int ks = 0; ks < nks; ++ks) {
+        const int G = ci * nks + ks;
+        const int s = G % kOpStages;
+        if (abort_sh ||
+            !mbar_wait_bounded(&full_bar[s], (uint32_t)(G / kOpStages) & 1u, &abort_sh, a.err,
+                               DEV_ERR_WAIT_FULL, a.wait_limit_ns)) {
+          go = false;
           break;
+        }
+        // (channel ci's first stage was written after the epilogue of
+        // channel ci - 1 read its accumulators, which these MMAs overwrite)
         tc_fence_after();
         const uint32_t stage = sbase + (uint32_t)s * kStageBytes;
 #pragma unroll
@@ -723,69 +864,13 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
         }
         umma_commit(&empty_bar[s]);
       }
-      umma_commit(&accum_bar);
+      if (go) umma_commit(&accum_bar);   // channel ci's accumulators are complete
+      }
+      umma_commit(&final_bar);           // every MMA issued here is complete
     }
     __syncwarp();
   }
 
-  // ---------------------------------------------------------------- epilogue
-  if (warp < NW) {
-    bool ok = mbar_wait_bounded(&accum_bar, 0u, &abort_sh, a.err, DEV_ERR_WAIT_ACCUM,
-                                a.wait_limit_ns);
-    tc_fence_after();
-    ok = __all_sync(0xffffffffu, ok && !abort_sh);
-    // TMEM lane quadrant q (warp % 4), time slot t; with NW = 16 the two
-    // warps of each (q, t) take alternate column blocks (hh)
-    constexpr int kCbStep = NW / 8;
-    const int q = warp & 3, t = (warp >> 2) & 1, hh = warp >> 3;
-    const int m = 32 * q + lane;                   // row = 2 * antenna + pol
-    const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)t * 256u;
-    // C^T through shared memory (every MMA has completed, so the operand
-    // stages are free): row m of C at word (col ^ (m & 31)) of a 512-byte row.
-    uint32_t *Cs = reinterpret_cast<uint32_t *>(gbase + t * (128 * 128 * 4));
-    if (ok) {
-#pragma unroll
-      for (int cb = hh; cb < 8; cb += kCbStep) {
-        uint32_t cv[16];
-        tmem_ld16(trow + 128u + 16u * cb, cv);
-        tmem_wait_ld();
-#pragma unroll
-        for (int e = 0; e < 16; ++e) Cs[m * 128 + ((16 * cb + e) ^ lane)] = cv[e];
-      }
-    }
-    named_bar(1, kUnpackThreads);
-    if (ok) {
-      const int i = m >> 1, pi = m & 1;
-      float *vis = a.vis + (int64_t)(2 * ch + t) * (2080 * 8);
-      const int64_t tri = (int64_t)i * (i + 1) / 2;
-      const int ncb = 2 * q + 2;
-      for (int cb = hh; cb < ncb; cb += kCbStep) {
-        uint32_t re[16], cr[16];
-        tmem_ld16(trow + 16u * cb, re);
-        tmem_ld16(trow + 128u + 16u * cb, cr);
-        tmem_wait_ld();
-#pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {
-          const int j = 8 * cb + jj;
-          if (j <= i) {
-            const int b0 = 2 * j, b1 = 2 * j + 1;
-            const int32_t ct0 = (int32_t)Cs[b0 * 128 + (m ^ (b0 & 31))];
-            const int32_t ct1 = (int32_t)Cs[b1 * 128 + (m ^ (b1 & 31))];
-            // cr = E[m][.] = C[.][m], ct = C[m][.]: Im = C[m][.] - C[.][m]
-            float4 o = make_float4((float)(int32_t)re[2 * jj], (float)(ct0 - (int32_t)cr[2 * jj]),
-                                   (float)(int32_t)re[2 * jj + 1],
-                                   (float)(ct1 - (int32_t)cr[2 * jj + 1]));
-            float4 *dst = reinterpret_cast<float4 *>(vis + ((tri + j) * 4 + 2 * pi) * 2);
-            if (a.accumulate) {
-              const float4 old = *dst;
-              o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
-            }
-            *dst = o;
-          }
-        }
-      }
-    }
-  }
   tc_fence_before();
   __syncthreads();
   // no CTA leaves while another may still address its shared memory
@@ -793,7 +878,7 @@ __global__ void __launch_bounds__(corrcm::threads<FEED, NW>(), 1)
   if (warp == NW) {
     if (lane == 0) {
       volatile int no_abort = 0;
-      mbar_wait_bounded(&accum_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, drain_limit(a.wait_limit_ns));
+      mbar_wait_bounded(&final_bar, 0u, &no_abort, a.err, DEV_ERR_WAIT_ACCUM, drain_limit(a.wait_limit_ns));
     }
     __syncwarp();
     tc_fence_after();
@@ -827,7 +912,18 @@ static int launch_cm(const CorrArgs &a, cudaStream_t st) {
   memset(&tmap, 0, sizeof(tmap));
   if (FEED == 2 && encode_captured_map(&tmap, a) != 0) return -2;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)a.nchan, 1, 1);
+  // FEED 0 / 1: persistent, one CTA per SM (the 512 TMEM columns), each
+  // looping over channels blockIdx.x, + gridDim.x, ...; FEED 2: one CTA
+  // per channel (clusters of four channels)
+  unsigned grid = (unsigned)a.nchan;
+  if (FEED != 2) {
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return -2;
+    if (nsm > 0 && (unsigned)nsm < grid) grid = (unsigned)nsm;
+  }
+  cfg.gridDim = dim3(grid, 1, 1);
   cfg.blockDim = dim3(corrcm::threads<FEED, NW>(), 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
@@ -844,6 +940,7 @@ static int launch_cm(const CorrArgs &a, cudaStream_t st) {
 int launch_correlate_chanmajor(const CorrArgs &a, cudaStream_t st, int corr_path) {
   switch (corr_path) {
     case 3: return launch_cm<0, 8>(a, st);
+
     case 5:
     case 7: return launch_cm<1, 16>(a, st);
     default: return launch_cm<1, 8>(a, st);
