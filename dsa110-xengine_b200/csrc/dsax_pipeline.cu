@@ -6,8 +6,7 @@
 // before it reads the next (src/dsaX_xgpu.cu:300-357).  Here block i+1's
 // corner turn (HBM-bound) runs on a side stream while block i is correlated
 // (bound by the unpack warps, with HBM bandwidth to spare), and in host mode
-// the PCIe copies in and out overlap both (in device mode the corner turn
-// stays on the context stream, see below).  The fused paths (corr_path 6,
+// the PCIe copies in and out overlap both.  The fused paths (corr_path 6,
 // 7) have no corner turn: only the copies overlap the correlations.  Buffers are double-buffered and
 // every reuse waits on the event of the stage that last read the buffer.
 #include <cuda_runtime.h>
@@ -68,14 +67,16 @@ extern "C" int dsax_correlate_many(dsax_ctx *c, const void *const *blocks, void 
   uint8_t *din[2] = {base + oreo, base + oreo + up(nin)};
   uint8_t *dvis[2] = {din[1] + up(nin), din[1] + up(nin) + up(nvis)};
 
-  // In device mode each block's corner turn runs on the context stream right
-  // before its correlation: overlapping it with the previous block's
-  // correlation on a side stream measured slower (0.29 against 0.165 ms per
-  // block on a B200), because the corner turn's CTAs take the SMs that the
-  // correlator's later waves need.  With host buffers the PCIe copies set
-  // the pace and the corner turn overlaps them on its own stream.
+  // The corner turns run on their own stream in both modes.  In device mode
+  // block i+1's corner turn takes the SMs that the persistent correlator's
+  // CTAs free as they finish their last channel (60 of 148 SMs idle for
+  // the last third of a 384-channel block): 0.146 against 0.162 ms per
+  // block with both on one stream.  (With one correlator CTA per channel
+  // the overlap measured slower, 0.29 against 0.165 ms: the corner turn's
+  // CTAs took the SMs the correlator's later waves needed.)  With host
+  // buffers the PCIe copies set the pace.
   cudaStream_t cs = c->stream, h2d = c->side[S_H2D], d2h = c->side[S_D2H];
-  cudaStream_t rs = host ? c->side[S_REO] : cs;
+  cudaStream_t rs = c->side[S_REO];
   cudaEvent_t *ev = c->pev;
   // the side streams start after everything already queued on the context stream
   cudaError_t e = cudaEventRecord(ev[E_START], cs);

@@ -149,8 +149,9 @@ int dsax_correlate(dsax_ctx *ctx, const void *in, void *vis, int mem);
  * mem = DSAX_MEM_HOST the stages of consecutive blocks overlap: block i+1's
  * copy in and corner turn run on side streams while block i is correlated
  * and block i-1 copied out (pinned host buffers give asynchronous DMA).  In
- * device mode each block is corner-turned and correlated in sequence on the
- * context stream (overlapping the two on the GPU measured slower).  Replaces the per-block loop of src/dsaX_xgpu.cu:300-357 (H2D,
+ * device mode block i+1's corner turn runs on a side stream beside block
+ * i's correlation, on the SMs the correlator's CTAs free as they finish.
+ * Replaces the per-block loop of src/dsaX_xgpu.cu:300-357 (H2D,
  * promoter, xgpuCudaXengine, matrix copy-out, one block at a time).  Device
  * mode enqueues (ordered on the context stream); host mode returns when all
  * visibilities are in the host buffers.  Output always overwrites.  Uses
