@@ -360,22 +360,30 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
         ctx.set_weights(wre, wim)
         st = torch.cuda.ExternalStream(ctx.stream)
         ms8 = _time_loop(st, lambda i: ctx.beamform(blk_dev[i % len(blk_dev)], out), steps)
+        ctx.beamform(blk_dev[0], out, f32)
         ctx.sync()
-    # per-output error on groups 0 and 47 against the oracle on the same block
+        got8 = f32.cpu().numpy().reshape(128, 256, 48).astype(np.float64)
+        gu8_8 = out.cpu().numpy().reshape(128, 256, 48)
+    # per-output error on groups 0 and 47 against the FP64 oracle (unrounded
+    # weights) on the same block, for the BF16 and the FP8 operands
     blk0 = blk_dev[0].cpu().numpy().reshape(2048, 63, 384, 2, 2)
-    err = {}
-    rel_all, lsb_all = [], []
-    for g in (0, 47):
-        ref = oracle.beamform_power(blk0, wre, wim, 16, g0=g, ng=1)[:, :, 0]
-        rel = np.abs(got[:, :, g] - ref) / np.maximum(ref, 1e-30)
-        lsb = np.abs(gu8[:, :, g].astype(int) - oracle.quantize_u8(ref, scale).astype(int))
-        rel_all.append(rel.reshape(-1))
-        lsb_all.append(lsb.reshape(-1))
-    rel_all = np.concatenate(rel_all)
-    lsb_all = np.concatenate(lsb_all)
-    err = {"outputs_checked": int(rel_all.size), "groups": [0, 47],
-           "fp32_rel_max": float(rel_all.max()), "fp32_rel_mean": float(rel_all.mean()),
-           "u8_max_lsb": int(lsb_all.max()), "u8_frac_off_by_1": float((lsb_all == 1).mean())}
+    refs = {g: oracle.beamform_power(blk0, wre, wim, 16, g0=g, ng=1)[:, :, 0] for g in (0, 47)}
+
+    def _err(gp, gu):
+        rel_all, lsb_all = [], []
+        for g, ref in refs.items():
+            rel = np.abs(gp[:, :, g] - ref) / np.maximum(ref, 1e-30)
+            lsb = np.abs(gu[:, :, g].astype(int) - oracle.quantize_u8(ref, scale).astype(int))
+            rel_all.append(rel.reshape(-1))
+            lsb_all.append(lsb.reshape(-1))
+        rel_all = np.concatenate(rel_all)
+        lsb_all = np.concatenate(lsb_all)
+        return {"outputs_checked": int(rel_all.size), "groups": [0, 47],
+                "fp32_rel_max": float(rel_all.max()), "fp32_rel_mean": float(rel_all.mean()),
+                "u8_max_lsb": int(lsb_all.max()),
+                "u8_frac_off_by_1": float((lsb_all == 1).mean())}
+    err = _err(got, gu8)
+    err8 = _err(got8, gu8_8)
     # CPU baseline: the oracle's FP64 beamformer on the host cores, a sample
     # of channel groups scaled to the block
     t0 = time.perf_counter()
@@ -408,7 +416,8 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
                                       f"block, scaled"},
            "fp8": {"ms_per_block": ms8, "blocks_per_s": 1e3 / ms8, "achieved_tflops": tf8,
                    "frac_of_2x_bf16_peak": tf8 / (2 * burst),
-                   "peak_kind": "E4M3 dense taken as 2x the measured BF16 burst"}}
+                   "peak_kind": "E4M3 dense taken as 2x the measured BF16 burst",
+                   "error_vs_fp64": err8}}
     if fp8_peak:
         res["fp8"]["frac_of_probe"] = tf8 / fp8_peak
         res["fp8"]["probe_tflops"] = fp8_peak
