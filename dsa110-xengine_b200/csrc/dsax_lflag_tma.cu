@@ -75,7 +75,10 @@ __device__ __forceinline__ uint32_t tma_pack_bf16x2(float lo, float hi) {
   return r;
 }
 
-template <int COUT, bool PROJ>
+// CIN: the real input channels of the 64-channel grid rows (32 for layer 2,
+// whose upper 32 channels carry zero weights): the MMAs cover K = CIN per
+// tap, so layer 2 issues half of layer 3's.
+template <int COUT, bool PROJ, int CIN>
 __global__ void __launch_bounds__(lftma::kThreads, 1)
     lf_conv_tma_kernel(const __grid_constant__ CUtensorMap tin, LfTmaArgs a) {
   using namespace lftma;
@@ -84,6 +87,8 @@ __global__ void __launch_bounds__(lftma::kThreads, 1)
   constexpr uint32_t TCOLS = 2 * COUT;
   constexpr int kStages = stages<COUT>();
   static_assert(COUT == 64, "64 output channels");
+  static_assert(CIN == 32 || CIN == 64, "32 or 64 real input channels");
+  constexpr int KK = CIN / 16;   // 16-channel K steps per tap
 
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kStages];
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(lftma::kThreads, 1)
 #pragma unroll
           for (int dx = 0; dx < 3; ++dx)   // tap (band, dx): window starting dx rows in
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk)   // K = 64 bf16 = 4 x 16
+            for (int kk = 0; kk < KK; ++kk)   // K = CIN bf16 = KK x 16
               umma_f16(dcol, ab + (uint64_t)((128 * dx + 32 * kk) >> 4),
                        bdesc0 + (uint64_t)(((3 * band + dx) * COUT * 128 + 32 * kk) >> 4), IDESC,
                        (band | dx | kk) != 0);
@@ -590,16 +595,16 @@ int encode_grid_map(CUtensorMap *map, const uint16_t *grid, int64_t npp, int ch)
   return r == CUDA_SUCCESS ? 0 : -1;
 }
 
-template <int COUT, bool PROJ>
+template <int COUT, bool PROJ, int CIN>
 int conv_tma_launch(const CUtensorMap &map, const LfTmaArgs &a, int num_sms, cudaStream_t st) {
   constexpr int smem = 1024 + lftma::kTaps * COUT * 128 + lftma::stages<COUT>() * lftma::kABytes;
   static SmemAttrOnce attr;
-  if (smem_attr_once(attr, lf_conv_tma_kernel<COUT, PROJ>, smem) != cudaSuccess) return -2;
+  if (smem_attr_once(attr, lf_conv_tma_kernel<COUT, PROJ, CIN>, smem) != cudaSuccess) return -2;
   const int64_t npp = (int64_t)a.B * (a.H + 2) * (a.W + 2);
   const int ntiles = (int)((npp + 127) / 128);
   const int grid = ntiles < num_sms ? ntiles : num_sms;
   if (grid < 1) return 0;
-  lf_conv_tma_kernel<COUT, PROJ><<<grid, lftma::kThreads, smem, st>>>(map, a);
+  lf_conv_tma_kernel<COUT, PROJ, CIN><<<grid, lftma::kThreads, smem, st>>>(map, a);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -661,10 +666,10 @@ int lf_tma_layers23(const LfNet &net, const uint8_t *wimg, const uint16_t *act1p
   a.B = B; a.H = H; a.W = W;
   a.wait_limit_ns = wait_limit_ns;
   a.wimg = wimg; a.bias = net.b[1]; a.out = act2p;
-  int e = conv_tma_launch<64, false>(m1, a, num_sms, st);
+  int e = conv_tma_launch<64, false, kLfCin[1]>(m1, a, num_sms, st);
   a.wimg = wimg + lftma::kTaps * 64 * 128; a.bias = net.b[2]; a.out = nullptr;
   a.w4 = net.w[3]; a.z9 = z9;
-  e |= conv_tma_launch<64, true>(m2, a, num_sms, st);
+  e |= conv_tma_launch<64, true, kLfCin[2]>(m2, a, num_sms, st);
   return e;
 }
 
