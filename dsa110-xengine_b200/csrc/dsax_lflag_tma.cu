@@ -341,7 +341,7 @@ __global__ void lf_pad_border_kernel(uint16_t *act, int B, int H, int W, int chu
 // kernel row) land in a band slot, and four builder warps copy each pixel's
 // nine taps into the K-major 128-byte-swizzled A tile (K = 72 in two 64-wide
 // blocks, k = 8 tap + ci; the rest of the second block stays zero), then
-// 8 MMAs of N = 32.  The epilogue writes channels 0-31 of the interior
+// 5 MMAs of N = 32 (K 64 + 16).  The epilogue writes channels 0-31 of the interior
 // pixels of the 64-channel grid the next layer reads (channels 32-63 are
 // zero there).
 //   warps 0-3 : A-tile builders      warps 4-7 : epilogue
@@ -549,10 +549,12 @@ __global__ void __launch_bounds__(lf1::kThreads, 1)
         tc_fence_after();
         const uint64_t ab = adesc0 + (uint64_t)(((uint32_t)s2 * kABytes) >> 4);
         const uint32_t dcol = tmem + (uint32_t)(bf * kCout);
+        // K = 72: block 0 holds taps 0-7, block 1 tap 8 in its first 16
+        // K elements (the rest is zero and not issued)
 #pragma unroll
         for (int kb = 0; kb < 2; ++kb)
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk)
+          for (int kk = 0; kk < (kb == 0 ? 4 : 1); ++kk)
             umma_f16(dcol, ab + (uint64_t)((kb * 16384 + 32 * kk) >> 4),
                      bdesc0 + (uint64_t)((kb * kCout * 128 + 32 * kk) >> 4), IDESC, (kb | kk) != 0);
         umma_commit(&aempty_bar[s2]);
