@@ -346,6 +346,11 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
         e2e_ms = (time.perf_counter() - t0) * 1e3 / e_steps
         lib.dsax_host_free(ctx.handle, p_in)
         lib.dsax_host_free(ctx.handle, p_out)
+    # the autotuner's candidates on this GPU: the one-CTA form and the CTA
+    # pairs with each stage-parameter variant
+    with dsax.Context(dsax.default_config(bf_scale=scale), device=dev) as ctx:
+        ctx.set_weights(wre, wim)
+        tune_ms, tune_best = ctx.autotune_beamformer(reps=5)
     # the one-CTA-per-beam-tile form (bf_path 1), for comparison with the
     # default CTA pairs
     cfg1 = dsax.default_config(bf_scale=scale, bf_path=1)
@@ -403,6 +408,10 @@ def bench_beamformer(dsax, synth, dev, blk_dev, steps, peaks=None):
                           "tcgen05.mma.cta_group::2 (M = 256)",
            "one_cta_form": {"ms_per_block": ms1, "achieved_tflops": BF_FLOPS / (ms1 * 1e-3) / 1e12,
                             "kernel": "bf_kernel (bf_path 1)"},
+           "autotune": {"candidates_ms": {("one CTA" if k == 1 else f"pairs, variant {k - 1}"): v
+                                          for k, v in tune_ms.items()},
+                        "chosen": "one CTA" if tune_best == 1 else f"pairs, variant {tune_best - 1}",
+                        "call": "dsax_autotune_beamformer (BF16)"},
            "roofline": {"bound": "tensor", "kernel": "bf_pair_kernel", "achieved": tf,
                         "peak": burst, "unit": "TFLOP/s", "frac": tf / burst,
                         "frac_of_sustained": tf / sust, "peak_kind": f"{kind} BF16 dense (cuBLAS)"},

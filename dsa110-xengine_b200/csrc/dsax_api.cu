@@ -127,7 +127,8 @@ int dsax_create(dsax_ctx **out, const dsax_config *cfg, int device) {
   if (!out || !cfg) return DSAX_ERR_ARG;
   *out = nullptr;
   if (cfg->npkt < 1 || cfg->npkt > (1 << 16) || cfg->nant_in < 1 || cfg->nant_in > 64 ||
-      cfg->nchan < 1 || cfg->nchan > 8192 || cfg->bf_path < 0 || cfg->bf_path > 2)
+      cfg->nchan < 1 || cfg->nchan > 8192 || cfg->bf_path < 0 || cfg->bf_path > 2 ||
+      cfg->bf_variant < 0 || cfg->bf_variant > 4)
     return DSAX_ERR_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)

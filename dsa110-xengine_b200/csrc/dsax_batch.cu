@@ -67,6 +67,7 @@ int enqueue_block(dsax_ctx *c, const dsax_block_desc &d, uint8_t *scratch, float
     b.ppo = ppo;
     b.scale = cf.bf_scale;
     b.path = cf.bf_path;
+    b.variant = cf.bf_variant;
     b.wait_limit_ns = cf.wait_limit_ns;
     if (launch_beamform(b, c->num_sms, sb) != 0) return -2;
   }

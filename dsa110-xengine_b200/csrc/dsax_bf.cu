@@ -1021,9 +1021,25 @@ int launch_beamform(const BfArgs &a, int num_sms, cudaStream_t st) {
   // FP8: two raw staging slots beside its six 16 KB stages (1 % faster);
   // BF16 keeps one slot and four 32 KB stages (three stages and two slots
   // measured 4 % slower)
-  if (a.path != 1 && beamform_pair_ok(a))
-    return a.fp8 ? launch_bf_pair<true, 8, 2, 2>(a, num_sms, st)
-                 : launch_bf_pair<false, 8, 1, 1>(a, num_sms, st);
+  if (a.path != 1 && beamform_pair_ok(a)) {
+    // variant: (TMEM loads per wait, raw staging slots) = 1 (1,1), 2 (2,1),
+    // 3 (1,2), 4 (2,2); 0 = the default above per operand type
+    const int v = a.variant ? a.variant : (a.fp8 ? 4 : 1);
+    if (a.fp8) {
+      switch (v) {
+        case 1: return launch_bf_pair<true, 8, 1, 1>(a, num_sms, st);
+        case 2: return launch_bf_pair<true, 8, 2, 1>(a, num_sms, st);
+        case 3: return launch_bf_pair<true, 8, 1, 2>(a, num_sms, st);
+        default: return launch_bf_pair<true, 8, 2, 2>(a, num_sms, st);
+      }
+    }
+    switch (v) {
+      case 2: return launch_bf_pair<false, 8, 2, 1>(a, num_sms, st);
+      case 3: return launch_bf_pair<false, 8, 1, 2>(a, num_sms, st);
+      case 4: return launch_bf_pair<false, 8, 2, 2>(a, num_sms, st);
+      default: return launch_bf_pair<false, 8, 1, 1>(a, num_sms, st);
+    }
+  }
   return a.fp8 ? launch_bf<true, 4>(a, num_sms, st) : launch_bf<false, 4>(a, num_sms, st);
 }
 

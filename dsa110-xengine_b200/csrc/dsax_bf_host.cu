@@ -266,6 +266,7 @@ int dsax_beamform(dsax_ctx *c, const void *blk, void *out_u8, void *out_f32, int
   a.wait_limit_ns = cf.wait_limit_ns;
   a.pscale = 1.0f;
   a.path = cf.bf_path;
+  a.variant = cf.bf_variant;
   if (cf.bf_fp8) {   // E4M3 operands, per-antenna data exponents, power by 2^-2E
     a.fp8 = 1;
     a.wimg = static_cast<const uint8_t *>(c->aux[AUX_WIMG_FP8].ptr);

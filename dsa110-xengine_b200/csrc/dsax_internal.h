@@ -72,6 +72,7 @@ struct BfArgs {
   const signed char *e4m3_add;  // FP8: per-antenna data exponent 8d (64 entries) or null
   int fp8;                 // operands: 0 BF16 (kind::f16), 1 FP8 E4M3 (kind::f8f6f4)
   int path;                // kernel form (dsax_config.bf_path)
+  int variant;             // CTA-pair stage parameters (dsax_config.bf_variant)
   const float *agc_scale;  // per-beam AGC scale: u8 = rint(P * s) / 2 (or null: fixed scale)
   float *beam_power;       // per-beam total power of the block, accumulated (or null)
   int *err;

@@ -7,8 +7,10 @@
 // (4) the same correlator fed by one bulk copy per 64-packet stage and
 // unpacked by 8 warps, (5) as 4 with 16 unpack warps, (6) no corner turn:
 // the captured block read directly by clusters of four channel CTAs, (7) as
-// 6 with 16 unpack warps.  Candidates for the beamformer (bf_path): (1)
-// one CTA per 64-beam tile, (2) CTA pairs sharing a cta_group::2 MMA.
+// 6 with 16 unpack warps.  Candidates for the beamformer: (1) one CTA per
+// 64-beam tile (bf_path 1), (2-5) CTA pairs sharing a cta_group::2 MMA
+// (bf_path 2) with stage parameters bf_variant 1-4 (TMEM loads in flight
+// per epilogue wait x raw staging slots).
 #include <cstring>
 #include <cuda_runtime.h>
 
@@ -95,16 +97,18 @@ extern "C" int dsax_autotune_beamformer(dsax_ctx *c, int reps, float *times_ms, 
   uint8_t *blk = static_cast<uint8_t *>(c->aux[AUX_TUNE].ptr);
   uint8_t *beams = blk + ((nin + 255) & ~(size_t)255);
   fill_pattern<<<1024, 256, 0, c->stream>>>(blk, nin, 54321u);
-  const int saved = c->cfg.bf_path;
-  constexpr int kNumPaths = 2;
-  const int paths[kNumPaths] = {1, 2};
+  const int saved = c->cfg.bf_path, saved_v = c->cfg.bf_variant;
+  constexpr int kNumCand = 5;
+  const int paths[kNumCand] = {1, 2, 2, 2, 2};
+  const int variants[kNumCand] = {0, 1, 2, 3, 4};
   float best = 1e30f;
-  int bestp = 2;
+  int bestk = 1;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int k = 0; k < kNumPaths; ++k) {
+  for (int k = 0; k < kNumCand; ++k) {
     c->cfg.bf_path = paths[k];
+    c->cfg.bf_variant = variants[k];
     for (int w = 0; w < 2; ++w)
       if ((rc = dsax_beamform(c, blk, beams, nullptr, DSAX_MEM_DEVICE)) != DSAX_OK) break;
     if (rc != DSAX_OK) break;
@@ -118,15 +122,17 @@ extern "C" int dsax_autotune_beamformer(dsax_ctx *c, int reps, float *times_ms, 
     cudaEventElapsedTime(&ms, e0, e1);
     ms /= reps;
     if (times_ms && k < ntimes) times_ms[k] = ms;
-    if (ms < best) { best = ms; bestp = paths[k]; }
+    if (ms < best) { best = ms; bestk = k; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != DSAX_OK) {
     c->cfg.bf_path = saved;
+    c->cfg.bf_variant = saved_v;
     return rc;
   }
-  c->cfg.bf_path = bestp;
-  if (best_path) *best_path = bestp;
+  c->cfg.bf_path = paths[bestk];
+  c->cfg.bf_variant = variants[bestk];
+  if (best_path) *best_path = bestk + 1;
   return DSAX_OK;
 }

@@ -54,6 +54,7 @@ class Config(ctypes.Structure):
         ("corr_path", ctypes.c_int),
         ("bf_fp8", ctypes.c_int),
         ("bf_path", ctypes.c_int),
+        ("bf_variant", ctypes.c_int),
     ]
 
 
@@ -477,15 +478,17 @@ class Context:
         return {k + 1: float(t[k]) for k in range(7)}, best.value
 
     def autotune_beamformer(self, reps: int = 10):
-        """Returns ({bf_path: ms}, chosen bf_path); the context keeps the
-        choice (dsax_set_weights first)."""
+        """Returns ({candidate: ms}, chosen candidate): 1 = the one-CTA form,
+        2-5 = CTA pairs with bf_variant 1-4; the context keeps the choice
+        (dsax_set_weights first)."""
         import numpy as np
-        t = np.zeros(2, np.float32)
+        t = np.zeros(5, np.float32)
         best = ctypes.c_int(0)
-        self._check(lib().dsax_autotune_beamformer(self._h, reps, _ptr(t), 2, ctypes.byref(best)),
+        self._check(lib().dsax_autotune_beamformer(self._h, reps, _ptr(t), 5, ctypes.byref(best)),
                     "dsax_autotune_beamformer")
-        self.cfg.bf_path = best.value
-        return {k + 1: float(t[k]) for k in range(2)}, best.value
+        self.cfg.bf_path = 1 if best.value == 1 else 2
+        self.cfg.bf_variant = 0 if best.value == 1 else best.value - 1
+        return {k + 1: float(t[k]) for k in range(5)}, best.value
 
     # -- batches -----------------------------------------------------------
     def run_batch(self, descs, use_graph: bool = True):

@@ -93,6 +93,13 @@ typedef struct dsax_config {
                                 cluster share each data stage through one
                                 cta_group::2 MMA of M = 256 (BF16 or
                                 FP8, nbeam % 128 == 0; else as 1) */
+    int bf_variant;      /* CTA-pair beamformer stage parameters: 0 = the
+                            default for the operand type (BF16 1, FP8 4);
+                            1..4 = (TMEM loads in flight per epilogue wait,
+                            raw staging slots of packet groups in flight) =
+                            (1, 1), (2, 1), (1, 2), (2, 2); two slots cost
+                            BF16 one of its four operand stages.  All give
+                            the same beams; dsax_autotune_beamformer picks */
 } dsax_config;
 
 typedef struct dsax_ctx dsax_ctx;
@@ -206,11 +213,13 @@ int dsax_correlate_extract_ex(dsax_ctx *ctx, const void *in, void *out, int orde
  * milliseconds (times_ms[0..6] for paths 1..7, up to ntimes) and the choice. */
 int dsax_autotune(dsax_ctx *ctx, int reps, float *times_ms, int ntimes, int *best_path);
 
-/* Beamformer autotuner: times the kernel forms (bf_path 1 and 2) with the
- * context's weights (dsax_set_weights first) on a synthetic block of its
- * geometry, sets bf_path to the faster, and returns the milliseconds
- * (times_ms[0..1] for paths 1..2, up to ntimes) and the choice.  Both forms
- * compute the same beams (FP32 power within 1e-5 relative). */
+/* Beamformer autotuner: times, with the context's weights (dsax_set_weights
+ * first) on a synthetic block of its geometry, five candidates: (1) the
+ * one-CTA form (bf_path 1) and (2-5) the CTA-pair form (bf_path 2) with
+ * bf_variant 1-4; keeps the fastest in the context's bf_path / bf_variant,
+ * and returns the milliseconds (times_ms[0..4], up to ntimes) and the
+ * candidate number (1-5).  Every candidate computes the same beams (FP32
+ * power within 1e-5 relative). */
 int dsax_autotune_beamformer(dsax_ctx *ctx, int reps, float *times_ms, int ntimes,
                              int *best_path);
 

@@ -13,11 +13,13 @@ REL_TOL = 5e-3
 MEAN_TOL = 1e-3
 
 
-def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None, set_w=True, bf_path=0, fp8=0):
+def _beamform(dsax, blk, wre, wim, nbeam, ppo, scale, ctx=None, set_w=True, bf_path=0, fp8=0,
+              bf_variant=0):
     import torch
     npkt, nant, nchan = blk.shape[:3]
     cfg = dsax.default_config(npkt=npkt, nant_in=nant, nchan=nchan, nbeam=nbeam,
-                              bf_pkt_per_out=ppo, bf_scale=scale, bf_path=bf_path, bf_fp8=fp8)
+                              bf_pkt_per_out=ppo, bf_scale=scale, bf_path=bf_path, bf_fp8=fp8,
+                              bf_variant=bf_variant)
     own = ctx is None
     ctx = ctx or dsax.Context(cfg)
     try:
@@ -77,18 +79,19 @@ def test_beamformer_shapes(dsax, oracle, nbeam, ppo, npkt, nant, nchan, bf_path)
 
 @pytest.mark.parametrize("fp8", [0, 1])
 def test_beamformer_paths_agree_full_block(dsax, oracle, fp8):
-    """The CTA-pair kernel (cta_group::2) against the one-CTA kernel on a
-    full block, BF16 and FP8: the same products, the epilogue's partial
-    sums added in another order, so FP32 power within 1e-5 relative and
-    uint8 within 1 LSB."""
+    """The CTA-pair kernel (cta_group::2), with each of its stage-parameter
+    variants, against the one-CTA kernel on a full block, BF16 and FP8: the
+    same products, the epilogue's partial sums added in another order, so
+    FP32 power within 1e-5 relative and uint8 within 1 LSB."""
     blk = oracle.gen_block(304, 2048, 63, 384, "gauss")
     wre, wim = oracle.random_phase_weights(10, 48, 256)
     scale = 128.0 / (512 * 64 * 2 * 6.25)
     u8a, fa = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=1, fp8=fp8)
-    u8b, fb = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=2, fp8=fp8)
-    rel = np.abs(fb.astype(np.float64) - fa) / np.maximum(fa, 1e-30)
-    assert rel.max() < 1e-5, rel.max()
-    assert np.abs(u8b.astype(int) - u8a.astype(int)).max() <= 1
+    for v in (1, 2, 3, 4):
+        u8b, fb = _beamform(dsax, blk, wre, wim, 256, 16, scale, bf_path=2, fp8=fp8, bf_variant=v)
+        rel = np.abs(fb.astype(np.float64) - fa) / np.maximum(fa, 1e-30)
+        assert rel.max() < 1e-5, (v, rel.max())
+        assert np.abs(u8b.astype(int) - u8a.astype(int)).max() <= 1, v
 
 
 def test_beamformer_geometric_weights(dsax, oracle):
@@ -245,9 +248,10 @@ def test_beamformer_fp8(dsax, oracle, weights, bf_path):
 
 
 def test_autotune_beamformer_picks_fastest_and_stays_correct(dsax, oracle):
-    """dsax_autotune_beamformer times both kernel forms on the context's
-    geometry, keeps the faster, and the beams stay within the oracle
-    tolerances afterwards."""
+    """dsax_autotune_beamformer times the one-CTA form and the CTA-pair form
+    with its four stage-parameter variants on the context's geometry, keeps
+    the fastest, and the beams stay within the oracle tolerances
+    afterwards."""
     blk = oracle.gen_block(707, 256, 63, 64, "gauss")
     wre, wim = oracle.random_phase_weights(12, 8, 256)
     scale = 128.0 / (2 * 16 * 16 * 63 * 2 * 6.25 * 0.93)
@@ -255,7 +259,7 @@ def test_autotune_beamformer_picks_fastest_and_stays_correct(dsax, oracle):
     with dsax.Context(cfg) as ctx:
         ctx.set_weights(wre, wim)
         times, best = ctx.autotune_beamformer(reps=3)
-        assert best in (1, 2) and all(t > 0 for t in times.values())
+        assert best in (1, 2, 3, 4, 5) and all(t > 0 for t in times.values())
         assert times[best] == min(times.values())
         u8, f32 = _beamform(dsax, blk, wre, wim, 256, 16, scale, ctx=ctx, set_w=False)
     _check(oracle, blk, wre, wim, u8, f32, 16, scale)
